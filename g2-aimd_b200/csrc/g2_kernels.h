@@ -1,0 +1,87 @@
+// g2_kernels.h - argument blocks and launchers of the device kernels
+// (internal to libg2aimd.so; the public surface is include/g2_aimd.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "g2_aimd.h"
+
+namespace g2 {
+
+// Bits of the device status word.
+constexpr int kStatusDeferOverflow = 1;  // deferred-task list full
+constexpr int kStatusHistOverflow = 2;   // clique larger than the histogram
+constexpr int kStatusStackOverflow = 4;  // GMatch candidate stack exhausted
+constexpr int kStatusBadPlan = 8;        // plan arrays inconsistent
+
+struct MceArgs {
+    const uint64_t *rp;
+    const uint32_t *ci;
+    const uint32_t *tasks;          // root vertex of each task
+    const uint32_t *task_index;     // optional: the task ids this pass runs (else 0..ntasks-1)
+    uint64_t ntasks;                // tasks in this pass (if ntasks_dev is null)
+    const unsigned long long *ntasks_dev;  // else: task count read from device memory
+    unsigned long long *head;       // device queue head
+    uint32_t chunk;                 // tasks grabbed per atomic
+    uint32_t hist_len;
+    uint32_t *scratch;              // warps * words_per_warp words
+    uint64_t words_per_warp;        // multiple of 64
+    unsigned long long *out;        // [0] count, [1 + s] hist[s]
+    uint32_t *deferred;             // task ids deferred to a larger pass
+    unsigned long long *ndeferred;
+    uint64_t deferred_cap;
+    uint64_t *root_nodes;           // optional, per task id
+    int *status;
+    int final_pass;
+};
+
+size_t mce_smem_bytes(int wpl, int warps_per_block);
+cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_block, cudaStream_t st);
+
+// Plan in device-friendly form: everything by POSITION.
+struct DevPlan {
+    uint32_t k;
+    uint32_t bn_count[G2_MAX_QUERY];
+    uint32_t bn_pos[G2_MAX_QUERY][G2_MAX_QUERY];       // back neighbours as positions
+    uint32_t cond_count[G2_MAX_QUERY];
+    uint32_t cond_op[G2_MAX_QUERY][G2_MAX_QUERY];      // condition of position p vs ...
+    uint32_t cond_pos[G2_MAX_QUERY][G2_MAX_QUERY];     // ... the vertex matched at this position
+    uint32_t share[G2_MAX_QUERY];                      // prefix intersection computed one level early
+    uint32_t pre_bn_count[G2_MAX_QUERY];
+    uint32_t pre_bn_pos[G2_MAX_QUERY][G2_MAX_QUERY];
+    uint32_t pre_cond_count[G2_MAX_QUERY];
+    uint32_t pre_cond_op[G2_MAX_QUERY][G2_MAX_QUERY];
+    uint32_t pre_cond_pos[G2_MAX_QUERY][G2_MAX_QUERY];
+    uint32_t after_bn_count[G2_MAX_QUERY];
+    uint32_t after_bn_pos[G2_MAX_QUERY][G2_MAX_QUERY];
+    uint32_t after_cond_count[G2_MAX_QUERY];
+    uint32_t after_cond_op[G2_MAX_QUERY][G2_MAX_QUERY];
+    uint32_t after_cond_pos[G2_MAX_QUERY][G2_MAX_QUERY];
+    uint32_t clique;        // 1: every position adjacent to all earlier ones, strictly increasing images
+};
+
+struct MatchArgs {
+    const uint64_t *rp;
+    const uint32_t *ci;
+    const uint32_t *tasks;
+    const uint32_t *task_index;
+    uint64_t ntasks;
+    unsigned long long *head;
+    uint32_t chunk;
+    uint32_t *scratch;
+    uint64_t words_per_warp;
+    unsigned long long *out;        // [0] count
+    uint32_t *deferred;
+    unsigned long long *ndeferred;
+    uint64_t deferred_cap;
+    uint64_t *root_nodes;           // optional: embeddings counted per task
+    int *status;
+};
+
+cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block,
+                         cudaStream_t st, bool clique_path, int wpl);
+
+}  // namespace g2

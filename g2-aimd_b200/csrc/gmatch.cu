@@ -1,0 +1,283 @@
+// gmatch.cu - plan-driven subgraph enumeration for sm_100a.
+//
+// Replaces GMatchApp (app_gmatch/gmatch.h:15-736), which materialises every
+// partial embedding level by level in BFS buffers, with a persistent kernel:
+// each warp pulls a root (the image of matchOrder[0]) from a device atomic
+// queue and extends it depth first.  Two paths, chosen per plan:
+//
+//  * generic (any plan): the candidates of position i are N(M(parent)) with
+//    parent = the back neighbour whose image has the least degree (first on
+//    ties, app_gmatch/gmatch.h:516-536), filtered by the plan's conditions
+//    (<, >, != against earlier positions, :559-588) and by membership in the
+//    other back neighbours' lists (:589-601).  The `<` / `>` conditions are
+//    also turned into a [lo, hi) window on the sorted neighbour list before the
+//    scan, which removes only candidates the filter rejects.  Candidate lists
+//    live in the warp's HBM slab and are generated in chunks (the reference's
+//    TEMPSIZE chunking, :617-622), so any degree fits.  The last position is
+//    counted, never materialised (:602-609).
+//  * clique (plans whose every position is adjacent to all earlier ones with
+//    images strictly increasing - presets 0, 23-27): every candidate lies in
+//    P0 = N(v) ∩ (v, ∞), so the root's P0 adjacency is built once as bitmap
+//    rows and the (k-1)-cliques of that local graph are counted with AND +
+//    popc.  Roots whose P0 needs more than 32*WPL words, or whose rows do not
+//    fit the slab, take the generic path inside the same kernel.
+// Both paths count exactly the embeddings the plan admits, so the result equals
+// the reference's "Total counts:".
+#include <cstdint>
+
+#include "g2_bitrows.cuh"
+#include "g2_device.cuh"
+#include "g2_kernels.h"
+
+namespace g2 {
+
+namespace {
+
+__constant__ DevPlan c_plan;
+
+__device__ __forceinline__ bool cond_ok(uint32_t op, uint32_t w, uint32_t m) {
+    return op == G2_COND_LESS_THAN ? w < m : op == G2_COND_LARGER_THAN ? w > m : w != m;
+}
+
+struct Level {
+    uint64_t pos, end;   // scan window in the parent's neighbour list
+    uint32_t len, idx;   // materialised chunk
+    uint32_t parent;     // position of the parent back neighbour
+};
+
+// Set up the scan window of position i given M[0..i-1].
+__device__ void level_init(const uint64_t *rp, const uint32_t *ci, const uint32_t *M, uint32_t i, Level &L) {
+    const DevPlan &pl = c_plan;
+    uint32_t parent = pl.bn_pos[i][0];
+    uint64_t pd = ldg(rp + M[parent] + 1) - ldg(rp + M[parent]);
+    for (uint32_t j = 1; j < pl.bn_count[i]; j++) {
+        uint32_t b = pl.bn_pos[i][j];
+        uint64_t d = ldg(rp + M[b] + 1) - ldg(rp + M[b]);
+        if (d < pd) pd = d, parent = b;
+    }
+    uint32_t lo = 0, hi = 0xffffffffu;
+    bool hi_set = false;
+    for (uint32_t c = 0; c < pl.cond_count[i]; c++) {
+        uint32_t m = M[pl.cond_pos[i][c]];
+        if (pl.cond_op[i][c] == G2_COND_LARGER_THAN) lo = m + 1 > lo ? m + 1 : lo;
+        else if (pl.cond_op[i][c] == G2_COND_LESS_THAN) hi = m < hi ? m : hi, hi_set = true;
+    }
+    uint64_t s = ldg(rp + M[parent]), e = ldg(rp + M[parent] + 1);
+    uint64_t ps = s, pe = e;
+    if (lane_id() == 0) {
+        ps = lo ? lower_bound(ci, s, e, lo) : s;
+        pe = hi_set ? lower_bound(ci, ps, e, hi) : e;
+    }
+    L.pos = __shfl_sync(G2_FULL, ps, 0);
+    L.end = __shfl_sync(G2_FULL, pe, 0);
+    L.len = 0;
+    L.idx = 0;
+    L.parent = parent;
+}
+
+// Does w qualify for position i (conditions + other back neighbours)?
+__device__ __forceinline__ bool cand_ok(const uint64_t *rp, const uint32_t *ci, const uint32_t *M, uint32_t i,
+                                        uint32_t parent, uint32_t w) {
+    const DevPlan &pl = c_plan;
+    for (uint32_t c = 0; c < pl.cond_count[i]; c++)
+        if (!cond_ok(pl.cond_op[i][c], w, M[pl.cond_pos[i][c]])) return false;
+    for (uint32_t j = 0; j < pl.bn_count[i]; j++) {
+        uint32_t b = pl.bn_pos[i][j];
+        if (b == parent) continue;
+        if (!contains(ci, ldg(rp + M[b]), ldg(rp + M[b] + 1), w)) return false;
+    }
+    return true;
+}
+
+// Generic plan-driven walk of one root; returns the number of embeddings.
+__device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v, uint32_t *S) {
+    const DevPlan &pl = c_plan;
+    const uint32_t k = pl.k;
+    const uint32_t lane = lane_id();
+    const uint64_t *rp = a.rp;
+    const uint32_t *ci = a.ci;
+    uint32_t M[G2_MAX_QUERY];
+    Level Ls[G2_MAX_QUERY];
+    M[0] = v;
+    const uint32_t nlists = k > 2 ? k - 2 : 1;
+    const uint32_t CH = (uint32_t)((a.words_per_warp / nlists) & ~31ull);
+    unsigned long long count = 0;
+    if (CH < 64) {  // a chunk must hold at least two warp-widths of candidates
+        if (lane == 0) atomicOr(a.status, kStatusStackOverflow);
+        return 0;
+    }
+    uint32_t i = 1;
+    level_init(rp, ci, M, 1, Ls[1]);
+    for (;;) {
+        Level &L = Ls[i];
+        if (i == k - 1) {
+            // last position: count, never materialise
+            for (uint64_t e = L.pos; e < L.end; e += 32) {
+                uint64_t x = e + lane;
+                bool ok = x < L.end && cand_ok(rp, ci, M, i, L.parent, ldg(ci + x));
+                count += __popc(__ballot_sync(G2_FULL, ok));
+            }
+            if (i == 1) break;
+            i--;
+            continue;
+        }
+        uint32_t *buf = S + (uint64_t)(i - 1) * CH;
+        if (L.idx == L.len) {
+            if (L.pos >= L.end) {
+                if (i == 1) break;
+                i--;
+                continue;
+            }
+            // next chunk of candidates
+            uint32_t len = 0;
+            while (L.pos < L.end && len + 32 <= CH) {
+                uint64_t x = L.pos + lane;
+                uint32_t w = x < L.end ? ldg(ci + x) : 0u;
+                bool ok = x < L.end && cand_ok(rp, ci, M, i, L.parent, w);
+                uint32_t tot;
+                uint32_t pos = warp_scan(ok, tot);
+                if (ok) buf[len + pos] = w;
+                len += tot;
+                L.pos += 32;
+            }
+            __syncwarp();
+            L.len = len;
+            L.idx = 0;
+            continue;
+        }
+        M[i] = buf[L.idx];
+        L.idx++;
+        i++;
+        level_init(rp, ci, M, i, Ls[i]);
+    }
+    return count;
+}
+
+// Clique plans on P0 bitmaps.  Returns false if the root does not fit (caller
+// falls back to the generic walk).
+template <int WPL>
+__device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, uint32_t *rowbuf,
+                                  unsigned long long &count) {
+    const DevPlan &pl = c_plan;
+    const uint32_t k = pl.k;
+    const uint32_t lane = lane_id();
+    const uint64_t *rp = a.rp;
+    const uint32_t *ci = a.ci;
+    const uint64_t lo = ldg(rp + v), hi = ldg(rp + v + 1);
+    count = 0;
+    if (lo == hi) return true;
+    uint64_t split = 0;
+    if (lane == 0) split = lower_bound(ci, lo, hi, v + 1);
+    split = __shfl_sync(G2_FULL, split, 0);
+    const uint32_t p = (uint32_t)(hi - split);
+    if (p + 1 < k) return true;
+    if (k == 2) {
+        count = p;
+        return true;
+    }
+    const uint32_t W = (p + 31u) >> 5;
+    if (W > 32u * WPL) return false;
+    // slab: [A p*W] [frames (k) * (W + 1)]
+    const uint64_t a0 = 0, f0 = (uint64_t)p * W;
+    if (f0 + (uint64_t)k * (W + 1) > a.words_per_warp) return false;
+    const uint32_t pmax = ldg(ci + hi - 1);
+    Row<WPL> row;
+    for (uint32_t i = 0; i < p; i++) {
+        build_row<WPL>(rp, ci, v, split, p, W, pmax, ldg(ci + split + i), row, rowbuf);
+        row_store(row, S + a0 + (uint64_t)i * W, W);
+    }
+    __syncwarp();
+    // C = remaining candidates at the current depth; depth = vertices chosen (v included)
+    Row<WPL> C;
+#pragma unroll
+    for (int s = 0; s < WPL; s++) {
+        uint32_t w = lane + 32u * s;
+        C.w[s] = w < W ? (w + 1 < W || (p & 31u) == 0 ? G2_FULL : ((1u << (p & 31u)) - 1u)) : 0u;
+    }
+    uint32_t depth = 1;
+    unsigned long long cnt = 0;
+    for (;;) {
+        // lowest remaining candidate x
+        uint32_t key = 0xffffffffu;
+#pragma unroll
+        for (int s = WPL - 1; s >= 0; s--)
+            if (C.w[s]) key = 32u * (uint32_t)s + lane;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            uint32_t y = __shfl_xor_sync(G2_FULL, key, o);
+            key = y < key ? y : key;
+        }
+        if (key == 0xffffffffu) {
+            if (depth == 1) break;
+            depth--;
+            row_load(C, S + f0 + (uint64_t)depth * (W + 1), W);
+            __syncwarp();
+            continue;
+        }
+        const uint32_t x = key * 32u + (uint32_t)(__ffs(row_word(C, key)) - 1);
+#pragma unroll
+        for (int s = 0; s < WPL; s++)
+            if (lane + 32u * s == key) C.w[s] &= ~(1u << (x & 31u));
+        Row<WPL> ax;
+        row_load(ax, S + a0 + (uint64_t)x * W, W);
+        if (depth + 2 == k) {
+            // children would be the last position: count C ∩ A[x]
+            uint32_t c = 0;
+#pragma unroll
+            for (int s = 0; s < WPL; s++) c += __popc(C.w[s] & ax.w[s]);
+            cnt += warp_sum_u64(c);
+            continue;
+        }
+        row_store(C, S + f0 + (uint64_t)depth * (W + 1), W);
+        __syncwarp();
+#pragma unroll
+        for (int s = 0; s < WPL; s++) C.w[s] &= ax.w[s];
+        depth++;
+    }
+    count = cnt;
+    return true;
+}
+
+template <int WPL>
+__global__ void __launch_bounds__(256) match_kernel(MatchArgs a, int clique_path) {
+    extern __shared__ uint32_t smem[];
+    const uint32_t wib = threadIdx.x >> 5;
+    uint32_t *rowbuf = smem + wib * 32u * WPL;
+    const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t *S = a.scratch + gw * a.words_per_warp;
+    unsigned long long total = 0;
+    for (;;) {
+        unsigned long long t0 = grab(a.head, a.chunk);
+        if (t0 >= a.ntasks) break;
+        unsigned long long t1 = t0 + a.chunk < a.ntasks ? t0 + a.chunk : a.ntasks;
+        for (unsigned long long t = t0; t < t1; t++) {
+            uint64_t task = a.task_index ? a.task_index[t] : t;
+            uint32_t v = a.tasks[task];
+            unsigned long long c = 0;
+            if (!clique_path || !match_root_clique<WPL>(a, v, S, rowbuf, c)) c = match_root_generic(a, v, S);
+            total += c;
+            if (a.root_nodes && lane_id() == 0) a.root_nodes[task] = c;
+        }
+    }
+    if (lane_id() == 0 && total) atomicAdd(a.out, total);
+}
+
+}  // namespace
+
+cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block, cudaStream_t st,
+                         bool clique_path, int wpl) {
+    cudaError_t e = cudaMemcpyToSymbolAsync(c_plan, &plan, sizeof(DevPlan), 0, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    size_t sm = (size_t)warps_per_block * 32u * wpl * sizeof(uint32_t);
+    dim3 g(blocks), b(32 * warps_per_block);
+    switch (wpl) {
+        case 1: match_kernel<1><<<g, b, sm, st>>>(a, clique_path ? 1 : 0); break;
+        case 2: match_kernel<2><<<g, b, sm, st>>>(a, clique_path ? 1 : 0); break;
+        case 4: match_kernel<4><<<g, b, sm, st>>>(a, clique_path ? 1 : 0); break;
+        case 8: match_kernel<8><<<g, b, sm, st>>>(a, clique_path ? 1 : 0); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace g2

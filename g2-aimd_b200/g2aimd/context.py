@@ -1,0 +1,189 @@
+"""Python side of the C ABI: a device context, query plans, and the two
+enumerations (maximal cliques, plan-driven subgraph counts).
+
+This mirrors the reference's app plugin surface: `Context.mce` is what
+Worker<BKExpandSequential> computes (sum of the "Total No. of Cliques:" lines,
+app_BK/BK.h:72-76) and `Context.match` is Worker<GMatchApp>'s "Total counts:"
+(system/worker.h:273-279).  All work runs in libg2aimd.so on the GPU; errors
+are raised, never hidden.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import G2_MAX_QUERY, G2Opts, G2Plan, check, lib
+
+SCHED = {"given": 0, "heuristic": 1, "scores": 2}
+
+
+class Plan:
+    """A query plan (GMContext arrays, system/appbase.h:11-68)."""
+
+    def __init__(self, raw: G2Plan):
+        self.raw = raw
+
+    @staticmethod
+    def preset(query_id: int) -> "Plan":
+        p = G2Plan()
+        check(lib().g2_plan_preset(int(query_id), C.byref(p)), f"plan preset {query_id}")
+        return Plan(p)
+
+    @staticmethod
+    def from_edges(k: int, edges) -> "Plan":
+        e = np.ascontiguousarray(np.asarray(edges, dtype=np.uint32).reshape(-1, 2))
+        p = G2Plan()
+        check(lib().g2_plan_build(k, e.ctypes.data_as(C.c_void_p), e.shape[0], C.byref(p)), "plan build")
+        return Plan(p)
+
+    @property
+    def k(self) -> int:
+        return self.raw.k
+
+    def to_dict(self) -> dict:
+        """Same field layout as the reference-planner fixtures."""
+        r, k = self.raw, self.raw.k
+        lst = lambda cnt, arr: [[arr[i][j] for j in range(cnt[i])] for i in range(k)]  # noqa: E731
+        lst2 = lambda cnt, arr: [[[arr[i][j][0], arr[i][j][1]] for j in range(cnt[i])] for i in range(k)]  # noqa
+        return {
+            "k": k, "hop": r.hop, "root_degree": r.root_degree,
+            "order": list(r.order[:k]), "id2order": list(r.id2order[:k]),
+            "bn_count": list(r.bn_count[:k]), "bn": lst(r.bn_count, r.bn), "share": list(r.share[:k]),
+            "pre_bn": lst(r.pre_bn_count, r.pre_bn), "after_bn": lst(r.after_bn_count, r.after_bn),
+            "cond": lst2(r.cond_count, r.cond), "pre_cond": lst2(r.pre_cond_count, r.pre_cond),
+            "after_cond": lst2(r.after_cond_count, r.after_cond),
+            "strategy": list(r.strategy[:k + 1]), "moving_lvl": list(r.moving_lvl[:k]),
+        }
+
+    def flat(self):
+        """(order, id2order, bn_count, bn[k*k], cond_count, cond[k*k*2]) with
+        the reference's strides, for the oracle."""
+        r, k = self.raw, self.raw.k
+        bn = np.zeros(k * k, np.uint32)
+        cond = np.zeros(k * k * 2, np.uint32)
+        for i in range(k):
+            for j in range(r.bn_count[i]):
+                bn[i * k + j] = r.bn[i][j]
+            for j in range(r.cond_count[i]):
+                cond[(i * k + j) * 2] = r.cond[i][j][0]
+                cond[(i * k + j) * 2 + 1] = r.cond[i][j][1]
+        return (np.array(r.order[:k], np.uint32), np.array(r.id2order[:k], np.uint32),
+                np.array(r.bn_count[:k], np.uint32), bn, np.array(r.cond_count[:k], np.uint32), cond)
+
+
+def _opts(warps_per_block=0, blocks=0, schedule="given", scores=None, root_nodes=None, intersect_mode=0,
+          split_threshold=0):
+    o = G2Opts()
+    o.warps_per_block = warps_per_block
+    o.blocks = blocks
+    o.schedule = SCHED[schedule]
+    o.split_threshold = split_threshold
+    o.intersect_mode = intersect_mode
+    keep = []
+    if scores is not None:
+        s = np.ascontiguousarray(scores, dtype=np.float32)
+        keep.append(s)
+        o.scores = s.ctypes.data_as(C.POINTER(C.c_float))
+    if root_nodes is not None:
+        o.root_nodes = root_nodes.ctypes.data_as(C.POINTER(C.c_uint64))
+    return o, keep
+
+
+class Context:
+    """One device context (g2_open).  Load a graph, then run enumerations."""
+
+    def __init__(self, device: int = 0, scratch_bytes: int = 0):
+        self._h = C.c_void_p()
+        check(lib().g2_open(device, scratch_bytes, C.byref(self._h)), "g2_open")
+        self.graph = None
+
+    def close(self):
+        if self._h:
+            check(lib().g2_close(self._h), "g2_close")
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def cuda_error(self) -> str:
+        return lib().g2_last_cuda_error(self._h).decode()
+
+    def launches(self) -> int:
+        return int(lib().g2_last_launch_count(self._h))
+
+    def _check(self, rc, where):
+        if rc != 0:
+            err = self.cuda_error()
+            check(rc, where + (f" [{err}]" if err else ""))
+
+    def load(self, graph):
+        self._check(lib().g2_load_csr(self._h, graph.row_ptrs.ctypes.data_as(C.c_void_p),
+                                      graph.cols.ctypes.data_as(C.c_void_p), graph.n, graph.m), "g2_load_csr")
+        self.graph = graph
+        return self
+
+    def load_device(self, d_row_ptrs: int, d_cols: int, n: int, m: int):
+        """Borrow a CSR already in device memory (raw device pointers)."""
+        self._check(lib().g2_load_csr_device(self._h, C.c_void_p(d_row_ptrs), C.c_void_p(d_cols), n, m),
+                    "g2_load_csr_device")
+        return self
+
+    def set_plan(self, plan: Plan):
+        self._check(lib().g2_set_plan(self._h, C.byref(plan.raw)), "g2_set_plan")
+        return self
+
+    def mce(self, sources=None, hist_len=256, root_nodes=False, **kw):
+        """(count, hist) of maximal cliques rooted at `sources` (default: all);
+        with root_nodes=True also the search-tree node count per source."""
+        src = None if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+        nsrc = 0 if src is None else src.size
+        rn = np.zeros(nsrc if src is not None else self.graph.n, np.uint64) if root_nodes else None
+        o, keep = _opts(root_nodes=rn, **kw)
+        count = C.c_uint64()
+        hist = np.zeros(hist_len, np.uint64)
+        self._check(lib().g2_mce_run(self._h, None if src is None else src.ctypes.data_as(C.c_void_p), nsrc,
+                                     C.byref(o), C.byref(count), hist.ctypes.data_as(C.c_void_p), hist_len),
+                    "g2_mce_run")
+        del keep
+        return (count.value, hist, rn) if root_nodes else (count.value, hist)
+
+    def match(self, plan: Plan = None, sources=None, **kw):
+        if plan is not None:
+            self.set_plan(plan)
+        src = None if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+        o, keep = _opts(**kw)
+        count = C.c_uint64()
+        self._check(lib().g2_match_run(self._h, None if src is None else src.ctypes.data_as(C.c_void_p),
+                                       0 if src is None else src.size, C.byref(o), C.byref(count)), "g2_match_run")
+        del keep
+        return count.value
+
+    # device-resident entry points (timing): pointers are raw device addresses
+    def mce_device(self, d_out: int, hist_len: int, d_sources: int = 0, nsrc: int = 0, stream: int = 0, **kw):
+        o, keep = _opts(**kw)
+        self._check(lib().g2_mce_run_device(self._h, C.c_void_p(d_sources) if d_sources else None, nsrc,
+                                            C.byref(o), C.c_void_p(d_out), hist_len, C.c_void_p(stream)),
+                    "g2_mce_run_device")
+
+    def match_device(self, d_out: int, d_sources: int = 0, nsrc: int = 0, stream: int = 0, **kw):
+        o, keep = _opts(**kw)
+        self._check(lib().g2_match_run_device(self._h, C.c_void_p(d_sources) if d_sources else None, nsrc,
+                                              C.byref(o), C.c_void_p(d_out), C.c_void_p(stream)),
+                    "g2_match_run_device")
+
+
+__all__ = ["Context", "Plan", "G2_MAX_QUERY"]

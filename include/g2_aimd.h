@@ -1,0 +1,252 @@
+/*
+ * g2_aimd.h - C ABI of the B200 subgraph-search library (libg2aimd.so).
+ *
+ * The reference (lyuheng/g2-aimd) exposes its hot path as a compile-time C++
+ * template plugin: Worker<App>::run (system/worker.h:28) builds a
+ * PipelineExecutor<App> (system/pipeline_executor.h:44), which uploads one CSR
+ * view bin (Transfer, system/pipeline_executor.h:121-147), runs the BFS level
+ * loop (Run, system/pipeline_executor.h:151-207) and reads the app's counters
+ * (BK: totalCliques, app_BK/BK.h:38-76; GMatch: total_counts_ summed in
+ * system/worker.h:250-279).  This header replaces that plugin boundary with plain
+ * functions over plain pointers: one context per device, a CSR upload, a
+ * query-plan upload and one call per enumeration.  Every call returns an int
+ * status (0 = G2_OK, negative = error; see g2_strerror), outputs are
+ * caller-owned, and no call exits the process (the reference prints and calls
+ * exit(-1), common/gpu_env.h:85-92).
+ *
+ * Types follow the reference .bin format (common/graph.h:360-398):
+ * vertex ids uint32_t (uintV, common/meta.h:15), edge offsets uint64_t (uintE,
+ * common/meta.h:16); neighbour lists sorted, deduplicated, no self loops,
+ * every edge stored in both directions.
+ */
+#ifndef G2_AIMD_H
+#define G2_AIMD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define G2_OK 0
+#define G2_ERR_INVALID (-1)      /* bad argument (null pointer, size, range)  */
+#define G2_ERR_CUDA (-2)         /* CUDA runtime error; see g2_last_cuda_error */
+#define G2_ERR_OOM (-3)          /* device or pinned allocation failed         */
+#define G2_ERR_TIMEOUT (-4)      /* a bounded device wait ran out (hang guard) */
+#define G2_ERR_OVERFLOW (-5)     /* scratch and host spill both exhausted      */
+#define G2_ERR_NO_GRAPH (-6)     /* no CSR loaded in this context              */
+#define G2_ERR_NO_PLAN (-7)      /* g2_match_run without g2_set_plan           */
+#define G2_ERR_UNSUPPORTED (-8)  /* e.g. query larger than G2_MAX_QUERY        */
+#define G2_ERR_IO (-9)           /* file could not be read or written          */
+#define G2_ERR_HIST (-10)        /* clique larger than the histogram supplied  */
+
+/* Largest query pattern: the reference keeps a partial embedding in
+ * partial_subgraphs[WARPS_EACH_BLK][8] (app_gmatch/gmatch.h:87). */
+#define G2_MAX_QUERY 8
+
+/* Condition operators, same values as CondOperator (common/meta.h:22). */
+#define G2_COND_LESS_THAN 0
+#define G2_COND_LARGER_THAN 1
+#define G2_COND_NON_EQUAL 2
+
+/* Store strategies, same values as StoreStrategy (common/meta.h:24). */
+#define G2_STORE_EXPAND 0
+#define G2_STORE_PREFIX 1
+#define G2_STORE_COUNT 2
+
+/*
+ * Query plan: the flat arrays of GMContext (system/appbase.h:11-68) as built by
+ * Plan (system/plan.h:51-372) and uploaded by AppBase::allocateGMMemory
+ * (system/appbase.h:156-216), with fixed capacity G2_MAX_QUERY.
+ * Indexing follows the reference exactly:
+ *   - by POSITION p in the match order: bn_*, pre_bn_*, after_bn_*, share,
+ *     strategy (strategy has k+1 entries, strategy[k] = COUNT);
+ *   - by QUERY VERTEX u: cond_*, pre_cond_*, after_cond_*;
+ *   - entries of bn / cond lists are QUERY VERTEX ids (map with id2order).
+ * cond[u][j] = {op, query vertex}: LESS_THAN means M(u) < M(vertex).
+ */
+typedef struct g2_plan {
+    uint32_t k;                                   /* query vertices          */
+    uint32_t hop;                                 /* Plan::GetHop            */
+    uint32_t root_degree;                         /* Plan::root_degree_      */
+    uint32_t order[G2_MAX_QUERY];                 /* matchOrder (seq_)       */
+    uint32_t id2order[G2_MAX_QUERY];              /* ID2order (reverse_seq_) */
+    uint32_t bn_count[G2_MAX_QUERY];
+    uint32_t bn[G2_MAX_QUERY][G2_MAX_QUERY];
+    uint32_t parent[G2_MAX_QUERY];                /* parentHost (unused on device) */
+    uint32_t cond_count[G2_MAX_QUERY];
+    uint32_t cond[G2_MAX_QUERY][G2_MAX_QUERY][2];
+    uint32_t share[G2_MAX_QUERY];                 /* shareIntersection (0/1) */
+    uint32_t pre_bn_count[G2_MAX_QUERY];
+    uint32_t pre_bn[G2_MAX_QUERY][G2_MAX_QUERY];
+    uint32_t pre_cond_count[G2_MAX_QUERY];
+    uint32_t pre_cond[G2_MAX_QUERY][G2_MAX_QUERY][2];
+    uint32_t after_bn_count[G2_MAX_QUERY];
+    uint32_t after_bn[G2_MAX_QUERY][G2_MAX_QUERY];
+    uint32_t after_cond_count[G2_MAX_QUERY];
+    uint32_t after_cond[G2_MAX_QUERY][G2_MAX_QUERY][2];
+    uint32_t strategy[G2_MAX_QUERY + 1];
+    uint32_t moving_lvl[G2_MAX_QUERY];
+} g2_plan;
+
+/* Root schedule (task order of the device work queue). */
+#define G2_SCHED_GIVEN 0      /* sources in the order given                      */
+#define G2_SCHED_HEURISTIC 1  /* plain heuristic: descending forward degree x core */
+#define G2_SCHED_SCORES 2     /* descending caller scores (learned cost model)     */
+
+/*
+ * Run options.  Zero-initialise and set what you need; 0 means "default".
+ */
+typedef struct g2_opts {
+    uint32_t blocks;            /* persistent CTAs (default: 148 x occupancy)       */
+    uint32_t warps_per_block;   /* default 8                                        */
+    uint32_t schedule;          /* G2_SCHED_*                                       */
+    uint32_t split_threshold;   /* MCE: split roots whose |P0| exceeds this into one
+                                   task per branch (0 = default, ~0u = never)      */
+    const float *scores;        /* host, nsrc entries, for G2_SCHED_SCORES          */
+    uint64_t *root_nodes;       /* optional host out: search-tree nodes per source  */
+    uint64_t *work_bytes;       /* optional host out: algorithmic bytes W (MCE)     */
+    uint32_t intersect_mode;    /* GMatch: 0 auto, 1 binary search, 2 merge          */
+    uint32_t reserved[7];
+} g2_opts;
+
+typedef struct g2_ctx g2_ctx;
+
+/* Library version string and the text of an error code. */
+const char *g2_version(void);
+const char *g2_strerror(int code);
+/* Text of the last CUDA error seen in this context (or "" if none). */
+const char *g2_last_cuda_error(const g2_ctx *ctx);
+
+/* Open a context on `device` (replaces the PipelineExecutor constructor,
+ * system/pipeline_executor.h:44-99; no memory is pinned to "all free memory").
+ * scratch_bytes = device scratch budget for DFS frames (0 = default 4 GiB). */
+int g2_open(int device, uint64_t scratch_bytes, g2_ctx **out);
+int g2_close(g2_ctx *ctx);
+
+/* Upload a CSR from host memory (replaces Transfer,
+ * system/pipeline_executor.h:121-147).  The context keeps a device copy. */
+int g2_load_csr(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols,
+                uint64_t n, uint64_t m);
+/* Borrow a CSR that already lives in device memory of this context's device.
+ * The caller keeps it alive until the next load or g2_close. */
+int g2_load_csr_device(g2_ctx *ctx, const uint64_t *d_row_ptrs,
+                       const uint32_t *d_cols, uint64_t n, uint64_t m);
+
+/* Upload a query plan (replaces AppBase::allocateGMMemory,
+ * system/appbase.h:156-216). */
+int g2_set_plan(g2_ctx *ctx, const g2_plan *plan);
+
+/*
+ * Maximal clique enumeration (Bron-Kerbosch with Tomita pivot) rooted at
+ * `sources` (host array; NULL = every vertex 0..n-1).  Replaces app_BK
+ * (BKExpandSequential, app_BK/BK.h:400-480) run through Worker/PipelineExecutor;
+ * the result equals the sum of the reference's "Total No. of Cliques:" lines.
+ * Root v starts with R={v}, P=N(v)∩(v,∞), X=N(v)∩[0,v) (app_BK/BK.h:323-355);
+ * vertices without neighbours are skipped (app_BK/BK.h:335-336).
+ * count: number of maximal cliques; hist[s] = maximal cliques with s vertices
+ * (hist may be NULL; G2_ERR_HIST if a clique has >= hist_len vertices).
+ */
+int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc,
+               const g2_opts *opts, uint64_t *count, uint64_t *hist,
+               uint32_t hist_len);
+
+/*
+ * Plan-driven subgraph enumeration of the plan set by g2_set_plan, rooted at
+ * `sources` (host array; NULL = all vertices).  Replaces GMatchApp
+ * (app_gmatch/gmatch.h:15-736); *count equals the reference's "Total counts:"
+ * line (system/worker.h:273-279): the number of embeddings that satisfy the
+ * plan's symmetry-breaking conditions.
+ */
+int g2_match_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc,
+                 const g2_opts *opts, uint64_t *count);
+
+/*
+ * Device-resident variants used for timing: sources and outputs live in device
+ * memory of this context; work is enqueued on `stream` (a cudaStream_t, may be
+ * NULL for the legacy default stream) and the call returns without
+ * synchronising.  d_out receives the counters:
+ *   MCE:   d_out[0] = count, d_out[1 + s] = hist[s] for s < hist_len;
+ *   match: d_out[0] = count.
+ * d_out must hold 1 + hist_len (MCE) or 1 (match) uint64_t.
+ */
+int g2_mce_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc,
+                      const g2_opts *opts, uint64_t *d_out, uint32_t hist_len,
+                      void *stream);
+int g2_match_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc,
+                        const g2_opts *opts, uint64_t *d_out, void *stream);
+
+/* Number of kernels the last run launched (for launch accounting). */
+uint64_t g2_last_launch_count(const g2_ctx *ctx);
+
+/* ------------------------------------------------------ host-side helpers */
+
+/* Query planner: preset pattern id (0..27 as PresetPatternType,
+ * common/graph.h:25-55) -> plan, following Graph(QUERY) + ReMapVertexId
+ * (common/graph.h:127-266), GetConditions (common/graph.h:658-699) and
+ * Plan::FindRoot..GenerateStoreStrategy (system/plan.h:51-372). */
+int g2_plan_preset(int query_id, g2_plan *out);
+/* Same for an arbitrary connected query given as an edge list over 0..k-1. */
+int g2_plan_build(uint32_t k, const uint32_t *edges, uint32_t nedges,
+                  g2_plan *out);
+
+/* .bin CSR I/O (common/graph.h:360-398 and :539-562).  g2_read_bin allocates
+ * *row_ptrs / *cols with malloc; free them with g2_free. */
+int g2_read_bin(const char *path, uint64_t **row_ptrs, uint32_t **cols,
+                uint64_t *n, uint64_t *m);
+int g2_write_bin(const char *path, const uint64_t *row_ptrs,
+                 const uint32_t *cols, uint64_t n, uint64_t m);
+void g2_free(void *p);
+
+/* .vbmap view-bin partition (view/view_bin_manager.h:34-94): "nbins b0 b1 ...".
+ * Writes `n` bin ids; all-zero when nbins == 1. */
+int g2_write_vbmap(const char *path, uint32_t nbins, const uint32_t *bins,
+                   uint64_t n);
+int g2_read_vbmap(const char *path, uint64_t n, uint32_t *nbins,
+                  uint32_t *bins);
+
+/*
+ * Degeneracy order (kmeans/kcore.cpp:103-191): k-core shells in increasing core
+ * number, vertices of a shell by increasing degree (ties: lower old id), then
+ * recode ids so that u < v means "u earlier in the order".
+ * core (optional, n entries) receives core numbers in OLD ids; perm (n entries)
+ * receives new_id[old_id].  g2_recode applies a permutation to a CSR
+ * (neighbour lists re-sorted); outputs preallocated by the caller.
+ */
+int g2_degeneracy_order(const uint64_t *row_ptrs, const uint32_t *cols,
+                        uint64_t n, uint32_t *perm, uint32_t *core);
+int g2_recode(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n,
+              const uint32_t *perm, uint64_t *out_row_ptrs,
+              uint32_t *out_cols);
+
+/*
+ * Seeded synthetic graphs, written as a symmetric, deduplicated, self-loop free
+ * CSR (*row_ptrs / *cols malloc'd; free with g2_free).  Every random draw is a
+ * counter-based hash of (seed, stream, index), so any thread count gives the
+ * same graph.
+ *   er:      G(n, p) plus `nplanted` cliques of size `planted_size` on disjoint
+ *            random vertex sets;
+ *   rmat:    2^scale vertices, edge_factor * 2^scale generated edges with
+ *            quadrant probabilities (a, b, c, 1-a-b-c), plus `nplanted` cliques
+ *            of sizes uniform in [planted_min, planted_max];
+ *   chunglu: n vertices, expected degree w_i ~ (i+1)^(-1/(gamma-1)) scaled to
+ *            avg_degree, n*avg_degree/2 edges drawn proportional to w.
+ */
+int g2_gen_er(uint64_t n, double p, uint32_t nplanted, uint32_t planted_size,
+              uint64_t seed, uint64_t **row_ptrs, uint32_t **cols,
+              uint64_t *out_n, uint64_t *out_m);
+int g2_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b,
+                double c, uint32_t nplanted, uint32_t planted_min,
+                uint32_t planted_max, uint64_t seed, uint64_t **row_ptrs,
+                uint32_t **cols, uint64_t *out_n, uint64_t *out_m);
+int g2_gen_chunglu(uint64_t n, double gamma, double avg_degree, uint64_t seed,
+                   uint64_t **row_ptrs, uint32_t **cols, uint64_t *out_n,
+                   uint64_t *out_m);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* G2_AIMD_H */

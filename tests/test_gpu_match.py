@@ -1,0 +1,51 @@
+"""Plan-driven subgraph counts on the GPU against the CPU oracle."""
+import numpy as np
+import pytest
+
+from helpers import random_graph
+
+pytestmark = pytest.mark.gpu
+
+QUERIES = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16, 17, 18, 23, 24, 25, 26]
+
+
+@pytest.mark.parametrize("q", QUERIES)
+def test_presets_small(g2, orc, ctx, q):
+    from g2aimd.context import Plan
+    plan = Plan.preset(q)
+    for g in (random_graph(g2.Graph, 40, 0.3, 5 + q, planted=[tuple(range(0, 9))]),
+              g2.Graph.rmat(9, 8, seed=q).degeneracy_recoded()):
+        ctx.load(g)
+        want = orc.match(g, plan)["count"]
+        assert ctx.match(plan) == want, (q, g.name)
+        assert ctx.match(plan, intersect_mode=1) == want, (q, g.name, "generic")
+
+
+@pytest.mark.parametrize("q", [0, 1, 2, 24, 25])
+def test_rmat_s14(g2, orc, ctx, q):
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(14, 16, seed=3).degeneracy_recoded()
+    plan = Plan.preset(q)
+    ctx.load(g)
+    want = orc.match(g, plan, threads=8)["count"]
+    assert ctx.match(plan) == want
+    assert ctx.match(plan, schedule="heuristic") == want
+
+
+def test_raw_ids_and_sources(g2, orc, ctx):
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(12, 8, seed=8)
+    ctx.load(g)
+    src = np.arange(0, g.n, 3, dtype=np.uint32)
+    for q in (0, 2, 24):
+        plan = Plan.preset(q)
+        assert ctx.match(plan, sources=src) == orc.match(g, plan, roots=src, threads=8)["count"]
+
+
+def test_empty_and_tiny(g2, ctx):
+    from g2aimd.context import Plan
+    ctx.load(g2.Graph.from_edges(5, []))
+    assert ctx.match(Plan.preset(0)) == 0
+    ctx.load(g2.Graph.from_edges(3, [(0, 1), (1, 2), (0, 2)]))
+    assert ctx.match(Plan.preset(0)) == 1
+    assert ctx.match(Plan.preset(24)) == 0

@@ -1,0 +1,87 @@
+"""Maximal clique enumeration on the GPU against the CPU oracle (bit-exact
+count, size histogram and per-root search-tree size)."""
+import numpy as np
+import pytest
+
+from helpers import random_graph, small_graphs
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(got, want, name):
+    c, h = got[0], got[1]
+    assert c == want["count"], name
+    assert np.array_equal(h[: want["hist"].size], want["hist"][: h.size]), name
+
+
+def test_small_graphs(g2, orc, ctx):
+    for g in small_graphs(g2.Graph):
+        for recode in (False, True):
+            gg = g.degeneracy_recoded() if recode else g
+            ctx.load(gg)
+            want = orc.mce(gg, per_root=True)
+            c, h, rn = ctx.mce(root_nodes=True)
+            _same((c, h), want, gg.name)
+            assert np.array_equal(rn, want["root_nodes"]), gg.name
+
+
+def test_config1_er_planted(orc, ctx, c1_graph):
+    """ER(2000, 0.01) + 5 x K12: count, histogram and tree shape."""
+    ctx.load(c1_graph)
+    want = orc.mce(c1_graph, threads=4, per_root=True)
+    c, h, rn = ctx.mce(root_nodes=True)
+    _same((c, h), want, "c1")
+    assert h[12] >= 5
+    assert np.array_equal(rn, want["root_nodes"])
+
+
+def test_rmat_and_schedules(g2, orc, ctx):
+    g = g2.Graph.rmat(14, 16, seed=11).degeneracy_recoded()
+    ctx.load(g)
+    want = orc.mce(g, threads=8, per_root=True)
+    for sched in ("given", "heuristic"):
+        c, h, rn = ctx.mce(root_nodes=True, schedule=sched)
+        _same((c, h), want, sched)
+        assert np.array_equal(rn, want["root_nodes"]), sched
+    scores = np.random.default_rng(0).random(g.n).astype(np.float32)
+    c, h = ctx.mce(schedule="scores", scores=scores)
+    _same((c, h), want, "scores")
+
+
+def test_sources_subset_and_order(g2, orc, ctx):
+    g = random_graph(g2.Graph, 400, 0.05, 3, planted=[tuple(range(0, 200, 17))]).degeneracy_recoded()
+    ctx.load(g)
+    src = np.random.default_rng(1).permutation(g.n)[:150].astype(np.uint32)
+    want = orc.mce(g, roots=src, per_root=True)
+    c, h, rn = ctx.mce(sources=src, root_nodes=True)
+    _same((c, h), want, "subset")
+    assert np.array_equal(rn, want["root_nodes"])
+    c2, h2, rn2 = ctx.mce(sources=src, root_nodes=True, schedule="heuristic")
+    assert c2 == c and np.array_equal(h2, h) and np.array_equal(rn2, rn)
+
+
+def test_deferral_passes_with_tiny_scratch(g2, orc):
+    """A slab too small for the big roots sends them through the deferred
+    passes (bigger slab per warp); results do not change."""
+    from g2aimd.context import Context
+    g = g2.Graph.rmat(13, 16, seed=5).degeneracy_recoded()
+    want = orc.mce(g, threads=8)
+    with Context(0, scratch_bytes=64 << 20) as c:
+        c.load(g)
+        got = c.mce()
+    _same(got, want, "tiny-scratch")
+
+
+def test_not_degeneracy_ordered(g2, orc, ctx):
+    """Raw R-MAT ids (hubs early): large forward sets, wide rows."""
+    g = g2.Graph.rmat(12, 8, seed=21)
+    ctx.load(g)
+    want = orc.mce(g, threads=8)
+    _same(ctx.mce(), want, "raw-ids")
+
+
+def test_histogram_too_short_is_an_error(g2, ctx):
+    g = g2.Graph.from_edges(6, [(a, b) for a in range(6) for b in range(a + 1, 6)])
+    ctx.load(g)
+    with pytest.raises(g2.G2Error):
+        ctx.mce(hist_len=4)
