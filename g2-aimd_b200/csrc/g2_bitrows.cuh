@@ -62,47 +62,206 @@ __device__ __forceinline__ uint32_t row_word(const Row<WPL> &r, uint32_t w) {
 
 __device__ __forceinline__ uint32_t ilog2p1(uint64_t x) { return 64u - (uint32_t)__clzll((long long)x); }
 
-// Row of u against P0 = ci[split, split+p), all lanes participate; rowbuf is this
-// warp's shared scratch of 32*WPL words.
-template <int WPL>
-__device__ void build_row(const uint64_t *rp, const uint32_t *ci, uint32_t v, uint64_t split, uint32_t p,
-                          uint32_t W, uint32_t pmax, uint32_t u, Row<WPL> &row, uint32_t *rowbuf) {
+// Transpose of a 32x32 bit tile held one word per lane: on return lane L
+// holds the word whose bit l is bit L of lane l's input.
+__device__ __forceinline__ uint32_t transpose32(uint32_t w) {
     const uint32_t lane = lane_id();
-    const uint64_t ulo = ldg(rp + u), uhi = ldg(rp + u + 1);
-    const uint64_t du = uhi - ulo;
-    row_zero(row);
-    if (du == 0) return;
-    if ((uint64_t)p * ilog2p1(du) <= du * ilog2p1(p)) {
-        // test every P0 member in N(u)
-        for (uint32_t c = 0; c < W; c++) {
-            uint32_t j = 32u * c + lane;
-            bool f = j < p && contains(ci, ulo, uhi, ldg(ci + split + j));
-            uint32_t bits = __ballot_sync(G2_FULL, f);
+    uint32_t t = 0;
 #pragma unroll
-            for (int s = 0; s < WPL; s++)
-                if ((c >> 5) == (uint32_t)s && lane == (c & 31u)) row.w[s] = bits;
-        }
-    } else {
-        // locate every neighbour of u inside P0
-#pragma unroll
-        for (int s = 0; s < WPL; s++)
-            if (lane + 32u * s < W) rowbuf[lane + 32u * s] = 0u;
-        __syncwarp();
-        for (uint64_t e = ulo + lane; e < uhi; e += 32) {
-            uint32_t y = ldg(ci + e);
-            if (y > v && y <= pmax) {
-                uint64_t j = lower_bound(ci, split, split + p, y);
-                if (j < split + p && ldg(ci + j) == y) {
-                    uint32_t jj = (uint32_t)(j - split);
-                    atomicOr(rowbuf + (jj >> 5), 1u << (jj & 31u));
+    for (int b = 0; b < 32; b++) {
+        uint32_t col = __ballot_sync(G2_FULL, (w >> b) & 1u);
+        if (lane == (uint32_t)b) t = col;
+    }
+    return t;
+}
+
+// First index in [lo, hi) of the shared-memory array a with a[i] >= key.
+__device__ __forceinline__ uint32_t smem_lower_bound(const uint32_t *a, uint32_t lo, uint32_t hi, uint32_t key) {
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+constexpr uint32_t kLongList = 96;  // forward lists longer than this are scanned by the whole warp
+
+// Adjacency rows of the root's forward neighbourhood.
+//   p0s   : P0 = N(v) ∩ (v, ∞) staged in shared memory (p sorted ids)
+//   fo    : fo[u] = offset of the first neighbour of u larger than u
+//   A     : p rows of W words (slab), row i = N(P0[i]) ∩ P0
+// Upper parts come from forward lists (P0[j] ∈ N+(P0[i]) for j > i), one lane
+// per row (the warp together for long lists); the lower parts are the
+// transpose, added 32x32 tile by tile.
+__device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo,
+                                   const uint32_t *p0s, uint32_t p, uint32_t W, uint32_t *A, uint32_t *rowbuf) {
+    const uint32_t lane = lane_id();
+    const uint32_t pmax = p0s[p - 1];
+    for (uint64_t w = lane; w < (uint64_t)p * W; w += 32) A[w] = 0u;
+    __syncwarp();
+    for (uint32_t i0 = 0; i0 < p; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        bool big = false;
+        if (i < p) {
+            const uint32_t u = p0s[i];
+            uint64_t e = ldg(rp + u) + ldg(fo + u);
+            const uint64_t end = ldg(rp + u + 1);
+            if (end - e > kLongList) big = true;
+            else {
+                uint32_t *row = A + (uint64_t)i * W;
+                uint32_t j = i + 1;
+                for (; e < end; e++) {
+                    const uint32_t y = ldg(ci + e);
+                    if (y > pmax) break;
+                    j = smem_lower_bound(p0s, j, p, y);
+                    if (j < p && p0s[j] == y) row[j >> 5] |= 1u << (j & 31u);
                 }
             }
         }
-        __syncwarp();
-#pragma unroll
-        for (int s = 0; s < WPL; s++) row.w[s] = (lane + 32u * s < W) ? rowbuf[lane + 32u * s] : 0u;
+        uint32_t bigmask = __ballot_sync(G2_FULL, big);
+        while (bigmask) {
+            const uint32_t l = __ffs(bigmask) - 1;
+            bigmask &= bigmask - 1;
+            const uint32_t ii = i0 + l;
+            const uint32_t u = p0s[ii];
+            const uint64_t e0 = ldg(rp + u) + ldg(fo + u), end = ldg(rp + u + 1);
+            for (uint32_t w = lane; w < W; w += 32) rowbuf[w] = 0u;
+            __syncwarp();
+            for (uint64_t e = e0 + lane; e < end; e += 32) {
+                const uint32_t y = ldg(ci + e);
+                if (y > pmax) break;
+                const uint32_t j = smem_lower_bound(p0s, ii + 1, p, y);
+                if (j < p && p0s[j] == y) atomicOr(rowbuf + (j >> 5), 1u << (j & 31u));
+            }
+            __syncwarp();
+            for (uint32_t w = lane; w < W; w += 32) A[(uint64_t)ii * W + w] = rowbuf[w];
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+    // A |= A^T over upper tiles (tr <= tc)
+    for (uint32_t tr = 0; tr < W; tr++) {
+        for (uint32_t tc = tr; tc < W; tc++) {
+            const uint32_t r = 32u * tr + lane;
+            const uint32_t w = r < p ? A[(uint64_t)r * W + tc] : 0u;
+            const uint32_t t = transpose32(w);
+            const uint32_t r2 = 32u * tc + lane;
+            if (r2 < p) A[(uint64_t)r2 * W + tr] |= t;
+            __syncwarp();
+        }
+    }
+}
+
+// B rows of the root's backward neighbours X0 = ci[lo, lo+nx) (ids < v):
+// row = N+(x) ∩ P0.  Only non-zero rows are kept, compacted in X0 order into
+// B (nb rows of W words); xv (optional) receives the vertex of each kept row.
+// Returns nb, or ~0u if more than cap rows would be needed.
+__device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, uint32_t v,
+                                    uint64_t lo, uint32_t nx, const uint32_t *p0s, uint32_t p, uint32_t W,
+                                    uint32_t *B, uint32_t *xv, uint32_t cap, uint32_t *rowbuf) {
+    const uint32_t lane = lane_id();
+    const uint32_t pmin = p0s[0], pmax = p0s[p - 1];
+    uint32_t nb = 0;
+    for (uint32_t c = 0; c < nx; c += 32) {
+        const uint32_t i = c + lane;
+        uint32_t x = 0;
+        uint64_t e = 0, end = 0;
+        bool hit = false, big = false;
+        if (i < nx) {
+            x = ldg(ci + lo + i);
+            e = ldg(rp + x) + ldg(fo + x);
+            end = ldg(rp + x + 1);
+            if (end - e > kLongList) big = true;
+            else {
+                e = lower_bound(ci, e, end, pmin);
+                // any element of N+(x) in P0?
+                uint32_t j = 0;
+                for (uint64_t f = e; f < end; f++) {
+                    const uint32_t y = ldg(ci + f);
+                    if (y > pmax) break;
+                    j = smem_lower_bound(p0s, j, p, y);
+                    if (j < p && p0s[j] == y) {
+                        hit = true;
+                        break;
+                    }
+                }
+            }
+        }
+        // long lists: decide with the whole warp
+        uint32_t bigmask = __ballot_sync(G2_FULL, big);
+        uint32_t bighit = 0;
+        while (bigmask) {
+            const uint32_t l = __ffs(bigmask) - 1;
+            bigmask &= bigmask - 1;
+            const uint32_t xx = __shfl_sync(G2_FULL, x, l);
+            uint64_t b0 = ldg(rp + xx) + ldg(fo + xx), b1 = ldg(rp + xx + 1);
+            uint64_t s = 0;
+            if (lane == 0) s = lower_bound(ci, b0, b1, pmin);
+            s = __shfl_sync(G2_FULL, s, 0);
+            bool any = false;
+            for (uint64_t base = s; base < b1; base += 32) {  // uniform trip count
+                const uint64_t f = base + lane;
+                const uint32_t y = f < b1 ? ldg(ci + f) : 0xffffffffu;
+                const bool inr = f < b1 && y <= pmax;
+                bool found = false;
+                if (inr) {
+                    const uint32_t j = smem_lower_bound(p0s, 0, p, y);
+                    found = j < p && p0s[j] == y;
+                }
+                if (__any_sync(G2_FULL, found)) {
+                    any = true;
+                    break;
+                }
+                if (!__any_sync(G2_FULL, inr)) break;  // sorted: the rest lies beyond P0
+            }
+            any = __any_sync(G2_FULL, any);
+            if (any) bighit |= 1u << l;
+        }
+        hit = hit || ((bighit >> lane) & 1u);
+        uint32_t tot;
+        const uint32_t pos = warp_scan(hit, tot);
+        if (nb + tot > cap) return ~0u;
+        // second pass: write the kept rows at their compacted position
+        if (hit && !big) {
+            uint32_t *row = B + (uint64_t)(nb + pos) * W;
+            for (uint32_t w = 0; w < W; w++) row[w] = 0u;
+            uint32_t j = 0;
+            for (uint64_t f = e; f < end; f++) {
+                const uint32_t y = ldg(ci + f);
+                if (y > pmax) break;
+                j = smem_lower_bound(p0s, j, p, y);
+                if (j < p && p0s[j] == y) row[j >> 5] |= 1u << (j & 31u);
+            }
+            if (xv) xv[nb + pos] = x;
+        }
+        uint32_t bm = __ballot_sync(G2_FULL, hit && big);
+        while (bm) {
+            const uint32_t l = __ffs(bm) - 1;
+            bm &= bm - 1;
+            const uint32_t xx = __shfl_sync(G2_FULL, x, l);
+            const uint32_t dst = nb + __shfl_sync(G2_FULL, pos, l);
+            uint64_t b0 = ldg(rp + xx) + ldg(fo + xx), b1 = ldg(rp + xx + 1);
+            uint64_t s = 0;
+            if (lane == 0) s = lower_bound(ci, b0, b1, pmin);
+            s = __shfl_sync(G2_FULL, s, 0);
+            for (uint32_t w = lane; w < W; w += 32) rowbuf[w] = 0u;
+            __syncwarp();
+            for (uint64_t f = s + lane; f < b1; f += 32) {
+                const uint32_t y = ldg(ci + f);
+                if (y > pmax) break;
+                const uint32_t j = smem_lower_bound(p0s, 0, p, y);
+                if (j < p && p0s[j] == y) atomicOr(rowbuf + (j >> 5), 1u << (j & 31u));
+            }
+            __syncwarp();
+            for (uint32_t w = lane; w < W; w += 32) B[(uint64_t)dst * W + w] = rowbuf[w];
+            if (xv && lane == 0) xv[dst] = xx;
+            __syncwarp();
+        }
+        nb += tot;
         __syncwarp();
     }
+    return nb;
 }
 
 }  // namespace g2

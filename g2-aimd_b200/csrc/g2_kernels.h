@@ -20,6 +20,7 @@ constexpr int kStatusBadPlan = 8;        // plan arrays inconsistent
 struct MceArgs {
     const uint64_t *rp;
     const uint32_t *ci;
+    const uint32_t *fo;             // fo[v]: offset in N(v) of the first neighbour > v
     const uint32_t *tasks;          // root vertex of each task
     const uint32_t *task_index;     // optional: the task ids this pass runs (else 0..ntasks-1)
     uint64_t ntasks;                // tasks in this pass (if ntasks_dev is null)
@@ -34,6 +35,7 @@ struct MceArgs {
     unsigned long long *ndeferred;
     uint64_t deferred_cap;
     uint64_t *root_nodes;           // optional, per task id
+    unsigned long long *work;       // optional: work model W in bytes (metrics kernel)
     int *status;
     int final_pass;
 };
@@ -66,6 +68,7 @@ struct DevPlan {
 struct MatchArgs {
     const uint64_t *rp;
     const uint32_t *ci;
+    const uint32_t *fo;
     const uint32_t *tasks;
     const uint32_t *task_index;
     uint64_t ntasks;
@@ -74,6 +77,7 @@ struct MatchArgs {
     uint32_t *scratch;
     uint64_t words_per_warp;
     unsigned long long *out;        // [0] count
+    unsigned long long *work;       // optional: work model W in bytes (metrics kernel)
     uint32_t *deferred;
     unsigned long long *ndeferred;
     uint64_t deferred_cap;
@@ -81,6 +85,7 @@ struct MatchArgs {
     int *status;
 };
 
+size_t match_smem_bytes(int wpl, int warps_per_block);
 cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block,
                          cudaStream_t st, bool clique_path, int wpl);
 

@@ -45,14 +45,17 @@ struct Level {
     uint32_t parent;     // position of the parent back neighbour
 };
 
-// Set up the scan window of position i given M[0..i-1].
-__device__ void level_init(const uint64_t *rp, const uint32_t *ci, const uint32_t *M, uint32_t i, Level &L) {
+// Set up the scan window of position i given M[0..i-1].  Returns the sum of
+// the back neighbours' degrees (one partial embedding's share of the work model).
+__device__ uint64_t level_init(const uint64_t *rp, const uint32_t *ci, const uint32_t *M, uint32_t i, Level &L) {
     const DevPlan &pl = c_plan;
     uint32_t parent = pl.bn_pos[i][0];
     uint64_t pd = ldg(rp + M[parent] + 1) - ldg(rp + M[parent]);
+    uint64_t dsum = pd;
     for (uint32_t j = 1; j < pl.bn_count[i]; j++) {
         uint32_t b = pl.bn_pos[i][j];
         uint64_t d = ldg(rp + M[b] + 1) - ldg(rp + M[b]);
+        dsum += d;
         if (d < pd) pd = d, parent = b;
     }
     uint32_t lo = 0, hi = 0xffffffffu;
@@ -73,6 +76,7 @@ __device__ void level_init(const uint64_t *rp, const uint32_t *ci, const uint32_
     L.len = 0;
     L.idx = 0;
     L.parent = parent;
+    return dsum;
 }
 
 // Does w qualify for position i (conditions + other back neighbours)?
@@ -89,8 +93,10 @@ __device__ __forceinline__ bool cand_ok(const uint64_t *rp, const uint32_t *ci, 
     return true;
 }
 
-// Generic plan-driven walk of one root; returns the number of embeddings.
-__device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v, uint32_t *S) {
+// Generic plan-driven walk of one root; returns the number of embeddings and
+// adds the work model (4 x back-neighbour degrees per partial embedding) to work.
+__device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v, uint32_t *S,
+                                                 unsigned long long &work) {
     const DevPlan &pl = c_plan;
     const uint32_t k = pl.k;
     const uint32_t lane = lane_id();
@@ -107,7 +113,7 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
         return 0;
     }
     uint32_t i = 1;
-    level_init(rp, ci, M, 1, Ls[1]);
+    work += 4ull * level_init(rp, ci, M, 1, Ls[1]);
     for (;;) {
         Level &L = Ls[i];
         if (i == k - 1) {
@@ -148,16 +154,16 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
         M[i] = buf[L.idx];
         L.idx++;
         i++;
-        level_init(rp, ci, M, i, Ls[i]);
+        work += 4ull * level_init(rp, ci, M, i, Ls[i]);
     }
     return count;
 }
 
 // Clique plans on P0 bitmaps.  Returns false if the root does not fit (caller
 // falls back to the generic walk).
-template <int WPL>
-__device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, uint32_t *rowbuf,
-                                  unsigned long long &count) {
+template <int WPL, bool METRICS>
+__device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, uint32_t *p0s, uint32_t *rowbuf,
+                                  unsigned long long &count, unsigned long long &work) {
     const DevPlan &pl = c_plan;
     const uint32_t k = pl.k;
     const uint32_t lane = lane_id();
@@ -165,14 +171,18 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
     const uint32_t *ci = a.ci;
     const uint64_t lo = ldg(rp + v), hi = ldg(rp + v + 1);
     count = 0;
-    if (lo == hi) return true;
-    uint64_t split = 0;
-    if (lane == 0) split = lower_bound(ci, lo, hi, v + 1);
-    split = __shfl_sync(G2_FULL, split, 0);
+    unsigned long long w = METRICS ? (hi - lo) : 0;  // the root's own partial embedding
+    if (lo == hi) {
+        work += 4ull * w;
+        return true;
+    }
+    const uint64_t split = lo + ldg(a.fo + v);
     const uint32_t p = (uint32_t)(hi - split);
-    if (p + 1 < k) return true;
-    if (k == 2) {
-        count = p;
+    if (k == 2 || p == 0 || (!METRICS && p + 1 < k)) {
+        // k == 2: every forward neighbour is a match; otherwise no k-clique here
+        // (the metrics build still walks short roots to count their partial embeddings)
+        if (k == 2) count = p;
+        work += 4ull * w;
         return true;
     }
     const uint32_t W = (p + 31u) >> 5;
@@ -180,12 +190,9 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
     // slab: [A p*W] [frames (k) * (W + 1)]
     const uint64_t a0 = 0, f0 = (uint64_t)p * W;
     if (f0 + (uint64_t)k * (W + 1) > a.words_per_warp) return false;
-    const uint32_t pmax = ldg(ci + hi - 1);
-    Row<WPL> row;
-    for (uint32_t i = 0; i < p; i++) {
-        build_row<WPL>(rp, ci, v, split, p, W, pmax, ldg(ci + split + i), row, rowbuf);
-        row_store(row, S + a0 + (uint64_t)i * W, W);
-    }
+    for (uint32_t i = lane; i < p; i += 32) p0s[i] = ldg(ci + split + i);
+    __syncwarp();
+    build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf);
     __syncwarp();
     // C = remaining candidates at the current depth; depth = vertices chosen (v included)
     Row<WPL> C;
@@ -196,6 +203,8 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
     }
     uint32_t depth = 1;
     unsigned long long cnt = 0;
+    unsigned long long sdeg[G2_MAX_QUERY];  // degree sum of the chosen vertices per depth (metrics)
+    sdeg[1] = hi - lo;
     for (;;) {
         // lowest remaining candidate x
         uint32_t key = 0xffffffffu;
@@ -220,6 +229,12 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
             if (lane + 32u * s == key) C.w[s] &= ~(1u << (x & 31u));
         Row<WPL> ax;
         row_load(ax, S + a0 + (uint64_t)x * W, W);
+        unsigned long long dx = 0;
+        if (METRICS) {
+            const uint32_t u = p0s[x];
+            dx = ldg(rp + u + 1) - ldg(rp + u);
+            w += sdeg[depth] + dx;  // partial embedding of length depth + 1
+        }
         if (depth + 2 == k) {
             // children would be the last position: count C ∩ A[x]
             uint32_t c = 0;
@@ -232,20 +247,23 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
         __syncwarp();
 #pragma unroll
         for (int s = 0; s < WPL; s++) C.w[s] &= ax.w[s];
+        if (METRICS) sdeg[depth + 1] = sdeg[depth] + dx;
         depth++;
     }
     count = cnt;
+    work += 4ull * w;
     return true;
 }
 
-template <int WPL>
+template <int WPL, bool METRICS>
 __global__ void __launch_bounds__(256) match_kernel(MatchArgs a, int clique_path) {
     extern __shared__ uint32_t smem[];
     const uint32_t wib = threadIdx.x >> 5;
-    uint32_t *rowbuf = smem + wib * 32u * WPL;
+    uint32_t *rowbuf = smem + wib * (32u * WPL + 1024u * WPL);
+    uint32_t *p0s = rowbuf + 32u * WPL;
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t *S = a.scratch + gw * a.words_per_warp;
-    unsigned long long total = 0;
+    unsigned long long total = 0, work = 0;
     for (;;) {
         unsigned long long t0 = grab(a.head, a.chunk);
         if (t0 >= a.ntasks) break;
@@ -254,27 +272,41 @@ __global__ void __launch_bounds__(256) match_kernel(MatchArgs a, int clique_path
             uint64_t task = a.task_index ? a.task_index[t] : t;
             uint32_t v = a.tasks[task];
             unsigned long long c = 0;
-            if (!clique_path || !match_root_clique<WPL>(a, v, S, rowbuf, c)) c = match_root_generic(a, v, S);
+            if (!clique_path || !match_root_clique<WPL, METRICS>(a, v, S, p0s, rowbuf, c, work))
+                c = match_root_generic(a, v, S, work);
             total += c;
             if (a.root_nodes && lane_id() == 0) a.root_nodes[task] = c;
         }
     }
     if (lane_id() == 0 && total) atomicAdd(a.out, total);
+    if (METRICS && lane_id() == 0 && work) atomicAdd(a.work, work);
 }
 
 }  // namespace
+
+size_t match_smem_bytes(int wpl, int warps_per_block) {
+    return (size_t)warps_per_block * (32u * wpl + 1024u * wpl) * sizeof(uint32_t);
+}
+
+template <int WPL, bool M>
+static void launch_match(const MatchArgs &a, dim3 g, dim3 b, size_t sm, cudaStream_t st, int cp) {
+    cudaFuncSetAttribute(match_kernel<WPL, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    match_kernel<WPL, M><<<g, b, sm, st>>>(a, cp);
+}
 
 cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block, cudaStream_t st,
                          bool clique_path, int wpl) {
     cudaError_t e = cudaMemcpyToSymbolAsync(c_plan, &plan, sizeof(DevPlan), 0, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
-    size_t sm = (size_t)warps_per_block * 32u * wpl * sizeof(uint32_t);
+    size_t sm = match_smem_bytes(wpl, warps_per_block);
     dim3 g(blocks), b(32 * warps_per_block);
+    const int cp = clique_path ? 1 : 0;
+    const bool m = a.work != nullptr;
     switch (wpl) {
-        case 1: match_kernel<1><<<g, b, sm, st>>>(a, clique_path ? 1 : 0); break;
-        case 2: match_kernel<2><<<g, b, sm, st>>>(a, clique_path ? 1 : 0); break;
-        case 4: match_kernel<4><<<g, b, sm, st>>>(a, clique_path ? 1 : 0); break;
-        case 8: match_kernel<8><<<g, b, sm, st>>>(a, clique_path ? 1 : 0); break;
+        case 1: m ? launch_match<1, true>(a, g, b, sm, st, cp) : launch_match<1, false>(a, g, b, sm, st, cp); break;
+        case 2: m ? launch_match<2, true>(a, g, b, sm, st, cp) : launch_match<2, false>(a, g, b, sm, st, cp); break;
+        case 4: m ? launch_match<4, true>(a, g, b, sm, st, cp) : launch_match<4, false>(a, g, b, sm, st, cp); break;
+        case 8: m ? launch_match<8, true>(a, g, b, sm, st, cp) : launch_match<8, false>(a, g, b, sm, st, cp); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

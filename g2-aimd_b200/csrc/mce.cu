@@ -30,8 +30,6 @@ namespace g2 {
 
 namespace {
 
-constexpr uint32_t kSmallDeg = 128;  // X0 rows built one lane per vertex below this degree
-
 struct Frame {  // offsets inside the warp slab
     static __device__ __forceinline__ uint32_t size(uint32_t W) { return 3u * W + 2u; }
 };
@@ -45,8 +43,38 @@ __device__ void defer_root(const MceArgs &a, uint64_t t) {
     }
 }
 
-// Walk one root.  Returns false if the root had to be deferred.
+// Sum of degrees of the P0 vertices whose bits are set in a distributed row.
 template <int WPL>
+__device__ __forceinline__ unsigned long long row_degree_sum(const Row<WPL> &r, const uint64_t *rp,
+                                                             const uint32_t *ci, uint64_t split) {
+    const uint32_t lane = lane_id();
+    unsigned long long s = 0;
+#pragma unroll
+    for (int k = 0; k < WPL; k++) {
+        uint32_t word = r.w[k];
+        while (word) {
+            uint32_t b = __ffs(word) - 1;
+            word &= word - 1;
+            uint32_t u = ldg(ci + split + (lane + 32u * k) * 32u + b);
+            s += ldg(rp + u + 1) - ldg(rp + u);
+        }
+    }
+    return warp_sum_u64(s);
+}
+
+template <int WPL>
+__device__ __forceinline__ uint32_t row_popc(const Row<WPL> &r) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < WPL; k++) c += __popc(r.w[k]);
+    return (uint32_t)warp_sum_u64(c);
+}
+
+// Walk one root.  Returns false if the root had to be deferred.  With METRICS
+// the work model W (in 4-byte words) of the reference's tree is accumulated:
+// per node with P ∪ X non-empty, sum_{u in P∪X} (|P| + deg u) for pivot
+// scoring plus sum_{q in P \ N(pivot)} (|P ∪ X| + deg q) for the children.
+template <int WPL, bool METRICS>
 __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *cand, uint32_t *rowbuf) {
     const uint32_t lane = lane_id();
     const uint64_t *rp = a.rp;
@@ -57,9 +85,7 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
         if (a.root_nodes && lane == 0) a.root_nodes[t] = 0;
         return true;
     }
-    uint64_t split = 0;
-    if (lane == 0) split = lower_bound(ci, lo, hi, v + 1);
-    split = __shfl_sync(G2_FULL, split, 0);
+    const uint64_t split = lo + ldg(a.fo + v);
     const uint32_t p = (uint32_t)(hi - split);
     const uint32_t nx = (uint32_t)(split - lo);
     if (p == 0) {  // P empty, X non-empty: one record, not maximal
@@ -70,71 +96,25 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
     if (W > 32u * WPL) return false;
     const uint64_t SW = a.words_per_warp;
     const uint32_t FR = Frame::size(W);
-    // slab layout: [hist u64 (p+2)] [A p*W] [B nb*W ...] [lists ...] ... [frames (p+1)*FR]
-    const uint64_t h0 = 0, a0 = 2ull * (p + 2), b0 = a0 + (uint64_t)p * W;
+    // slab: [hist u64 (p+2)] [A p*W] [xv nx (metrics)] [B nb*W] [lists ...] ... [frames (p+1)*FR]
+    const uint64_t h0 = 0, a0 = 2ull * (p + 2), xv0 = a0 + (uint64_t)p * W;
+    const uint64_t b0 = xv0 + (METRICS ? nx : 0);  // metrics: X0 vertex of each kept B row
     const uint64_t fr0 = SW >= (uint64_t)(p + 1) * FR ? SW - (uint64_t)(p + 1) * FR : 0;
-    // uncompacted B rows and the root list must fit below the frames
-    if (fr0 == 0 || b0 + (uint64_t)nx * W + nx + 64 > fr0) return false;
+    if (fr0 < b0 + 64) return false;
     unsigned long long *hist_local = reinterpret_cast<unsigned long long *>(S + h0);
     for (uint32_t s = lane; s < p + 2; s += 32) hist_local[s] = 0ull;
-    const uint32_t pmax = ldg(ci + hi - 1);
-
-    // ---- A rows
-    Row<WPL> row;
-    for (uint32_t i = 0; i < p; i++) {
-        uint32_t u = ldg(ci + split + i);
-        build_row<WPL>(rp, ci, v, split, p, W, pmax, u, row, rowbuf);
-        row_store(row, S + a0 + (uint64_t)i * W, W);
-    }
-    // ---- B rows (uncompacted at b0 + i*W), small-degree X0 vertices one per lane
+    // ---- stage P0 in shared memory, then the rows
+    for (uint32_t i = lane; i < p; i += 32) cand[i] = ldg(ci + split + i);
+    __syncwarp();
+    build_forward_rows(rp, ci, a.fo, cand, p, W, S + a0, rowbuf);
     uint32_t *Bfull = S + b0;
-    for (uint32_t c = 0; c < nx; c += 32) {
-        uint32_t i = c + lane;
-        bool big = false;
-        if (i < nx) {
-            uint32_t x = ldg(ci + lo + i);
-            uint64_t xlo = ldg(rp + x), xhi = ldg(rp + x + 1);
-            uint32_t *r = Bfull + (uint64_t)i * W;
-            for (uint32_t w = 0; w < W; w++) r[w] = 0u;
-            if (xhi - xlo > kSmallDeg) big = true;
-            else {
-                uint64_t e = lower_bound(ci, xlo, xhi, v + 1);
-                for (; e < xhi; e++) {
-                    uint32_t y = ldg(ci + e);
-                    if (y > pmax) break;
-                    uint64_t j = lower_bound(ci, split, split + p, y);
-                    if (j < split + p && ldg(ci + j) == y) {
-                        uint32_t jj = (uint32_t)(j - split);
-                        r[jj >> 5] |= 1u << (jj & 31u);
-                    }
-                }
-            }
-        }
-        uint32_t bigmask = __ballot_sync(G2_FULL, big);
-        __syncwarp();
-        while (bigmask) {
-            uint32_t l = __ffs(bigmask) - 1;
-            bigmask &= bigmask - 1;
-            uint32_t ii = c + l;
-            uint32_t x = ldg(ci + lo + ii);
-            build_row<WPL>(rp, ci, v, split, p, W, pmax, x, row, rowbuf);
-            row_store(row, Bfull + (uint64_t)ii * W, W);
-        }
-        __syncwarp();
-    }
-    // compact non-zero B rows in place (destination index <= source index)
-    uint32_t nb = 0;
-    for (uint32_t i = 0; i < nx; i++) {
-        row_load(row, Bfull + (uint64_t)i * W, W);
-        if (row_any(row)) {
-            if (nb != i) {
-                __syncwarp();
-                row_store(row, Bfull + (uint64_t)nb * W, W);
-            }
-            nb++;
-        }
-        __syncwarp();
-    }
+    // kept B rows plus their root-list entries must stay below the frames
+    const uint64_t cap64 = (fr0 - b0 - 64) / (W + 1);
+    const uint32_t cap = cap64 > 0xfffffff0ull ? 0xfffffff0u : (uint32_t)cap64;
+    const uint32_t nb = build_back_rows(rp, ci, a.fo, v, lo, nx, cand, p, W, Bfull, METRICS ? S + xv0 : nullptr,
+                                        cap, rowbuf);
+    if (nb == ~0u) return false;
+    __syncwarp();
     // ---- root list (identity over the nb kept rows), right after B
     const uint64_t l0 = b0 + (uint64_t)nb * W;
     for (uint32_t i = lane; i < nb; i += 32) S[l0 + i] = i;
@@ -152,7 +132,7 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
     uint64_t xoff = l0;
     uint32_t xlen = nb;
     uint32_t d = 0;  // |R| = d + 1
-    unsigned long long nodes = 0, cliques = 0;
+    unsigned long long nodes = 0, cliques = 0, work = 0;
     bool enter = true;
     bool overflow = false;
     for (;;) {
@@ -165,6 +145,28 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
             for (int s = 0; s < WPL; s++) anyp |= P.w[s], anyx |= X.w[s];
             const bool hp = __any_sync(G2_FULL, anyp != 0);
             const bool hx = __any_sync(G2_FULL, anyx != 0) || xlen > 0;
+            unsigned long long npx = 0;  // |P| + |X| (metrics)
+            if (METRICS && (hp || hx)) {
+                // the reference's root record keeps every X0 vertex, also those
+                // with no neighbour in P0 that the B list drops (they fall out of
+                // every child), so the root node counts all of X0
+                const uint32_t np = row_popc(P);
+                npx = np + row_popc(X) + (d == 0 ? nx : xlen);
+                unsigned long long sd = row_degree_sum(P, rp, ci, split) + row_degree_sum(X, rp, ci, split);
+                unsigned long long sx = 0;
+                if (d == 0) {
+                    for (uint32_t li = lane; li < nx; li += 32) {
+                        const uint32_t u = ldg(ci + lo + li);
+                        sx += ldg(rp + u + 1) - ldg(rp + u);
+                    }
+                } else {
+                    for (uint32_t li = lane; li < xlen; li += 32) {
+                        const uint32_t u = S[xv0 + S[xoff + li]];
+                        sx += ldg(rp + u + 1) - ldg(rp + u);
+                    }
+                }
+                work += npx * np + sd + warp_sum_u64(sx);
+            }
             if (!hp) {
                 if (!hx) {  // no P and no X: maximal (app_BK/BK.h:78-91)
                     cliques++;
@@ -235,6 +237,7 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
                 row_load(pr, prow, W);
 #pragma unroll
                 for (int s = 0; s < WPL; s++) Qr.w[s] = P.w[s] & ~pr.w[s];
+                if (METRICS) work += npx * row_popc(Qr) + row_degree_sum(Qr, rp, ci, split);
             }
         }
         if (!want_pop) {
@@ -322,6 +325,7 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
     if (lane == 0) {
         atomicAdd(a.out, cliques);
         if (a.root_nodes) a.root_nodes[t] = nodes;
+        if (METRICS) atomicAdd(a.work, work * 4ull);
     }
     for (uint32_t s = lane; s < p + 2; s += 32) {
         unsigned long long h = hist_local[s];
@@ -334,7 +338,7 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
     return true;
 }
 
-template <int WPL>
+template <int WPL, bool METRICS>
 __global__ void __launch_bounds__(256) mce_kernel(MceArgs a) {
     extern __shared__ uint32_t smem[];
     const uint32_t wib = threadIdx.x >> 5;
@@ -353,7 +357,7 @@ __global__ void __launch_bounds__(256) mce_kernel(MceArgs a) {
         unsigned long long t1 = t0 + a.chunk < ntasks ? t0 + a.chunk : ntasks;
         for (unsigned long long t = t0; t < t1; t++) {
             uint64_t task = a.task_index ? a.task_index[t] : t;
-            if (!mce_root<WPL>(a, task, S, cand, rowbuf)) defer_root<WPL>(a, task);
+            if (!mce_root<WPL, METRICS>(a, task, S, cand, rowbuf)) defer_root<WPL>(a, task);
         }
     }
 }
@@ -364,28 +368,22 @@ size_t mce_smem_bytes(int wpl, int warps_per_block) {
     return (size_t)warps_per_block * (32u * 32u * wpl + 32u * wpl) * sizeof(uint32_t);
 }
 
+template <int WPL, bool M>
+static void launch_one(const MceArgs &a, dim3 g, dim3 b, size_t sm, cudaStream_t st) {
+    cudaFuncSetAttribute(mce_kernel<WPL, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    mce_kernel<WPL, M><<<g, b, sm, st>>>(a);
+}
+
 cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_block, cudaStream_t st) {
     size_t sm = mce_smem_bytes(wpl, warps_per_block);
     dim3 g(blocks), b(32 * warps_per_block);
+    const bool m = a.work != nullptr;
     switch (wpl) {
-        case 1:
-            cudaFuncSetAttribute(mce_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            mce_kernel<1><<<g, b, sm, st>>>(a);
-            break;
-        case 2:
-            cudaFuncSetAttribute(mce_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            mce_kernel<2><<<g, b, sm, st>>>(a);
-            break;
-        case 4:
-            cudaFuncSetAttribute(mce_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            mce_kernel<4><<<g, b, sm, st>>>(a);
-            break;
-        case 8:
-            cudaFuncSetAttribute(mce_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            mce_kernel<8><<<g, b, sm, st>>>(a);
-            break;
-        default:
-            return cudaErrorInvalidValue;
+        case 1: m ? launch_one<1, true>(a, g, b, sm, st) : launch_one<1, false>(a, g, b, sm, st); break;
+        case 2: m ? launch_one<2, true>(a, g, b, sm, st) : launch_one<2, false>(a, g, b, sm, st); break;
+        case 4: m ? launch_one<4, true>(a, g, b, sm, st) : launch_one<4, false>(a, g, b, sm, st); break;
+        case 8: m ? launch_one<8, true>(a, g, b, sm, st) : launch_one<8, false>(a, g, b, sm, st); break;
+        default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }

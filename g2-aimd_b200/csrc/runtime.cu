@@ -30,6 +30,8 @@ struct g2_ctx {
     bool owns_csr = false;
     uint64_t n = 0, m = 0;
     uint32_t max_fwd = 0;  // max |N(v) ∩ (v, ∞)|
+    uint32_t *d_fo = nullptr;  // forward-list offsets
+    uint64_t fo_cap = 0;
     // work buffers
     uint32_t *d_scratch = nullptr;
     uint64_t scratch_words = 0;
@@ -56,6 +58,10 @@ struct g2_ctx {
     // diagnostics
     std::string cuda_err;
     uint64_t launches = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around the three passes
+    bool timed = false;
+    unsigned long long *d_work = nullptr;
+    cudaStream_t last_stream = nullptr;
 };
 
 namespace {
@@ -85,7 +91,10 @@ int grow(g2_ctx *ctx, T *&p, uint64_t &cap, uint64_t need, const char *what) {
     return G2_OK;
 }
 
-__global__ void fwd_max_kernel(const uint64_t *rp, const uint32_t *ci, uint64_t n, unsigned int *out) {
+// fo[v] = offset in N(v) of the first neighbour larger than v (forward list
+// start); out = max forward degree.
+__global__ void forward_offsets_kernel(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint32_t *fo,
+                                       unsigned int *out) {
     unsigned int best = 0;
     for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t lo = rp[v], hi = rp[v + 1];
@@ -95,6 +104,7 @@ __global__ void fwd_max_kernel(const uint64_t *rp, const uint32_t *ci, uint64_t 
             if (ci[mid] <= (uint32_t)v) a = mid + 1;
             else b = mid;
         }
+        fo[v] = (uint32_t)(a - lo);
         unsigned int f = (unsigned int)(hi - a);
         best = f > best ? f : best;
     }
@@ -232,6 +242,19 @@ int status_to_code(int st) {
     return G2_OK;
 }
 
+// Events for pass timing and the device work counter, as the flags ask.
+int prepare_flags(g2_ctx *ctx, uint32_t flags, cudaStream_t st) {
+    ctx->timed = (flags & G2_FLAG_TIME_KERNELS) != 0;
+    ctx->last_stream = st;
+    if (ctx->timed && !ctx->ev[0])
+        for (auto &e : ctx->ev) G2_TRY(cudaEventCreate(&e));
+    if (flags & G2_FLAG_WORK_MODEL) {
+        if (!ctx->d_work) G2_TRY(cudaMalloc(&ctx->d_work, sizeof(unsigned long long)));
+        G2_TRY(cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), st));
+    }
+    return G2_OK;
+}
+
 int wpl_for(uint32_t p) {
     uint32_t W = (p + 31) / 32;
     return W <= 32 ? 1 : W <= 64 ? 2 : W <= 128 ? 4 : 8;
@@ -248,6 +271,9 @@ int mce_enqueue(g2_ctx *ctx, uint64_t ntasks, const g2_opts *o, unsigned long lo
     G2_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(unsigned long long) * 16, st));
     G2_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
     G2_TRY(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long) * (1 + hist_len), st));
+    const uint32_t flags = o ? o->flags : 0u;
+    rc = prepare_flags(ctx, flags, st);
+    if (rc) return rc;
     const int wpb = default_warps(o);
     const int blocks = default_blocks(ctx, o, wpb);
     // pass 1: every task, WPL=1, one slab per resident warp
@@ -260,6 +286,7 @@ int mce_enqueue(g2_ctx *ctx, uint64_t ntasks, const g2_opts *o, unsigned long lo
         g2::MceArgs a{};
         a.rp = ctx->d_rp;
         a.ci = ctx->d_ci;
+        a.fo = ctx->d_fo;
         a.tasks = ctx->d_tasks;
         a.task_index = k == 0 ? nullptr : ctx->d_defer + (uint64_t)(k - 1) * ctx->tasks_cap;
         a.ntasks = k == 0 ? ntasks : 0;
@@ -277,8 +304,11 @@ int mce_enqueue(g2_ctx *ctx, uint64_t ntasks, const g2_opts *o, unsigned long lo
         a.root_nodes = d_root_nodes;
         a.status = ctx->d_status;
         a.final_pass = k == 2;
+        a.work = (flags & G2_FLAG_WORK_MODEL) ? ctx->d_work : nullptr;
+        if (ctx->timed && k == 0) G2_TRY(cudaEventRecord(ctx->ev[0], st));
         cudaError_t e = g2::mce_launch(passes[k].wpl, a, passes[k].blocks, passes[k].wpb, st);
         if (e != cudaSuccess) return fail_cuda(ctx, e, "mce_launch");
+        if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[k + 1], st));
         ctx->launches++;
     }
     return G2_OK;
@@ -311,6 +341,22 @@ const char *g2_last_cuda_error(const g2_ctx *ctx) { return ctx ? ctx->cuda_err.c
 
 uint64_t g2_last_launch_count(const g2_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
+int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms) {
+    if (!ctx || !ms || pass < 0 || pass > 2 || !ctx->timed) return G2_ERR_INVALID;
+    G2_TRY(cudaEventSynchronize(ctx->ev[pass + 1]));
+    G2_TRY(cudaEventElapsedTime(ms, ctx->ev[pass], ctx->ev[pass + 1]));
+    return G2_OK;
+}
+
+int g2_last_work_bytes(g2_ctx *ctx, uint64_t *bytes) {
+    if (!ctx || !bytes || !ctx->d_work) return G2_ERR_INVALID;
+    unsigned long long h = 0;
+    G2_TRY(cudaStreamSynchronize(ctx->last_stream));
+    G2_TRY(cudaMemcpy(&h, ctx->d_work, sizeof(h), cudaMemcpyDeviceToHost));
+    *bytes = h;
+    return G2_OK;
+}
+
 int g2_open(int device, uint64_t scratch_bytes, g2_ctx **out) {
     if (!out) return G2_ERR_INVALID;
     *out = nullptr;
@@ -338,19 +384,24 @@ int g2_close(g2_ctx *ctx) {
         cudaFree(ctx->d_rp);
         cudaFree(ctx->d_ci);
     }
-    void *bufs[] = {ctx->d_scratch, ctx->d_tasks, ctx->d_defer, ctx->d_root_nodes, ctx->d_ctr, ctx->d_status,
+    void *bufs[] = {ctx->d_fo, ctx->d_scratch, ctx->d_tasks, ctx->d_defer, ctx->d_root_nodes, ctx->d_ctr, ctx->d_status,
                     ctx->d_out, ctx->d_keys, ctx->d_keys2, ctx->d_vals2, ctx->d_cub, ctx->d_scores};
     for (void *b : bufs)
         if (b) cudaFree(b);
+    if (ctx->d_work) cudaFree(ctx->d_work);
+    for (auto &e : ctx->ev)
+        if (e) cudaEventDestroy(e);
     delete ctx;
     return G2_OK;
 }
 
 static int after_load(g2_ctx *ctx) {
+    int rc = grow(ctx, ctx->d_fo, ctx->fo_cap, std::max<uint64_t>(ctx->n, 1), "forward offsets");
+    if (rc) return rc;
     unsigned int *d_max = nullptr;
     G2_TRY(cudaMalloc(&d_max, sizeof(unsigned int)));
     G2_TRY(cudaMemset(d_max, 0, sizeof(unsigned int)));
-    if (ctx->n) fwd_max_kernel<<<ctx->sm_count * 4, 256>>>(ctx->d_rp, ctx->d_ci, ctx->n, d_max);
+    if (ctx->n) forward_offsets_kernel<<<ctx->sm_count * 4, 256>>>(ctx->d_rp, ctx->d_ci, ctx->n, ctx->d_fo, d_max);
     ctx->launches++;
     unsigned int h = 0;
     cudaError_t e = cudaMemcpy(&h, d_max, sizeof(unsigned int), cudaMemcpyDeviceToHost);
@@ -468,7 +519,10 @@ int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opt
     rc = grow(ctx, ctx->d_out, oc, 1 + hl, "out");
     ctx->out_cap = (uint32_t)oc;
     if (rc) return rc;
-    rc = mce_enqueue(ctx, nsrc, opts, ctx->d_out, hl, want_nodes ? ctx->d_root_nodes : nullptr, st);
+    g2_opts o2{};
+    if (opts) o2 = *opts;
+    if (o2.work_bytes) o2.flags |= G2_FLAG_WORK_MODEL;
+    rc = mce_enqueue(ctx, nsrc, &o2, ctx->d_out, hl, want_nodes ? ctx->d_root_nodes : nullptr, st);
     if (rc) return rc;
     std::vector<unsigned long long> h(1 + hl);
     int status = 0;
@@ -480,6 +534,10 @@ int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opt
     *count = h[0];
     if (hist)
         for (uint32_t s = 0; s < hist_len; s++) hist[s] = h[1 + s];
+    if (o2.work_bytes) {
+        rc = g2_last_work_bytes(ctx, o2.work_bytes);
+        if (rc) return rc;
+    }
     if (want_nodes) {
         std::vector<uint64_t> rn(nsrc);
         G2_TRY(cudaMemcpy(rn.data(), ctx->d_root_nodes, sizeof(uint64_t) * nsrc, cudaMemcpyDeviceToHost));
@@ -517,11 +575,17 @@ int g2_match_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc, c
     G2_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(unsigned long long) * 16, st));
     G2_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
     G2_TRY(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
-    const int wpb = default_warps(opts);
+    const uint32_t flags = opts ? opts->flags : 0u;
+    rc = prepare_flags(ctx, flags, st);
+    if (rc) return rc;
+    int wpl = wpl_for(ctx->max_fwd);
+    int wpb = default_warps(opts);
+    while (wpb > 1 && g2::match_smem_bytes(wpl, wpb) > 200 * 1024) wpb /= 2;
     const int blocks = default_blocks(ctx, opts, wpb);
     g2::MatchArgs a{};
     a.rp = ctx->d_rp;
     a.ci = ctx->d_ci;
+    a.fo = ctx->d_fo;
     a.tasks = ctx->d_tasks;
     a.ntasks = nsrc;
     a.head = ctx->d_ctr;
@@ -532,10 +596,12 @@ int g2_match_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc, c
     a.out = reinterpret_cast<unsigned long long *>(d_out);
     a.root_nodes = nullptr;
     a.status = ctx->d_status;
+    a.work = (flags & G2_FLAG_WORK_MODEL) ? ctx->d_work : nullptr;
     const bool clique = ctx->clique_plan && !(opts && opts->intersect_mode == 1);
-    int wpl = wpl_for(ctx->max_fwd);
+    if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
     cudaError_t e = g2::match_launch(ctx->plan, a, blocks, wpb, st, clique, wpl);
     if (e != cudaSuccess) return fail_cuda(ctx, e, "match_launch");
+    if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[1], st));
     ctx->launches++;
     return G2_OK;
 }
@@ -557,7 +623,11 @@ int g2_match_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_o
     uint64_t oc = ctx->out_cap;
     int rc = grow(ctx, ctx->d_out, oc, 1, "out");
     ctx->out_cap = (uint32_t)oc;
-    if (!rc) rc = g2_match_run_device(ctx, sources ? d_src : nullptr, nsrc, opts, (uint64_t *)ctx->d_out, nullptr);
+    g2_opts o2{};
+    if (opts) o2 = *opts;
+    if (o2.work_bytes) o2.flags |= G2_FLAG_WORK_MODEL;
+    if (!rc) rc = g2_match_run_device(ctx, sources ? d_src : nullptr, nsrc, &o2, (uint64_t *)ctx->d_out, nullptr);
+    if (!rc && o2.work_bytes) rc = g2_last_work_bytes(ctx, o2.work_bytes);
     unsigned long long h = 0;
     int status = 0;
     if (!rc) {

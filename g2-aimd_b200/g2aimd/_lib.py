@@ -37,7 +37,7 @@ class G2Opts(C.Structure):
         ("blocks", u32), ("warps_per_block", u32), ("schedule", u32),
         ("split_threshold", u32), ("scores", P(C.c_float)),
         ("root_nodes", P(u64)), ("work_bytes", P(u64)),
-        ("intersect_mode", u32), ("reserved", u32 * 7),
+        ("intersect_mode", u32), ("flags", u32), ("reserved", u32 * 6),
     ]
 
 
@@ -66,6 +66,8 @@ def lib():
         "g2_mce_run_device": (i32, [C.c_void_p, C.c_void_p, u64, P(G2Opts), C.c_void_p, u32, C.c_void_p]),
         "g2_match_run_device": (i32, [C.c_void_p, C.c_void_p, u64, P(G2Opts), C.c_void_p, C.c_void_p]),
         "g2_last_launch_count": (u64, [C.c_void_p]),
+        "g2_pass_time_ms": (i32, [C.c_void_p, i32, P(C.c_float)]),
+        "g2_last_work_bytes": (i32, [C.c_void_p, P(u64)]),
         "g2_plan_preset": (i32, [i32, P(G2Plan)]),
         "g2_plan_build": (i32, [u32, C.c_void_p, u32, P(G2Plan)]),
         "g2_read_bin": (i32, [C.c_char_p, P(C.c_void_p), P(C.c_void_p), P(u64), P(u64)]),

@@ -73,8 +73,9 @@ class Plan:
 
 
 def _opts(warps_per_block=0, blocks=0, schedule="given", scores=None, root_nodes=None, intersect_mode=0,
-          split_threshold=0):
+          split_threshold=0, flags=0, work_bytes=None):
     o = G2Opts()
+    o.flags = flags
     o.warps_per_block = warps_per_block
     o.blocks = blocks
     o.schedule = SCHED[schedule]
@@ -87,6 +88,8 @@ def _opts(warps_per_block=0, blocks=0, schedule="given", scores=None, root_nodes
         o.scores = s.ctypes.data_as(C.POINTER(C.c_float))
     if root_nodes is not None:
         o.root_nodes = root_nodes.ctypes.data_as(C.POINTER(C.c_uint64))
+    if work_bytes is not None:
+        o.work_bytes = work_bytes.ctypes.data_as(C.POINTER(C.c_uint64))
     return o, keep
 
 

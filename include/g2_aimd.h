@@ -108,9 +108,15 @@ typedef struct g2_opts {
     const float *scores;        /* host, nsrc entries, for G2_SCHED_SCORES          */
     uint64_t *root_nodes;       /* optional host out: search-tree nodes per source  */
     uint64_t *work_bytes;       /* optional host out: algorithmic bytes W (MCE)     */
-    uint32_t intersect_mode;    /* GMatch: 0 auto, 1 binary search, 2 merge          */
-    uint32_t reserved[7];
+    uint32_t intersect_mode;    /* GMatch: 0 auto (clique bitmap path when the plan is
+                                   a clique), 1 generic plan-driven path only        */
+    uint32_t flags;             /* G2_FLAG_* bits                                    */
+    uint32_t reserved[6];
 } g2_opts;
+
+/* g2_opts.flags */
+#define G2_FLAG_TIME_KERNELS 1u  /* record CUDA events around each enumeration pass */
+#define G2_FLAG_WORK_MODEL 2u    /* count the work model W on the device (slower)    */
 
 typedef struct g2_ctx g2_ctx;
 
@@ -180,6 +186,17 @@ int g2_match_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc,
 
 /* Number of kernels the last run launched (for launch accounting). */
 uint64_t g2_last_launch_count(const g2_ctx *ctx);
+
+/* After a run with G2_FLAG_TIME_KERNELS: device milliseconds of enumeration
+ * pass `pass` (0 = main pass, 1-2 = deferred passes) of the last run, measured
+ * with CUDA events on the run's stream.  Synchronises on the events. */
+int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms);
+
+/* After a run with G2_FLAG_WORK_MODEL: the work model W of the last run in
+ * bytes (MCE: merge-intersection bytes of the reference's search tree; match:
+ * 4 x sum over partial embeddings of the back neighbours' degrees).
+ * Synchronises the run's stream. */
+int g2_last_work_bytes(g2_ctx *ctx, uint64_t *bytes);
 
 /* ------------------------------------------------------ host-side helpers */
 

@@ -13,8 +13,9 @@ QUERIES = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16, 17, 18, 23, 24, 25,
 def test_presets_small(g2, orc, ctx, q):
     from g2aimd.context import Plan
     plan = Plan.preset(q)
-    for g in (random_graph(g2.Graph, 40, 0.3, 5 + q, planted=[tuple(range(0, 9))]),
-              g2.Graph.rmat(9, 8, seed=q).degeneracy_recoded()):
+    k = plan.k
+    for g in (random_graph(g2.Graph, 40 if k < 6 else 30, 0.3, 5 + q, planted=[tuple(range(0, 9))]),
+              g2.Graph.rmat(9 if k < 6 else 8, 8, seed=q).degeneracy_recoded()):
         ctx.load(g)
         want = orc.match(g, plan)["count"]
         assert ctx.match(plan) == want, (q, g.name)
@@ -22,9 +23,9 @@ def test_presets_small(g2, orc, ctx, q):
 
 
 @pytest.mark.parametrize("q", [0, 1, 2, 24, 25])
-def test_rmat_s14(g2, orc, ctx, q):
+def test_rmat_s13(g2, orc, ctx, q):
     from g2aimd.context import Plan
-    g = g2.Graph.rmat(14, 16, seed=3).degeneracy_recoded()
+    g = g2.Graph.rmat(13, 16, seed=3).degeneracy_recoded()
     plan = Plan.preset(q)
     ctx.load(g)
     want = orc.match(g, plan, threads=8)["count"]
@@ -49,3 +50,20 @@ def test_empty_and_tiny(g2, ctx):
     ctx.load(g2.Graph.from_edges(3, [(0, 1), (1, 2), (0, 2)]))
     assert ctx.match(Plan.preset(0)) == 1
     assert ctx.match(Plan.preset(24)) == 0
+
+
+@pytest.mark.parametrize("q", [0, 24, 25, 1, 2])
+def test_device_work_model_matches_oracle(g2, orc, ctx, q):
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(11, 16, seed=4).degeneracy_recoded()
+    plan = Plan.preset(q)
+    ctx.load(g)
+    w = np.zeros(1, np.uint64)
+    c = ctx.match(plan, work_bytes=w)
+    want = orc.match(g, plan, threads=8)
+    assert c == want["count"]
+    assert int(w[0]) == want["work"]
+    if plan.k > 2:
+        w2 = np.zeros(1, np.uint64)
+        assert ctx.match(plan, intersect_mode=1, work_bytes=w2) == want["count"]
+        assert int(w2[0]) == want["work"]

@@ -36,7 +36,7 @@ def test_config1_er_planted(orc, ctx, c1_graph):
 
 
 def test_rmat_and_schedules(g2, orc, ctx):
-    g = g2.Graph.rmat(14, 16, seed=11).degeneracy_recoded()
+    g = g2.Graph.rmat(12, 16, seed=11).degeneracy_recoded()
     ctx.load(g)
     want = orc.mce(g, threads=8, per_root=True)
     for sched in ("given", "heuristic"):
@@ -64,9 +64,9 @@ def test_deferral_passes_with_tiny_scratch(g2, orc):
     """A slab too small for the big roots sends them through the deferred
     passes (bigger slab per warp); results do not change."""
     from g2aimd.context import Context
-    g = g2.Graph.rmat(13, 16, seed=5).degeneracy_recoded()
+    g = g2.Graph.rmat(12, 16, seed=5).degeneracy_recoded()
     want = orc.mce(g, threads=8)
-    with Context(0, scratch_bytes=64 << 20) as c:
+    with Context(0, scratch_bytes=32 << 20) as c:
         c.load(g)
         got = c.mce()
     _same(got, want, "tiny-scratch")
@@ -74,7 +74,7 @@ def test_deferral_passes_with_tiny_scratch(g2, orc):
 
 def test_not_degeneracy_ordered(g2, orc, ctx):
     """Raw R-MAT ids (hubs early): large forward sets, wide rows."""
-    g = g2.Graph.rmat(12, 8, seed=21)
+    g = g2.Graph.rmat(11, 8, seed=21)
     ctx.load(g)
     want = orc.mce(g, threads=8)
     _same(ctx.mce(), want, "raw-ids")
@@ -85,3 +85,23 @@ def test_histogram_too_short_is_an_error(g2, ctx):
     ctx.load(g)
     with pytest.raises(g2.G2Error):
         ctx.mce(hist_len=4)
+
+
+def test_device_work_model_matches_oracle(g2, orc, ctx, c1_graph):
+    """The work model W counted on the device equals the oracle's."""
+    for g in (c1_graph, g2.Graph.rmat(11, 16, seed=2).degeneracy_recoded()):
+        ctx.load(g)
+        w = np.zeros(1, np.uint64)
+        c, h = ctx.mce(work_bytes=w)
+        want = orc.mce(g, threads=8)
+        assert c == want["count"]
+        assert int(w[0]) == want["work"], g.name
+
+
+def test_chung_lu_power_law(g2, orc, ctx):
+    g = g2.Graph.chung_lu(1 << 15, 2.3, 16.0, seed=3).degeneracy_recoded()
+    ctx.load(g)
+    want = orc.mce(g, threads=8, per_root=True)
+    c, h, rn = ctx.mce(root_nodes=True, schedule="heuristic")
+    _same((c, h), want, g.name)
+    assert np.array_equal(rn, want["root_nodes"])
