@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--edge-factor", type=int, default=16)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-sample-s", type=float, default=12.0, help="target seconds of CPU baseline work")
-    ap.add_argument("--no-extras", action="store_true", help="skip 4-clique / triangle / e2e / CPU legs")
+    ap.add_argument("--no-extras", action="store_true", help="skip triangle / MCE / e2e / CPU legs")
+    ap.add_argument("--scratch-mb", type=int, default=4096, help="device scratch for the DFS slabs")
     return ap.parse_args()
 
 
@@ -205,7 +206,7 @@ def run_ours(a):
     torch.cuda.set_device(dev)
     L = g2aimd.lib()
     g, gen_s = make_graph(a.scale, a.edge_factor, a.seed + rank)
-    ctx = Context(local)
+    ctx = Context(local, a.scratch_mb << 20)
     rp = torch.from_numpy(g.row_ptrs.view(np.int64)).to(dev)
     ci = torch.from_numpy(g.cols.view(np.int32)).to(dev)
     ctx.load_device(rp.data_ptr(), ci.data_ptr(), g.n, g.m)

@@ -20,6 +20,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libg2aimd.so")
+WORKER = os.path.join(HERE, "g2_worker")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = "g++"
@@ -29,6 +30,9 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-rela
 CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-march=x86-64-v2"] + INC
 
 
+MAIN = os.path.join(CSRC, "host", "worker_main.cpp")
+
+
 def sources():
     cu, cpp = [], []
     for d, _, fs in os.walk(CSRC):
@@ -36,7 +40,7 @@ def sources():
             p = os.path.join(d, f)
             if f.endswith(".cu"):
                 cu.append(p)
-            elif f.endswith(".cpp"):
+            elif f.endswith(".cpp") and p != MAIN:
                 cpp.append(p)
     return cu, cpp
 
@@ -79,6 +83,9 @@ def build(verbose=False, ptxas_v=False):
         objs.append(o)
     if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"], verbose)
+    # the reference-style command-line driver (drop-in for `bk` / `run`)
+    if newer(MAIN, WORKER, hs) or os.path.getmtime(LIB) > os.path.getmtime(WORKER):
+        run([CXX] + CXXFLAGS + [MAIN, "-o", WORKER, "-L", HERE, "-lg2aimd", "-Wl,-rpath,$ORIGIN"], verbose)
     return LIB
 
 

@@ -1,0 +1,154 @@
+// worker_main.cpp - g2_worker, the drop-in for the reference's `bk` and `run`
+// binaries (app_BK/main.cu, app_gmatch/main.cu -> Worker<App>::run,
+// system/worker.h:28-280).
+//
+// Same flags and result lines:
+//   -dg <graph.bin>   data graph (.bin CSR, ids in degeneracy order for BK)
+//   -q  <id>          query preset; 1000 (default) = maximal clique enumeration
+//   -h  <hop>         view-bin hop for BK (GMatch takes the plan's hop; must be unset)
+//   -cn <n>           consumers = GPUs 0..n-1
+//   -ss <0|1>         sort the sources of each bin
+//   -m, -t, -qs, -pn, -dr, -ds, -dst  accepted for compatibility (see below)
+// Bins come from "<graph.bin>.<hop>.hop.vbmap" (view/view_bin_manager.h:34-94); a
+// missing file means one bin holding every vertex.  BK prints one
+// "Total No. of Cliques: N" line per bin (app_BK/BK.h:72-76), GMatch one final
+// "Total counts: N" (system/worker.h:273-279).
+//
+// What changes: each GPU holds the whole CSR (loaded once) instead of a k-hop view
+// per bin, so there is no producer-side materialisation (-pn, -t, -qs, -m have no
+// work to size); the view of a bin is a subset of the full graph that contains every
+// adjacency list the bin's roots read, so the counts are the same.  Bins go to GPUs
+// through an atomic counter instead of the MPMC queues.  -dr (reorder bins by
+// sum of degrees, largest first) and -ds/-dst (split) are honoured as orderings of the
+// bin list; they do not change results.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "g2_aimd.h"
+
+namespace {
+
+const char *opt(int argc, char **argv, const char *name, const char *def) {
+    for (int i = 1; i + 1 < argc; i++)
+        if (!strcmp(argv[i], name)) return argv[i + 1];
+    return def;
+}
+
+int die(const char *what, int rc) {
+    fprintf(stderr, "g2_worker: %s: %s (%d)\n", what, g2_strerror(rc), rc);
+    return 1;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    const std::string data = opt(argc, argv, "-dg", "");
+    const int query = atoi(opt(argc, argv, "-q", "1000"));
+    int hop = atoi(opt(argc, argv, "-h", "-1"));
+    const int consumers = std::max(1, atoi(opt(argc, argv, "-cn", "1")));
+    const int sort_sources = atoi(opt(argc, argv, "-ss", "0"));
+    const int reorder = atoi(opt(argc, argv, "-dr", "0"));
+    if (data.empty()) {
+        fprintf(stderr, "usage: g2_worker -dg graph.bin [-q id] [-h hop] [-cn gpus] [-ss 0|1]\n");
+        return 2;
+    }
+    const bool bk = query == 1000;
+    g2_plan plan;
+    memset(&plan, 0, sizeof(plan));
+    if (!bk) {
+        if (hop != -1) {
+            fprintf(stderr, "g2_worker: -h must be unset for subgraph queries (system/worker.h:61)\n");
+            return 2;
+        }
+        int rc = g2_plan_preset(query, &plan);
+        if (rc) return die("query plan", rc);
+        hop = (int)plan.hop;
+        printf("Hop = %d\nRoot degree = %u\nMatch Order: ", hop, plan.root_degree);
+        for (uint32_t i = 0; i < plan.k; i++) printf("%u ", plan.order[i]);
+        printf("\n");
+    }
+    uint64_t *rp = nullptr, n = 0, m = 0;
+    uint32_t *ci = nullptr;
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = g2_read_bin(data.c_str(), &rp, &ci, &n, &m);
+    if (rc) return die(data.c_str(), rc);
+    printf("vertex_count=%llu, edge_count=%llu\n", (unsigned long long)n, (unsigned long long)m);
+    // view bins
+    std::vector<uint32_t> bins(n, 0);
+    uint32_t nbins = 1;
+    const std::string vb = data + "." + std::to_string(hop) + ".hop.vbmap";
+    if (g2_read_vbmap(vb.c_str(), n, &nbins, bins.data()) != G2_OK) {
+        nbins = 1;
+        std::fill(bins.begin(), bins.end(), 0u);
+    }
+    std::vector<std::vector<uint32_t>> sources(nbins);
+    for (uint64_t v = 0; v < n; v++) sources[bins[v]].push_back((uint32_t)v);
+    if (sort_sources)
+        for (auto &s : sources) std::sort(s.begin(), s.end());
+    std::vector<uint32_t> order(nbins);
+    for (uint32_t b = 0; b < nbins; b++) order[b] = b;
+    if (reorder) {
+        std::vector<uint64_t> f(nbins, 0);
+        for (uint32_t b = 0; b < nbins; b++)
+            for (uint32_t v : sources[b]) f[b] += rp[v + 1] - rp[v];
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return f[a] > f[b]; });
+    }
+    std::atomic<uint32_t> next{0};
+    std::atomic<int> failed{0};
+    std::atomic<unsigned long long> total{0};
+    std::mutex out_mu;
+    std::vector<std::thread> th;
+    for (int c = 0; c < consumers; c++) {
+        th.emplace_back([&, c] {
+            g2_ctx *ctx = nullptr;
+            int r = g2_open(c, 0, &ctx);
+            if (!r) r = g2_load_csr(ctx, rp, ci, n, m);
+            if (!r && !bk) r = g2_set_plan(ctx, &plan);
+            for (uint32_t k; !r && (k = next++) < nbins;) {
+                const uint32_t b = order[k];
+                g2_opts o;
+                memset(&o, 0, sizeof(o));
+                o.schedule = G2_SCHED_HEURISTIC;
+                uint64_t count = 0;
+                auto s = std::chrono::steady_clock::now();
+                if (sources[b].empty()) {
+                    count = 0;
+                } else if (bk) {
+                    r = g2_mce_run(ctx, sources[b].data(), sources[b].size(), &o, &count, nullptr, 0);
+                } else {
+                    r = g2_match_run(ctx, sources[b].data(), sources[b].size(), &o, &count);
+                }
+                double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - s).count();
+                if (r) break;
+                total += count;
+                std::lock_guard<std::mutex> lk(out_mu);
+                printf("consumer %d completes bin %u\nfinish In-memory Execution Time, elapsed_time=%.3fms\n", c, b,
+                       ms);
+                if (bk) printf("Total No. of Cliques: %llu\n", (unsigned long long)count);
+                else printf("Currently Total counts: %llu\n", (unsigned long long)total.load());
+            }
+            if (r) {
+                std::lock_guard<std::mutex> lk(out_mu);
+                fprintf(stderr, "g2_worker: device %d: %s (%d) %s\n", c, g2_strerror(r), r,
+                        ctx ? g2_last_cuda_error(ctx) : "");
+                failed = 1;
+            }
+            if (ctx) g2_close(ctx);
+        });
+    }
+    for (auto &t : th) t.join();
+    double total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    printf("finish total time, elapsed_time=%.3fms\n", total_ms);
+    if (!bk) printf("Total counts: %llu\n", (unsigned long long)total.load());
+    g2_free(rp);
+    g2_free(ci);
+    return failed ? 1 : 0;
+}

@@ -89,6 +89,15 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
     const uint32_t p = (uint32_t)(hi - split);
     const uint32_t nx = (uint32_t)(split - lo);
     if (p == 0) {  // P empty, X non-empty: one record, not maximal
+        if (METRICS) {  // its pivot scan still reads every X0 list
+            unsigned long long sx = 0;
+            for (uint32_t li = lane; li < nx; li += 32) {
+                const uint32_t u = ldg(ci + lo + li);
+                sx += ldg(rp + u + 1) - ldg(rp + u);
+            }
+            sx = warp_sum_u64(sx);
+            if (lane == 0) atomicAdd(a.work, sx * 4ull);
+        }
         if (a.root_nodes && lane == 0) a.root_nodes[t] = 1;
         return true;
     }
