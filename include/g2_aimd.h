@@ -198,6 +198,28 @@ int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms);
  * Synchronises the run's stream. */
 int g2_last_work_bytes(g2_ctx *ctx, uint64_t *bytes);
 
+/*
+ * Plan-driven count that allocates no memory (no counterpart in the reference,
+ * which allocates all of its buffers itself).  For callers that cannot let a
+ * library call cudaMalloc / cudaFree: applications whose device memory is owned
+ * by their own caching allocator or a fixed budget, and latency-critical code
+ * where those calls may synchronise the device.  Counts the embeddings of `plan`
+ * rooted at every vertex of the device-resident CSR (same result as
+ * g2_match_run with sources = NULL) into *d_count (device memory), enqueued on
+ * `stream` of the current device; the count is ready when the stream is.
+ * Scratch is a file-scope device array of G2_NOALLOC_SCRATCH_BYTES that every
+ * GPU loading this library holds until exit.  Limits: n <= G2_NOALLOC_MAX_VERTICES,
+ * otherwise G2_ERR_UNSUPPORTED (also when the query leaves too little scratch
+ * per warp).  All calls on a device share that array: calls that overlap on the
+ * GPU race and must be serialised.  The first call on each device looks up the
+ * array's device address; make it before any stream capture.
+ */
+#define G2_NOALLOC_SCRATCH_BYTES (32u << 20)
+#define G2_NOALLOC_MAX_VERTICES (1u << 21)
+int g2_match_count_noalloc(const uint64_t *d_row_ptrs, const uint32_t *d_cols,
+                           uint64_t n, uint64_t m, const g2_plan *plan,
+                           uint64_t *d_count, void *stream);
+
 /* ------------------------------------------------------ host-side helpers */
 
 /* Query planner: preset pattern id (0..27 as PresetPatternType,
