@@ -23,6 +23,8 @@ struct MceArgs {
     const uint32_t *fo;             // fo[v]: offset in N(v) of the first neighbour > v
     const uint32_t *tasks;          // root vertex of each task
     const uint32_t *task_index;     // optional: the task ids this pass runs (else 0..ntasks-1)
+    const uint32_t *task_part;      // optional per task id: (nparts << 16) | part of a split root
+    uint64_t *root_cost;            // optional per task id: SM cycles spent on the task
     uint64_t ntasks;                // tasks in this pass (if ntasks_dev is null)
     const unsigned long long *ntasks_dev;  // else: task count read from device memory
     unsigned long long *head;       // device queue head
@@ -71,7 +73,10 @@ struct MatchArgs {
     const uint32_t *fo;
     const uint32_t *tasks;
     const uint32_t *task_index;
+    const uint32_t *task_part;      // optional per task: (nparts << 16) | part of a split root
+    uint64_t *root_cost;            // optional per task: SM cycles spent on the task
     uint64_t ntasks;
+    const unsigned long long *ntasks_dev;  // optional: task count read from device memory
     unsigned long long *head;
     uint32_t chunk;
     uint32_t *scratch;

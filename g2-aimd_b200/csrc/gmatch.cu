@@ -96,7 +96,7 @@ __device__ __forceinline__ bool cand_ok(const uint64_t *rp, const uint32_t *ci, 
 // Generic plan-driven walk of one root; returns the number of embeddings and
 // adds the work model (4 x back-neighbour degrees per partial embedding) to work.
 __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v, uint32_t *S,
-                                                 unsigned long long &work) {
+                                                 unsigned long long &work, uint32_t part, uint32_t nparts) {
     const DevPlan &pl = c_plan;
     const uint32_t k = pl.k;
     const uint32_t lane = lane_id();
@@ -113,7 +113,9 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
         return 0;
     }
     uint32_t i = 1;
-    work += 4ull * level_init(rp, ci, M, 1, Ls[1]);
+    uint32_t ord = 0;  // ordinal of the next position-1 candidate (heavy-root split)
+    const uint64_t w1 = 4ull * level_init(rp, ci, M, 1, Ls[1]);
+    if (part == 0) work += w1;
     for (;;) {
         Level &L = Ls[i];
         if (i == k - 1) {
@@ -121,7 +123,14 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
             for (uint64_t e = L.pos; e < L.end; e += 32) {
                 uint64_t x = e + lane;
                 bool ok = x < L.end && cand_ok(rp, ci, M, i, L.parent, ldg(ci + x));
-                count += __popc(__ballot_sync(G2_FULL, ok));
+                uint32_t b = __ballot_sync(G2_FULL, ok);
+                if (i == 1 && nparts > 1) {  // k == 2: split the candidates themselves
+                    uint32_t keep = 0;
+                    for (uint32_t bits = b; bits; bits &= bits - 1)
+                        if ((ord++ % nparts) == part) keep |= bits & (~bits + 1u);
+                    b = keep;
+                }
+                count += __popc(b);
             }
             if (i == 1) break;
             i--;
@@ -153,6 +162,7 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
         }
         M[i] = buf[L.idx];
         L.idx++;
+        if (i == 1 && nparts > 1 && (ord++ % nparts) != part) continue;  // another part's candidate
         i++;
         work += 4ull * level_init(rp, ci, M, i, Ls[i]);
     }
@@ -163,7 +173,8 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
 // falls back to the generic walk).
 template <int WPL, bool METRICS>
 __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, uint32_t *p0s, uint32_t *rowbuf,
-                                  unsigned long long &count, unsigned long long &work) {
+                                  unsigned long long &count, unsigned long long &work, uint32_t part,
+                                  uint32_t nparts) {
     const DevPlan &pl = c_plan;
     const uint32_t k = pl.k;
     const uint32_t lane = lane_id();
@@ -171,7 +182,7 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
     const uint32_t *ci = a.ci;
     const uint64_t lo = ldg(rp + v), hi = ldg(rp + v + 1);
     count = 0;
-    unsigned long long w = METRICS ? (hi - lo) : 0;  // the root's own partial embedding
+    unsigned long long w = (METRICS && part == 0) ? (hi - lo) : 0;  // the root's own partial embedding
     if (lo == hi) {
         work += 4ull * w;
         return true;
@@ -181,7 +192,7 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
     if (k == 2 || p == 0 || (!METRICS && p + 1 < k)) {
         // k == 2: every forward neighbour is a match; otherwise no k-clique here
         // (the metrics build still walks short roots to count their partial embeddings)
-        if (k == 2) count = p;
+        if (k == 2) count = nparts > 1 ? (p + nparts - 1 - part) / nparts : p;
         work += 4ull * w;
         return true;
     }
@@ -202,6 +213,7 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
         C.w[s] = w < W ? (w + 1 < W || (p & 31u) == 0 ? G2_FULL : ((1u << (p & 31u)) - 1u)) : 0u;
     }
     uint32_t depth = 1;
+    uint32_t ord = 0;  // ordinal of the next depth-1 pick (heavy-root split)
     unsigned long long cnt = 0;
     unsigned long long sdeg[G2_MAX_QUERY];  // degree sum of the chosen vertices per depth (metrics)
     sdeg[1] = hi - lo;
@@ -227,6 +239,7 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
 #pragma unroll
         for (int s = 0; s < WPL; s++)
             if (lane + 32u * s == key) C.w[s] &= ~(1u << (x & 31u));
+        if (depth == 1 && nparts > 1 && (ord++ % nparts) != part) continue;  // another part's branch
         Row<WPL> ax;
         row_load(ax, S + a0 + (uint64_t)x * W, W);
         unsigned long long dx = 0;
@@ -264,18 +277,25 @@ __global__ void __launch_bounds__(256) match_kernel(MatchArgs a, int clique_path
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t *S = a.scratch + gw * a.words_per_warp;
     unsigned long long total = 0, work = 0;
+    const unsigned long long ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
     for (;;) {
         unsigned long long t0 = grab(a.head, a.chunk);
-        if (t0 >= a.ntasks) break;
-        unsigned long long t1 = t0 + a.chunk < a.ntasks ? t0 + a.chunk : a.ntasks;
+        if (t0 >= ntasks) break;
+        unsigned long long t1 = t0 + a.chunk < ntasks ? t0 + a.chunk : ntasks;
         for (unsigned long long t = t0; t < t1; t++) {
-            uint64_t task = a.task_index ? a.task_index[t] : t;
-            uint32_t v = a.tasks[task];
+            const uint64_t task = a.task_index ? a.task_index[t] : t;
+            const uint32_t v = a.tasks[task];
+            const uint32_t tp = a.task_part ? a.task_part[task] : (1u << 16);
+            const uint32_t nparts = tp >> 16, part = tp & 0xffffu;
+            const long long c0 = clock64();
             unsigned long long c = 0;
-            if (!clique_path || !match_root_clique<WPL, METRICS>(a, v, S, p0s, rowbuf, c, work))
-                c = match_root_generic(a, v, S, work);
+            if (!clique_path || !match_root_clique<WPL, METRICS>(a, v, S, p0s, rowbuf, c, work, part, nparts))
+                c = match_root_generic(a, v, S, work, part, nparts);
             total += c;
-            if (a.root_nodes && lane_id() == 0) a.root_nodes[task] = c;
+            if (lane_id() == 0) {
+                if (a.root_nodes) a.root_nodes[task] = c;
+                if (a.root_cost) a.root_cost[task] = (uint64_t)(clock64() - c0);
+            }
         }
     }
     if (lane_id() == 0 && total) atomicAdd(a.out, total);

@@ -81,10 +81,15 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
     const uint32_t *ci = a.ci;
     const uint32_t v = a.tasks[t];
     const uint64_t lo = ldg(rp + v), hi = ldg(rp + v + 1);
-    if (lo == hi) {  // no neighbours: skipped, as app_BK/BK.h:335-336
+    // heavy-root split: this task owns the root's top-level branches whose ordinal
+    // is congruent to part mod nparts (the root record itself belongs to part 0)
+    const uint32_t tp = a.task_part ? a.task_part[t] : (1u << 16);
+    const uint32_t nparts = tp >> 16, part = tp & 0xffffu;
+    if (lo == hi || (part != 0 && ldg(a.fo + v) == hi - lo)) {  // no neighbours (app_BK/BK.h:335-336) or P empty
         if (a.root_nodes && lane == 0) a.root_nodes[t] = 0;
         return true;
     }
+    uint32_t branch = 0;  // ordinal of the next top-level branch
     const uint64_t split = lo + ldg(a.fo + v);
     const uint32_t p = (uint32_t)(hi - split);
     const uint32_t nx = (uint32_t)(split - lo);
@@ -148,14 +153,14 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
         bool want_pop = false;
         if (enter) {
             enter = false;
-            nodes++;
+            if (d > 0 || part == 0) nodes++;
             uint32_t anyp = 0, anyx = 0;
 #pragma unroll
             for (int s = 0; s < WPL; s++) anyp |= P.w[s], anyx |= X.w[s];
             const bool hp = __any_sync(G2_FULL, anyp != 0);
             const bool hx = __any_sync(G2_FULL, anyx != 0) || xlen > 0;
             unsigned long long npx = 0;  // |P| + |X| (metrics)
-            if (METRICS && (hp || hx)) {
+            if (METRICS && (hp || hx) && (d > 0 || part == 0)) {
                 // the reference's root record keeps every X0 vertex, also those
                 // with no neighbour in P0 that the B list drops (they fall out of
                 // every child), so the root node counts all of X0
@@ -246,7 +251,7 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
                 row_load(pr, prow, W);
 #pragma unroll
                 for (int s = 0; s < WPL; s++) Qr.w[s] = P.w[s] & ~pr.w[s];
-                if (METRICS) work += npx * row_popc(Qr) + row_degree_sum(Qr, rp, ci, split);
+                if (METRICS && (d > 0 || part == 0)) work += npx * row_popc(Qr) + row_degree_sum(Qr, rp, ci, split);
             }
         }
         if (!want_pop) {
@@ -275,6 +280,7 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
                         X.w[s] |= qbit;
                         Qr.w[s] &= ~qbit;
                     }
+                if (d == 0 && nparts > 1 && (branch++ % nparts) != part) continue;  // another part's branch
                 const uint64_t coff = xoff + xlen;
                 if (coff + xlen > fr0) {  // child list would reach the frames
                     overflow = true;
@@ -366,7 +372,9 @@ __global__ void __launch_bounds__(256) mce_kernel(MceArgs a) {
         unsigned long long t1 = t0 + a.chunk < ntasks ? t0 + a.chunk : ntasks;
         for (unsigned long long t = t0; t < t1; t++) {
             uint64_t task = a.task_index ? a.task_index[t] : t;
+            const long long c0 = clock64();
             if (!mce_root<WPL, METRICS>(a, task, S, cand, rowbuf)) defer_root<WPL>(a, task);
+            else if (a.root_cost && lane_id() == 0) a.root_cost[task] = (uint64_t)(clock64() - c0);
         }
     }
 }
