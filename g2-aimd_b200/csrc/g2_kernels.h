@@ -94,4 +94,16 @@ size_t match_smem_bytes(int wpl, int warps_per_block);
 cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block,
                          cudaStream_t st, bool clique_path, int wpl);
 
+// Learned root-cost model (costmodel.cu).
+size_t model_smem_bytes();
+cudaError_t features_launch(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, const uint32_t *core,
+                            const uint32_t *src, uint64_t n, float *out, int sms, cudaStream_t st);
+cudaError_t train_step_launch(const float *X, const float *Y, const uint32_t *idx, uint32_t n, const float *params,
+                              const float *norm, float *grad, float *loss, cudaStream_t st);
+cudaError_t adam_launch(float *params, float *mom, float *vel, const float *grad, float lr, int step,
+                        cudaStream_t st);
+cudaError_t score_launch(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, const uint32_t *core,
+                         const uint32_t *src, uint64_t n, const float *X, const float *params, const float *norm,
+                         float *pred, float *cost, float *total, int sms, cudaStream_t st);
+
 }  // namespace g2

@@ -5,16 +5,21 @@
 // kernel pass per slab size is enqueued on a stream; roots that do not fit a
 // warp's slab are deferred on the device to the next pass (bigger slab per
 // warp), which replaces the overflow -> chunk/8 retry of
-// system/subgraph_container.h:178-211 without host round trips.
+// system/subgraph_container.h:178-211 without host round trips.  Task
+// generation (root order, heavy-root splits, the learned cost model's
+// inference) also runs on the device.
 #include <cuda_runtime.h>
 
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
+#include <numeric>
+#include <random>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "g2_aimd.h"
@@ -29,28 +34,38 @@ struct g2_ctx {
     uint32_t *d_ci = nullptr;
     bool owns_csr = false;
     uint64_t n = 0, m = 0;
-    uint32_t max_fwd = 0;  // max |N(v) ∩ (v, ∞)|
+    uint32_t max_fwd = 0;      // max |N(v) ∩ (v, ∞)|
     uint32_t *d_fo = nullptr;  // forward-list offsets
     uint64_t fo_cap = 0;
+    uint32_t *d_core = nullptr;  // optional core numbers (cost-model feature)
+    uint64_t core_cap = 0;
     // work buffers
     uint32_t *d_scratch = nullptr;
     uint64_t scratch_words = 0;
-    uint32_t *d_tasks = nullptr;   // root vertex per task (ordered)
-    uint32_t *d_defer = nullptr;   // 3 deferred lists of tasks_cap each
+    uint32_t *d_tasks = nullptr;  // root vertex per task (schedule order)
+    uint32_t *d_defer = nullptr;  // 3 deferred lists of tasks_cap each
     uint64_t tasks_cap = 0;
-    uint64_t *d_root_nodes = nullptr;
-    uint64_t root_nodes_cap = 0;
+    uint64_t *d_root_nodes = nullptr, *d_root_cost = nullptr;
+    uint64_t root_nodes_cap = 0, root_cost_cap = 0;
     unsigned long long *d_ctr = nullptr;  // [0..3] queue heads, [4..6] deferred counts
     int *d_status = nullptr;
     unsigned long long *d_out = nullptr;  // counters for the host entry points
-    uint32_t out_cap = 0;
+    uint64_t out_cap = 0;
     // schedule
     uint64_t *d_keys = nullptr, *d_keys2 = nullptr;
-    uint32_t *d_vals2 = nullptr;
+    uint64_t keys_cap = 0, keys2_cap = 0;
+    uint32_t *d_roots = nullptr, *d_S = nullptr, *d_part = nullptr, *d_xroots = nullptr, *d_xparts = nullptr;
+    uint64_t roots_cap = 0, S_cap = 0, part_cap = 0, xroots_cap = 0, xparts_cap = 0;
+    float *d_cost = nullptr, *d_total = nullptr;
+    uint64_t cost_cap = 0, total_cap = 0;
+    unsigned long long *d_ntask = nullptr;
+    uint64_t ntask_cap = 0;
     void *d_cub = nullptr;
     size_t cub_bytes = 0;
-    uint64_t sched_cap = 0, sched2_cap = 0, scores_cap = 0;
-    float *d_scores = nullptr;
+    bool last_split = false;  // the last run's tasks carry parts
+    uint64_t last_cap = 0;    // tasks buffer entries used by the last run
+    // learned cost model: params (G2_MODEL_PARAMS) followed by norm (G2_MODEL_NORM)
+    float *d_model = nullptr;
     // plan
     g2::DevPlan plan{};
     bool has_plan = false;
@@ -58,7 +73,7 @@ struct g2_ctx {
     // diagnostics
     std::string cuda_err;
     uint64_t launches = 0;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around the three passes
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around the enumeration passes
     bool timed = false;
     unsigned long long *d_work = nullptr;
     cudaStream_t last_stream = nullptr;
@@ -66,16 +81,16 @@ struct g2_ctx {
 
 namespace {
 
-const char *kVersion = "g2aimd-b200 0.1 (sm_100a)";
+const char *kVersion = "g2aimd-b200 0.2 (sm_100a)";
 
 int fail_cuda(g2_ctx *c, cudaError_t e, const char *where) {
     if (c) c->cuda_err = std::string(where) + ": " + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? G2_ERR_OOM : G2_ERR_CUDA;
 }
 
-#define G2_TRY(call)                                          \
-    do {                                                      \
-        cudaError_t _e = (call);                              \
+#define G2_TRY(call)                                             \
+    do {                                                         \
+        cudaError_t _e = (call);                                 \
         if (_e != cudaSuccess) return fail_cuda(ctx, _e, #call); \
     } while (0)
 
@@ -88,6 +103,16 @@ int grow(g2_ctx *ctx, T *&p, uint64_t &cap, uint64_t need, const char *what) {
     cudaError_t e = cudaMalloc(&p, sizeof(T) * (need ? need : 1));
     if (e != cudaSuccess) return fail_cuda(ctx, e, what);
     cap = need;
+    return G2_OK;
+}
+
+int cub_space(g2_ctx *ctx, size_t need) {
+    if (need <= ctx->cub_bytes && ctx->d_cub) return G2_OK;
+    if (ctx->d_cub) cudaFree(ctx->d_cub);
+    ctx->d_cub = nullptr;
+    ctx->cub_bytes = 0;
+    G2_TRY(cudaMalloc(&ctx->d_cub, need ? need : 16));
+    ctx->cub_bytes = need;
     return G2_OK;
 }
 
@@ -120,29 +145,79 @@ __global__ void iota_kernel(uint32_t *t, uint64_t n) {
         t[i] = (uint32_t)i;
 }
 
-// Heuristic root cost: p * (p + |X0|) bitmap-row words of the root's local
-// graph, a proxy of its set-up and search work; descending order = largest first.
-__global__ void heuristic_keys_kernel(const uint64_t *rp, const uint32_t *ci, const uint32_t *src, uint64_t n,
-                                      uint64_t *keys) {
+// Plain heuristic root cost: p * (p + deg) + 1 (bitmap-row words of the root's
+// local graph, a proxy of its set-up and search work); total for the split target.
+__global__ void heuristic_cost_kernel(const uint64_t *rp, const uint32_t *fo, const uint32_t *src, uint64_t n,
+                                      float *cost, float *total) {
+    float local = 0.f;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t v = src[i];
-        uint64_t lo = rp[v], hi = rp[v + 1], a = lo, b = hi;
-        while (a < b) {
-            uint64_t mid = a + ((b - a) >> 1);
-            if (ci[mid] <= v) a = mid + 1;
-            else b = mid;
-        }
-        uint64_t p = hi - a, d = hi - lo;
-        uint64_t cost = p * (p + d);
-        keys[i] = ~cost;  // ascending sort of ~cost = descending cost
+        const uint32_t v = src[i];
+        const float d = (float)(rp[v + 1] - rp[v]), p = d - (float)fo[v];
+        const float c = p * (p + d) + 1.f;
+        cost[i] = c;
+        local += c;
+    }
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(total, local);
+}
+
+__device__ __forceinline__ uint32_t float_key(float c) {  // order-preserving float -> uint
+    uint32_t b = __float_as_uint(c);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+// One task per root: key = (descending cost, root slot).
+__global__ void cost_keys_kernel(const float *cost, uint64_t n, uint64_t *keys) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        keys[i] = ((uint64_t)(~float_key(cost[i])) << 32) | (uint32_t)i;
+}
+
+// Tasks per root: ceil(cost / target) in 1..64, target = total * share.
+__global__ void split_count_kernel(const float *cost, const float *total, uint64_t n, float share, uint32_t *S) {
+    const float target = fmaxf(*total * share, 1.f);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float k = ceilf(cost[i] / target);
+        S[i] = (uint32_t)fminf(fmaxf(k, 1.f), 64.f);
     }
 }
 
-__global__ void score_keys_kernel(const float *scores, uint64_t n, uint64_t *keys) {
+// Expand root i into S[i] tasks at off[i]; key = (descending per-task cost, slot).
+__global__ void split_scatter_kernel(const uint32_t *src, const float *cost, const uint32_t *S, const uint32_t *off,
+                                     uint64_t n, uint64_t cap, uint32_t *roots, uint32_t *parts, uint64_t *keys) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t b = __float_as_uint(scores[i]);
-        b = (b & 0x80000000u) ? ~b : (b | 0x80000000u);  // order-preserving float -> uint
-        keys[i] = ~(uint64_t)b;                           // descending score
+        const uint32_t s = S[i];
+        const uint32_t kb = ~float_key(cost[i] / (float)s);
+        for (uint32_t j = 0; j < s; j++) {
+            const uint64_t t = (uint64_t)off[i] + j;
+            if (t >= cap) break;
+            roots[t] = src[i];
+            parts[t] = (s << 16) | j;
+            keys[t] = ((uint64_t)kb << 32) | (uint32_t)t;
+        }
+    }
+}
+
+__global__ void split_total_kernel(const uint32_t *S, const uint32_t *off, uint64_t n, uint64_t cap,
+                                   unsigned long long *ntasks) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        unsigned long long t = n ? (unsigned long long)off[n - 1] + S[n - 1] : 0ull;
+        *ntasks = t < cap ? t : cap;
+    }
+}
+
+// tasks[i] = roots[slot of the i-th smallest key]; unused slots sort last.
+__global__ void gather_tasks_kernel(const uint64_t *keys_sorted, const uint32_t *roots, const uint32_t *parts,
+                                    uint64_t cap, uint32_t *tasks, uint32_t *task_part) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = keys_sorted[i];
+        if (k == ~0ull) {
+            tasks[i] = 0;
+            if (task_part) task_part[i] = 1u << 16;
+            continue;
+        }
+        const uint32_t t = (uint32_t)(k & 0xffffffffull);
+        tasks[i] = roots[t];
+        if (task_part) task_part[i] = parts ? parts[t] : (1u << 16);
     }
 }
 
@@ -155,67 +230,122 @@ int default_blocks(g2_ctx *ctx, const g2_opts *o, int wpb) {
     return ctx->sm_count * per_sm;
 }
 
-// Upload / order the task list: d_tasks[i] = root of task i.
-int prepare_tasks(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, bool on_device, const g2_opts *o,
-                  cudaStream_t st, std::vector<uint32_t> *order_out) {
-    if (!sources) nsrc = ctx->n;
-    uint64_t cap = ctx->tasks_cap;
-    int rc = grow(ctx, ctx->d_tasks, cap, nsrc, "tasks");
+// Result of task generation.
+struct TaskList {
+    uint64_t cap = 0;    // d_tasks entries in use (upper bound of the task count)
+    bool split = false;  // d_part valid; the task count is in d_ntask
+};
+
+int sort_keys(g2_ctx *ctx, uint64_t n, cudaStream_t st) {
+    size_t need = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, need, ctx->d_keys, ctx->d_keys2, (int)n, 0, 64, st);
+    int rc = cub_space(ctx, need);
     if (rc) return rc;
-    if (cap != ctx->tasks_cap || !ctx->d_defer) {
+    G2_TRY(cub::DeviceRadixSort::SortKeys(ctx->d_cub, need, ctx->d_keys, ctx->d_keys2, (int)n, 0, 64, st));
+    ctx->launches += 4;
+    return G2_OK;
+}
+
+// Task generation: upload the roots, compute the schedule's cost per root (the
+// learned model's features + MLP run here, in one kernel), optionally split
+// heavy roots, sort the tasks by descending cost.  No host synchronisation.
+int prepare_tasks(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, bool on_device, const g2_opts *o,
+                  uint64_t nwarps, cudaStream_t st, TaskList *tl) {
+    if (!sources) nsrc = ctx->n;
+    const uint32_t sched = o ? o->schedule : G2_SCHED_GIVEN;
+    const uint32_t flags = o ? o->flags : 0u;
+    if (sched > G2_SCHED_LEARNED) return G2_ERR_INVALID;
+    if (sched == G2_SCHED_SCORES && !(o && o->scores)) return G2_ERR_INVALID;
+    if (sched == G2_SCHED_LEARNED && !ctx->d_model) return G2_ERR_INVALID;
+    const bool split = nsrc > 0 && (sched == G2_SCHED_HEURISTIC || sched == G2_SCHED_LEARNED) &&
+                       ((flags & G2_FLAG_SPLIT) || (sched == G2_SCHED_LEARNED && !(flags & G2_FLAG_NO_SPLIT)));
+    // sum_i ceil(c_i / t) <= n + total / t = n + 4 * warps
+    const uint64_t cap = split ? nsrc + 4 * nwarps + 64 : nsrc;
+    uint64_t tc = ctx->tasks_cap;
+    int rc = grow(ctx, ctx->d_tasks, tc, cap, "tasks");
+    if (rc) return rc;
+    if (tc != ctx->tasks_cap || !ctx->d_defer) {
         // three deferred-task lists with stride tasks_cap
         if (ctx->d_defer) cudaFree(ctx->d_defer);
         ctx->d_defer = nullptr;
-        G2_TRY(cudaMalloc(&ctx->d_defer, sizeof(uint32_t) * 3 * std::max<uint64_t>(cap, 1)));
+        G2_TRY(cudaMalloc(&ctx->d_defer, sizeof(uint32_t) * 3 * std::max<uint64_t>(tc, 1)));
     }
-    ctx->tasks_cap = cap;
-    if (!sources) {
-        iota_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(ctx->d_tasks, nsrc);
-        ctx->launches++;
-    } else if (on_device) {
-        G2_TRY(cudaMemcpyAsync(ctx->d_tasks, sources, sizeof(uint32_t) * nsrc, cudaMemcpyDeviceToDevice, st));
-    } else {
-        G2_TRY(cudaMemcpyAsync(ctx->d_tasks, sources, sizeof(uint32_t) * nsrc, cudaMemcpyHostToDevice, st));
-    }
-    uint32_t sched = o ? o->schedule : G2_SCHED_GIVEN;
-    if (sched == G2_SCHED_GIVEN || nsrc < 2) return G2_OK;
-    if (sched == G2_SCHED_SCORES && !(o && o->scores)) return G2_ERR_INVALID;
-    // keys -> sort (task order) ; the permutation is kept for per-root outputs
-    rc = grow(ctx, ctx->d_keys, ctx->sched_cap, nsrc, "keys");
-    if (rc) return rc;
-    uint64_t c2 = ctx->sched2_cap, c3 = ctx->sched2_cap;
-    rc = grow(ctx, ctx->d_keys2, c2, nsrc, "keys2");
-    if (!rc) rc = grow(ctx, ctx->d_vals2, c3, nsrc, "vals2");
-    ctx->sched2_cap = std::min(c2, c3);
-    if (rc) return rc;
-    if (sched == G2_SCHED_HEURISTIC) {
-        heuristic_keys_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(ctx->d_rp, ctx->d_ci, ctx->d_tasks, nsrc,
-                                                                ctx->d_keys);
-    } else {
-        rc = grow(ctx, ctx->d_scores, ctx->scores_cap, nsrc, "scores");
+    ctx->tasks_cap = tc;
+    tl->cap = nsrc;
+    tl->split = false;
+    const bool reorder = sched != G2_SCHED_GIVEN && nsrc >= 2;
+    uint32_t *roots = ctx->d_tasks;
+    if (reorder) {
+        rc = grow(ctx, ctx->d_roots, ctx->roots_cap, nsrc, "roots");
         if (rc) return rc;
-        G2_TRY(cudaMemcpyAsync(ctx->d_scores, o->scores, sizeof(float) * nsrc, cudaMemcpyHostToDevice, st));
-        score_keys_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(ctx->d_scores, nsrc, ctx->d_keys);
+        roots = ctx->d_roots;
     }
-    ctx->launches++;
+    if (!sources) {
+        iota_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(roots, nsrc);
+        ctx->launches++;
+    } else if (nsrc) {
+        G2_TRY(cudaMemcpyAsync(roots, sources, sizeof(uint32_t) * nsrc,
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    }
+    if (!reorder) return G2_OK;
+    rc = grow(ctx, ctx->d_keys, ctx->keys_cap, cap, "keys");
+    if (!rc) rc = grow(ctx, ctx->d_keys2, ctx->keys2_cap, cap, "keys2");
+    if (!rc) rc = grow(ctx, ctx->d_cost, ctx->cost_cap, nsrc, "cost");
+    if (!rc && !ctx->d_total) rc = grow(ctx, ctx->d_total, ctx->total_cap, 2, "total");
+    if (rc) return rc;
+    // ---- cost per root
+    G2_TRY(cudaMemsetAsync(ctx->d_total, 0, sizeof(float), st));
+    if (sched == G2_SCHED_HEURISTIC) {
+        heuristic_cost_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(ctx->d_rp, ctx->d_fo, roots, nsrc, ctx->d_cost,
+                                                                ctx->d_total);
+        ctx->launches++;
+    } else if (sched == G2_SCHED_LEARNED) {
+        cudaError_t e = g2::score_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, ctx->d_core, roots, nsrc, nullptr,
+                                         ctx->d_model, ctx->d_model + G2_MODEL_PARAMS, nullptr, ctx->d_cost,
+                                         ctx->d_total, ctx->sm_count, st);
+        if (e != cudaSuccess) return fail_cuda(ctx, e, "score_launch");
+        ctx->launches++;
+    } else {
+        G2_TRY(cudaMemcpyAsync(ctx->d_cost, o->scores, sizeof(float) * nsrc, cudaMemcpyHostToDevice, st));
+    }
+    if (!split) {
+        // one task per root, descending cost
+        cost_keys_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(ctx->d_cost, nsrc, ctx->d_keys);
+        ctx->launches++;
+        rc = sort_keys(ctx, nsrc, st);
+        if (rc) return rc;
+        gather_tasks_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(ctx->d_keys2, roots, nullptr, nsrc, ctx->d_tasks,
+                                                              nullptr);
+        ctx->launches++;
+        return G2_OK;
+    }
+    // ---- split heavy roots: tasks per root, offsets, expansion, sort, gather
+    rc = grow(ctx, ctx->d_S, ctx->S_cap, 2 * nsrc, "split counts");
+    if (!rc) rc = grow(ctx, ctx->d_part, ctx->part_cap, ctx->tasks_cap, "task parts");
+    if (!rc) rc = grow(ctx, ctx->d_xroots, ctx->xroots_cap, cap, "expanded roots");
+    if (!rc) rc = grow(ctx, ctx->d_xparts, ctx->xparts_cap, cap, "expanded parts");
+    if (!rc && !ctx->d_ntask) rc = grow(ctx, ctx->d_ntask, ctx->ntask_cap, 1, "task count");
+    if (rc) return rc;
+    uint32_t *S = ctx->d_S, *off = ctx->d_S + nsrc;
+    split_count_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(ctx->d_cost, ctx->d_total, nsrc,
+                                                         1.f / (4.f * (float)nwarps), S);
     size_t need = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, need, ctx->d_keys, ctx->d_keys2, ctx->d_tasks, ctx->d_vals2,
-                                    (int)nsrc, 0, 64, st);
-    if (need > ctx->cub_bytes) {
-        if (ctx->d_cub) cudaFree(ctx->d_cub);
-        ctx->d_cub = nullptr;
-        G2_TRY(cudaMalloc(&ctx->d_cub, need));
-        ctx->cub_bytes = need;
-    }
-    G2_TRY(cub::DeviceRadixSort::SortPairs(ctx->d_cub, need, ctx->d_keys, ctx->d_keys2, ctx->d_tasks,
-                                           ctx->d_vals2, (int)nsrc, 0, 64, st));
+    cub::DeviceScan::ExclusiveSum(nullptr, need, S, off, (int)nsrc, st);
+    rc = cub_space(ctx, need);
+    if (rc) return rc;
+    G2_TRY(cub::DeviceScan::ExclusiveSum(ctx->d_cub, need, S, off, (int)nsrc, st));
+    G2_TRY(cudaMemsetAsync(ctx->d_keys, 0xff, sizeof(uint64_t) * cap, st));
+    split_scatter_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(roots, ctx->d_cost, S, off, nsrc, cap, ctx->d_xroots,
+                                                           ctx->d_xparts, ctx->d_keys);
+    split_total_kernel<<<1, 32, 0, st>>>(S, off, nsrc, cap, ctx->d_ntask);
     ctx->launches += 4;
-    G2_TRY(cudaMemcpyAsync(ctx->d_tasks, ctx->d_vals2, sizeof(uint32_t) * nsrc, cudaMemcpyDeviceToDevice, st));
-    if (order_out) {
-        order_out->resize(nsrc);
-        G2_TRY(cudaMemcpyAsync(order_out->data(), ctx->d_tasks, sizeof(uint32_t) * nsrc, cudaMemcpyDeviceToHost,
-                               st));
-    }
+    rc = sort_keys(ctx, cap, st);
+    if (rc) return rc;
+    gather_tasks_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(ctx->d_keys2, ctx->d_xroots, ctx->d_xparts, cap,
+                                                          ctx->d_tasks, ctx->d_part);
+    ctx->launches++;
+    tl->cap = cap;
+    tl->split = true;
     return G2_OK;
 }
 
@@ -260,9 +390,60 @@ int wpl_for(uint32_t p) {
     return W <= 32 ? 1 : W <= 64 ? 2 : W <= 128 ? 4 : 8;
 }
 
+// Per-task outputs of the last run: zeroed device buffers of tasks_cap entries.
+int prepare_root_outputs(g2_ctx *ctx, bool nodes, bool cost, cudaStream_t st) {
+    if (nodes) {
+        int rc = grow(ctx, ctx->d_root_nodes, ctx->root_nodes_cap, ctx->tasks_cap, "root nodes");
+        if (rc) return rc;
+        G2_TRY(cudaMemsetAsync(ctx->d_root_nodes, 0, sizeof(uint64_t) * ctx->tasks_cap, st));
+    }
+    if (cost) {
+        int rc = grow(ctx, ctx->d_root_cost, ctx->root_cost_cap, ctx->tasks_cap, "root cost");
+        if (rc) return rc;
+        G2_TRY(cudaMemsetAsync(ctx->d_root_cost, 0, sizeof(uint64_t) * ctx->tasks_cap, st));
+    }
+    return G2_OK;
+}
+
+// Sum per-task outputs into per-source arrays (caller's order).  Synchronous.
+int gather_root_outputs(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, uint64_t *nodes_out,
+                        uint64_t *cost_out) {
+    if (!nodes_out && !cost_out) return G2_OK;
+    const uint64_t cap = ctx->last_cap;
+    std::vector<uint32_t> tasks(cap);
+    std::vector<uint64_t> v(cap);
+    G2_TRY(cudaMemcpy(tasks.data(), ctx->d_tasks, sizeof(uint32_t) * cap, cudaMemcpyDeviceToHost));
+    uint64_t used = cap;
+    if (ctx->last_split) {
+        unsigned long long t = 0;
+        G2_TRY(cudaMemcpy(&t, ctx->d_ntask, sizeof(t), cudaMemcpyDeviceToHost));
+        used = t;
+    }
+    std::unordered_map<uint32_t, uint64_t> pos;
+    if (sources)
+        for (uint64_t i = nsrc; i-- > 0;) pos[sources[i]] = i;  // first occurrence wins
+    auto index_of = [&](uint32_t root) -> uint64_t {
+        if (!sources) return root;
+        auto it = pos.find(root);
+        return it == pos.end() ? ~0ull : it->second;
+    };
+    for (int which = 0; which < 2; which++) {
+        uint64_t *out = which == 0 ? nodes_out : cost_out;
+        uint64_t *dev = which == 0 ? ctx->d_root_nodes : ctx->d_root_cost;
+        if (!out) continue;
+        G2_TRY(cudaMemcpy(v.data(), dev, sizeof(uint64_t) * cap, cudaMemcpyDeviceToHost));
+        memset(out, 0, sizeof(uint64_t) * nsrc);
+        for (uint64_t i = 0; i < used; i++) {
+            const uint64_t j = index_of(tasks[i]);
+            if (j < nsrc) out[j] += v[i];
+        }
+    }
+    return G2_OK;
+}
+
 // Enqueue the MCE passes; counters land in d_out.
-int mce_enqueue(g2_ctx *ctx, uint64_t ntasks, const g2_opts *o, unsigned long long *d_out, uint32_t hist_len,
-                uint64_t *d_root_nodes, cudaStream_t st) {
+int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long long *d_out, uint32_t hist_len,
+                uint64_t *d_root_nodes, uint64_t *d_root_cost, cudaStream_t st) {
     int rc = ensure_scratch(ctx);
     if (rc) return rc;
     rc = ensure_counters(ctx);
@@ -288,9 +469,11 @@ int mce_enqueue(g2_ctx *ctx, uint64_t ntasks, const g2_opts *o, unsigned long lo
         a.ci = ctx->d_ci;
         a.fo = ctx->d_fo;
         a.tasks = ctx->d_tasks;
+        a.task_part = tl.split ? ctx->d_part : nullptr;
+        a.root_cost = d_root_cost;
         a.task_index = k == 0 ? nullptr : ctx->d_defer + (uint64_t)(k - 1) * ctx->tasks_cap;
-        a.ntasks = k == 0 ? ntasks : 0;
-        a.ntasks_dev = k == 0 ? nullptr : ctx->d_ctr + 4 + (k - 1);
+        a.ntasks = k == 0 ? tl.cap : 0;
+        a.ntasks_dev = k == 0 ? (tl.split ? ctx->d_ntask : nullptr) : ctx->d_ctr + 4 + (k - 1);
         a.head = ctx->d_ctr + k;
         a.chunk = k == 0 ? 2 : 1;
         a.hist_len = hist_len;
@@ -312,6 +495,66 @@ int mce_enqueue(g2_ctx *ctx, uint64_t ntasks, const g2_opts *o, unsigned long lo
         ctx->launches++;
     }
     return G2_OK;
+}
+
+// Persistent-grid geometry of the match kernel.
+void match_geometry(g2_ctx *ctx, const g2_opts *o, int *wpl, int *wpb, int *blocks) {
+    *wpl = wpl_for(ctx->max_fwd);
+    *wpb = default_warps(o);
+    while (*wpb > 1 && g2::match_smem_bytes(*wpl, *wpb) > 200 * 1024) *wpb /= 2;
+    *blocks = default_blocks(ctx, o, *wpb);
+}
+
+int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long long *d_out,
+                  uint64_t *d_root_nodes, uint64_t *d_root_cost, cudaStream_t st) {
+    int rc = ensure_scratch(ctx);
+    if (rc) return rc;
+    rc = ensure_counters(ctx);
+    if (rc) return rc;
+    G2_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(unsigned long long) * 16, st));
+    G2_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
+    G2_TRY(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
+    const uint32_t flags = o ? o->flags : 0u;
+    rc = prepare_flags(ctx, flags, st);
+    if (rc) return rc;
+    int wpl, wpb, blocks;
+    match_geometry(ctx, o, &wpl, &wpb, &blocks);
+    g2::MatchArgs a{};
+    a.rp = ctx->d_rp;
+    a.ci = ctx->d_ci;
+    a.fo = ctx->d_fo;
+    a.tasks = ctx->d_tasks;
+    a.task_part = tl.split ? ctx->d_part : nullptr;
+    a.root_cost = d_root_cost;
+    a.ntasks = tl.cap;
+    a.ntasks_dev = tl.split ? ctx->d_ntask : nullptr;
+    a.head = ctx->d_ctr;
+    a.chunk = 4;
+    a.scratch = ctx->d_scratch;
+    a.words_per_warp = (ctx->scratch_words / ((uint64_t)blocks * wpb)) & ~63ull;
+    if (a.words_per_warp / (ctx->plan.k > 2 ? ctx->plan.k - 2 : 1) < 64) return G2_ERR_OVERFLOW;
+    a.out = d_out;
+    a.root_nodes = d_root_nodes;
+    a.status = ctx->d_status;
+    a.work = (flags & G2_FLAG_WORK_MODEL) ? ctx->d_work : nullptr;
+    const bool clique = ctx->clique_plan && !(o && o->intersect_mode == 1);
+    if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
+    cudaError_t e = g2::match_launch(ctx->plan, a, blocks, wpb, st, clique, wpl);
+    if (e != cudaSuccess) return fail_cuda(ctx, e, "match_launch");
+    if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[1], st));
+    ctx->launches++;
+    return G2_OK;
+}
+
+uint64_t mce_warps(g2_ctx *ctx, const g2_opts *o) {
+    const int wpb = default_warps(o);
+    return (uint64_t)default_blocks(ctx, o, wpb) * wpb;
+}
+
+uint64_t match_warps(g2_ctx *ctx, const g2_opts *o) {
+    int wpl, wpb, blocks;
+    match_geometry(ctx, o, &wpl, &wpb, &blocks);
+    return (uint64_t)blocks * wpb;
 }
 
 }  // namespace
@@ -384,11 +627,12 @@ int g2_close(g2_ctx *ctx) {
         cudaFree(ctx->d_rp);
         cudaFree(ctx->d_ci);
     }
-    void *bufs[] = {ctx->d_fo, ctx->d_scratch, ctx->d_tasks, ctx->d_defer, ctx->d_root_nodes, ctx->d_ctr, ctx->d_status,
-                    ctx->d_out, ctx->d_keys, ctx->d_keys2, ctx->d_vals2, ctx->d_cub, ctx->d_scores};
+    void *bufs[] = {ctx->d_fo,     ctx->d_core,    ctx->d_scratch, ctx->d_tasks,  ctx->d_defer,      ctx->d_root_nodes,
+                    ctx->d_root_cost, ctx->d_ctr,  ctx->d_status,  ctx->d_out,    ctx->d_keys,       ctx->d_keys2,
+                    ctx->d_roots,  ctx->d_S,       ctx->d_part,    ctx->d_xroots, ctx->d_xparts,     ctx->d_cost,
+                    ctx->d_total,  ctx->d_ntask,   ctx->d_cub,     ctx->d_model,  ctx->d_work};
     for (void *b : bufs)
         if (b) cudaFree(b);
-    if (ctx->d_work) cudaFree(ctx->d_work);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     delete ctx;
@@ -398,6 +642,11 @@ int g2_close(g2_ctx *ctx) {
 static int after_load(g2_ctx *ctx) {
     int rc = grow(ctx, ctx->d_fo, ctx->fo_cap, std::max<uint64_t>(ctx->n, 1), "forward offsets");
     if (rc) return rc;
+    if (ctx->d_core) {  // core numbers belong to the previous graph
+        cudaFree(ctx->d_core);
+        ctx->d_core = nullptr;
+        ctx->core_cap = 0;
+    }
     unsigned int *d_max = nullptr;
     G2_TRY(cudaMalloc(&d_max, sizeof(unsigned int)));
     G2_TRY(cudaMemset(d_max, 0, sizeof(unsigned int)));
@@ -446,6 +695,16 @@ int g2_load_csr_device(g2_ctx *ctx, const uint64_t *d_row_ptrs, const uint32_t *
     return after_load(ctx);
 }
 
+int g2_load_core(g2_ctx *ctx, const uint32_t *core) {
+    if (!ctx || !core) return G2_ERR_INVALID;
+    if (!ctx->d_rp) return G2_ERR_NO_GRAPH;
+    G2_TRY(cudaSetDevice(ctx->device));
+    int rc = grow(ctx, ctx->d_core, ctx->core_cap, std::max<uint64_t>(ctx->n, 1), "core");
+    if (rc) return rc;
+    if (ctx->n) G2_TRY(cudaMemcpy(ctx->d_core, core, sizeof(uint32_t) * ctx->n, cudaMemcpyHostToDevice));
+    return G2_OK;
+}
+
 int g2_set_plan(g2_ctx *ctx, const g2_plan *p) {
     if (!ctx || !p) return G2_ERR_INVALID;
     const uint32_t k = p->k;
@@ -457,9 +716,11 @@ int g2_set_plan(g2_ctx *ctx, const g2_plan *p) {
     bool clique = true;
     for (uint32_t i = 0; i < k; i++) {
         const uint32_t u = p->order[i];  // query vertex at position i
-        if (i > 0 && p->bn_count[i] == 0) return G2_ERR_INVALID;
+        if (i > 0 && (p->bn_count[i] == 0 || p->bn_count[i] > k)) return G2_ERR_INVALID;
+        if (p->cond_count[u] > k) return G2_ERR_INVALID;
         d.bn_count[i] = p->bn_count[i];
         for (uint32_t j = 0; j < p->bn_count[i]; j++) {
+            if (p->bn[i][j] >= k) return G2_ERR_INVALID;
             uint32_t pos = p->id2order[p->bn[i][j]];
             if (pos >= i) return G2_ERR_INVALID;
             d.bn_pos[i][j] = pos;
@@ -467,6 +728,7 @@ int g2_set_plan(g2_ctx *ctx, const g2_plan *p) {
         d.cond_count[i] = p->cond_count[u];
         uint32_t larger = 0;
         for (uint32_t j = 0; j < p->cond_count[u]; j++) {
+            if (p->cond[u][j][1] >= k) return G2_ERR_INVALID;
             uint32_t pos = p->id2order[p->cond[u][j][1]];
             if (pos >= i || p->cond[u][j][0] > G2_COND_NON_EQUAL) return G2_ERR_INVALID;
             d.cond_op[i][j] = p->cond[u][j][0];
@@ -490,10 +752,13 @@ int g2_mce_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc, con
     G2_TRY(cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
     ctx->launches = 0;
-    int rc = prepare_tasks(ctx, d_sources, nsrc, true, opts, st, nullptr);
+    TaskList tl;
+    int rc = prepare_tasks(ctx, d_sources, nsrc, true, opts, mce_warps(ctx, opts), st, &tl);
     if (rc) return rc;
-    if (!d_sources) nsrc = ctx->n;
-    return mce_enqueue(ctx, nsrc, opts, reinterpret_cast<unsigned long long *>(d_out), hist_len, nullptr, st);
+    ctx->last_split = tl.split;
+    ctx->last_cap = tl.cap;
+    return mce_enqueue(ctx, tl, opts, reinterpret_cast<unsigned long long *>(d_out), hist_len, nullptr, nullptr,
+                       st);
 }
 
 int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opts *opts, uint64_t *count,
@@ -504,25 +769,21 @@ int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opt
     ctx->launches = 0;
     const uint32_t hl = hist ? hist_len : 1u;
     cudaStream_t st = nullptr;
-    std::vector<uint32_t> order;
-    const bool want_nodes = opts && opts->root_nodes;
-    int rc = prepare_tasks(ctx, sources, nsrc, false, opts, st, want_nodes ? &order : nullptr);
-    if (rc) return rc;
-    if (!sources) nsrc = ctx->n;
-    uint64_t rncap = ctx->root_nodes_cap;
-    if (want_nodes) {
-        rc = grow(ctx, ctx->d_root_nodes, rncap, nsrc, "root_nodes");
-        ctx->root_nodes_cap = rncap;
-        if (rc) return rc;
-    }
-    uint64_t oc = ctx->out_cap;
-    rc = grow(ctx, ctx->d_out, oc, 1 + hl, "out");
-    ctx->out_cap = (uint32_t)oc;
-    if (rc) return rc;
     g2_opts o2{};
     if (opts) o2 = *opts;
     if (o2.work_bytes) o2.flags |= G2_FLAG_WORK_MODEL;
-    rc = mce_enqueue(ctx, nsrc, &o2, ctx->d_out, hl, want_nodes ? ctx->d_root_nodes : nullptr, st);
+    TaskList tl;
+    int rc = prepare_tasks(ctx, sources, nsrc, false, &o2, mce_warps(ctx, &o2), st, &tl);
+    if (rc) return rc;
+    if (!sources) nsrc = ctx->n;
+    ctx->last_split = tl.split;
+    ctx->last_cap = tl.cap;
+    rc = prepare_root_outputs(ctx, o2.root_nodes != nullptr, o2.root_cost != nullptr, st);
+    if (rc) return rc;
+    rc = grow(ctx, ctx->d_out, ctx->out_cap, 1 + hl, "out");
+    if (rc) return rc;
+    rc = mce_enqueue(ctx, tl, &o2, ctx->d_out, hl, o2.root_nodes ? ctx->d_root_nodes : nullptr,
+                     o2.root_cost ? ctx->d_root_cost : nullptr, st);
     if (rc) return rc;
     std::vector<unsigned long long> h(1 + hl);
     int status = 0;
@@ -538,22 +799,8 @@ int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opt
         rc = g2_last_work_bytes(ctx, o2.work_bytes);
         if (rc) return rc;
     }
-    if (want_nodes) {
-        std::vector<uint64_t> rn(nsrc);
-        G2_TRY(cudaMemcpy(rn.data(), ctx->d_root_nodes, sizeof(uint64_t) * nsrc, cudaMemcpyDeviceToHost));
-        if (!order.empty()) {
-            // task i ran root order[i]; map back to the caller's source index
-            std::vector<uint64_t> pos_of(ctx->n, ~0ull);
-            if (sources)
-                for (uint64_t i = 0; i < nsrc; i++) pos_of[sources[i]] = i;
-            for (uint64_t i = 0; i < nsrc; i++) {
-                uint64_t j = sources ? pos_of[order[i]] : order[i];
-                opts->root_nodes[j] = rn[i];
-            }
-        } else {
-            memcpy(opts->root_nodes, rn.data(), sizeof(uint64_t) * nsrc);
-        }
-    }
+    rc = gather_root_outputs(ctx, sources, nsrc, o2.root_nodes, o2.root_cost);
+    if (rc) return rc;
     return status_to_code(status);
 }
 
@@ -565,45 +812,12 @@ int g2_match_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc, c
     G2_TRY(cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
     ctx->launches = 0;
-    int rc = prepare_tasks(ctx, d_sources, nsrc, true, opts, st, nullptr);
+    TaskList tl;
+    int rc = prepare_tasks(ctx, d_sources, nsrc, true, opts, match_warps(ctx, opts), st, &tl);
     if (rc) return rc;
-    if (!d_sources) nsrc = ctx->n;
-    rc = ensure_scratch(ctx);
-    if (rc) return rc;
-    rc = ensure_counters(ctx);
-    if (rc) return rc;
-    G2_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(unsigned long long) * 16, st));
-    G2_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
-    G2_TRY(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
-    const uint32_t flags = opts ? opts->flags : 0u;
-    rc = prepare_flags(ctx, flags, st);
-    if (rc) return rc;
-    int wpl = wpl_for(ctx->max_fwd);
-    int wpb = default_warps(opts);
-    while (wpb > 1 && g2::match_smem_bytes(wpl, wpb) > 200 * 1024) wpb /= 2;
-    const int blocks = default_blocks(ctx, opts, wpb);
-    g2::MatchArgs a{};
-    a.rp = ctx->d_rp;
-    a.ci = ctx->d_ci;
-    a.fo = ctx->d_fo;
-    a.tasks = ctx->d_tasks;
-    a.ntasks = nsrc;
-    a.head = ctx->d_ctr;
-    a.chunk = 4;
-    a.scratch = ctx->d_scratch;
-    a.words_per_warp = (ctx->scratch_words / ((uint64_t)blocks * wpb)) & ~63ull;
-    if (a.words_per_warp / (ctx->plan.k > 2 ? ctx->plan.k - 2 : 1) < 64) return G2_ERR_OVERFLOW;
-    a.out = reinterpret_cast<unsigned long long *>(d_out);
-    a.root_nodes = nullptr;
-    a.status = ctx->d_status;
-    a.work = (flags & G2_FLAG_WORK_MODEL) ? ctx->d_work : nullptr;
-    const bool clique = ctx->clique_plan && !(opts && opts->intersect_mode == 1);
-    if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
-    cudaError_t e = g2::match_launch(ctx->plan, a, blocks, wpb, st, clique, wpl);
-    if (e != cudaSuccess) return fail_cuda(ctx, e, "match_launch");
-    if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[1], st));
-    ctx->launches++;
-    return G2_OK;
+    ctx->last_split = tl.split;
+    ctx->last_cap = tl.cap;
+    return match_enqueue(ctx, tl, opts, reinterpret_cast<unsigned long long *>(d_out), nullptr, nullptr, st);
 }
 
 int g2_match_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opts *opts, uint64_t *count) {
@@ -611,34 +825,203 @@ int g2_match_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_o
     if (!ctx->d_rp) return G2_ERR_NO_GRAPH;
     if (!ctx->has_plan) return G2_ERR_NO_PLAN;
     G2_TRY(cudaSetDevice(ctx->device));
-    uint32_t *d_src = nullptr;
-    if (sources) {
-        G2_TRY(cudaMalloc(&d_src, sizeof(uint32_t) * std::max<uint64_t>(nsrc, 1)));
-        cudaError_t e = cudaMemcpy(d_src, sources, sizeof(uint32_t) * nsrc, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) {
-            cudaFree(d_src);
-            return fail_cuda(ctx, e, "sources");
-        }
-    }
-    uint64_t oc = ctx->out_cap;
-    int rc = grow(ctx, ctx->d_out, oc, 1, "out");
-    ctx->out_cap = (uint32_t)oc;
+    ctx->launches = 0;
+    cudaStream_t st = nullptr;
     g2_opts o2{};
     if (opts) o2 = *opts;
     if (o2.work_bytes) o2.flags |= G2_FLAG_WORK_MODEL;
-    if (!rc) rc = g2_match_run_device(ctx, sources ? d_src : nullptr, nsrc, &o2, (uint64_t *)ctx->d_out, nullptr);
-    if (!rc && o2.work_bytes) rc = g2_last_work_bytes(ctx, o2.work_bytes);
+    TaskList tl;
+    int rc = prepare_tasks(ctx, sources, nsrc, false, &o2, match_warps(ctx, &o2), st, &tl);
+    if (rc) return rc;
+    if (!sources) nsrc = ctx->n;
+    ctx->last_split = tl.split;
+    ctx->last_cap = tl.cap;
+    rc = prepare_root_outputs(ctx, o2.root_nodes != nullptr, o2.root_cost != nullptr, st);
+    if (!rc) rc = grow(ctx, ctx->d_out, ctx->out_cap, 1, "out");
+    if (!rc)
+        rc = match_enqueue(ctx, tl, &o2, ctx->d_out, o2.root_nodes ? ctx->d_root_nodes : nullptr,
+                           o2.root_cost ? ctx->d_root_cost : nullptr, st);
+    if (rc) return rc;
     unsigned long long h = 0;
     int status = 0;
-    if (!rc) {
-        cudaError_t e = cudaMemcpy(&h, ctx->d_out, sizeof(h), cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) rc = fail_cuda(ctx, e, "match result");
-    }
-    if (d_src) cudaFree(d_src);
-    if (rc) return rc;
+    G2_TRY(cudaMemcpy(&h, ctx->d_out, sizeof(h), cudaMemcpyDeviceToHost));
+    G2_TRY(cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     *count = h;
+    if (o2.work_bytes) {
+        rc = g2_last_work_bytes(ctx, o2.work_bytes);
+        if (rc) return rc;
+    }
+    rc = gather_root_outputs(ctx, sources, nsrc, o2.root_nodes, o2.root_cost);
+    if (rc) return rc;
     return status_to_code(status);
+}
+
+// ---------------------------------------------------------- cost model
+
+int g2_root_features(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, float *out) {
+    if (!ctx || !out) return G2_ERR_INVALID;
+    if (!ctx->d_rp) return G2_ERR_NO_GRAPH;
+    G2_TRY(cudaSetDevice(ctx->device));
+    if (!sources) nsrc = ctx->n;
+    uint32_t *d_src = nullptr;
+    float *d_f = nullptr;
+    if (sources) G2_TRY(cudaMalloc(&d_src, sizeof(uint32_t) * std::max<uint64_t>(nsrc, 1)));
+    cudaError_t e = cudaMalloc(&d_f, sizeof(float) * G2_MODEL_FEATURES * std::max<uint64_t>(nsrc, 1));
+    if (e == cudaSuccess && sources)
+        e = cudaMemcpy(d_src, sources, sizeof(uint32_t) * nsrc, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nsrc)
+        e = g2::features_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, ctx->d_core, d_src, nsrc, d_f, ctx->sm_count, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(out, d_f, sizeof(float) * G2_MODEL_FEATURES * nsrc, cudaMemcpyDeviceToHost);
+    cudaFree(d_src);
+    cudaFree(d_f);
+    if (e != cudaSuccess) return fail_cuda(ctx, e, "g2_root_features");
+    return G2_OK;
+}
+
+// Scratch of one training / gradient call, freed on return.
+struct TrainBufs {
+    float *X = nullptr, *Y = nullptr, *params = nullptr, *norm = nullptr, *grad = nullptr, *mom = nullptr,
+          *vel = nullptr, *loss = nullptr;
+    uint32_t *idx = nullptr;
+    ~TrainBufs() {
+        void *b[] = {X, Y, params, norm, grad, mom, vel, loss, idx};
+        for (void *p : b)
+            if (p) cudaFree(p);
+    }
+};
+
+static int upload_train(g2_ctx *ctx, TrainBufs &b, const float *X, const float *Y, uint64_t n, const float *norm,
+                        const float *params) {
+    const uint64_t nn = std::max<uint64_t>(n, 1);
+    G2_TRY(cudaMalloc(&b.X, sizeof(float) * G2_MODEL_FEATURES * nn));
+    G2_TRY(cudaMalloc(&b.Y, sizeof(float) * nn));
+    G2_TRY(cudaMalloc(&b.idx, sizeof(uint32_t) * nn));
+    G2_TRY(cudaMalloc(&b.params, sizeof(float) * G2_MODEL_PARAMS));
+    G2_TRY(cudaMalloc(&b.norm, sizeof(float) * G2_MODEL_NORM));
+    G2_TRY(cudaMalloc(&b.grad, sizeof(float) * G2_MODEL_PARAMS));
+    G2_TRY(cudaMalloc(&b.loss, sizeof(float)));
+    G2_TRY(cudaMemcpy(b.X, X, sizeof(float) * G2_MODEL_FEATURES * n, cudaMemcpyHostToDevice));
+    G2_TRY(cudaMemcpy(b.Y, Y, sizeof(float) * n, cudaMemcpyHostToDevice));
+    G2_TRY(cudaMemcpy(b.params, params, sizeof(float) * G2_MODEL_PARAMS, cudaMemcpyHostToDevice));
+    G2_TRY(cudaMemcpy(b.norm, norm, sizeof(float) * G2_MODEL_NORM, cudaMemcpyHostToDevice));
+    return G2_OK;
+}
+
+int g2_model_grad(g2_ctx *ctx, const float *X, const float *y, uint32_t n, const float *norm, const float *params,
+                  float *grad, float *loss) {
+    if (!ctx || !X || !y || !norm || !params || !grad || n == 0) return G2_ERR_INVALID;
+    G2_TRY(cudaSetDevice(ctx->device));
+    TrainBufs b;
+    int rc = upload_train(ctx, b, X, y, n, norm, params);
+    if (rc) return rc;
+    std::vector<uint32_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0u);
+    G2_TRY(cudaMemcpy(b.idx, idx.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    G2_TRY(cudaMemset(b.grad, 0, sizeof(float) * G2_MODEL_PARAMS));
+    G2_TRY(cudaMemset(b.loss, 0, sizeof(float)));
+    G2_TRY(g2::train_step_launch(b.X, b.Y, b.idx, n, b.params, b.norm, b.grad, b.loss, 0));
+    G2_TRY(cudaMemcpy(grad, b.grad, sizeof(float) * G2_MODEL_PARAMS, cudaMemcpyDeviceToHost));
+    float l = 0.f;
+    G2_TRY(cudaMemcpy(&l, b.loss, sizeof(float), cudaMemcpyDeviceToHost));
+    if (loss) *loss = l / (float)n;
+    return G2_OK;
+}
+
+int g2_model_train(g2_ctx *ctx, const float *X, const float *cost, uint64_t n, uint32_t epochs, uint32_t batch,
+                   float lr, uint64_t seed, float *params, float *norm, float *epoch_loss) {
+    if (!ctx || !X || !cost || !params || !norm || n < 2 || n >= (1ull << 31) || batch == 0) return G2_ERR_INVALID;
+    G2_TRY(cudaSetDevice(ctx->device));
+    const int F = G2_MODEL_FEATURES;
+    // normalisation of features and of the log-cost targets
+    std::vector<double> mean(F, 0.0), var(F, 0.0);
+    std::vector<float> y(n);
+    double ym = 0.0, yv = 0.0;
+    for (uint64_t i = 0; i < n; i++) {
+        for (int k = 0; k < F; k++) mean[k] += X[i * F + k];
+        y[i] = std::log1p(std::max(0.f, cost[i]));
+        ym += y[i];
+    }
+    for (int k = 0; k < F; k++) mean[k] /= (double)n;
+    ym /= (double)n;
+    for (uint64_t i = 0; i < n; i++) {
+        for (int k = 0; k < F; k++) var[k] += (X[i * F + k] - mean[k]) * (X[i * F + k] - mean[k]);
+        yv += (y[i] - ym) * (y[i] - ym);
+    }
+    for (int k = 0; k < F; k++) {
+        norm[k] = (float)mean[k];
+        norm[F + k] = (float)std::max(1e-3, std::sqrt(var[k] / (double)n));
+    }
+    norm[2 * F] = (float)ym;
+    norm[2 * F + 1] = (float)std::max(1e-3, std::sqrt(yv / (double)n));
+    for (uint64_t i = 0; i < n; i++) y[i] = (y[i] - norm[2 * F]) / norm[2 * F + 1];
+    // He-uniform initialisation
+    std::mt19937_64 rng(seed);
+    auto uni = [&](float lim) { return std::uniform_real_distribution<float>(-lim, lim)(rng); };
+    for (int i = 0; i < 64 * F; i++) params[i] = uni(std::sqrt(6.f / F));
+    for (int i = 0; i < 64; i++) params[64 * F + i] = 0.f;
+    for (int i = 0; i < 64 * 64; i++) params[64 * F + 64 + i] = uni(std::sqrt(6.f / 64));
+    for (int i = 0; i < 64; i++) params[64 * F + 64 + 4096 + i] = 0.f;
+    for (int i = 0; i < 64; i++) params[64 * F + 128 + 4096 + i] = uni(std::sqrt(6.f / 64));
+    params[G2_MODEL_PARAMS - 1] = 0.f;
+    TrainBufs b;
+    int rc = upload_train(ctx, b, X, y.data(), n, norm, params);
+    if (rc) return rc;
+    G2_TRY(cudaMalloc(&b.mom, sizeof(float) * G2_MODEL_PARAMS));
+    G2_TRY(cudaMalloc(&b.vel, sizeof(float) * G2_MODEL_PARAMS));
+    G2_TRY(cudaMemset(b.mom, 0, sizeof(float) * G2_MODEL_PARAMS));
+    G2_TRY(cudaMemset(b.vel, 0, sizeof(float) * G2_MODEL_PARAMS));
+    std::vector<uint32_t> perm(n);
+    std::iota(perm.begin(), perm.end(), 0u);
+    int step = 0;
+    for (uint32_t ep = 0; ep < epochs; ep++) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        G2_TRY(cudaMemcpy(b.idx, perm.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+        G2_TRY(cudaMemset(b.loss, 0, sizeof(float)));
+        for (uint64_t s = 0; s < n; s += batch) {
+            const uint32_t m = (uint32_t)std::min<uint64_t>(batch, n - s);
+            G2_TRY(cudaMemsetAsync(b.grad, 0, sizeof(float) * G2_MODEL_PARAMS));
+            G2_TRY(g2::train_step_launch(b.X, b.Y, b.idx + s, m, b.params, b.norm, b.grad, b.loss, 0));
+            G2_TRY(g2::adam_launch(b.params, b.mom, b.vel, b.grad, lr, ++step, 0));
+        }
+        if (epoch_loss) {
+            float l = 0.f;
+            G2_TRY(cudaMemcpy(&l, b.loss, sizeof(float), cudaMemcpyDeviceToHost));
+            epoch_loss[ep] = l / (float)n;
+        }
+    }
+    G2_TRY(cudaMemcpy(params, b.params, sizeof(float) * G2_MODEL_PARAMS, cudaMemcpyDeviceToHost));
+    return G2_OK;
+}
+
+int g2_model_predict(g2_ctx *ctx, const float *X, uint64_t n, const float *norm, const float *params, float *out) {
+    if (!ctx || !X || !norm || !params || !out) return G2_ERR_INVALID;
+    G2_TRY(cudaSetDevice(ctx->device));
+    if (n == 0) return G2_OK;
+    TrainBufs b;
+    int rc = upload_train(ctx, b, X, X, 0, norm, params);  // X / params / norm only
+    if (rc) return rc;
+    float *d_x = nullptr, *d_p = nullptr;
+    G2_TRY(cudaMalloc(&d_x, sizeof(float) * G2_MODEL_FEATURES * n));
+    cudaError_t e = cudaMalloc(&d_p, sizeof(float) * n);
+    if (e == cudaSuccess) e = cudaMemcpy(d_x, X, sizeof(float) * G2_MODEL_FEATURES * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = g2::score_launch(nullptr, nullptr, nullptr, nullptr, nullptr, n, d_x, b.params, b.norm, d_p, nullptr,
+                             nullptr, ctx->sm_count, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d_p, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d_x);
+    cudaFree(d_p);
+    if (e != cudaSuccess) return fail_cuda(ctx, e, "g2_model_predict");
+    return G2_OK;
+}
+
+int g2_set_model(g2_ctx *ctx, const float *params, const float *norm) {
+    if (!ctx || !params || !norm) return G2_ERR_INVALID;
+    G2_TRY(cudaSetDevice(ctx->device));
+    if (!ctx->d_model) G2_TRY(cudaMalloc(&ctx->d_model, sizeof(float) * (G2_MODEL_PARAMS + G2_MODEL_NORM)));
+    G2_TRY(cudaMemcpy(ctx->d_model, params, sizeof(float) * G2_MODEL_PARAMS, cudaMemcpyHostToDevice));
+    G2_TRY(cudaMemcpy(ctx->d_model + G2_MODEL_PARAMS, norm, sizeof(float) * G2_MODEL_NORM, cudaMemcpyHostToDevice));
+    return G2_OK;
 }
 
 }  // extern "C"

@@ -37,7 +37,8 @@ class G2Opts(C.Structure):
         ("blocks", u32), ("warps_per_block", u32), ("schedule", u32),
         ("split_threshold", u32), ("scores", P(C.c_float)),
         ("root_nodes", P(u64)), ("work_bytes", P(u64)),
-        ("intersect_mode", u32), ("flags", u32), ("reserved", u32 * 6),
+        ("intersect_mode", u32), ("flags", u32), ("reserved0", u32), ("root_cost", P(u64)),
+        ("reserved", u32 * 2),
     ]
 
 
@@ -68,6 +69,15 @@ def lib():
         "g2_last_launch_count": (u64, [C.c_void_p]),
         "g2_pass_time_ms": (i32, [C.c_void_p, i32, P(C.c_float)]),
         "g2_last_work_bytes": (i32, [C.c_void_p, P(u64)]),
+        "g2_load_core": (i32, [C.c_void_p, C.c_void_p]),
+        "g2_root_features": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p]),
+        "g2_model_train": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, u32, u32, C.c_float, u64, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]),
+        "g2_model_grad": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_void_p]),
+        "g2_model_predict": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "g2_set_model": (i32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+        "g2_match_count_noalloc": (i32, [C.c_void_p, C.c_void_p, u64, u64, C.c_void_p, C.c_void_p, C.c_void_p]),
         "g2_plan_preset": (i32, [i32, P(G2Plan)]),
         "g2_plan_build": (i32, [u32, C.c_void_p, u32, P(G2Plan)]),
         "g2_read_bin": (i32, [C.c_char_p, P(C.c_void_p), P(C.c_void_p), P(u64), P(u64)]),

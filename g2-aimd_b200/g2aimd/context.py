@@ -15,7 +15,9 @@ import numpy as np
 
 from ._lib import G2_MAX_QUERY, G2Opts, G2Plan, check, lib
 
-SCHED = {"given": 0, "heuristic": 1, "scores": 2}
+SCHED = {"given": 0, "heuristic": 1, "scores": 2, "learned": 3}
+FLAG_TIME_KERNELS, FLAG_WORK_MODEL, FLAG_SPLIT, FLAG_NO_SPLIT = 1, 2, 4, 8
+MODEL_FEATURES, MODEL_PARAMS, MODEL_NORM = 8, 4801, 18
 
 
 class Plan:
@@ -73,9 +75,9 @@ class Plan:
 
 
 def _opts(warps_per_block=0, blocks=0, schedule="given", scores=None, root_nodes=None, intersect_mode=0,
-          split_threshold=0, flags=0, work_bytes=None):
+          split_threshold=0, flags=0, work_bytes=None, root_cost=None, split=False):
     o = G2Opts()
-    o.flags = flags
+    o.flags = flags | (FLAG_SPLIT if split else 0)
     o.warps_per_block = warps_per_block
     o.blocks = blocks
     o.schedule = SCHED[schedule]
@@ -90,6 +92,8 @@ def _opts(warps_per_block=0, blocks=0, schedule="given", scores=None, root_nodes
         o.root_nodes = root_nodes.ctypes.data_as(C.POINTER(C.c_uint64))
     if work_bytes is not None:
         o.work_bytes = work_bytes.ctypes.data_as(C.POINTER(C.c_uint64))
+    if root_cost is not None:
+        o.root_cost = root_cost.ctypes.data_as(C.POINTER(C.c_uint64))
     return o, keep
 
 
@@ -149,13 +153,14 @@ class Context:
         self._check(lib().g2_set_plan(self._h, C.byref(plan.raw)), "g2_set_plan")
         return self
 
-    def mce(self, sources=None, hist_len=256, root_nodes=False, **kw):
+    def mce(self, sources=None, hist_len=256, root_nodes=False, root_cost=None, **kw):
         """(count, hist) of maximal cliques rooted at `sources` (default: all);
-        with root_nodes=True also the search-tree node count per source."""
+        with root_nodes=True also the search-tree node count per source.  A
+        uint64 array passed as root_cost receives SM cycles per source."""
         src = None if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
         nsrc = 0 if src is None else src.size
         rn = np.zeros(nsrc if src is not None else self.graph.n, np.uint64) if root_nodes else None
-        o, keep = _opts(root_nodes=rn, **kw)
+        o, keep = _opts(root_nodes=rn, root_cost=root_cost, **kw)
         count = C.c_uint64()
         hist = np.zeros(hist_len, np.uint64)
         self._check(lib().g2_mce_run(self._h, None if src is None else src.ctypes.data_as(C.c_void_p), nsrc,
@@ -164,11 +169,14 @@ class Context:
         del keep
         return (count.value, hist, rn) if root_nodes else (count.value, hist)
 
-    def match(self, plan: Plan = None, sources=None, **kw):
+    def match(self, plan: Plan = None, sources=None, root_counts=None, root_cost=None, **kw):
+        """Embeddings admitted by the plan, rooted at `sources` (default: all).
+        Optional uint64 arrays: root_counts (embeddings per source), root_cost
+        (SM cycles per source)."""
         if plan is not None:
             self.set_plan(plan)
         src = None if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
-        o, keep = _opts(**kw)
+        o, keep = _opts(root_nodes=root_counts, root_cost=root_cost, **kw)
         count = C.c_uint64()
         self._check(lib().g2_match_run(self._h, None if src is None else src.ctypes.data_as(C.c_void_p),
                                        0 if src is None else src.size, C.byref(o), C.byref(count)), "g2_match_run")
@@ -189,4 +197,79 @@ class Context:
                     "g2_match_run_device")
 
 
-__all__ = ["Context", "Plan", "G2_MAX_QUERY"]
+    # ------------------------------------------------------ cost model
+    def load_core(self, core):
+        c = np.ascontiguousarray(core, dtype=np.uint32)
+        self._check(lib().g2_load_core(self._h, c.ctypes.data_as(C.c_void_p)), "g2_load_core")
+
+    def root_features(self, sources=None):
+        src = None if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+        n = self.graph.n if src is None else src.size
+        out = np.zeros((n, MODEL_FEATURES), np.float32)
+        self._check(lib().g2_root_features(self._h, None if src is None else src.ctypes.data_as(C.c_void_p),
+                                           0 if src is None else src.size, out.ctypes.data_as(C.c_void_p)),
+                    "g2_root_features")
+        return out
+
+    def set_model(self, model: "CostModel"):
+        self._check(lib().g2_set_model(self._h, model.params.ctypes.data_as(C.c_void_p),
+                                       model.norm.ctypes.data_as(C.c_void_p)), "g2_set_model")
+
+
+class CostModel:
+    """The learned root-cost model: 8 features -> 64 -> 64 -> 1, trained and
+    evaluated by the library's tensor-core kernels (g2_model_*)."""
+
+    def __init__(self, params, norm):
+        self.params = np.ascontiguousarray(params, dtype=np.float32)
+        self.norm = np.ascontiguousarray(norm, dtype=np.float32)
+        assert self.params.size == MODEL_PARAMS and self.norm.size == MODEL_NORM
+
+    @staticmethod
+    def train(ctx: Context, X, cost, epochs=30, batch=1024, lr=3e-3, seed=0):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        cost = np.ascontiguousarray(cost, dtype=np.float32)
+        params = np.zeros(MODEL_PARAMS, np.float32)
+        norm = np.zeros(MODEL_NORM, np.float32)
+        losses = np.zeros(epochs, np.float32)
+        ctx._check(lib().g2_model_train(ctx.handle, X.ctypes.data_as(C.c_void_p), cost.ctypes.data_as(C.c_void_p),
+                                        X.shape[0], epochs, batch, lr, seed, params.ctypes.data_as(C.c_void_p),
+                                        norm.ctypes.data_as(C.c_void_p), losses.ctypes.data_as(C.c_void_p)),
+                   "g2_model_train")
+        m = CostModel(params, norm)
+        m.losses = losses
+        return m
+
+    def predict(self, ctx: Context, X):
+        """Normalised log-cost predictions of feature rows X (n x 8)."""
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        out = np.zeros(X.shape[0], np.float32)
+        ctx._check(lib().g2_model_predict(ctx.handle, X.ctypes.data_as(C.c_void_p), X.shape[0],
+                                          self.norm.ctypes.data_as(C.c_void_p),
+                                          self.params.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)),
+                   "g2_model_predict")
+        return out
+
+    def grad(self, ctx: Context, X, y):
+        """(gradient of the mean squared error w.r.t. the parameters, loss) for
+        normalised targets y, computed by the training kernel."""
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        g = np.zeros(MODEL_PARAMS, np.float32)
+        loss = C.c_float()
+        ctx._check(lib().g2_model_grad(ctx.handle, X.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p),
+                                       X.shape[0], self.norm.ctypes.data_as(C.c_void_p),
+                                       self.params.ctypes.data_as(C.c_void_p), g.ctypes.data_as(C.c_void_p),
+                                       C.byref(loss)), "g2_model_grad")
+        return g, loss.value
+
+    def save(self, path):
+        np.savez(path, params=self.params, norm=self.norm)
+
+    @staticmethod
+    def load(path):
+        d = np.load(path)
+        return CostModel(d["params"], d["norm"])
+
+
+__all__ = ["Context", "Plan", "CostModel", "G2_MAX_QUERY"]

@@ -94,7 +94,10 @@ typedef struct g2_plan {
 /* Root schedule (task order of the device work queue). */
 #define G2_SCHED_GIVEN 0      /* sources in the order given                      */
 #define G2_SCHED_HEURISTIC 1  /* plain heuristic: descending forward degree x core */
-#define G2_SCHED_SCORES 2     /* descending caller scores (learned cost model)     */
+#define G2_SCHED_SCORES 2     /* descending caller scores                          */
+#define G2_SCHED_LEARNED 3    /* descending cost predicted on the device by the model
+                                 set with g2_set_model (features + MLP fused into
+                                 task generation); heavy roots split by default  */
 
 /*
  * Run options.  Zero-initialise and set what you need; 0 means "default".
@@ -106,17 +109,27 @@ typedef struct g2_opts {
     uint32_t split_threshold;   /* MCE: split roots whose |P0| exceeds this into one
                                    task per branch (0 = default, ~0u = never)      */
     const float *scores;        /* host, nsrc entries, for G2_SCHED_SCORES          */
-    uint64_t *root_nodes;       /* optional host out: search-tree nodes per source  */
+    uint64_t *root_nodes;       /* optional host out: search-tree nodes per source
+                                   (MCE) or embeddings per source (match), summed
+                                   over a source's split tasks                      */
     uint64_t *work_bytes;       /* optional host out: algorithmic bytes W (MCE)     */
     uint32_t intersect_mode;    /* GMatch: 0 auto (clique bitmap path when the plan is
                                    a clique), 1 generic plan-driven path only        */
     uint32_t flags;             /* G2_FLAG_* bits                                    */
-    uint32_t reserved[6];
+    uint32_t reserved0;
+    uint64_t *root_cost;        /* optional host out: SM cycles per source (summed
+                                   over its split tasks)                            */
+    uint32_t reserved[2];
 } g2_opts;
 
 /* g2_opts.flags */
 #define G2_FLAG_TIME_KERNELS 1u  /* record CUDA events around each enumeration pass */
 #define G2_FLAG_WORK_MODEL 2u    /* count the work model W on the device (slower)    */
+#define G2_FLAG_SPLIT 4u         /* split heavy roots by the schedule's cost estimate:
+                                    a root of estimated cost c becomes ceil(c / t)
+                                    tasks (at most 64), t = total / (4 x warps); each
+                                    task owns every k-th top-level branch            */
+#define G2_FLAG_NO_SPLIT 8u      /* G2_SCHED_LEARNED without splitting               */
 
 typedef struct g2_ctx g2_ctx;
 
@@ -219,6 +232,37 @@ int g2_last_work_bytes(g2_ctx *ctx, uint64_t *bytes);
 int g2_match_count_noalloc(const uint64_t *d_row_ptrs, const uint32_t *d_cols,
                            uint64_t n, uint64_t m, const g2_plan *plan,
                            uint64_t *d_count, void *stream);
+
+/*
+ * Learned root-cost model (no counterpart in the reference; it only orders and
+ * splits root tasks).  MLP 8 -> 64 -> 64 -> 1 with ReLU, fp32 master weights,
+ * bf16 tensor-core arithmetic with fp32 accumulation.  params (G2_MODEL_PARAMS
+ * floats): W1[64][8], b1[64], W2[64][64], b2[64], w3[64], b3.  norm
+ * (G2_MODEL_NORM floats): feature mean[8], feature std[8], target mean, target
+ * std; targets are log1p(cost), cost = SM cycles of a root's search.
+ */
+#define G2_MODEL_FEATURES 8
+#define G2_MODEL_PARAMS 4801
+#define G2_MODEL_NORM 18
+/* Core numbers (n entries, host) used by feature f1; without them p stands in. */
+int g2_load_core(g2_ctx *ctx, const uint32_t *core);
+/* Features of each source (host out, nsrc x 8; sources NULL = all vertices). */
+int g2_root_features(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, float *out);
+/* Train on (X, cost): computes norm, initialises params from seed (He uniform)
+ * and runs `epochs` of mini-batch Adam on the device.  epoch_loss (optional,
+ * epochs entries) receives the mean squared error in normalised units. */
+int g2_model_train(g2_ctx *ctx, const float *X, const float *cost, uint64_t n, uint32_t epochs,
+                   uint32_t batch, float lr, uint64_t seed, float *params, float *norm,
+                   float *epoch_loss);
+/* One forward+backward on (X, y_normalised) without updating: gradient of the
+ * mean squared error w.r.t. params (G2_MODEL_PARAMS floats) and the loss. */
+int g2_model_grad(g2_ctx *ctx, const float *X, const float *y, uint32_t n, const float *norm,
+                  const float *params, float *grad, float *loss);
+/* Predicted normalised log-cost of given feature rows (host in / out). */
+int g2_model_predict(g2_ctx *ctx, const float *X, uint64_t n, const float *norm,
+                     const float *params, float *out);
+/* Model used by G2_SCHED_LEARNED in this context. */
+int g2_set_model(g2_ctx *ctx, const float *params, const float *norm);
 
 /* ------------------------------------------------------ host-side helpers */
 

@@ -1,0 +1,147 @@
+"""The learned root-cost model: tensor-core training/inference kernels against
+the CPU fp32 oracle, and the schedules it drives (order + heavy-root splits)
+leaving every result unchanged."""
+import numpy as np
+import pytest
+
+from helpers import random_graph
+
+pytestmark = pytest.mark.gpu
+
+
+def _he(seed):
+    rng = np.random.default_rng(seed)
+    F, H = 8, 64
+    parts = [rng.uniform(-np.sqrt(6 / F), np.sqrt(6 / F), H * F), rng.normal(0, 0.1, H),
+             rng.uniform(-np.sqrt(6 / H), np.sqrt(6 / H), H * H), rng.normal(0, 0.1, H),
+             rng.uniform(-np.sqrt(6 / H), np.sqrt(6 / H), H), [0.3]]
+    return np.concatenate(parts).astype(np.float32)
+
+
+def _data(n, seed):
+    rng = np.random.default_rng(seed)
+    X = rng.gamma(2.0, 1.5, (n, 8)).astype(np.float32)
+    norm = np.concatenate([X.mean(0), X.std(0) + 1e-3, [0.0, 1.0]]).astype(np.float32)
+    y = rng.normal(0, 1, n).astype(np.float32)
+    return X, y, norm
+
+
+@pytest.mark.parametrize("n", [1, 16, 37, 300])
+def test_gradient_matches_cpu_fp32_oracle(g2, ctx, n):
+    import mlp_oracle
+    from g2aimd.context import CostModel
+    X, y, norm = _data(n, 10 + n)
+    m = CostModel(_he(n), norm)
+    g, loss = m.grad(ctx, X, y)
+    want, wloss = mlp_oracle.grad(X, y, m.params, norm)
+    scale = np.abs(want).max()
+    assert np.allclose(g, want, rtol=1e-2, atol=1e-3 * scale), np.abs(g - want).max() / scale
+    assert abs(loss - wloss) <= 1e-3 * max(1.0, wloss)
+
+
+def test_prediction_matches_cpu_fp32_oracle(g2, ctx):
+    import mlp_oracle
+    from g2aimd.context import CostModel
+    X, _, norm = _data(1000, 3)
+    m = CostModel(_he(3), norm)
+    got = m.predict(ctx, X)
+    want, _ = mlp_oracle.forward(X, m.params, norm)
+    assert np.allclose(got, want, rtol=1e-3, atol=1e-3 * np.abs(want).max())
+
+
+def test_training_fits_a_smooth_target(g2, ctx):
+    from g2aimd.context import CostModel
+    rng = np.random.default_rng(5)
+    X = rng.gamma(2.0, 1.0, (20000, 8)).astype(np.float32)
+    cost = np.expm1(1.0 + X[:, 0] + 0.5 * X[:, 1] * X[:, 2] / (1 + X[:, 2])).astype(np.float32)
+    m = CostModel.train(ctx, X, cost, epochs=20, batch=512, lr=3e-3, seed=1)
+    assert m.losses[-1] < 0.1 * m.losses[0], m.losses
+    assert m.losses[-1] < 0.05
+
+
+def _np_features(g, v):
+    nb = g.neighbors(v)
+    fwd = nb[nb > v]
+    p = fwd.size
+    deg = g.degrees()
+    wedge = sum(int((g.neighbors(u) > u).sum()) for u in fwd)
+    ns = min(p, 4)
+    inter = []
+    for j in range(ns):
+        u = fwd[j * p // ns]
+        fu = g.neighbors(u)
+        inter.append(np.intersect1d(fu[fu > u], fwd).size)
+    mean = float(np.mean(inter)) if inter else 0.0
+    return np.array([np.log1p(deg[v]), np.log1p(g.core[v]), np.log1p(p), np.log1p(nb.size - p), np.log1p(wedge),
+                     np.log1p(mean), mean / p if p else 0.0, np.log1p(max(inter) if inter else 0)], np.float32)
+
+
+def test_root_features(g2, ctx):
+    g = g2.Graph.rmat(10, 8, seed=2).degeneracy_recoded()
+    ctx.load(g)
+    ctx.load_core(g.core)
+    f = ctx.root_features()
+    for v in range(0, g.n, 7):
+        assert np.allclose(f[v], _np_features(g, v), rtol=1e-5, atol=1e-5), v
+
+
+def test_split_and_learned_schedules_keep_results(g2, orc, ctx):
+    from g2aimd.context import CostModel, Plan
+    g = g2.Graph.rmat(12, 16, seed=9).degeneracy_recoded()
+    ctx.load(g)
+    ctx.load_core(g.core)
+    want = orc.mce(g, threads=8, per_root=True)
+    # a model trained on this graph's own root costs (any model keeps results exact)
+    cost = np.zeros(g.n, np.uint64)
+    ctx.mce(root_cost=cost)
+    model = CostModel.train(ctx, ctx.root_features(), cost.astype(np.float32), epochs=5, batch=256, seed=3)
+    ctx.set_model(model)
+    for kw in ({"schedule": "heuristic", "split": True}, {"schedule": "learned"},
+               {"schedule": "learned", "flags": 8}):
+        c, h, rn = ctx.mce(root_nodes=True, **kw)
+        assert c == want["count"] and np.array_equal(h[:want["hist"].size], want["hist"][:h.size]), kw
+        assert np.array_equal(rn, want["root_nodes"]), kw
+    src = np.arange(1, g.n, 5, dtype=np.uint32)
+    for q in (24, 2, 0):
+        plan = Plan.preset(q)
+        base = orc.match(g, plan, roots=src, threads=8, per_root=True)
+        for kw in ({"schedule": "heuristic", "split": True}, {"schedule": "learned"}, {"intersect_mode": 1,
+                   "schedule": "learned"}):
+            rc = np.zeros(src.size, np.uint64)
+            assert ctx.match(plan, sources=src, root_counts=rc, **kw) == base["count"], (q, kw)
+            assert np.array_equal(rc, base["root_counts"]), (q, kw)
+
+
+def test_learned_order_tracks_measured_cost(g2, ctx):
+    """Trained on root costs of seeded R-MAT graphs, the model ranks the roots of
+    a held-out graph by cost at least as well as the plain heuristic does."""
+    from g2aimd.context import CostModel, Plan
+    plan = Plan.preset(24)
+    Xs, cs = [], []
+    for seed in (101, 102, 103):
+        g = g2.Graph.rmat(13, 16, seed=seed).degeneracy_recoded()
+        ctx.load(g)
+        ctx.load_core(g.core)
+        cost = np.zeros(g.n, np.uint64)
+        ctx.match(plan, root_cost=cost)
+        Xs.append(ctx.root_features())
+        cs.append(cost.astype(np.float32))
+    model = CostModel.train(ctx, np.concatenate(Xs), np.concatenate(cs), epochs=40, batch=1024, seed=7)
+    g = g2.Graph.rmat(13, 16, seed=104).degeneracy_recoded()
+    ctx.load(g)
+    ctx.load_core(g.core)
+    cost = np.zeros(g.n, np.uint64)
+    ctx.match(plan, root_cost=cost)
+    pred = model.predict(ctx, ctx.root_features())
+    d = g.degrees().astype(np.float64)
+    p = np.array([int((g.neighbors(v) > v).sum()) for v in range(g.n)], np.float64)
+    heur = p * (p + d)
+
+    def spearman(a, b):
+        ra, rb = np.argsort(np.argsort(a)), np.argsort(np.argsort(b))
+        return float(np.corrcoef(ra, rb)[0, 1])
+
+    busy = cost > np.percentile(cost, 50)
+    s_model, s_heur = spearman(pred[busy], cost[busy]), spearman(heur[busy], cost[busy])
+    print(f"spearman on the costlier half: model {s_model:.3f}, heuristic {s_heur:.3f}")
+    assert s_model >= s_heur - 0.02
