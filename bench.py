@@ -6,11 +6,15 @@ power-law (Chung-Lu) graph reported beside it.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One step = one pass of the hot path over one batch: every root of the graph
-expanded by the persistent plan-driven kernel for the 4-clique plan (preset 24;
-task generation and the heuristic root schedule included).  `value` is
-4-clique matches per second with the CSR resident in HBM; `e2e` is the same
-metric through the host C ABI (g2_load_csr from pinned host memory +
-g2_match_run, count read back) every step.  Maximal-clique enumeration is not
+expanded by the persistent plan-driven kernel for the 4-clique plan (preset 24),
+task generation included: the learned cost model's features + MLP inference,
+heavy-root splits, the device sort of the task list.  `value` is 4-clique
+matches per second with the CSR resident in HBM, on the learned schedule whose
+launch parameters the autotuner picked before the timed steps; the plain
+schedule (heuristic order, one task per root) is timed the same way and
+reported beside it.  `e2e` is the same metric through the host C ABI
+(g2_load_csr + g2_load_core from pinned host memory, g2_match_run, count read
+back) every step.  Maximal-clique enumeration is not
 the headline on this graph: R-MAT graphs with edge factor 16 have a dense core
 whose maximal-clique count grows ~10x per scale (measured up to scale 14), so
 no implementation enumerates them at scale 20.  Under torchrun each rank runs
@@ -193,7 +197,8 @@ def run_ours(a):
     import torch
 
     import g2aimd
-    from g2aimd.context import Context, Plan
+    from g2aimd.autotune import DEFAULT_SPACE, tune
+    from g2aimd.context import Context, CostModel, Plan
     world, rank, local = dist_env()
     dist = world > 1
     if dist:
@@ -205,15 +210,19 @@ def run_ours(a):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     L = g2aimd.lib()
+    models = os.path.join(ROOT, "g2-aimd_b200", "models")
     g, gen_s = make_graph(a.scale, a.edge_factor, a.seed + rank)
     ctx = Context(local, a.scratch_mb << 20)
     rp = torch.from_numpy(g.row_ptrs.view(np.int64)).to(dev)
     ci = torch.from_numpy(g.cols.view(np.int32)).to(dev)
     ctx.load_device(rp.data_ptr(), ci.data_ptr(), g.n, g.m)
+    ctx.load_core(g.core)
+    ctx.set_model(CostModel.load(os.path.join(models, "k4.npz")))
     out = torch.zeros(1 + HIST, dtype=torch.int64, device=dev)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
+    cur = {"ctx": ctx}
 
     def timed(fn, steps, warm):
         """Device time of each step (CUDA events on the launching stream, L2
@@ -231,30 +240,38 @@ def run_ours(a):
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
             f = ctypes.c_float()
-            if L.g2_pass_time_ms(ctx.handle, 0, ctypes.byref(f)) == 0:
+            if L.g2_pass_time_ms(cur["ctx"].handle, 0, ctypes.byref(f)) == 0:
                 pass_ms.append(f.value)
         return ms, pass_ms
 
-    def work_of(fn):
-        fn(2)
+    def work_of(c):
         wb = ctypes.c_uint64()
-        g2aimd._lib.check(L.g2_last_work_bytes(ctx.handle, ctypes.byref(wb)), "work")
+        g2aimd._lib.check(L.g2_last_work_bytes(c.handle, ctypes.byref(wb)), "work")
         return wb.value
 
-    # ---- headline: 4-clique count over every root, heuristic schedule
+    def count():
+        torch.cuda.synchronize(dev)
+        return int(out[0].item())
+
+    # ---- 4-clique count over every root (preset 24 plan)
     ctx.set_plan(Plan.preset(K4))
-
-    def k4_step(flags=1):
-        ctx.match_device(out.data_ptr(), stream=sptr, schedule="heuristic", flags=flags)
-
-    work_bytes = work_of(k4_step)
-    torch.cuda.synchronize(dev)
-    k4 = int(out[0].item())
+    run = lambda **kw: ctx.match_device(out.data_ptr(), stream=sptr, **kw)  # noqa: E731
+    run(schedule="heuristic", flags=2)  # work-model build (schedule-independent), untimed
+    work_bytes = work_of(ctx)
+    k4 = count()
+    # plain schedule: heuristic order, one task per root (no model, no splits)
+    plain_ms, _ = timed(lambda: run(schedule="heuristic", flags=1), a.steps, a.warmup)
+    # learned schedule: autotuned launch/split parameters (untimed search)
+    tuned, _, tlog = tune(lambda **kw: run(schedule="learned", flags=1, **kw),
+                          {"granularity": 4, "warps_per_block": 8, "chunk": 4}, DEFAULT_SPACE)
+    step = lambda: run(schedule="learned", flags=1, **tuned)  # noqa: E731
+    step()
+    assert count() == k4
     if dist:
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
     with Clocks(local) as clk:
-        ms, pass_ms = timed(k4_step, a.steps, a.warmup)
+        ms, pass_ms = timed(step, a.steps, a.warmup)
     launches_per_step = ctx.launches()
     if dist:
         torch.distributed.barrier()
@@ -270,16 +287,21 @@ def run_ours(a):
         step_ms_all, total = step_ms, float(k4)
     value = total / (step_ms_all / 1000.0)
     kern_ms = float(np.mean(pass_ms)) if pass_ms else None
-    extras, e2e, cpu = {}, None, None
+    plain = float(np.mean(plain_ms))
+    extras = {"schedules": {
+        "plain_heuristic_ms": plain, "learned_ms": step_ms, "learned_vs_plain": plain / step_ms,
+        "tuned": tuned, "tuning_log": [[c, round(t, 3)] for c, t in tlog]}}
+    e2e, cpu = None, None
     if not a.no_extras:
-        # ---- plain (given) order for comparison, triangles on the same graph
-        ms_given, _ = timed(lambda: ctx.match_device(out.data_ptr(), stream=sptr, flags=1), 3, 1)
-        extras["k4_given_order_ms"] = float(np.mean(ms_given))
+        hs, _ = timed(lambda: run(schedule="heuristic", split=True, flags=1, **tuned), 3, 1)
+        extras["schedules"]["heuristic_split_ms"] = float(np.mean(hs))
+        gs, _ = timed(lambda: run(flags=1), 3, 1)
+        extras["schedules"]["given_order_ms"] = float(np.mean(gs))
+        # ---- triangles on the same graph (heuristic splits)
         ctx.set_plan(Plan.preset(0))
-        tri_step = lambda: ctx.match_device(out.data_ptr(), stream=sptr, schedule="heuristic", flags=1)  # noqa
+        tri_step = lambda: run(schedule="heuristic", split=True, flags=1, **tuned)  # noqa: E731
         tri_step()
-        torch.cuda.synchronize(dev)
-        tri = int(out[0].item())
+        tri = count()
         tms, _ = timed(tri_step, 3, 1)
         extras["triangle"] = {"count": tri, "ms_per_step": float(np.mean(tms)),
                               "per_s": tri / (float(np.mean(tms)) / 1000.0)}
@@ -289,22 +311,26 @@ def run_ours(a):
         cci = torch.from_numpy(cl.cols.view(np.int32)).to(dev)
         mctx = Context(local)
         mctx.load_device(crp.data_ptr(), cci.data_ptr(), cl.n, cl.m)
-        mstep = lambda f=1: mctx.mce_device(out.data_ptr(), HIST, stream=sptr, schedule="heuristic", flags=f)  # noqa
-        mstep(2)
-        wb = ctypes.c_uint64()
-        g2aimd._lib.check(L.g2_last_work_bytes(mctx.handle, ctypes.byref(wb)), "work")
-        torch.cuda.synchronize(dev)
-        cliques = int(out[0].item())
-        saved = ctx
-        ctx = mctx
-        mms, mpass = timed(mstep, 3, 1)
-        ctx = saved
+        mctx.load_core(cl.core)
+        mctx.set_model(CostModel.load(os.path.join(models, "mce.npz")))
+        mrun = lambda **kw: mctx.mce_device(out.data_ptr(), HIST, stream=sptr, **kw)  # noqa: E731
+        mrun(schedule="heuristic", flags=2)
+        mwork = work_of(mctx)
+        cliques = count()
+        cur["ctx"] = mctx
+        mplain, _ = timed(lambda: mrun(schedule="heuristic", flags=1), 3, 1)
+        mtuned, _, _ = tune(lambda **kw: mrun(schedule="learned", flags=1, **kw),
+                            {"granularity": 4, "warps_per_block": 8, "chunk": 2}, DEFAULT_SPACE)
+        mms, mpass = timed(lambda: mrun(schedule="learned", flags=1, **mtuned), 3, 1)
+        assert count() == cliques
+        cur["ctx"] = ctx
         mk = float(np.mean(mpass)) if mpass else None
         extras["mce_chung_lu"] = {
             "graph": {"n": cl.n, "m": cl.m, "gamma": 2.3, "avg_degree": 16},
-            "maximal_cliques": cliques, "ms_per_step": float(np.mean(mms)),
-            "per_s": cliques / (float(np.mean(mms)) / 1000.0), "kernel_ms": mk,
-            "work_bytes": wb.value, "achieved_gbs": wb.value / (mk / 1000.0) / 1e9 if mk else None}
+            "maximal_cliques": cliques, "plain_heuristic_ms": float(np.mean(mplain)),
+            "learned_ms": float(np.mean(mms)), "learned_vs_plain": float(np.mean(mplain)) / float(np.mean(mms)),
+            "tuned": mtuned, "per_s": cliques / (float(np.mean(mms)) / 1000.0), "kernel_ms": mk,
+            "work_bytes": mwork, "achieved_gbs": mwork / (mk / 1000.0) / 1e9 if mk else None}
         if rank == 0 and world == 1:
             cs = cpu_sample(cl, a.cpu_sample_s / 2, os.cpu_count() or 1, what="mce")
             extras["mce_chung_lu"]["cpu_port_per_s"] = cs["value"]
@@ -312,21 +338,29 @@ def run_ours(a):
         # ---- end to end through the host ABI with pinned host buffers
         prp = torch.from_numpy(g.row_ptrs.view(np.int64)).pin_memory()
         pci = torch.from_numpy(g.cols.view(np.int32)).pin_memory()
+        pcore = torch.from_numpy(g.core.view(np.int32)).pin_memory()
         pg = g2aimd.Graph(prp.numpy().view(np.uint64), pci.numpy().view(np.uint32))
+        core_h = pcore.numpy().view(np.uint32)
         e2c = Context(local)
+        e2c.set_model(CostModel.load(os.path.join(models, "k4.npz")))
         plan = Plan.preset(K4)
-        for _ in range(a.warmup):
+
+        def e2e_step():
             e2c.load(pg)
-            e2c.match(plan, schedule="heuristic")
+            e2c.load_core(core_h)
+            return e2c.match(plan, schedule="learned", **tuned)
+
+        for _ in range(a.warmup):
+            e2e_step()
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         for _ in range(a.steps):
-            e2c.load(pg)
-            c2 = e2c.match(plan, schedule="heuristic")
+            c2 = e2e_step()
         e2e_s = (time.perf_counter() - t0) / a.steps
         assert c2 == k4, (c2, k4)
         e2c.close()
-        e2e = {"value": k4 / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(g.row_ptrs.nbytes + g.cols.nbytes),
+        e2e = {"value": k4 / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(g.row_ptrs.nbytes + g.cols.nbytes + g.core.nbytes),
                "d2h_bytes_per_step": 8}
         if rank == 0 and world == 1:
             cs = cpu_sample(g, a.cpu_sample_s, os.cpu_count() or 1)
@@ -341,7 +375,8 @@ def run_ours(a):
             "warmup": a.warmup, "ms_per_step": step_ms_all, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": f"rmat-s{a.scale}-ef{a.edge_factor} (a=.57,b=c=.19) degeneracy-ordered: "
-                                   "4-clique count (preset 24 plan) over all roots, heuristic schedule",
+                                   "4-clique count (preset 24 plan) over all roots, learned schedule "
+                                   "(cost-model order + heavy-root splits, autotuned launch parameters)",
                        "graph": {"n": g.n, "m": g.m, "seed": a.seed, "gen_s": round(gen_s, 2)},
                        "k4_matches": k4, "l2": "512 MiB flush before every timed step",
                        "parallelism": f"dp{world} (one graph instance per rank)"},

@@ -172,12 +172,12 @@ __global__ void cost_keys_kernel(const float *cost, uint64_t n, uint64_t *keys) 
         keys[i] = ((uint64_t)(~float_key(cost[i])) << 32) | (uint32_t)i;
 }
 
-// Tasks per root: ceil(cost / target) in 1..64, target = total * share.
+// Tasks per root: ceil(cost / target) in 1..256, target = total * share.
 __global__ void split_count_kernel(const float *cost, const float *total, uint64_t n, float share, uint32_t *S) {
     const float target = fmaxf(*total * share, 1.f);
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const float k = ceilf(cost[i] / target);
-        S[i] = (uint32_t)fminf(fmaxf(k, 1.f), 64.f);
+        S[i] = (uint32_t)fminf(fmaxf(k, 1.f), 256.f);
     }
 }
 
@@ -259,8 +259,9 @@ int prepare_tasks(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, bool on_d
     if (sched == G2_SCHED_LEARNED && !ctx->d_model) return G2_ERR_INVALID;
     const bool split = nsrc > 0 && (sched == G2_SCHED_HEURISTIC || sched == G2_SCHED_LEARNED) &&
                        ((flags & G2_FLAG_SPLIT) || (sched == G2_SCHED_LEARNED && !(flags & G2_FLAG_NO_SPLIT)));
-    // sum_i ceil(c_i / t) <= n + total / t = n + 4 * warps
-    const uint64_t cap = split ? nsrc + 4 * nwarps + 64 : nsrc;
+    // sum_i ceil(c_i / t) <= n + total / t = n + g * warps
+    const uint32_t gran = (o && o->split_granularity) ? std::min<uint32_t>(o->split_granularity, 1024u) : 4u;
+    const uint64_t cap = split ? nsrc + (uint64_t)gran * nwarps + 64 : nsrc;
     uint64_t tc = ctx->tasks_cap;
     int rc = grow(ctx, ctx->d_tasks, tc, cap, "tasks");
     if (rc) return rc;
@@ -328,7 +329,7 @@ int prepare_tasks(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, bool on_d
     if (rc) return rc;
     uint32_t *S = ctx->d_S, *off = ctx->d_S + nsrc;
     split_count_kernel<<<ctx->sm_count * 4, 256, 0, st>>>(ctx->d_cost, ctx->d_total, nsrc,
-                                                         1.f / (4.f * (float)nwarps), S);
+                                                         1.f / ((float)gran * (float)nwarps), S);
     size_t need = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, need, S, off, (int)nsrc, st);
     rc = cub_space(ctx, need);
@@ -475,7 +476,7 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
         a.ntasks = k == 0 ? tl.cap : 0;
         a.ntasks_dev = k == 0 ? (tl.split ? ctx->d_ntask : nullptr) : ctx->d_ctr + 4 + (k - 1);
         a.head = ctx->d_ctr + k;
-        a.chunk = k == 0 ? 2 : 1;
+        a.chunk = k == 0 ? ((o && o->chunk) ? o->chunk : 2u) : 1u;
         a.hist_len = hist_len;
         a.scratch = ctx->d_scratch;
         uint64_t nw = (uint64_t)passes[k].blocks * passes[k].wpb;
@@ -529,7 +530,7 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
     a.ntasks = tl.cap;
     a.ntasks_dev = tl.split ? ctx->d_ntask : nullptr;
     a.head = ctx->d_ctr;
-    a.chunk = 4;
+    a.chunk = (o && o->chunk) ? o->chunk : 4u;
     a.scratch = ctx->d_scratch;
     a.words_per_warp = (ctx->scratch_words / ((uint64_t)blocks * wpb)) & ~63ull;
     if (a.words_per_warp / (ctx->plan.k > 2 ? ctx->plan.k - 2 : 1) < 64) return G2_ERR_OVERFLOW;

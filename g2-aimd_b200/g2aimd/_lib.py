@@ -35,10 +35,10 @@ class G2Plan(C.Structure):
 class G2Opts(C.Structure):
     _fields_ = [
         ("blocks", u32), ("warps_per_block", u32), ("schedule", u32),
-        ("split_threshold", u32), ("scores", P(C.c_float)),
+        ("split_granularity", u32), ("scores", P(C.c_float)),
         ("root_nodes", P(u64)), ("work_bytes", P(u64)),
         ("intersect_mode", u32), ("flags", u32), ("reserved0", u32), ("root_cost", P(u64)),
-        ("reserved", u32 * 2),
+        ("chunk", u32), ("reserved1", u32),
     ]
 
 

@@ -75,13 +75,14 @@ class Plan:
 
 
 def _opts(warps_per_block=0, blocks=0, schedule="given", scores=None, root_nodes=None, intersect_mode=0,
-          split_threshold=0, flags=0, work_bytes=None, root_cost=None, split=False):
+          granularity=0, chunk=0, flags=0, work_bytes=None, root_cost=None, split=False):
     o = G2Opts()
     o.flags = flags | (FLAG_SPLIT if split else 0)
+    o.chunk = chunk
     o.warps_per_block = warps_per_block
     o.blocks = blocks
     o.schedule = SCHED[schedule]
-    o.split_threshold = split_threshold
+    o.split_granularity = granularity
     o.intersect_mode = intersect_mode
     keep = []
     if scores is not None:

@@ -106,8 +106,8 @@ typedef struct g2_opts {
     uint32_t blocks;            /* persistent CTAs (default: 148 x occupancy)       */
     uint32_t warps_per_block;   /* default 8                                        */
     uint32_t schedule;          /* G2_SCHED_*                                       */
-    uint32_t split_threshold;   /* MCE: split roots whose |P0| exceeds this into one
-                                   task per branch (0 = default, ~0u = never)      */
+    uint32_t split_granularity; /* heavy-root splits aim at tasks of cost
+                                   total / (granularity x warps) (0 = 4)           */
     const float *scores;        /* host, nsrc entries, for G2_SCHED_SCORES          */
     uint64_t *root_nodes;       /* optional host out: search-tree nodes per source
                                    (MCE) or embeddings per source (match), summed
@@ -119,7 +119,8 @@ typedef struct g2_opts {
     uint32_t reserved0;
     uint64_t *root_cost;        /* optional host out: SM cycles per source (summed
                                    over its split tasks)                            */
-    uint32_t reserved[2];
+    uint32_t chunk;             /* tasks taken per queue atomic (0 = 2 MCE, 4 match) */
+    uint32_t reserved1;
 } g2_opts;
 
 /* g2_opts.flags */
@@ -127,8 +128,9 @@ typedef struct g2_opts {
 #define G2_FLAG_WORK_MODEL 2u    /* count the work model W on the device (slower)    */
 #define G2_FLAG_SPLIT 4u         /* split heavy roots by the schedule's cost estimate:
                                     a root of estimated cost c becomes ceil(c / t)
-                                    tasks (at most 64), t = total / (4 x warps); each
-                                    task owns every k-th top-level branch            */
+                                    tasks (at most 256), t = total / (g x warps) with
+                                    g = split_granularity; each task owns every k-th
+                                    top-level branch of its root                     */
 #define G2_FLAG_NO_SPLIT 8u      /* G2_SCHED_LEARNED without splitting               */
 
 typedef struct g2_ctx g2_ctx;
