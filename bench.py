@@ -42,6 +42,9 @@ METRIC = "maximal cliques/s and 4-clique matches/s on 1 B200, learned vs plain s
 UNIT = "4-clique matches/s"
 HIST = 256
 K4 = 24
+# DRAM bytes (read + write) of one main-pass launch of the headline kernel on the
+# default graph, from the ncu capture summarised in profiles/ (null until captured).
+TRAFFIC_K4_S20 = None
 
 
 def parse():
@@ -56,6 +59,8 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=12.0, help="target seconds of CPU baseline work")
     ap.add_argument("--no-extras", action="store_true", help="skip triangle / MCE / e2e / CPU legs")
     ap.add_argument("--scratch-mb", type=int, default=4096, help="device scratch for the DFS slabs")
+    ap.add_argument("--fixed", action="store_true",
+                    help="skip the plain-schedule timing and the autotuner (profiling runs)")
     return ap.parse_args()
 
 
@@ -259,11 +264,14 @@ def run_ours(a):
     run(schedule="heuristic", flags=2)  # work-model build (schedule-independent), untimed
     work_bytes = work_of(ctx)
     k4 = count()
-    # plain schedule: heuristic order, one task per root (no model, no splits)
-    plain_ms, _ = timed(lambda: run(schedule="heuristic", flags=1), a.steps, a.warmup)
-    # learned schedule: autotuned launch/split parameters (untimed search)
-    tuned, _, tlog = tune(lambda **kw: run(schedule="learned", flags=1, **kw),
-                          {"granularity": 4, "warps_per_block": 8, "chunk": 4}, DEFAULT_SPACE)
+    if a.fixed:
+        plain_ms, tuned, tlog = [float("nan")], {"granularity": 4, "warps_per_block": 8, "chunk": 1}, []
+    else:
+        # plain schedule: heuristic order, one task per root (no model, no splits)
+        plain_ms, _ = timed(lambda: run(schedule="heuristic", flags=1), a.steps, a.warmup)
+        # learned schedule: autotuned launch/split parameters (untimed search)
+        tuned, _, tlog = tune(lambda **kw: run(schedule="learned", flags=1, **kw),
+                              {"granularity": 4, "warps_per_block": 8, "chunk": 4}, DEFAULT_SPACE)
     step = lambda: run(schedule="learned", flags=1, **tuned)  # noqa: E731
     step()
     assert count() == k4
@@ -325,12 +333,14 @@ def run_ours(a):
         assert count() == cliques
         cur["ctx"] = ctx
         mk = float(np.mean(mpass)) if mpass else None
+        mstream = cl.mce_stream_bytes()
         extras["mce_chung_lu"] = {
             "graph": {"n": cl.n, "m": cl.m, "gamma": 2.3, "avg_degree": 16},
+            "stream_bytes": mstream, "stream_gbs": mstream / (mk / 1000.0) / 1e9 if mk else None,
             "maximal_cliques": cliques, "plain_heuristic_ms": float(np.mean(mplain)),
             "learned_ms": float(np.mean(mms)), "learned_vs_plain": float(np.mean(mplain)) / float(np.mean(mms)),
             "tuned": mtuned, "per_s": cliques / (float(np.mean(mms)) / 1000.0), "kernel_ms": mk,
-            "work_bytes": mwork, "achieved_gbs": mwork / (mk / 1000.0) / 1e9 if mk else None}
+            "merge_model_bytes": mwork, "merge_model_gbs": mwork / (mk / 1000.0) / 1e9 if mk else None}
         if rank == 0 and world == 1:
             cs = cpu_sample(cl, a.cpu_sample_s / 2, os.cpu_count() or 1, what="mce")
             extras["mce_chung_lu"]["cpu_port_per_s"] = cs["value"]
@@ -368,7 +378,8 @@ def run_ours(a):
                    "sample": f"{cs['roots']} random roots of the same graph, {cs['seconds']:.1f} s, plan-driven "
                              "enumeration with the reference planner's plan (oracle/g2_oracle.c)"}
     peak, peak_kind = measured_peak()
-    achieved = work_bytes / (kern_ms / 1000.0) / 1e9 if kern_ms else None
+    stream_bytes = g.clique_stream_bytes(4)
+    achieved = stream_bytes / (kern_ms / 1000.0) / 1e9 if kern_ms else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -381,9 +392,11 @@ def run_ours(a):
                        "k4_matches": k4, "l2": "512 MiB flush before every timed step",
                        "parallelism": f"dp{world} (one graph instance per rank)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
-                         "kernel": "match_kernel<1> (clique bitmap path)", "kernel_ms": kern_ms,
-                         "algorithmic_bytes": work_bytes, "peak_kind": peak_kind},
+                         "frac": (achieved / peak) if achieved else None, "traffic": TRAFFIC_K4_S20,
+                         "kernel": "match_kernel<1,0> (clique bitmap path), main pass", "kernel_ms": kern_ms,
+                         "algorithmic_bytes": stream_bytes, "peak_kind": peak_kind,
+                         "merge_model_bytes": work_bytes,
+                         "merge_model_gbs": work_bytes / (kern_ms / 1000.0) / 1e9 if kern_ms else None},
             "clocks": clk.summary(), "gpu_launches": int(launches_per_step * a.steps),
             "e2e": e2e, "cpu_baseline": cpu, "extras": extras,
         }

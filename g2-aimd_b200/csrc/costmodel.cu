@@ -356,7 +356,8 @@ __global__ void adam_kernel(float *params, float *mom, float *vel, const float *
 // Features + MLP of every root in one kernel (the inference fused into task
 // generation).  pred[i] (optional) = normalised log-cost of root src[i];
 // cost[i] (optional) = decoded cost (>= 1); *total (optional) += sum of costs.
-// With X given, the features are read from X (n x 8) instead.
+// With X given, the features are read from X instead: row src[i] (per-vertex
+// features cached for the loaded graph) or row i when src is null.
 __global__ void __launch_bounds__(128) score_kernel(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo,
                                                     const uint32_t *core, const uint32_t *src, uint64_t n,
                                                     const float *X, const float *params, const float *norm,
@@ -374,8 +375,10 @@ __global__ void __launch_bounds__(128) score_kernel(const uint64_t *rp, const ui
             const uint64_t i = base + lane;
             if (i < n) {
                 float f[F];
-                if (X)
-                    for (int k = 0; k < F; k++) f[k] = X[i * F + k];
+                if (X) {  // precomputed features, rows indexed by vertex when src is given
+                    const uint64_t row = src ? (uint64_t)src[i] : i;
+                    for (int k = 0; k < F; k++) f[k] = X[row * F + k];
+                }
                 else
                     root_features(rp, ci, fo, core, src ? src[i] : (uint32_t)i, f);
                 normalise_row(m, f, t.x[lane]);

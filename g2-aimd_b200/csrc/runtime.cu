@@ -66,6 +66,9 @@ struct g2_ctx {
     uint64_t last_cap = 0;    // tasks buffer entries used by the last run
     // learned cost model: params (G2_MODEL_PARAMS) followed by norm (G2_MODEL_NORM)
     float *d_model = nullptr;
+    float *d_feat = nullptr;  // per-vertex features of the loaded graph (n x 8), cached
+    uint64_t feat_cap = 0;
+    bool feat_valid = false;
     // plan
     g2::DevPlan plan{};
     bool has_plan = false;
@@ -301,7 +304,19 @@ int prepare_tasks(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, bool on_d
                                                                 ctx->d_total);
         ctx->launches++;
     } else if (sched == G2_SCHED_LEARNED) {
-        cudaError_t e = g2::score_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, ctx->d_core, roots, nsrc, nullptr,
+        // features depend on the graph only: computed once per loaded graph (and
+        // core numbers), then every run is MLP inference over the task list
+        if (!ctx->feat_valid) {
+            rc = grow(ctx, ctx->d_feat, ctx->feat_cap, (uint64_t)G2_MODEL_FEATURES * std::max<uint64_t>(ctx->n, 1),
+                      "features");
+            if (rc) return rc;
+            cudaError_t e = g2::features_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, ctx->d_core, nullptr, ctx->n,
+                                                ctx->d_feat, ctx->sm_count, st);
+            if (e != cudaSuccess) return fail_cuda(ctx, e, "features_launch");
+            ctx->launches++;
+            ctx->feat_valid = true;
+        }
+        cudaError_t e = g2::score_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, ctx->d_core, roots, nsrc, ctx->d_feat,
                                          ctx->d_model, ctx->d_model + G2_MODEL_PARAMS, nullptr, ctx->d_cost,
                                          ctx->d_total, ctx->sm_count, st);
         if (e != cudaSuccess) return fail_cuda(ctx, e, "score_launch");
@@ -631,7 +646,8 @@ int g2_close(g2_ctx *ctx) {
     void *bufs[] = {ctx->d_fo,     ctx->d_core,    ctx->d_scratch, ctx->d_tasks,  ctx->d_defer,      ctx->d_root_nodes,
                     ctx->d_root_cost, ctx->d_ctr,  ctx->d_status,  ctx->d_out,    ctx->d_keys,       ctx->d_keys2,
                     ctx->d_roots,  ctx->d_S,       ctx->d_part,    ctx->d_xroots, ctx->d_xparts,     ctx->d_cost,
-                    ctx->d_total,  ctx->d_ntask,   ctx->d_cub,     ctx->d_model,  ctx->d_work};
+                    ctx->d_total,  ctx->d_ntask,   ctx->d_cub,     ctx->d_model,  ctx->d_work,
+                    ctx->d_feat};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (auto &e : ctx->ev)
@@ -643,6 +659,7 @@ int g2_close(g2_ctx *ctx) {
 static int after_load(g2_ctx *ctx) {
     int rc = grow(ctx, ctx->d_fo, ctx->fo_cap, std::max<uint64_t>(ctx->n, 1), "forward offsets");
     if (rc) return rc;
+    ctx->feat_valid = false;
     if (ctx->d_core) {  // core numbers belong to the previous graph
         cudaFree(ctx->d_core);
         ctx->d_core = nullptr;
@@ -702,6 +719,7 @@ int g2_load_core(g2_ctx *ctx, const uint32_t *core) {
     G2_TRY(cudaSetDevice(ctx->device));
     int rc = grow(ctx, ctx->d_core, ctx->core_cap, std::max<uint64_t>(ctx->n, 1), "core");
     if (rc) return rc;
+    ctx->feat_valid = false;
     if (ctx->n) G2_TRY(cudaMemcpy(ctx->d_core, core, sizeof(uint32_t) * ctx->n, cudaMemcpyHostToDevice));
     return G2_OK;
 }
@@ -992,6 +1010,30 @@ int g2_model_train(g2_ctx *ctx, const float *X, const float *cost, uint64_t n, u
         }
     }
     G2_TRY(cudaMemcpy(params, b.params, sizeof(float) * G2_MODEL_PARAMS, cudaMemcpyDeviceToHost));
+    // Calibration of the decoded cost: a least-squares fit in log space shrinks
+    // the spread of its predictions, which shrinks exactly the heavy roots that
+    // splitting must see.  Rescale the decode so that the predictions on the
+    // training set have the targets' mean and spread (variance matching).
+    {
+        float *d_pred = nullptr;
+        G2_TRY(cudaMalloc(&d_pred, sizeof(float) * n));
+        cudaError_t e = g2::score_launch(nullptr, nullptr, nullptr, nullptr, nullptr, n, b.X, b.params, b.norm,
+                                         d_pred, nullptr, nullptr, ctx->sm_count, 0);
+        std::vector<float> pred(n);
+        if (e == cudaSuccess) e = cudaMemcpy(pred.data(), d_pred, sizeof(float) * n, cudaMemcpyDeviceToHost);
+        cudaFree(d_pred);
+        if (e != cudaSuccess) return fail_cuda(ctx, e, "calibration");
+        double pm = 0.0, pv = 0.0;
+        for (float p : pred) pm += p;
+        pm /= (double)n;
+        for (float p : pred) pv += (p - pm) * (p - pm);
+        const double ps = std::sqrt(pv / (double)n);
+        if (ps > 1e-3) {  // decode(y) = y * ystd' + ymean' with (y - pm) / ps rescaled to unit spread
+            const double ystd = norm[2 * F + 1], ymean = norm[2 * F];
+            norm[2 * F + 1] = (float)(ystd / ps);
+            norm[2 * F] = (float)(ymean - pm * ystd / ps);
+        }
+    }
     return G2_OK;
 }
 

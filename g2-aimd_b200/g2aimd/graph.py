@@ -132,3 +132,33 @@ class Graph:
         g.core = np.zeros(self.n, np.uint32)
         g.core[perm] = core
         return g
+
+    # ------------------------------------------------ stream-byte models
+    def _forward_degrees(self):
+        rp = self.row_ptrs.astype(np.int64)
+        src = np.repeat(np.arange(self.n, dtype=np.int64), np.diff(rp))
+        fwd = self.cols.astype(np.int64) > src
+        p = np.bincount(src[fwd], minlength=self.n).astype(np.int64)
+        return src, fwd, p
+
+    def clique_stream_bytes(self, k):
+        """Bytes of the CSR the bitmap clique path must read once per root:
+        the root's offsets and forward list, and for each forward neighbour its
+        offsets and forward list (an upper bound: scans stop at the largest
+        member of the root's forward list).  Roots with fewer than k-1 forward
+        neighbours read their offsets only."""
+        src, fwd, p = self._forward_degrees()
+        s = np.bincount(src[fwd], weights=p[self.cols[fwd].astype(np.int64)], minlength=self.n)
+        per = np.where(p >= k - 1, 20 + 24 * p + 4 * s, 20)
+        return int(per.sum())
+
+    def mce_stream_bytes(self):
+        """Bytes of the CSR the MCE kernel must read once per root: offsets and
+        neighbour list of the root, and offsets + forward list of every
+        neighbour (rows of P0 and of the back neighbours)."""
+        src, fwd, p = self._forward_degrees()
+        deg = np.diff(self.row_ptrs.astype(np.int64))
+        s = np.bincount(src, weights=p[self.cols.astype(np.int64)], minlength=self.n)
+        per = np.where(p > 0, 20 + 24 * deg + 4 * s, 20)
+        return int(per.sum())
+

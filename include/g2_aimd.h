@@ -252,7 +252,10 @@ int g2_load_core(g2_ctx *ctx, const uint32_t *core);
 int g2_root_features(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, float *out);
 /* Train on (X, cost): computes norm, initialises params from seed (He uniform)
  * and runs `epochs` of mini-batch Adam on the device.  epoch_loss (optional,
- * epochs entries) receives the mean squared error in normalised units. */
+ * epochs entries) receives the mean squared error in normalised units.  The
+ * target mean/std in norm are then recalibrated so that the decoded training
+ * predictions have the targets' mean and spread in log space (the fit shrinks
+ * the spread, and with it the heavy roots that splitting must see). */
 int g2_model_train(g2_ctx *ctx, const float *X, const float *cost, uint64_t n, uint32_t epochs,
                    uint32_t batch, float lr, uint64_t seed, float *params, float *norm,
                    float *epoch_loss);
