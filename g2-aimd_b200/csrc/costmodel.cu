@@ -77,12 +77,52 @@ __device__ void root_features(const uint64_t *rp, const uint32_t *ci, const uint
     f[7] = log1pf(imax);
 }
 
+// One warp per root: lanes share the wedge sum and each sampled intersection
+// (integer sums, so the result equals root_features() exactly).
 __global__ void features_kernel(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, const uint32_t *core,
                                 const uint32_t *src, uint64_t n, float *out) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        float f[F];
-        root_features(rp, ci, fo, core, src ? src[i] : (uint32_t)i, f);
-        for (int k = 0; k < F; k++) out[i * F + k] = f[k];
+    const uint32_t lane = lane_id();
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = warp; i < n; i += nwarps) {
+        const uint32_t v = src ? src[i] : (uint32_t)i;
+        const uint64_t lo = rp[v], hi = rp[v + 1];
+        const uint64_t s = lo + fo[v];
+        const uint32_t p = (uint32_t)(hi - s), nx = (uint32_t)(s - lo);
+        unsigned long long wedge = 0;
+        for (uint32_t j = lane; j < p; j += 32) {
+            const uint32_t u = ci[s + j];
+            wedge += rp[u + 1] - rp[u] - fo[u];
+        }
+        wedge = warp_sum_u64(wedge);
+        const uint32_t ns = p < 4 ? p : 4;
+        const uint32_t pmax = p ? ci[hi - 1] : 0u;
+        uint32_t isum = 0, imax = 0;
+        for (uint32_t j = 0; j < ns; j++) {
+            const uint32_t u = ci[s + (uint64_t)j * p / ns];
+            const uint64_t us = rp[u] + fo[u], ue = rp[u + 1];
+            uint32_t c = 0;
+            for (uint64_t e = us + lane; e < ue; e += 32) {  // |N+(u) ∩ N+(v)|
+                const uint32_t y = ci[e];
+                if (y > pmax) break;
+                c += contains(ci, s, hi, y);
+            }
+            c = (uint32_t)warp_sum_u64(c);
+            isum += c;
+            imax = c > imax ? c : imax;
+        }
+        if (lane == 0) {
+            const float imean = ns ? (float)isum / (float)ns : 0.f;
+            float *f = out + i * F;
+            f[0] = log1pf((float)(hi - lo));
+            f[1] = log1pf((float)(core ? core[v] : p));
+            f[2] = log1pf((float)p);
+            f[3] = log1pf((float)nx);
+            f[4] = log1pf((float)wedge);
+            f[5] = log1pf(imean);
+            f[6] = p ? imean / (float)p : 0.f;
+            f[7] = log1pf((float)imax);
+        }
     }
 }
 
@@ -411,7 +451,7 @@ size_t model_smem_bytes() { return sizeof(SharedModel) + 4 * sizeof(WarpTile); }
 
 cudaError_t features_launch(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, const uint32_t *core,
                             const uint32_t *src, uint64_t n, float *out, int sms, cudaStream_t st) {
-    features_kernel<<<sms * 8, 128, 0, st>>>(rp, ci, fo, core, src, n, out);
+    features_kernel<<<sms * 16, 256, 0, st>>>(rp, ci, fo, core, src, n, out);
     return cudaGetLastError();
 }
 

@@ -169,6 +169,46 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
     return count;
 }
 
+// Bits of word w of the mask {j : j > x}.
+__device__ __forceinline__ uint32_t above(uint32_t x, uint32_t w) {
+    const uint32_t xw = x >> 5;
+    return w > xw ? G2_FULL : w < xw ? 0u : ~((2u << (x & 31u)) - 1u);
+}
+
+// Number of (k-1)-cliques of the local graph rows A (p rows x W words) with
+// increasing indices, k = 3, 4 or 5, summed over the warp.  Lane l owns the
+// first indices x = l, l+32, ... with x % nparts == part.
+__device__ unsigned long long clique_count_lanes(const uint32_t *A, uint32_t p, uint32_t W, uint32_t k,
+                                                 uint32_t part, uint32_t nparts) {
+    unsigned long long c = 0;
+    for (uint32_t x = lane_id(); x < p; x += 32) {
+        if (nparts > 1 && x % nparts != part) continue;
+        const uint32_t *ax = A + (uint64_t)x * W;
+        if (k == 3) {
+            for (uint32_t w = x >> 5; w < W; w++) c += __popc(ax[w] & above(x, w));
+            continue;
+        }
+        for (uint32_t w = x >> 5; w < W; w++) {
+            for (uint32_t m = ax[w] & above(x, w); m; m &= m - 1) {
+                const uint32_t y = (w << 5) + (uint32_t)(__ffs(m) - 1);
+                const uint32_t *ay = A + (uint64_t)y * W;
+                if (k == 4) {
+                    for (uint32_t w2 = y >> 5; w2 < W; w2++) c += __popc(ax[w2] & ay[w2] & above(y, w2));
+                    continue;
+                }
+                for (uint32_t w2 = y >> 5; w2 < W; w2++) {
+                    for (uint32_t m2 = ax[w2] & ay[w2] & above(y, w2); m2; m2 &= m2 - 1) {
+                        const uint32_t z = (w2 << 5) + (uint32_t)(__ffs(m2) - 1);
+                        const uint32_t *az = A + (uint64_t)z * W;
+                        for (uint32_t w3 = z >> 5; w3 < W; w3++) c += __popc(ax[w3] & ay[w3] & az[w3] & above(z, w3));
+                    }
+                }
+            }
+        }
+    }
+    return warp_sum_u64(c);
+}
+
 // Clique plans on P0 bitmaps.  Returns false if the root does not fit (caller
 // falls back to the generic walk).
 template <int WPL, bool METRICS>
@@ -205,6 +245,13 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
     __syncwarp();
     build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf);
     __syncwarp();
+    if (!METRICS && k <= 5) {
+        // lane-parallel counting: lane takes the depth-1 vertices x = lane, lane+32, ...
+        // (in ordinal order, so the split filter is x % nparts) and counts the
+        // (k-2)-cliques above x in its row serially; no warp traffic per pair.
+        count = clique_count_lanes(S + a0, p, W, k, part, nparts);
+        return true;
+    }
     // C = remaining candidates at the current depth; depth = vertices chosen (v included)
     Row<WPL> C;
 #pragma unroll
