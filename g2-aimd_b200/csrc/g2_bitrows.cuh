@@ -94,11 +94,18 @@ constexpr uint32_t kLongList = 96;  // forward lists longer than this are scanne
 // Upper parts come from forward lists (P0[j] ∈ N+(P0[i]) for j > i), one lane
 // per row (the warp together for long lists); the lower parts are the
 // transpose, added 32x32 tile by tile.
+// With symmetric = false only the upper part of each row (words from i / 32
+// on, bits j > i) is built: enough for walks that only look above the row.
 __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo,
-                                   const uint32_t *p0s, uint32_t p, uint32_t W, uint32_t *A, uint32_t *rowbuf) {
+                                   const uint32_t *p0s, uint32_t p, uint32_t W, uint32_t *A, uint32_t *rowbuf,
+                                   bool symmetric = true) {
     const uint32_t lane = lane_id();
     const uint32_t pmax = p0s[p - 1];
-    for (uint64_t w = lane; w < (uint64_t)p * W; w += 32) A[w] = 0u;
+    if (symmetric)
+        for (uint64_t w = lane; w < (uint64_t)p * W; w += 32) A[w] = 0u;
+    else
+        for (uint32_t i = lane; i < p; i += 32)
+            for (uint32_t w = i >> 5; w < W; w++) A[(uint64_t)i * W + w] = 0u;
     __syncwarp();
     for (uint32_t i0 = 0; i0 < p; i0 += 32) {
         const uint32_t i = i0 + lane;
@@ -140,6 +147,7 @@ __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const
         }
     }
     __syncwarp();
+    if (!symmetric) return;
     // A |= A^T over upper tiles (tr <= tc)
     for (uint32_t tr = 0; tr < W; tr++) {
         for (uint32_t tc = tr; tc < W; tc++) {
@@ -151,6 +159,51 @@ __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const
             __syncwarp();
         }
     }
+}
+
+// Number of edges of the root's forward neighbourhood (triangles rooted at v)
+// with i % nparts == part for the lower end i, counted during the forward-list
+// scan without building rows.  Warp total.
+__device__ __noinline__ static unsigned long long count_forward_edges(const uint64_t *rp, const uint32_t *ci,
+                                                                      const uint32_t *fo, const uint32_t *p0s,
+                                                                      uint32_t p, uint32_t part, uint32_t nparts) {
+    const uint32_t lane = lane_id();
+    const uint32_t pmax = p0s[p - 1];
+    unsigned long long c = 0;
+    for (uint32_t i0 = 0; i0 < p; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        bool big = false;
+        if (i < p && (nparts <= 1 || i % nparts == part)) {
+            const uint32_t u = p0s[i];
+            uint64_t e = ldg(rp + u) + ldg(fo + u);
+            const uint64_t end = ldg(rp + u + 1);
+            if (end - e > kLongList) big = true;
+            else {
+                uint32_t j = i + 1;
+                for (; e < end; e++) {
+                    const uint32_t y = ldg(ci + e);
+                    if (y > pmax) break;
+                    j = smem_lower_bound(p0s, j, p, y);
+                    c += j < p && p0s[j] == y;
+                }
+            }
+        }
+        uint32_t bigmask = __ballot_sync(G2_FULL, big);
+        while (bigmask) {
+            const uint32_t l = __ffs(bigmask) - 1;
+            bigmask &= bigmask - 1;
+            const uint32_t ii = i0 + l;
+            const uint32_t u = p0s[ii];
+            const uint64_t e0 = ldg(rp + u) + ldg(fo + u), end = ldg(rp + u + 1);
+            for (uint64_t e = e0 + lane; e < end; e += 32) {
+                const uint32_t y = ldg(ci + e);
+                if (y > pmax) break;
+                const uint32_t j = smem_lower_bound(p0s, ii + 1, p, y);
+                c += j < p && p0s[j] == y;
+            }
+        }
+    }
+    return warp_sum_u64(c);
 }
 
 // B rows of the root's backward neighbours X0 = ci[lo, lo+nx) (ids < v):

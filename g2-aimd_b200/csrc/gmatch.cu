@@ -243,15 +243,21 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
     if (f0 + (uint64_t)k * (W + 1) > a.words_per_warp) return false;
     for (uint32_t i = lane; i < p; i += 32) p0s[i] = ldg(ci + split + i);
     __syncwarp();
-    build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf);
-    __syncwarp();
+    if (!METRICS && k == 3) {  // triangles: count forward-neighbourhood edges while scanning
+        count = count_forward_edges(rp, ci, a.fo, p0s, p, part, nparts);
+        return true;
+    }
     if (!METRICS && k <= 5) {
         // lane-parallel counting: lane takes the depth-1 vertices x = lane, lane+32, ...
         // (in ordinal order, so the split filter is x % nparts) and counts the
-        // (k-2)-cliques above x in its row serially; no warp traffic per pair.
+        // (k-2)-cliques above x serially; it reads only the upper part of rows.
+        build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf, false);
+        __syncwarp();
         count = clique_count_lanes(S + a0, p, W, k, part, nparts);
         return true;
     }
+    build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf);
+    __syncwarp();
     // C = remaining candidates at the current depth; depth = vertices chosen (v included)
     Row<WPL> C;
 #pragma unroll
