@@ -203,6 +203,8 @@ def run_ours(a):
 
     import g2aimd
     from g2aimd.autotune import DEFAULT_SPACE, tune
+    # learned schedule search: heavy-root splits on (flags 1) or off (1 | G2_FLAG_NO_SPLIT)
+    LEARNED_SPACE = dict({"flags": [1, 1 | 8]}, **DEFAULT_SPACE)
     from g2aimd.context import Context, CostModel, Plan
     world, rank, local = dist_env()
     dist = world > 1
@@ -265,14 +267,14 @@ def run_ours(a):
     work_bytes = work_of(ctx)
     k4 = count()
     if a.fixed:
-        plain_ms, tuned, tlog = [float("nan")], {"granularity": 4, "warps_per_block": 8, "chunk": 1}, []
+        plain_ms, tuned, tlog = [float("nan")], {"flags": 1, "granularity": 4, "warps_per_block": 8, "chunk": 1}, []
     else:
         # plain schedule: heuristic order, one task per root (no model, no splits)
         plain_ms, _ = timed(lambda: run(schedule="heuristic", flags=1), a.steps, a.warmup)
         # learned schedule: autotuned launch/split parameters (untimed search)
-        tuned, _, tlog = tune(lambda **kw: run(schedule="learned", flags=1, **kw),
-                              {"granularity": 4, "warps_per_block": 8, "chunk": 4}, DEFAULT_SPACE)
-    step = lambda: run(schedule="learned", flags=1, **tuned)  # noqa: E731
+        tuned, _, tlog = tune(lambda **kw: run(schedule="learned", **kw),
+                              {"flags": 1, "granularity": 4, "warps_per_block": 8, "chunk": 4}, LEARNED_SPACE)
+    step = lambda: run(schedule="learned", **tuned)  # noqa: E731
     step()
     assert count() == k4
     if dist:
@@ -301,13 +303,13 @@ def run_ours(a):
         "tuned": tuned, "tuning_log": [[c, round(t, 3)] for c, t in tlog]}}
     e2e, cpu = None, None
     if not a.no_extras:
-        hs, _ = timed(lambda: run(schedule="heuristic", split=True, flags=1, **tuned), 3, 1)
+        hs, _ = timed(lambda: run(schedule="heuristic", split=True, **dict(tuned, flags=1)), 3, 1)
         extras["schedules"]["heuristic_split_ms"] = float(np.mean(hs))
         gs, _ = timed(lambda: run(flags=1), 3, 1)
         extras["schedules"]["given_order_ms"] = float(np.mean(gs))
         # ---- triangles on the same graph (heuristic splits)
         ctx.set_plan(Plan.preset(0))
-        tri_step = lambda: run(schedule="heuristic", split=True, flags=1, **tuned)  # noqa: E731
+        tri_step = lambda: run(schedule="heuristic", **dict(tuned, flags=1))  # noqa: E731
         tri_step()
         tri = count()
         tms, _ = timed(tri_step, 3, 1)
@@ -327,9 +329,9 @@ def run_ours(a):
         cliques = count()
         cur["ctx"] = mctx
         mplain, _ = timed(lambda: mrun(schedule="heuristic", flags=1), 3, 1)
-        mtuned, _, _ = tune(lambda **kw: mrun(schedule="learned", flags=1, **kw),
-                            {"granularity": 4, "warps_per_block": 8, "chunk": 2}, DEFAULT_SPACE)
-        mms, mpass = timed(lambda: mrun(schedule="learned", flags=1, **mtuned), 3, 1)
+        mtuned, _, _ = tune(lambda **kw: mrun(schedule="learned", **kw),
+                            {"flags": 1, "granularity": 4, "warps_per_block": 8, "chunk": 2}, LEARNED_SPACE)
+        mms, mpass = timed(lambda: mrun(schedule="learned", **mtuned), 3, 1)
         assert count() == cliques
         cur["ctx"] = ctx
         mk = float(np.mean(mpass)) if mpass else None
@@ -358,7 +360,7 @@ def run_ours(a):
         def e2e_step():
             e2c.load(pg)
             e2c.load_core(core_h)
-            return e2c.match(plan, schedule="learned", **tuned)
+            return e2c.match(plan, schedule="learned", **dict(tuned, flags=tuned["flags"] & ~1))
 
         for _ in range(a.warmup):
             e2e_step()
