@@ -303,7 +303,7 @@ def run_ours(a):
         "tuned": tuned, "tuning_log": [[c, round(t, 3)] for c, t in tlog]}}
     e2e, cpu = None, None
     if not a.no_extras:
-        hs, _ = timed(lambda: run(schedule="heuristic", split=True, **dict(tuned, flags=1)), 3, 1)
+        hs, _ = timed(lambda: run(schedule="heuristic", split=True, **dict(tuned, flags=1, granularity=4)), 3, 1)
         extras["schedules"]["heuristic_split_ms"] = float(np.mean(hs))
         gs, _ = timed(lambda: run(flags=1), 3, 1)
         extras["schedules"]["given_order_ms"] = float(np.mean(gs))

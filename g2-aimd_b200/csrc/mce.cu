@@ -346,7 +346,7 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
         unsigned long long h = hist_local[s];
         if (h) {
             if (s < a.hist_len) atomicAdd(a.out + 1 + s, h);
-            else atomicOr(a.status, kStatusHistOverflow);
+            else if (a.hist_len) atomicOr(a.status, kStatusHistOverflow);  // hist_len 0: no histogram
         }
     }
     __syncwarp();

@@ -786,7 +786,7 @@ int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opt
     if (!ctx->d_rp) return G2_ERR_NO_GRAPH;
     G2_TRY(cudaSetDevice(ctx->device));
     ctx->launches = 0;
-    const uint32_t hl = hist ? hist_len : 1u;
+    const uint32_t hl = hist ? hist_len : 0u;  // no histogram requested: count only
     cudaStream_t st = nullptr;
     g2_opts o2{};
     if (opts) o2 = *opts;
