@@ -205,6 +205,9 @@ def run_ours(a):
     from g2aimd.autotune import DEFAULT_SPACE, tune
     # learned schedule search: heavy-root splits on (flags 1) or off (1 | G2_FLAG_NO_SPLIT)
     LEARNED_SPACE = dict({"flags": [1, 1 | 8]}, **DEFAULT_SPACE)
+    # MCE: hand-off check interval and queue chunk
+    FLAG_NO_SPILL = 16
+    MCE_SPACE = {"spill_kcycles": [5, 20, 100], "chunk": [1, 2], "warps_per_block": [4, 8]}
     from g2aimd.context import Context, CostModel, Plan
     world, rank, local = dist_env()
     dist = world > 1
@@ -328,9 +331,11 @@ def run_ours(a):
         mwork = work_of(mctx)
         cliques = count()
         cur["ctx"] = mctx
-        mplain, _ = timed(lambda: mrun(schedule="heuristic", flags=1), 3, 1)
-        mtuned, _, _ = tune(lambda **kw: mrun(schedule="learned", **kw),
-                            {"flags": 1, "granularity": 4, "warps_per_block": 8, "chunk": 2}, LEARNED_SPACE)
+        # plain: one warp per root, no hand-off; then walks handing branches to idle warps
+        mplain, _ = timed(lambda: mrun(schedule="heuristic", flags=1 | FLAG_NO_SPILL), 3, 1)
+        mlplain, _ = timed(lambda: mrun(schedule="learned", flags=1 | FLAG_NO_SPILL), 3, 1)
+        mhand, _ = timed(lambda: mrun(schedule="heuristic", flags=1), 3, 1)
+        mtuned, _, _ = tune(lambda **kw: mrun(schedule="learned", **kw), {"flags": 1, "chunk": 1}, MCE_SPACE)
         mms, mpass = timed(lambda: mrun(schedule="learned", **mtuned), 3, 1)
         assert count() == cliques
         cur["ctx"] = ctx
@@ -340,6 +345,7 @@ def run_ours(a):
             "graph": {"n": cl.n, "m": cl.m, "gamma": 2.3, "avg_degree": 16},
             "stream_bytes": mstream, "stream_gbs": mstream / (mk / 1000.0) / 1e9 if mk else None,
             "maximal_cliques": cliques, "plain_heuristic_ms": float(np.mean(mplain)),
+            "learned_no_handoff_ms": float(np.mean(mlplain)), "heuristic_handoff_ms": float(np.mean(mhand)),
             "learned_ms": float(np.mean(mms)), "learned_vs_plain": float(np.mean(mplain)) / float(np.mean(mms)),
             "tuned": mtuned, "per_s": cliques / (float(np.mean(mms)) / 1000.0), "kernel_ms": mk,
             "merge_model_bytes": mwork, "merge_model_gbs": mwork / (mk / 1000.0) / 1e9 if mk else None}

@@ -16,6 +16,12 @@ constexpr int kStatusDeferOverflow = 1;  // deferred-task list full
 constexpr int kStatusHistOverflow = 2;   // clique larger than the histogram
 constexpr int kStatusStackOverflow = 4;  // GMatch candidate stack exhausted
 constexpr int kStatusBadPlan = 8;        // plan arrays inconsistent
+constexpr int kStatusWaitLimit = 16;     // a bounded device wait ran out
+
+// An MCE pass entry with this bit set is a spilled record id, else a task id.
+constexpr uint32_t kRecordBit = 0x80000000u;
+// Depth word of a record slot whose reservation ran past the buffer's end.
+constexpr uint32_t kVoidRecord = 0xffffffffu;
 
 struct MceArgs {
     const uint64_t *rp;
@@ -24,6 +30,7 @@ struct MceArgs {
     const uint32_t *tasks;          // root vertex of each task
     const uint32_t *task_index;     // optional: the task ids this pass runs (else 0..ntasks-1)
     const uint32_t *task_part;      // optional per task id: (nparts << 16) | part of a split root
+    uint32_t split_depth;           // split roots deal out their depth-split_depth subtrees (>= 1)
     uint64_t *root_cost;            // optional per task id: SM cycles spent on the task
     uint64_t ntasks;                // tasks in this pass (if ntasks_dev is null)
     const unsigned long long *ntasks_dev;  // else: task count read from device memory
@@ -39,8 +46,22 @@ struct MceArgs {
     uint64_t *root_nodes;           // optional, per task id
     unsigned long long *work;       // optional: work model W in bytes (metrics kernel)
     int *status;
-    int final_pass;
+    // handed-off search-tree nodes (record: task, depth, pool offset / 64, nb,
+    // then P, X, R rows of rec_words words; rec_stride words each)
+    uint32_t *records;
+    uint32_t *ready;                // per record slot: epoch of the run that published it
+    unsigned long long *nrec;       // records written in this run (append-only)
+    uint64_t rec_cap;
+    uint32_t rec_stride, rec_words;
+    uint32_t *pool;                 // A and B rows of the roots whose tasks spilled
+    unsigned long long *npool;      // 64-word units used
+    uint64_t pool_cap;              // words
+    uint64_t spill_cycles;          // 0: no hand-off in this pass
+    unsigned long long *qctl;       // record queue: [kQHead] tickets taken, [kQOut] outstanding work
+    uint32_t epoch;                 // ready word of records published in this run
+    uint64_t wait_cycles;           // longest wait of a warp for its ticket's record
 };
+constexpr int kQHead = 0, kQOut = 1;
 
 size_t mce_smem_bytes(int wpl, int warps_per_block);
 cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_block, cudaStream_t st);

@@ -17,6 +17,17 @@
 // (app_BK/BK.h:314; X0 ids < v < P0 ids and both are kept sorted), so the tree
 // is exactly the reference's and per-root node counts match the oracle.
 //
+// Spilling (load balance inside a root): once the pass's task queue is empty,
+// a task that has run for more than spill_cycles SM cycles stops and writes one
+// record per pending branch of every open level of its walk (node depth, P, X
+// and the path R as P0 bitmaps); its rows go once to a shared row pool.  The
+// next pass (a wave) runs those records on the whole grid, each rebuilding its
+// B list as the root's kept rows that contain R.  Every node is still visited
+// exactly once, in the same tree, so counts, histograms and per-root node
+// counts do not change.  Search trees of the dense cores of power-law graphs are
+// chains at the top (one branch per node for many levels), which is why the
+// split is taken where the walk is, not at a fixed depth.
+//
 // A root whose rows or frames do not fit in the warp's slab (or whose p needs
 // more than 32*WPL words) is deferred: the host re-runs deferred roots with a
 // larger slab per warp (fewer warps) or a wider WPL.  No spin waits exist.
@@ -30,15 +41,18 @@ namespace g2 {
 
 namespace {
 
-struct Frame {  // offsets inside the warp slab
-    static __device__ __forceinline__ uint32_t size(uint32_t W) { return 3u * W + 2u; }
-};
+__device__ __forceinline__ unsigned long long vload(const unsigned long long *p) {
+    return *reinterpret_cast<const volatile unsigned long long *>(p);
+}
+__device__ __forceinline__ uint32_t vload32(const uint32_t *p) { return *reinterpret_cast<const volatile uint32_t *>(p); }
 
-template <int WPL>
-__device__ void defer_root(const MceArgs &a, uint64_t t) {
+// slab frame per open level: P, X, Qr rows, list offset, list length, branch taken
+__device__ __forceinline__ uint32_t frame_words(uint32_t W) { return 3u * W + 3u; }
+
+__device__ void defer_entry(const MceArgs &a, uint32_t entry) {
     if (lane_id() == 0) {
         unsigned long long d = atomicAdd(a.ndeferred, 1ull);
-        if (d < a.deferred_cap) a.deferred[d] = (uint32_t)t;
+        if (d < a.deferred_cap) a.deferred[d] = entry;
         else atomicOr(a.status, kStatusDeferOverflow);
     }
 }
@@ -70,26 +84,306 @@ __device__ __forceinline__ uint32_t row_popc(const Row<WPL> &r) {
     return (uint32_t)warp_sum_u64(c);
 }
 
-// Walk one root.  Returns false if the root had to be deferred.  With METRICS
-// the work model W (in 4-byte words) of the reference's tree is accumulated:
-// per node with P ∪ X non-empty, sum_{u in P∪X} (|P| + deg u) for pivot
-// scoring plus sum_{q in P \ N(pivot)} (|P ∪ X| + deg q) for the children.
+// Lowest set bit of a distributed row (all lanes), ~0u if the row is empty.
+template <int WPL>
+__device__ __forceinline__ uint32_t row_lowest(const Row<WPL> &r) {
+    const uint32_t lane = lane_id();
+    uint32_t key = 0xffffffffu;
+#pragma unroll
+    for (int s = WPL - 1; s >= 0; s--)
+        if (r.w[s]) key = 32u * (uint32_t)s + lane;  // word index lane + 32*s
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        uint32_t y = __shfl_xor_sync(G2_FULL, key, o);
+        key = y < key ? y : key;
+    }
+    if (key == 0xffffffffu) return key;
+    return key * 32u + (uint32_t)(__ffs(row_word(r, key)) - 1);
+}
+
+template <int WPL>
+__device__ __forceinline__ void row_assign_bit(Row<WPL> &r, uint32_t q, bool on) {
+    const uint32_t lane = lane_id(), qw = q >> 5, bit = 1u << (q & 31u);
+#pragma unroll
+    for (int s = 0; s < WPL; s++)
+        if (lane + 32u * s == qw) r.w[s] = on ? (r.w[s] | bit) : (r.w[s] & ~bit);
+}
+
+template <int WPL>
+__device__ __forceinline__ void row_load_cg(Row<WPL> &r, const uint32_t *src, uint32_t W) {
+    const uint32_t lane = lane_id();
+#pragma unroll
+    for (int s = 0; s < WPL; s++) {
+        uint32_t w = lane + 32u * s;
+        r.w[s] = w < W ? __ldcg(src + w) : 0u;
+    }
+}
+
+// The rows a walk reads: slab rows of a root task, or pool rows of a record.
+struct Rows {
+    const uint32_t *A;   // p rows of W words
+    const uint32_t *B;   // nb kept X0 rows of W words
+    const uint32_t *xv;  // metrics: X0 vertex of each kept row
+    uint64_t pool_off;   // offset of the rows in the pool, ~0 while they live in the slab
+};
+
+// Record layout: [task, depth, pool offset / 64, nb, P (W), X (W), R (W)]; the
+// ready word of slot i is ready[i] (a separate array that holds nothing but
+// epochs, whatever the record stride of earlier runs was).
+constexpr uint32_t kRecRows = 4;
+
+// Reserve n consecutive records with one atomic (no retries: many warps hand
+// off work at the same moment).  The slots that exist are added to the
+// outstanding count before any of them is published (the caller is itself
+// outstanding, so the count cannot touch zero meanwhile).  If the slots run
+// past the end of the buffer the ones below the end are published as void
+// (their ticket holders skip them) and ~0 is returned.
+__device__ __forceinline__ unsigned long long reserve_records(const MceArgs &a, uint32_t n) {
+    unsigned long long base = 0;
+    if (lane_id() == 0) {
+        base = atomicAdd(a.nrec, (unsigned long long)n);
+        const unsigned long long end = base + n < a.rec_cap ? base + n : a.rec_cap;
+        if (end > base) atomicAdd(a.qctl + kQOut, end - base);
+    }
+    base = __shfl_sync(G2_FULL, base, 0);
+    if (base + n <= a.rec_cap) return base;
+    for (unsigned long long i = base + lane_id(); i < a.rec_cap && i < base + n; i += 32)
+        a.records[i * a.rec_stride + 1] = kVoidRecord;
+    __syncwarp();
+    __threadfence();
+    for (unsigned long long i = base + lane_id(); i < a.rec_cap && i < base + n; i += 32)
+        *reinterpret_cast<volatile uint32_t *>(a.ready + i) = a.epoch;
+    __syncwarp();
+    return ~0ull;
+}
+
+// Rows of a root task go to the pool before its first records reference them.
+template <bool METRICS>
+__device__ bool ensure_pooled(const MceArgs &a, uint32_t p, uint32_t nb, uint32_t W, Rows &rows) {
+    const uint32_t lane = lane_id();
+    if (rows.pool_off != ~0ull) return true;
+    const uint64_t words = (uint64_t)(p + nb) * W + (METRICS ? nb : 0u);
+    const uint64_t units = (words + 63u) >> 6;
+    unsigned long long off = 0;
+    if (lane == 0) off = atomicAdd(a.npool, (unsigned long long)units);
+    off = __shfl_sync(G2_FULL, off, 0);
+    if ((off + units) << 6 > a.pool_cap) return false;
+    uint32_t *dst = a.pool + (off << 6);
+    for (uint64_t i = lane; i < (uint64_t)p * W; i += 32) dst[i] = rows.A[i];
+    for (uint64_t i = lane; i < (uint64_t)nb * W; i += 32) dst[(uint64_t)p * W + i] = rows.B[i];
+    if (METRICS)
+        for (uint32_t i = lane; i < nb; i += 32) dst[(uint64_t)(p + nb) * W + i] = rows.xv[i];
+    __syncwarp();
+    rows.pool_off = off << 6;
+    rows.A = dst;
+    rows.B = dst + (uint64_t)p * W;
+    rows.xv = dst + (uint64_t)(p + nb) * W;
+    return true;
+}
+
+// Write records k, k+1, ... for the branches Q of one level (ascending; each
+// branch's P and X see the earlier ones moved from P to X, sequential BK).
+// R is the level's path; depth the children's depth.  Returns the next slot.
+template <int WPL>
+__device__ unsigned long long emit_level(const MceArgs &a, unsigned long long k, uint32_t task, uint32_t depth,
+                                         Row<WPL> Pl, Row<WPL> Xl, Row<WPL> Ql, const Row<WPL> &R,
+                                         const Rows &rows, uint32_t nb, uint32_t W) {
+    const uint32_t lane = lane_id();
+    for (;;) {
+        const uint32_t q = row_lowest(Ql);
+        if (q == 0xffffffffu) break;
+        row_assign_bit(Ql, q, false);
+        Row<WPL> aq, cp, cx, cr;
+        row_load(aq, rows.A + (uint64_t)q * W, W);
+#pragma unroll
+        for (int s = 0; s < WPL; s++) {
+            cp.w[s] = Pl.w[s] & aq.w[s];
+            cx.w[s] = Xl.w[s] & aq.w[s];
+            cr.w[s] = R.w[s];
+        }
+        row_assign_bit(cr, q, true);
+        uint32_t *rec = a.records + k * a.rec_stride;
+        k++;
+        if (lane == 0) {
+            rec[0] = task;
+            rec[1] = depth;
+            rec[2] = (uint32_t)(rows.pool_off >> 6);
+            rec[3] = nb;
+        }
+        row_store(cp, rec + kRecRows, W);
+        row_store(cx, rec + kRecRows + W, W);
+        row_store(cr, rec + kRecRows + 2u * W, W);
+        row_assign_bit(Pl, q, false);
+        row_assign_bit(Xl, q, true);
+    }
+    return k;
+}
+
+// Make records [k0, k1) visible to claimers: data first, then the ready words.
+__device__ __forceinline__ void publish(const MceArgs &a, unsigned long long k0, unsigned long long k1) {
+    __syncwarp();
+    __threadfence();
+    for (unsigned long long i = k0 + lane_id(); i < k1; i += 32)
+        *reinterpret_cast<volatile uint32_t *>(a.ready + i) = a.epoch;
+    __syncwarp();
+}
+
+// Pending-branch count of every frame level below d, as (first level with any, its count).
+template <int WPL>
+__device__ void shallowest_pending(const uint32_t *frames, uint32_t d, uint32_t W, uint32_t *level,
+                                   uint32_t *count) {
+    const uint32_t lane = lane_id(), FR = frame_words(W);
+    *level = d;
+    *count = 0;
+    for (uint32_t l = 0; l < d; l++) {
+        uint32_t c = 0;
+        for (uint32_t w = lane; w < W; w += 32) c += __popc(frames[(uint64_t)l * FR + 2u * W + w]);
+        c = (uint32_t)warp_sum_u64(c);
+        if (c) {
+            *level = l;
+            *count = c;
+            return;
+        }
+    }
+}
+
+// Path R of frame level l: the entry node's R plus the branches taken at levels < l.
+template <int WPL>
+__device__ Row<WPL> path_of(const uint32_t *frames, uint32_t l, uint32_t W, const Row<WPL> &Rbase) {
+    const uint32_t FR = frame_words(W);
+    Row<WPL> R = Rbase;
+    for (uint32_t j = 0; j < l; j++) row_assign_bit(R, frames[(uint64_t)j * FR + 3u * W + 2u], true);
+    return R;
+}
+
+// Hand the pending branches of the shallowest open level (its subtrees are the
+// largest) to idle warps and keep walking.  At the current level d the first
+// branch stays with this warp.  Returns false if nothing was handed off.
 template <int WPL, bool METRICS>
-__device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *cand, uint32_t *rowbuf) {
+__device__ __noinline__ bool donate(const MceArgs &a, uint32_t task, uint32_t d0, uint32_t d, const Row<WPL> &P,
+                                    const Row<WPL> &X, Row<WPL> &Qr, const Row<WPL> &Rbase, uint32_t *frames,
+                                    uint32_t W, uint32_t p, uint32_t nb, Rows &rows, bool *full) {
+    const uint32_t FR = frame_words(W);
+    uint32_t l, cnt;
+    shallowest_pending<WPL>(frames, d, W, &l, &cnt);
+    uint32_t q0 = 0xffffffffu;
+    if (cnt == 0) {  // only the current level: keep its first branch
+        q0 = row_lowest(Qr);
+        cnt = row_popc(Qr);
+        cnt = cnt ? cnt - 1 : 0;
+        if (cnt == 0) return false;
+    }
+    if (!ensure_pooled<METRICS>(a, p, nb, W, rows)) {
+        *full = true;
+        return false;
+    }
+    const unsigned long long k0 = reserve_records(a, cnt);
+    if (k0 == ~0ull) {
+        *full = true;
+        return false;
+    }
+    const Row<WPL> R = path_of<WPL>(frames, l, W, Rbase);
+    Row<WPL> Pl, Xl, Ql;
+    uint32_t *f = frames + (uint64_t)l * FR;
+    if (l < d) {
+        row_load(Pl, f, W);
+        row_load(Xl, f + W, W);
+        row_load(Ql, f + 2u * W, W);
+    } else {
+        Pl = P;
+        Xl = X;
+        Ql = Qr;
+        row_assign_bit(Pl, q0, false);  // q0 runs first here, so later siblings see it in X
+        row_assign_bit(Xl, q0, true);
+        row_assign_bit(Ql, q0, false);
+    }
+    const unsigned long long k1 = emit_level<WPL>(a, k0, task, d0 + l + 1u, Pl, Xl, Ql, R, rows, nb, W);
+    publish(a, k0, k1);
+    if (l < d) {
+        Row<WPL> z;
+        row_zero(z);
+        row_store(z, f + 2u * W, W);  // the donated branches leave the frame
+        __syncwarp();
+    } else {
+        row_zero(Qr);
+        row_assign_bit(Qr, q0, true);
+    }
+    return true;
+}
+
+// Hand every pending branch of levels 0..d to records (level d is the register
+// state P, X, Qr) and end the walk.  Returns false, with nothing published
+// that a claimer would run, if the buffers are full.
+template <int WPL, bool METRICS>
+__device__ __noinline__ bool spill_all(const MceArgs &a, uint32_t task, uint32_t d0, uint32_t d, const Row<WPL> &P,
+                                       const Row<WPL> &X, const Row<WPL> &Qr, const Row<WPL> &Rbase,
+                                       const uint32_t *frames, uint32_t W, uint32_t p, uint32_t nb, Rows &rows) {
+    const uint32_t lane = lane_id(), FR = frame_words(W);
+    uint32_t need = row_popc(Qr);
+    for (uint32_t l = 0; l < d; l++) {
+        uint32_t c = 0;
+        for (uint32_t w = lane; w < W; w += 32) c += __popc(frames[(uint64_t)l * FR + 2u * W + w]);
+        need += (uint32_t)warp_sum_u64(c);
+    }
+    if (need == 0) return true;  // nothing pending: the walk is complete
+    if (!ensure_pooled<METRICS>(a, p, nb, W, rows)) return false;
+    const unsigned long long k0 = reserve_records(a, need);
+    if (k0 == ~0ull) return false;
+    unsigned long long k = k0;
+    Row<WPL> R = Rbase;
+    for (uint32_t l = 0; l <= d; l++) {
+        const uint32_t *f = frames + (uint64_t)l * FR;
+        if (l < d) {
+            Row<WPL> Pl, Xl, Ql;
+            row_load(Pl, f, W);
+            row_load(Xl, f + W, W);
+            row_load(Ql, f + 2u * W, W);
+            k = emit_level<WPL>(a, k, task, d0 + l + 1u, Pl, Xl, Ql, R, rows, nb, W);
+            row_assign_bit(R, f[3u * W + 2u], true);
+        } else {
+            k = emit_level<WPL>(a, k, task, d0 + l + 1u, P, X, Qr, R, rows, nb, W);
+        }
+    }
+    publish(a, k0, k);
+    return true;
+}
+
+enum : int { kTaskDone = 0, kTaskDeferred = 1 };
+
+// Run one entry: a root task (entry < 2^31) or a handed-off record (entry has
+// kRecordBit set).  With METRICS the work model W (in 4-byte words) of the
+// reference's tree is accumulated: per node with P ∪ X non-empty,
+// sum_{u in P∪X} (|P| + deg u) for pivot scoring plus
+// sum_{q in P \ N(pivot)} (|P ∪ X| + deg q) for the children.
+template <int WPL, bool METRICS>
+__device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t *cand, uint32_t *rowbuf,
+                        long long c0, uint32_t *task_out) {
     const uint32_t lane = lane_id();
     const uint64_t *rp = a.rp;
     const uint32_t *ci = a.ci;
-    const uint32_t v = a.tasks[t];
-    const uint64_t lo = ldg(rp + v), hi = ldg(rp + v + 1);
-    // heavy-root split: this task owns the root's top-level branches whose ordinal
-    // is congruent to part mod nparts (the root record itself belongs to part 0)
-    const uint32_t tp = a.task_part ? a.task_part[t] : (1u << 16);
-    const uint32_t nparts = tp >> 16, part = tp & 0xffffu;
-    if (lo == hi || (part != 0 && ldg(a.fo + v) == hi - lo)) {  // no neighbours (app_BK/BK.h:335-336) or P empty
-        if (a.root_nodes && lane == 0) a.root_nodes[t] = 0;
-        return true;
+    const bool is_rec = (entry & kRecordBit) != 0;
+    const uint32_t *rec = is_rec ? a.records + (uint64_t)(entry & ~kRecordBit) * a.rec_stride : nullptr;
+    // record words are read past L1 (two records share a cache line, and a line
+    // another warp of this SM read earlier may predate this record)
+    if (is_rec && __ldcg(rec + 1) == kVoidRecord) {  // slot of a reservation that did not fit
+        *task_out = ~0u;
+        return kTaskDone;
     }
-    uint32_t branch = 0;  // ordinal of the next top-level branch
+    const uint32_t task = is_rec ? __ldcg(rec) : entry;
+    const uint32_t d0 = is_rec ? __ldcg(rec + 1) : 0u;  // depth of the entry node (R has d0 + 1 vertices)
+    *task_out = task;
+    const uint32_t v = a.tasks[task];
+    const uint64_t lo = ldg(rp + v), hi = ldg(rp + v + 1);
+    // static heavy-root split: every part walks the nodes above depth D (they are
+    // the same in every part; part 0 counts them) and owns the depth-D subtrees
+    // whose ordinal, in depth-first order, is congruent to part mod nparts
+    const uint32_t tp = (a.task_part && !is_rec) ? a.task_part[task] : (1u << 16);
+    const uint32_t nparts = tp >> 16, part = tp & 0xffffu;
+    const uint32_t D = nparts > 1 ? (a.split_depth ? a.split_depth : 1u) : 0u;
+    if (!is_rec && (lo == hi || (part != 0 && ldg(a.fo + v) == hi - lo))) {  // no neighbours (app_BK/BK.h:335-336) or P empty
+        return kTaskDone;
+    }
+    uint32_t branch = 0;  // ordinal of the next depth-D subtree
     const uint64_t split = lo + ldg(a.fo + v);
     const uint32_t p = (uint32_t)(hi - split);
     const uint32_t nx = (uint32_t)(split - lo);
@@ -103,88 +397,132 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
             sx = warp_sum_u64(sx);
             if (lane == 0) atomicAdd(a.work, sx * 4ull);
         }
-        if (a.root_nodes && lane == 0) a.root_nodes[t] = 1;
-        return true;
+        if (a.root_nodes && lane == 0) atomicAdd(reinterpret_cast<unsigned long long *>(a.root_nodes + task), 1ull);
+        return kTaskDone;
     }
     const uint32_t W = (p + 31u) >> 5;
-    if (W > 32u * WPL) return false;
+    if (W > 32u * WPL) return kTaskDeferred;
     const uint64_t SW = a.words_per_warp;
-    const uint32_t FR = Frame::size(W);
-    // slab: [hist u64 (p+2)] [A p*W] [xv nx (metrics)] [B nb*W] [lists ...] ... [frames (p+1)*FR]
-    const uint64_t h0 = 0, a0 = 2ull * (p + 2), xv0 = a0 + (uint64_t)p * W;
-    const uint64_t b0 = xv0 + (METRICS ? nx : 0);  // metrics: X0 vertex of each kept B row
+    const uint32_t FR = frame_words(W);
     const uint64_t fr0 = SW >= (uint64_t)(p + 1) * FR ? SW - (uint64_t)(p + 1) * FR : 0;
-    if (fr0 < b0 + 64) return false;
-    unsigned long long *hist_local = reinterpret_cast<unsigned long long *>(S + h0);
+    unsigned long long *hist_local = reinterpret_cast<unsigned long long *>(S);
+    const uint64_t a0 = 2ull * (p + 2);  // after the histogram
     for (uint32_t s = lane; s < p + 2; s += 32) hist_local[s] = 0ull;
-    // ---- stage P0 in shared memory, then the rows
-    for (uint32_t i = lane; i < p; i += 32) cand[i] = ldg(ci + split + i);
+    Rows rows;
+    uint32_t nb;
+    uint64_t l0;  // list region
+    Row<WPL> P, X, Qr, Rb;
+    uint32_t xlen;
+    if (!is_rec) {
+        // slab: [hist u64 (p+2)] [A p*W] [xv nx (metrics)] [B nb*W] [lists ...] ... [frames (p+1)*FR]
+        const uint64_t xv0 = a0 + (uint64_t)p * W;
+        const uint64_t b0 = xv0 + (METRICS ? nx : 0);
+        if (fr0 < b0 + 64) return kTaskDeferred;
+        // stage P0 in shared memory, then the rows
+        for (uint32_t i = lane; i < p; i += 32) cand[i] = ldg(ci + split + i);
+        __syncwarp();
+        build_forward_rows(rp, ci, a.fo, cand, p, W, S + a0, rowbuf);
+        // kept B rows plus their root-list entries must stay below the frames
+        const uint64_t cap64 = (fr0 - b0 - 64) / (W + 1);
+        const uint32_t cap = cap64 > 0xfffffff0ull ? 0xfffffff0u : (uint32_t)cap64;
+        nb = build_back_rows(rp, ci, a.fo, v, lo, nx, cand, p, W, S + b0, METRICS ? S + xv0 : nullptr, cap, rowbuf);
+        if (nb == ~0u) return kTaskDeferred;
+        __syncwarp();
+        rows.A = S + a0;
+        rows.B = S + b0;
+        rows.xv = S + xv0;
+        rows.pool_off = ~0ull;
+        // root list: identity over the nb kept rows
+        l0 = b0 + (uint64_t)nb * W;
+        for (uint32_t i = lane; i < nb; i += 32) S[l0 + i] = i;
+        xlen = nb;
+#pragma unroll
+        for (int s = 0; s < WPL; s++) {
+            uint32_t w = lane + 32u * s;
+            P.w[s] = w < W ? (w + 1 < W || (p & 31u) == 0 ? G2_FULL : ((1u << (p & 31u)) - 1u)) : 0u;
+            X.w[s] = 0u;
+            Rb.w[s] = 0u;
+        }
+    } else {
+        // slab: [hist u64 (p+2)] [lists ...] ... [frames]; rows in the pool
+        nb = __ldcg(rec + 3);
+        rows.pool_off = (uint64_t)__ldcg(rec + 2) << 6;
+        rows.A = a.pool + rows.pool_off;
+        rows.B = rows.A + (uint64_t)p * W;
+        rows.xv = rows.B + (uint64_t)nb * W;
+        l0 = a0;
+        if (fr0 < l0 + nb + 64) return kTaskDeferred;
+        row_load_cg(P, rec + kRecRows, W);
+        row_load_cg(X, rec + kRecRows + W, W);
+        row_load_cg(Rb, rec + kRecRows + 2u * W, W);
+        // the entry node's B list: kept rows adjacent to every vertex of R \ {v}
+        xlen = 0;
+        for (uint32_t c = 0; c < nb; c += 32) {
+            const uint32_t i = c + lane;
+            bool ok = i < nb;
+            for (uint32_t w = 0; w < W; w++) {
+                const uint32_t rw = row_word(Rb, w);
+                if (ok && (rows.B[(uint64_t)i * W + w] & rw) != rw) ok = false;
+            }
+            uint32_t tot;
+            const uint32_t pos = warp_scan(ok, tot);
+            if (ok) S[l0 + xlen + pos] = i;
+            xlen += tot;
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < WPL; s++) Qr.w[s] = 0u;
     __syncwarp();
-    build_forward_rows(rp, ci, a.fo, cand, p, W, S + a0, rowbuf);
-    uint32_t *Bfull = S + b0;
-    // kept B rows plus their root-list entries must stay below the frames
-    const uint64_t cap64 = (fr0 - b0 - 64) / (W + 1);
-    const uint32_t cap = cap64 > 0xfffffff0ull ? 0xfffffff0u : (uint32_t)cap64;
-    const uint32_t nb = build_back_rows(rp, ci, a.fo, v, lo, nx, cand, p, W, Bfull, METRICS ? S + xv0 : nullptr,
-                                        cap, rowbuf);
-    if (nb == ~0u) return false;
-    __syncwarp();
-    // ---- root list (identity over the nb kept rows), right after B
-    const uint64_t l0 = b0 + (uint64_t)nb * W;
-    for (uint32_t i = lane; i < nb; i += 32) S[l0 + i] = i;
-    __syncwarp();
+    const uint32_t *Bfull = rows.B;
 
     // ---- depth-first walk
-    Row<WPL> P, X, Qr;
-#pragma unroll
-    for (int s = 0; s < WPL; s++) {
-        uint32_t w = lane + 32u * s;
-        P.w[s] = w < W ? (w + 1 < W || (p & 31u) == 0 ? G2_FULL : ((1u << (p & 31u)) - 1u)) : 0u;
-        X.w[s] = 0u;
-        Qr.w[s] = 0u;
-    }
     uint64_t xoff = l0;
-    uint32_t xlen = nb;
-    uint32_t d = 0;  // |R| = d + 1
+    uint32_t d = 0;  // depth below the entry node
     unsigned long long nodes = 0, cliques = 0, work = 0;
     bool enter = true;
-    bool overflow = false;
+    bool overflow = false, spilled = false;
+    bool donated = false;  // some branches went to records: the entry can no longer be re-run
+    bool may_spill = a.spill_cycles != 0 && nparts == 1 && W <= a.rec_words;
+    long long next_check = (long long)a.spill_cycles;
+    const unsigned long long *qc = a.qctl;
     for (;;) {
         bool want_pop = false;
         if (enter) {
             enter = false;
-            if (d > 0 || part == 0) nodes++;
+            const bool own = d >= D || part == 0;  // this part counts the node
+            const bool at_root = !is_rec && d == 0;
+            if (own) nodes++;
             uint32_t anyp = 0, anyx = 0;
 #pragma unroll
             for (int s = 0; s < WPL; s++) anyp |= P.w[s], anyx |= X.w[s];
             const bool hp = __any_sync(G2_FULL, anyp != 0);
             const bool hx = __any_sync(G2_FULL, anyx != 0) || xlen > 0;
             unsigned long long npx = 0;  // |P| + |X| (metrics)
-            if (METRICS && (hp || hx) && (d > 0 || part == 0)) {
+            if (METRICS && (hp || hx) && own) {
                 // the reference's root record keeps every X0 vertex, also those
                 // with no neighbour in P0 that the B list drops (they fall out of
                 // every child), so the root node counts all of X0
                 const uint32_t np = row_popc(P);
-                npx = np + row_popc(X) + (d == 0 ? nx : xlen);
+                npx = np + row_popc(X) + (at_root ? nx : xlen);
                 unsigned long long sd = row_degree_sum(P, rp, ci, split) + row_degree_sum(X, rp, ci, split);
                 unsigned long long sx = 0;
-                if (d == 0) {
+                if (at_root) {
                     for (uint32_t li = lane; li < nx; li += 32) {
                         const uint32_t u = ldg(ci + lo + li);
                         sx += ldg(rp + u + 1) - ldg(rp + u);
                     }
                 } else {
                     for (uint32_t li = lane; li < xlen; li += 32) {
-                        const uint32_t u = S[xv0 + S[xoff + li]];
+                        const uint32_t u = rows.xv[S[xoff + li]];
                         sx += ldg(rp + u + 1) - ldg(rp + u);
                     }
                 }
                 work += npx * np + sd + warp_sum_u64(sx);
             }
             if (!hp) {
-                if (!hx) {  // no P and no X: maximal (app_BK/BK.h:78-91)
+                if (!hx && own) {  // no P and no X: maximal (app_BK/BK.h:78-91)
                     cliques++;
-                    if (lane == 0) hist_local[d + 1]++;
+                    if (lane == 0) hist_local[d0 + d + 1]++;
                 }
                 want_pop = true;
             } else {
@@ -216,7 +554,7 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
                     const uint32_t k = c + lane;
                     const bool valid = k < ncand;
                     const uint32_t idx = valid ? cand[k] : 0u;
-                    const uint32_t *r = S + a0 + (uint64_t)idx * W;
+                    const uint32_t *r = rows.A + (uint64_t)idx * W;
                     uint32_t sc = 0;
                     for (uint32_t w = 0; w < W; w++) {
                         const uint32_t pw = row_word(P, w);
@@ -246,43 +584,57 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
                 best = warp_max_u64(best);
                 const uint32_t rank = (uint32_t)(best & 0xffffffffull);
                 const uint32_t *prow =
-                    rank >= nb ? S + a0 + (uint64_t)(rank - nb) * W : Bfull + (uint64_t)rank * W;
+                    rank >= nb ? rows.A + (uint64_t)(rank - nb) * W : Bfull + (uint64_t)rank * W;
                 Row<WPL> pr;
                 row_load(pr, prow, W);
 #pragma unroll
                 for (int s = 0; s < WPL; s++) Qr.w[s] = P.w[s] & ~pr.w[s];
-                if (METRICS && (d > 0 || part == 0)) work += npx * row_popc(Qr) + row_degree_sum(Qr, rp, ci, split);
+                if (METRICS && own) work += npx * row_popc(Qr) + row_degree_sum(Qr, rp, ci, split);
+                // ---- every spill_cycles: hand work to idle warps while they
+                // outnumber the records waiting to be claimed
+                if (may_spill) {
+                    long long el = 0;
+                    if (lane == 0) el = clock64() - c0;
+                    el = __shfl_sync(G2_FULL, el, 0);
+                    if (el > next_check) {
+                        // idle warps hold tickets past the last reserved record
+                        int want = 0;
+                        if (lane == 0) want = vload(qc + kQHead) > vload(a.nrec);
+                        if (__shfl_sync(G2_FULL, want, 0)) {
+                            bool full = false;
+                            if (donate<WPL, METRICS>(a, task, d0, d, P, X, Qr, Rb, S + fr0, W, p, nb, rows, &full))
+                                donated = true;
+                            if (full) may_spill = false;  // buffers full: finish the walk here
+                        }
+                        next_check = el + (long long)a.spill_cycles;
+                    }
+                }
             }
         }
         if (!want_pop) {
             // ---- next branch q of the current node: lowest set bit of Qr
-            uint32_t key = 0xffffffffu;
-#pragma unroll
-            for (int s = WPL - 1; s >= 0; s--)
-                if (Qr.w[s]) key = 32u * (uint32_t)s + lane;  // word index lane + 32*s
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                uint32_t y = __shfl_xor_sync(G2_FULL, key, o);
-                key = y < key ? y : key;
-            }
-            if (key == 0xffffffffu) {
+            const uint32_t q = row_lowest(Qr);
+            if (q == 0xffffffffu) {
                 want_pop = true;
             } else {
-                const uint32_t qw = key;  // word index
-                const uint32_t qword = row_word(Qr, qw);
-                const uint32_t q = qw * 32u + (uint32_t)(__ffs(qword) - 1);
-                const uint32_t qbit = 1u << (q & 31u);
+                const uint32_t qw = q >> 5;
                 // q moves from P to X and is consumed from Q
-#pragma unroll
-                for (int s = 0; s < WPL; s++)
-                    if (lane + 32u * s == qw) {
-                        P.w[s] &= ~qbit;
-                        X.w[s] |= qbit;
-                        Qr.w[s] &= ~qbit;
-                    }
-                if (d == 0 && nparts > 1 && (branch++ % nparts) != part) continue;  // another part's branch
+                row_assign_bit(P, q, false);
+                row_assign_bit(X, q, true);
+                row_assign_bit(Qr, q, false);
+                if (d + 1 == D && (branch++ % nparts) != part) continue;  // another part's subtree
                 const uint64_t coff = xoff + xlen;
-                if (coff + xlen > fr0) {  // child list would reach the frames
+                if (coff + xlen > fr0) {         // child list would reach the frames
+                    if (may_spill || donated) {  // hand this level and the ones below to records
+                        Row<WPL> P1 = P, X1 = X, Q1 = Qr;
+                        row_assign_bit(P1, q, true);
+                        row_assign_bit(X1, q, false);
+                        row_assign_bit(Q1, q, true);
+                        if (spill_all<WPL, METRICS>(a, task, d0, d, P1, X1, Q1, Rb, S + fr0, W, p, nb, rows)) {
+                            spilled = true;
+                            break;
+                        }
+                    }
                     overflow = true;
                     break;
                 }
@@ -292,12 +644,13 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
                 row_store(X, f + W, W);
                 row_store(Qr, f + 2 * W, W);
                 if (lane == 0) {
-                    f[3 * W] = (uint32_t)(xoff - b0);
+                    f[3 * W] = (uint32_t)(xoff - l0);
                     f[3 * W + 1] = xlen;
+                    f[3 * W + 2] = q;
                 }
                 // child: P ∩ A[q], X_P0 ∩ A[q], B entries adjacent to q
                 Row<WPL> aq;
-                row_load(aq, S + a0 + (uint64_t)q * W, W);
+                row_load(aq, rows.A + (uint64_t)q * W, W);
 #pragma unroll
                 for (int s = 0; s < WPL; s++) {
                     P.w[s] &= aq.w[s];
@@ -329,17 +682,20 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
             row_load(P, f, W);
             row_load(X, f + W, W);
             row_load(Qr, f + 2 * W, W);
-            xoff = b0 + f[3 * W];
+            xoff = l0 + f[3 * W];
             xlen = f[3 * W + 1];
         }
         __syncwarp();
     }
-    if (overflow) return false;
-    // ---- commit this root's results
+    if (overflow && !spilled) {
+        if (!donated) return kTaskDeferred;  // re-run from scratch by a pass with a bigger slab
+        if (lane == 0) atomicOr(a.status, kStatusDeferOverflow);  // record buffers full: incomplete
+    }
+    // ---- commit this entry's results
     __syncwarp();
     if (lane == 0) {
         atomicAdd(a.out, cliques);
-        if (a.root_nodes) a.root_nodes[t] = nodes;
+        if (a.root_nodes) atomicAdd(reinterpret_cast<unsigned long long *>(a.root_nodes + task), nodes);
         if (METRICS) atomicAdd(a.work, work * 4ull);
     }
     for (uint32_t s = lane; s < p + 2; s += 32) {
@@ -350,32 +706,98 @@ __device__ bool mce_root(const MceArgs &a, uint64_t t, uint32_t *S, uint32_t *ca
         }
     }
     __syncwarp();
-    return true;
+    return kTaskDone;
 }
 
+template <int WPL, bool METRICS>
+__device__ __forceinline__ void run_entry(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t *cand,
+                                          uint32_t *rowbuf) {
+    long long c0 = 0;
+    if (lane_id() == 0) c0 = clock64();
+    c0 = __shfl_sync(G2_FULL, c0, 0);
+    uint32_t task = 0;
+    if (mce_task<WPL, METRICS>(a, entry, S, cand, rowbuf, c0, &task) == kTaskDeferred)
+        defer_entry(a, entry);
+    else if (a.root_cost && lane_id() == 0 && task != ~0u)
+        atomicAdd(reinterpret_cast<unsigned long long *>(a.root_cost + task), (unsigned long long)(clock64() - c0));
+}
+
+// Persistent pass.  Phase 1: entries from the task queue (or a deferred list).
+// Phase 2 (passes that hand off work): a warp takes a ticket (the index of the
+// next record, reserved or not yet) and runs that record once it is published.
+// kQOut counts the work that exists: warps holding queue tasks plus reserved,
+// unfinished records.  It is raised before work is published and lowered when
+// it is done, by warps that are themselves counted, so once it reads zero no
+// record can appear any more and a warp still waiting on a ticket leaves.
+// The wait is bounded by wait_cycles; past that the warp flags the run and
+// leaves (its ticket's record, if one comes, would be lost: an error).
 template <int WPL, bool METRICS>
 __global__ void __launch_bounds__(256) mce_kernel(MceArgs a) {
     extern __shared__ uint32_t smem[];
     const uint32_t wib = threadIdx.x >> 5;
+    const uint32_t lane = lane_id();
     uint32_t *cand = smem + wib * (32u * 32u * WPL + 32u * WPL);
     uint32_t *rowbuf = cand + 32u * 32u * WPL;
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t *S = a.scratch + gw * a.words_per_warp;
-    unsigned long long ntasks = a.ntasks;
+    unsigned long long *qc = a.qctl;
+    const bool handoff = a.spill_cycles != 0;
+    unsigned long long n = a.ntasks;
     if (a.ntasks_dev) {
-        ntasks = *a.ntasks_dev;
-        if (ntasks > a.deferred_cap) ntasks = a.deferred_cap;
+        n = *a.ntasks_dev;
+        if (n > a.deferred_cap) n = a.deferred_cap;
     }
     for (;;) {
-        unsigned long long t0 = grab(a.head, a.chunk);
-        if (t0 >= ntasks) break;
-        unsigned long long t1 = t0 + a.chunk < ntasks ? t0 + a.chunk : ntasks;
-        for (unsigned long long t = t0; t < t1; t++) {
-            uint64_t task = a.task_index ? a.task_index[t] : t;
-            const long long c0 = clock64();
-            if (!mce_root<WPL, METRICS>(a, task, S, cand, rowbuf)) defer_root<WPL>(a, task);
-            else if (a.root_cost && lane_id() == 0) a.root_cost[task] = (uint64_t)(clock64() - c0);
+        if (handoff && lane == 0) {
+            atomicAdd(qc + kQOut, 1ull);
+            __threadfence();  // counted before the task is taken
         }
+        const unsigned long long t0 = grab(a.head, a.chunk);
+        if (t0 >= n) {
+            if (handoff && lane == 0) atomicAdd(qc + kQOut, ~0ull);  // -1
+            break;
+        }
+        const unsigned long long t1 = t0 + a.chunk < n ? t0 + a.chunk : n;
+        for (unsigned long long t = t0; t < t1; t++)
+            run_entry<WPL, METRICS>(a, a.task_index ? a.task_index[t] : (uint32_t)t, S, cand, rowbuf);
+        if (handoff && lane == 0) atomicAdd(qc + kQOut, ~0ull);
+    }
+    if (!handoff) return;
+    unsigned long long h = 0;
+    if (lane == 0) h = atomicAdd(qc + kQHead, 1ull);
+    h = __shfl_sync(G2_FULL, h, 0);
+    uint32_t sleep_ns = 32;
+    long long w0 = clock64();
+    for (;;) {
+        int action = 0;  // 0 wait, 1 run record h, 2 leave
+        if (lane == 0) {
+            if (h < a.rec_cap && vload32(a.ready + h) == a.epoch) {
+                action = 1;
+            } else {
+                __threadfence();  // whatever this warp saw taken was counted first
+                if (vload(qc + kQOut) == 0) action = 2;
+            }
+        }
+        action = __shfl_sync(G2_FULL, action, 0);
+        if (action == 1) {
+            __threadfence();
+            run_entry<WPL, METRICS>(a, kRecordBit | (uint32_t)h, S, cand, rowbuf);
+            if (lane == 0) {
+                atomicAdd(qc + kQOut, ~0ull);
+                h = atomicAdd(qc + kQHead, 1ull);
+            }
+            h = __shfl_sync(G2_FULL, h, 0);
+            sleep_ns = 32;
+            w0 = clock64();
+            continue;
+        }
+        if (action == 2) break;
+        if (clock64() - w0 > (long long)a.wait_cycles) {
+            if (lane == 0) atomicOr(a.status, kStatusWaitLimit);
+            break;
+        }
+        __nanosleep(sleep_ns);
+        sleep_ns = sleep_ns < 2048 ? sleep_ns * 2 : 2048;
     }
 }
 

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <atomic>
 #include <random>
 #include <string>
 #include <unordered_map>
@@ -47,7 +48,10 @@ struct g2_ctx {
     uint64_t tasks_cap = 0;
     uint64_t *d_root_nodes = nullptr, *d_root_cost = nullptr;
     uint64_t root_nodes_cap = 0, root_cost_cap = 0;
-    unsigned long long *d_ctr = nullptr;  // [0..3] queue heads, [4..6] deferred counts
+    unsigned long long *d_ctr = nullptr;  // kCtr* layout below
+    uint32_t *d_rec = nullptr;            // MCE hand-off records
+    uint32_t *d_ready = nullptr;          // their ready words
+    uint32_t *d_pool = nullptr;           // MCE spill row pool
     int *d_status = nullptr;
     unsigned long long *d_out = nullptr;  // counters for the host entry points
     uint64_t out_cap = 0;
@@ -77,6 +81,7 @@ struct g2_ctx {
     std::string cuda_err;
     uint64_t launches = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around the enumeration passes
+    uint32_t epoch = 0;  // MCE runs so far (ready word of their records)
     bool timed = false;
     unsigned long long *d_work = nullptr;
     cudaStream_t last_stream = nullptr;
@@ -253,15 +258,18 @@ int sort_keys(g2_ctx *ctx, uint64_t n, cudaStream_t st) {
 // learned model's features + MLP run here, in one kernel), optionally split
 // heavy roots, sort the tasks by descending cost.  No host synchronisation.
 int prepare_tasks(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, bool on_device, const g2_opts *o,
-                  uint64_t nwarps, cudaStream_t st, TaskList *tl) {
+                  uint64_t nwarps, cudaStream_t st, TaskList *tl, bool mce) {
     if (!sources) nsrc = ctx->n;
     const uint32_t sched = o ? o->schedule : G2_SCHED_GIVEN;
     const uint32_t flags = o ? o->flags : 0u;
     if (sched > G2_SCHED_LEARNED) return G2_ERR_INVALID;
     if (sched == G2_SCHED_SCORES && !(o && o->scores)) return G2_ERR_INVALID;
     if (sched == G2_SCHED_LEARNED && !ctx->d_model) return G2_ERR_INVALID;
+    // MCE balances inside roots by handing branches to idle warps, which split
+    // tasks cannot do: there the static split is only taken when asked for
     const bool split = nsrc > 0 && (sched == G2_SCHED_HEURISTIC || sched == G2_SCHED_LEARNED) &&
-                       ((flags & G2_FLAG_SPLIT) || (sched == G2_SCHED_LEARNED && !(flags & G2_FLAG_NO_SPLIT)));
+                       ((flags & G2_FLAG_SPLIT) ||
+                        (!mce && sched == G2_SCHED_LEARNED && !(flags & G2_FLAG_NO_SPLIT)));
     // sum_i ceil(c_i / t) <= n + total / t = n + g * warps
     const uint32_t gran = (o && o->split_granularity) ? std::min<uint32_t>(o->split_granularity, 1024u) : 4u;
     const uint64_t cap = split ? nsrc + (uint64_t)gran * nwarps + 64 : nsrc;
@@ -374,8 +382,35 @@ int ensure_scratch(g2_ctx *ctx) {
     return G2_OK;
 }
 
+// Device counters: queue heads of the passes, deferred-list sizes, hand-off
+// record / pool allocation and the record queue.
+constexpr int kCtrHead = 0;    // 3 queue heads
+constexpr int kCtrDefer = 16;  // 3 deferred-list sizes
+constexpr int kCtrRec = 19;    // records reserved
+constexpr int kCtrPool = 20;   // pool units (64 words) used
+constexpr int kCtrQueue = 24;  // record queue: claimed, busy warps, idle warps
+constexpr int kCtrWords = 40;
+
+// Epoch of an MCE run: unique in the process and never 0, so a ready word left
+// in memory by an earlier run or context (buffers are reused by the allocator)
+// cannot match.
+uint32_t next_epoch() {
+    static std::atomic<uint32_t> counter{0};
+    uint32_t e;
+    do e = counter.fetch_add(1) + 1;
+    while (e == 0);
+    return e;
+}
+
+// MCE hand-off buffers and defaults.
+constexpr uint64_t kRecordBytes = 64ull << 20;  // records
+constexpr uint64_t kPoolBytes = 64ull << 20;    // rows of roots whose tasks handed off work
+constexpr uint64_t kMaxRecords = kRecordBytes / 32;  // slots at the smallest stride (8 words)
+constexpr uint32_t kSpillKcycles = 20;          // default check interval (x1000 SM cycles)
+constexpr uint64_t kWaitCycles = 1ull << 37;    // longest wait for a record (~70 s of SM clock)
+
 int ensure_counters(g2_ctx *ctx) {
-    if (!ctx->d_ctr) G2_TRY(cudaMalloc(&ctx->d_ctr, sizeof(unsigned long long) * 16));
+    if (!ctx->d_ctr) G2_TRY(cudaMalloc(&ctx->d_ctr, sizeof(unsigned long long) * kCtrWords));
     if (!ctx->d_status) G2_TRY(cudaMalloc(&ctx->d_status, sizeof(int)));
     return G2_OK;
 }
@@ -385,6 +420,7 @@ int status_to_code(int st) {
     if (st & g2::kStatusStackOverflow) return G2_ERR_OVERFLOW;
     if (st & g2::kStatusBadPlan) return G2_ERR_INVALID;
     if (st & g2::kStatusHistOverflow) return G2_ERR_HIST;
+    if (st & g2::kStatusWaitLimit) return G2_ERR_TIMEOUT;
     return G2_OK;
 }
 
@@ -392,8 +428,9 @@ int status_to_code(int st) {
 int prepare_flags(g2_ctx *ctx, uint32_t flags, cudaStream_t st) {
     ctx->timed = (flags & G2_FLAG_TIME_KERNELS) != 0;
     ctx->last_stream = st;
-    if (ctx->timed && !ctx->ev[0])
+    if (ctx->timed && !ctx->ev[0]) {
         for (auto &e : ctx->ev) G2_TRY(cudaEventCreate(&e));
+    }
     if (flags & G2_FLAG_WORK_MODEL) {
         if (!ctx->d_work) G2_TRY(cudaMalloc(&ctx->d_work, sizeof(unsigned long long)));
         G2_TRY(cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), st));
@@ -465,49 +502,90 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     rc = ensure_counters(ctx);
     if (rc) return rc;
     if (ctx->max_fwd > 32u * 32u * 8u) return G2_ERR_UNSUPPORTED;
-    G2_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(unsigned long long) * 16, st));
+    const uint32_t flags = o ? o->flags : 0u;
+    const bool spill = !(flags & G2_FLAG_NO_SPILL);
+    if (spill && !ctx->d_rec) {
+        G2_TRY(cudaMalloc(&ctx->d_rec, kRecordBytes));
+        G2_TRY(cudaMalloc(&ctx->d_pool, kPoolBytes));
+        G2_TRY(cudaMalloc(&ctx->d_ready, sizeof(uint32_t) * kMaxRecords));
+        // a ready word must never match a run's epoch by accident: a waiting warp
+        // polls the ready word of a slot before it is reserved
+        G2_TRY(cudaMemsetAsync(ctx->d_ready, 0, sizeof(uint32_t) * kMaxRecords, st));
+    }
+    G2_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(unsigned long long) * kCtrWords, st));
     G2_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
     G2_TRY(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long) * (1 + hist_len), st));
-    const uint32_t flags = o ? o->flags : 0u;
     rc = prepare_flags(ctx, flags, st);
     if (rc) return rc;
     const int wpb = default_warps(o);
     const int blocks = default_blocks(ctx, o, wpb);
-    // pass 1: every task, WPL=1, one slab per resident warp
-    // pass 2: deferred roots, 2 warps per SM, WPL for the widest root
-    // pass 3: what is still deferred, one warp owning the whole slab
+    // records hold rows of the WPL=1 main pass: at most 32 words
+    const uint32_t rec_words = std::min<uint32_t>((ctx->max_fwd + 31u) / 32u, 32u);
+    const uint32_t rec_stride = (4u + 3u * std::max<uint32_t>(rec_words, 1u) + 3u) & ~3u;
+    const uint64_t spill_cycles =
+        spill ? 1000ull * ((o && o->spill_kcycles) ? o->spill_kcycles : kSpillKcycles) : 0ull;
+    ctx->epoch = next_epoch();
+    g2::MceArgs base{};
+    base.rp = ctx->d_rp;
+    base.ci = ctx->d_ci;
+    base.fo = ctx->d_fo;
+    base.tasks = ctx->d_tasks;
+    base.task_part = tl.split ? ctx->d_part : nullptr;
+    base.split_depth = (o && o->split_depth) ? o->split_depth : 2u;
+    base.root_cost = d_root_cost;
+    base.hist_len = hist_len;
+    base.scratch = ctx->d_scratch;
+    base.out = d_out;
+    base.deferred_cap = ctx->tasks_cap;
+    base.root_nodes = d_root_nodes;
+    base.status = ctx->d_status;
+    base.work = (flags & G2_FLAG_WORK_MODEL) ? ctx->d_work : nullptr;
+    base.records = ctx->d_rec;
+    base.ready = ctx->d_ready;
+    base.nrec = ctx->d_ctr + kCtrRec;
+    base.rec_cap = spill ? std::min<uint64_t>(kRecordBytes / (4ull * rec_stride), g2::kRecordBit - 1u) : 0;
+    base.rec_stride = rec_stride;
+    base.rec_words = rec_words;
+    base.pool = ctx->d_pool;
+    base.npool = ctx->d_ctr + kCtrPool;
+    base.pool_cap = spill ? kPoolBytes / 4 : 0;
+    base.qctl = ctx->d_ctr + kCtrQueue;
+    base.epoch = ctx->epoch;
+    base.wait_cycles = kWaitCycles;
+    if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
+    {  // main pass: every task, WPL=1, one slab per resident warp; long walks
+       // hand branches to idle warps through the record queue
+        g2::MceArgs a = base;
+        a.head = ctx->d_ctr + kCtrHead;
+        a.chunk = (o && o->chunk) ? o->chunk : 1u;
+        a.words_per_warp = (ctx->scratch_words / ((uint64_t)blocks * wpb)) & ~63ull;
+        a.deferred = ctx->d_defer;
+        a.ndeferred = ctx->d_ctr + kCtrDefer;
+        a.spill_cycles = spill_cycles;
+        a.ntasks = tl.cap;
+        a.ntasks_dev = tl.split ? ctx->d_ntask : nullptr;
+        cudaError_t e = g2::mce_launch(1, a, blocks, wpb, st);
+        if (e != cudaSuccess) return fail_cuda(ctx, e, "mce_launch");
+        ctx->launches++;
+    }
+    if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[1], st));
+    // deferred entries: 2 warps per SM with WPL for the widest root, then one
+    // warp owning the whole slab; neither spills
     struct Pass {
         int blocks, wpb, wpl;
-    } passes[3] = {{blocks, wpb, 1}, {ctx->sm_count, 2, wpl_for(ctx->max_fwd)}, {1, 1, wpl_for(ctx->max_fwd)}};
-    for (int k = 0; k < 3; k++) {
-        g2::MceArgs a{};
-        a.rp = ctx->d_rp;
-        a.ci = ctx->d_ci;
-        a.fo = ctx->d_fo;
-        a.tasks = ctx->d_tasks;
-        a.task_part = tl.split ? ctx->d_part : nullptr;
-        a.root_cost = d_root_cost;
-        a.task_index = k == 0 ? nullptr : ctx->d_defer + (uint64_t)(k - 1) * ctx->tasks_cap;
-        a.ntasks = k == 0 ? tl.cap : 0;
-        a.ntasks_dev = k == 0 ? (tl.split ? ctx->d_ntask : nullptr) : ctx->d_ctr + 4 + (k - 1);
-        a.head = ctx->d_ctr + k;
-        a.chunk = k == 0 ? ((o && o->chunk) ? o->chunk : 2u) : 1u;
-        a.hist_len = hist_len;
-        a.scratch = ctx->d_scratch;
-        uint64_t nw = (uint64_t)passes[k].blocks * passes[k].wpb;
-        a.words_per_warp = (ctx->scratch_words / nw) & ~63ull;
-        a.out = d_out;
-        a.deferred = ctx->d_defer + (uint64_t)k * ctx->tasks_cap;
-        a.ndeferred = ctx->d_ctr + 4 + k;
-        a.deferred_cap = ctx->tasks_cap;
-        a.root_nodes = d_root_nodes;
-        a.status = ctx->d_status;
-        a.final_pass = k == 2;
-        a.work = (flags & G2_FLAG_WORK_MODEL) ? ctx->d_work : nullptr;
-        if (ctx->timed && k == 0) G2_TRY(cudaEventRecord(ctx->ev[0], st));
+    } passes[2] = {{ctx->sm_count, 2, wpl_for(ctx->max_fwd)}, {1, 1, wpl_for(ctx->max_fwd)}};
+    for (int k = 0; k < 2; k++) {
+        g2::MceArgs a = base;
+        a.task_index = ctx->d_defer + (uint64_t)k * ctx->tasks_cap;
+        a.ntasks_dev = ctx->d_ctr + kCtrDefer + k;
+        a.head = ctx->d_ctr + kCtrHead + 1 + k;
+        a.chunk = 1;
+        a.words_per_warp = (ctx->scratch_words / ((uint64_t)passes[k].blocks * passes[k].wpb)) & ~63ull;
+        a.deferred = ctx->d_defer + (uint64_t)(k + 1) * ctx->tasks_cap;
+        a.ndeferred = ctx->d_ctr + kCtrDefer + k + 1;
         cudaError_t e = g2::mce_launch(passes[k].wpl, a, passes[k].blocks, passes[k].wpb, st);
         if (e != cudaSuccess) return fail_cuda(ctx, e, "mce_launch");
-        if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[k + 1], st));
+        if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[k + 2], st));
         ctx->launches++;
     }
     return G2_OK;
@@ -527,7 +605,7 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
     if (rc) return rc;
     rc = ensure_counters(ctx);
     if (rc) return rc;
-    G2_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(unsigned long long) * 16, st));
+    G2_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(unsigned long long) * kCtrWords, st));
     G2_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
     G2_TRY(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
     const uint32_t flags = o ? o->flags : 0u;
@@ -607,6 +685,16 @@ int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms) {
     return G2_OK;
 }
 
+int g2_last_spill_stats(g2_ctx *ctx, uint64_t *records, uint64_t *pool_bytes) {
+    if (!ctx || !records || !pool_bytes || !ctx->d_ctr) return G2_ERR_INVALID;
+    unsigned long long h[2] = {0, 0};
+    G2_TRY(cudaStreamSynchronize(ctx->last_stream));
+    G2_TRY(cudaMemcpy(h, ctx->d_ctr + kCtrRec, sizeof(h), cudaMemcpyDeviceToHost));
+    *records = h[0];
+    *pool_bytes = h[1] * 64ull * 4ull;
+    return G2_OK;
+}
+
 int g2_last_work_bytes(g2_ctx *ctx, uint64_t *bytes) {
     if (!ctx || !bytes || !ctx->d_work) return G2_ERR_INVALID;
     unsigned long long h = 0;
@@ -647,7 +735,7 @@ int g2_close(g2_ctx *ctx) {
                     ctx->d_root_cost, ctx->d_ctr,  ctx->d_status,  ctx->d_out,    ctx->d_keys,       ctx->d_keys2,
                     ctx->d_roots,  ctx->d_S,       ctx->d_part,    ctx->d_xroots, ctx->d_xparts,     ctx->d_cost,
                     ctx->d_total,  ctx->d_ntask,   ctx->d_cub,     ctx->d_model,  ctx->d_work,
-                    ctx->d_feat};
+                    ctx->d_feat,   ctx->d_rec,     ctx->d_pool,    ctx->d_ready};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (auto &e : ctx->ev)
@@ -772,7 +860,7 @@ int g2_mce_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc, con
     cudaStream_t st = (cudaStream_t)stream;
     ctx->launches = 0;
     TaskList tl;
-    int rc = prepare_tasks(ctx, d_sources, nsrc, true, opts, mce_warps(ctx, opts), st, &tl);
+    int rc = prepare_tasks(ctx, d_sources, nsrc, true, opts, mce_warps(ctx, opts), st, &tl, true);
     if (rc) return rc;
     ctx->last_split = tl.split;
     ctx->last_cap = tl.cap;
@@ -792,7 +880,7 @@ int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opt
     if (opts) o2 = *opts;
     if (o2.work_bytes) o2.flags |= G2_FLAG_WORK_MODEL;
     TaskList tl;
-    int rc = prepare_tasks(ctx, sources, nsrc, false, &o2, mce_warps(ctx, &o2), st, &tl);
+    int rc = prepare_tasks(ctx, sources, nsrc, false, &o2, mce_warps(ctx, &o2), st, &tl, true);
     if (rc) return rc;
     if (!sources) nsrc = ctx->n;
     ctx->last_split = tl.split;
@@ -809,7 +897,7 @@ int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opt
     G2_TRY(cudaMemcpy(h.data(), ctx->d_out, sizeof(unsigned long long) * (1 + hl), cudaMemcpyDeviceToHost));
     G2_TRY(cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     unsigned long long ndef3 = 0;
-    G2_TRY(cudaMemcpy(&ndef3, ctx->d_ctr + 6, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    G2_TRY(cudaMemcpy(&ndef3, ctx->d_ctr + kCtrDefer + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
     if (ndef3) return G2_ERR_OVERFLOW;
     *count = h[0];
     if (hist)
@@ -832,7 +920,7 @@ int g2_match_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc, c
     cudaStream_t st = (cudaStream_t)stream;
     ctx->launches = 0;
     TaskList tl;
-    int rc = prepare_tasks(ctx, d_sources, nsrc, true, opts, match_warps(ctx, opts), st, &tl);
+    int rc = prepare_tasks(ctx, d_sources, nsrc, true, opts, match_warps(ctx, opts), st, &tl, false);
     if (rc) return rc;
     ctx->last_split = tl.split;
     ctx->last_cap = tl.cap;
@@ -850,7 +938,7 @@ int g2_match_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_o
     if (opts) o2 = *opts;
     if (o2.work_bytes) o2.flags |= G2_FLAG_WORK_MODEL;
     TaskList tl;
-    int rc = prepare_tasks(ctx, sources, nsrc, false, &o2, match_warps(ctx, &o2), st, &tl);
+    int rc = prepare_tasks(ctx, sources, nsrc, false, &o2, match_warps(ctx, &o2), st, &tl, false);
     if (rc) return rc;
     if (!sources) nsrc = ctx->n;
     ctx->last_split = tl.split;

@@ -37,8 +37,8 @@ class G2Opts(C.Structure):
         ("blocks", u32), ("warps_per_block", u32), ("schedule", u32),
         ("split_granularity", u32), ("scores", P(C.c_float)),
         ("root_nodes", P(u64)), ("work_bytes", P(u64)),
-        ("intersect_mode", u32), ("flags", u32), ("reserved0", u32), ("root_cost", P(u64)),
-        ("chunk", u32), ("reserved1", u32),
+        ("intersect_mode", u32), ("flags", u32), ("split_depth", u32), ("root_cost", P(u64)),
+        ("chunk", u32), ("spill_kcycles", u32),
     ]
 
 
@@ -69,6 +69,7 @@ def lib():
         "g2_last_launch_count": (u64, [C.c_void_p]),
         "g2_pass_time_ms": (i32, [C.c_void_p, i32, P(C.c_float)]),
         "g2_last_work_bytes": (i32, [C.c_void_p, P(u64)]),
+        "g2_last_spill_stats": (i32, [C.c_void_p, P(u64), P(u64)]),
         "g2_load_core": (i32, [C.c_void_p, C.c_void_p]),
         "g2_root_features": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p]),
         "g2_model_train": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, u32, u32, C.c_float, u64, C.c_void_p,

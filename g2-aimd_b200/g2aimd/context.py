@@ -16,7 +16,7 @@ import numpy as np
 from ._lib import G2_MAX_QUERY, G2Opts, G2Plan, check, lib
 
 SCHED = {"given": 0, "heuristic": 1, "scores": 2, "learned": 3}
-FLAG_TIME_KERNELS, FLAG_WORK_MODEL, FLAG_SPLIT, FLAG_NO_SPLIT = 1, 2, 4, 8
+FLAG_TIME_KERNELS, FLAG_WORK_MODEL, FLAG_SPLIT, FLAG_NO_SPLIT, FLAG_NO_SPILL = 1, 2, 4, 8, 16
 MODEL_FEATURES, MODEL_PARAMS, MODEL_NORM = 8, 4801, 18
 
 
@@ -75,8 +75,11 @@ class Plan:
 
 
 def _opts(warps_per_block=0, blocks=0, schedule="given", scores=None, root_nodes=None, intersect_mode=0,
-          granularity=0, chunk=0, flags=0, work_bytes=None, root_cost=None, split=False):
+          granularity=0, chunk=0, flags=0, work_bytes=None, root_cost=None, split=False, split_depth=0,
+          spill_kcycles=0):
     o = G2Opts()
+    o.split_depth = split_depth
+    o.spill_kcycles = spill_kcycles
     o.flags = flags | (FLAG_SPLIT if split else 0)
     o.chunk = chunk
     o.warps_per_block = warps_per_block
@@ -132,6 +135,21 @@ class Context:
 
     def launches(self) -> int:
         return int(lib().g2_last_launch_count(self._h))
+
+    def spill_stats(self):
+        """(records, pool bytes) the last MCE run handed from long walks to idle warps."""
+        r, b = C.c_uint64(), C.c_uint64()
+        self._check(lib().g2_last_spill_stats(self._h, C.byref(r), C.byref(b)), "g2_last_spill_stats")
+        return r.value, b.value
+
+    def pass_times(self):
+        """Device ms of the last run's passes (after a run with flags=1)."""
+        out = []
+        for k in range(3):
+            ms = C.c_float()
+            self._check(lib().g2_pass_time_ms(self._h, k, C.byref(ms)), "g2_pass_time_ms")
+            out.append(ms.value)
+        return out
 
     def _check(self, rc, where):
         if rc != 0:

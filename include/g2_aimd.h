@@ -97,7 +97,8 @@ typedef struct g2_plan {
 #define G2_SCHED_SCORES 2     /* descending caller scores                          */
 #define G2_SCHED_LEARNED 3    /* descending cost predicted on the device by the model
                                  set with g2_set_model (features + MLP fused into
-                                 task generation); heavy roots split by default  */
+                                 task generation); GMatch splits heavy roots by
+                                 default                                          */
 
 /*
  * Run options.  Zero-initialise and set what you need; 0 means "default".
@@ -116,11 +117,14 @@ typedef struct g2_opts {
     uint32_t intersect_mode;    /* GMatch: 0 auto (clique bitmap path when the plan is
                                    a clique), 1 generic plan-driven path only        */
     uint32_t flags;             /* G2_FLAG_* bits                                    */
-    uint32_t reserved0;
+    uint32_t split_depth;       /* MCE: a split root's tasks share out its subtrees
+                                   at this search-tree depth (0 = default 2)         */
     uint64_t *root_cost;        /* optional host out: SM cycles per source (summed
                                    over its split tasks)                            */
-    uint32_t chunk;             /* tasks taken per queue atomic (0 = 2 MCE, 4 match) */
-    uint32_t reserved1;
+    uint32_t chunk;             /* tasks taken per queue atomic (0 = 1 MCE, 4 match) */
+    uint32_t spill_kcycles;     /* MCE: every this many thousand SM cycles a walk
+                                   checks for idle warps and hands them the pending
+                                   branches of its shallowest open level (0 = 20)   */
 } g2_opts;
 
 /* g2_opts.flags */
@@ -130,8 +134,12 @@ typedef struct g2_opts {
                                     a root of estimated cost c becomes ceil(c / t)
                                     tasks (at most 256), t = total / (g x warps) with
                                     g = split_granularity; each task owns every k-th
-                                    top-level branch of its root                     */
-#define G2_FLAG_NO_SPLIT 8u      /* G2_SCHED_LEARNED without splitting               */
+                                    top-level branch of its root (GMatch) or every
+                                    k-th subtree at depth split_depth (MCE)          */
+#define G2_FLAG_NO_SPLIT 8u      /* GMatch G2_SCHED_LEARNED without splitting (MCE
+                                    splits only with G2_FLAG_SPLIT; its walks hand
+                                    branches to idle warps instead)                 */
+#define G2_FLAG_NO_SPILL 16u     /* MCE: no hand-off of branches to idle warps       */
 
 typedef struct g2_ctx g2_ctx;
 
@@ -212,6 +220,11 @@ int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms);
  * 4 x sum over partial embeddings of the back neighbours' degrees).
  * Synchronises the run's stream. */
 int g2_last_work_bytes(g2_ctx *ctx, uint64_t *bytes);
+
+/* Search-tree nodes the last MCE run handed from long walks to idle warps
+ * (records) and the bytes of root rows it moved to the record row pool.
+ * Synchronises the run's stream. */
+int g2_last_spill_stats(g2_ctx *ctx, uint64_t *records, uint64_t *pool_bytes);
 
 /*
  * Plan-driven count that allocates no memory (no counterpart in the reference,

@@ -105,3 +105,35 @@ def test_chung_lu_power_law(g2, orc, ctx):
     c, h, rn = ctx.mce(root_nodes=True, schedule="heuristic")
     _same((c, h), want, g.name)
     assert np.array_equal(rn, want["root_nodes"])
+
+
+def test_spilled_records_keep_results(g2, orc, ctx, c1_graph):
+    """Long tasks hand their pending branches to later waves as records (here
+    as early as possible: after 1000 SM cycles); count, histogram, per-root
+    tree size and the work model W stay the oracle's, with and without
+    spilling, and with a slab small enough to defer records."""
+    from g2aimd.context import Context
+    graphs = (c1_graph, g2.Graph.rmat(12, 16, seed=11).degeneracy_recoded(),
+              g2.Graph.chung_lu(1 << 15, 2.3, 16.0, seed=3).degeneracy_recoded())
+    for g in graphs:
+        ctx.load(g)
+        want = orc.mce(g, threads=8, per_root=True)
+        for kw in ({"spill_kcycles": 1}, {"spill_kcycles": 1, "schedule": "heuristic"}, {"flags": 16}):
+            c, h, rn = ctx.mce(root_nodes=True, **kw)
+            _same((c, h), want, (g.name, kw))
+            assert np.array_equal(rn, want["root_nodes"]), (g.name, kw)
+            records, pool = ctx.spill_stats()
+            if kw.get("flags") == 16:
+                assert records == 0 and pool == 0
+            else:
+                assert records > 0 and pool > 0, (g.name, kw)
+            w = np.zeros(1, np.uint64)
+            ctx.mce(work_bytes=w, **kw)
+            assert int(w[0]) == want["work"], (g.name, kw)
+    g = graphs[1]
+    want = orc.mce(g, threads=8, per_root=True)
+    with Context(0, scratch_bytes=32 << 20) as c:
+        c.load(g)
+        got = c.mce(root_nodes=True, spill_kcycles=1)
+        _same(got, want, "tiny-scratch-spill")
+        assert np.array_equal(got[2], want["root_nodes"])

@@ -101,6 +101,17 @@ def test_split_and_learned_schedules_keep_results(g2, orc, ctx):
         c, h, rn = ctx.mce(root_nodes=True, **kw)
         assert c == want["count"] and np.array_equal(h[:want["hist"].size], want["hist"][:h.size]), kw
         assert np.array_equal(rn, want["root_nodes"]), kw
+    # fine splits (up to 256 tasks per root) dealt out at several search-tree depths
+    w0 = np.zeros(1, np.uint64)
+    ctx.mce(flags=2, work_bytes=w0)
+    for depth in (1, 2, 3, 5):
+        kw = {"schedule": "heuristic", "split": True, "granularity": 512, "split_depth": depth}
+        c, h, rn = ctx.mce(root_nodes=True, **kw)
+        assert c == want["count"] and np.array_equal(h[:want["hist"].size], want["hist"][:h.size]), kw
+        assert np.array_equal(rn, want["root_nodes"]), kw
+        w = np.zeros(1, np.uint64)
+        ctx.mce(flags=2, work_bytes=w, **kw)
+        assert w[0] == w0[0], kw
     src = np.arange(1, g.n, 5, dtype=np.uint32)
     for q in (24, 2, 0):
         plan = Plan.preset(q)
