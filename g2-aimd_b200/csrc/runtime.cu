@@ -409,6 +409,17 @@ constexpr uint64_t kMaxRecords = kRecordBytes / 32;  // slots at the smallest st
 constexpr uint32_t kSpillKcycles = 20;          // default check interval (x1000 SM cycles)
 constexpr uint64_t kWaitCycles = 1ull << 37;    // longest wait for a record (~70 s of SM clock)
 
+int ensure_handoff(g2_ctx *ctx, cudaStream_t st) {
+    if (ctx->d_rec) return G2_OK;
+    G2_TRY(cudaMalloc(&ctx->d_rec, kRecordBytes));
+    G2_TRY(cudaMalloc(&ctx->d_pool, kPoolBytes));
+    G2_TRY(cudaMalloc(&ctx->d_ready, sizeof(uint32_t) * kMaxRecords));
+    // a ready word must never match a run's epoch by accident: a waiting warp
+    // polls the ready word of a slot before it is reserved
+    G2_TRY(cudaMemsetAsync(ctx->d_ready, 0, sizeof(uint32_t) * kMaxRecords, st));
+    return G2_OK;
+}
+
 int ensure_counters(g2_ctx *ctx) {
     if (!ctx->d_ctr) G2_TRY(cudaMalloc(&ctx->d_ctr, sizeof(unsigned long long) * kCtrWords));
     if (!ctx->d_status) G2_TRY(cudaMalloc(&ctx->d_status, sizeof(int)));
@@ -504,13 +515,9 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     if (ctx->max_fwd > 32u * 32u * 8u) return G2_ERR_UNSUPPORTED;
     const uint32_t flags = o ? o->flags : 0u;
     const bool spill = !(flags & G2_FLAG_NO_SPILL);
-    if (spill && !ctx->d_rec) {
-        G2_TRY(cudaMalloc(&ctx->d_rec, kRecordBytes));
-        G2_TRY(cudaMalloc(&ctx->d_pool, kPoolBytes));
-        G2_TRY(cudaMalloc(&ctx->d_ready, sizeof(uint32_t) * kMaxRecords));
-        // a ready word must never match a run's epoch by accident: a waiting warp
-        // polls the ready word of a slot before it is reserved
-        G2_TRY(cudaMemsetAsync(ctx->d_ready, 0, sizeof(uint32_t) * kMaxRecords, st));
+    if (spill) {
+        rc = ensure_handoff(ctx, st);
+        if (rc) return rc;
     }
     G2_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(unsigned long long) * kCtrWords, st));
     G2_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
@@ -682,6 +689,30 @@ int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms) {
     if (!ctx || !ms || pass < 0 || pass > 2 || !ctx->timed) return G2_ERR_INVALID;
     G2_TRY(cudaEventSynchronize(ctx->ev[pass + 1]));
     G2_TRY(cudaEventElapsedTime(ms, ctx->ev[pass], ctx->ev[pass + 1]));
+    return G2_OK;
+}
+
+int g2_reserve(g2_ctx *ctx, uint64_t max_sources) {
+    if (!ctx) return G2_ERR_INVALID;
+    G2_TRY(cudaSetDevice(ctx->device));
+    if (!max_sources) max_sources = ctx->n;
+    int rc = ensure_scratch(ctx);
+    if (!rc) rc = ensure_counters(ctx);
+    if (!rc) rc = ensure_handoff(ctx, nullptr);
+    if (rc) return rc;
+    if (max_sources) {
+        // tasks of an unsplit run plus the three deferred lists
+        uint64_t tc = ctx->tasks_cap;
+        rc = grow(ctx, ctx->d_tasks, tc, max_sources, "tasks");
+        if (rc) return rc;
+        if (tc != ctx->tasks_cap || !ctx->d_defer) {
+            if (ctx->d_defer) cudaFree(ctx->d_defer);
+            ctx->d_defer = nullptr;
+            G2_TRY(cudaMalloc(&ctx->d_defer, sizeof(uint32_t) * 3 * std::max<uint64_t>(tc, 1)));
+        }
+        ctx->tasks_cap = tc;
+    }
+    G2_TRY(cudaDeviceSynchronize());
     return G2_OK;
 }
 

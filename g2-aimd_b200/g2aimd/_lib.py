@@ -70,6 +70,7 @@ def lib():
         "g2_pass_time_ms": (i32, [C.c_void_p, i32, P(C.c_float)]),
         "g2_last_work_bytes": (i32, [C.c_void_p, P(u64)]),
         "g2_last_spill_stats": (i32, [C.c_void_p, P(u64), P(u64)]),
+        "g2_reserve": (i32, [C.c_void_p, u64]),
         "g2_load_core": (i32, [C.c_void_p, C.c_void_p]),
         "g2_root_features": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p]),
         "g2_model_train": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, u32, u32, C.c_float, u64, C.c_void_p,

@@ -108,6 +108,7 @@ class Context:
         self._h = C.c_void_p()
         check(lib().g2_open(device, scratch_bytes, C.byref(self._h)), "g2_open")
         self.graph = None
+        self.n = 0
 
     def close(self):
         if self._h:
@@ -136,6 +137,11 @@ class Context:
     def launches(self) -> int:
         return int(lib().g2_last_launch_count(self._h))
 
+    def reserve(self, max_sources: int = 0):
+        """Allocate the run buffers now (g2_reserve) instead of in the first run."""
+        self._check(lib().g2_reserve(self._h, max_sources), "g2_reserve")
+        return self
+
     def spill_stats(self):
         """(records, pool bytes) the last MCE run handed from long walks to idle warps."""
         r, b = C.c_uint64(), C.c_uint64()
@@ -160,12 +166,15 @@ class Context:
         self._check(lib().g2_load_csr(self._h, graph.row_ptrs.ctypes.data_as(C.c_void_p),
                                       graph.cols.ctypes.data_as(C.c_void_p), graph.n, graph.m), "g2_load_csr")
         self.graph = graph
+        self.n = graph.n
         return self
 
     def load_device(self, d_row_ptrs: int, d_cols: int, n: int, m: int):
         """Borrow a CSR already in device memory (raw device pointers)."""
         self._check(lib().g2_load_csr_device(self._h, C.c_void_p(d_row_ptrs), C.c_void_p(d_cols), n, m),
                     "g2_load_csr_device")
+        self.graph = None
+        self.n = n
         return self
 
     def set_plan(self, plan: Plan):

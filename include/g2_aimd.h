@@ -159,6 +159,13 @@ int g2_close(g2_ctx *ctx);
  * system/pipeline_executor.h:121-147).  The context keeps a device copy. */
 int g2_load_csr(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols,
                 uint64_t n, uint64_t m);
+/* Allocate the working buffers of runs over up to `max_sources` roots (0 = the
+ * loaded graph's n): DFS slabs, counters, task lists and the MCE hand-off
+ * record queue.  Optional; a run allocates what is missing.  Callers that time
+ * runs separately from set-up (as the reference's workers allocate their
+ * device buffers before the timed loop) call it once after loading. */
+int g2_reserve(g2_ctx *ctx, uint64_t max_sources);
+
 /* Borrow a CSR that already lives in device memory of this context's device.
  * The caller keeps it alive until the next load or g2_close. */
 int g2_load_csr_device(g2_ctx *ctx, const uint64_t *d_row_ptrs,

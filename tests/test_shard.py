@@ -1,0 +1,93 @@
+"""Root sharding over ranks (host logic of the multi-GPU path), checked with
+world_size-2 gloo process groups on the CPU.  The oracle stands in for each
+rank's device run; the shards, the cost balancing and the all-reduce of the
+count and the clique-size histogram are the library's."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from g2aimd.shard import shard
+
+
+def test_shards_partition_the_roots():
+    rng = np.random.default_rng(0)
+    for n in (0, 1, 7, 1000):
+        cost = rng.random(n) ** 4
+        for world in (1, 2, 3, 8):
+            for c in (None, cost):
+                parts = [shard(n, world, r, c) for r in range(world)]
+                allr = np.concatenate(parts) if parts else np.zeros(0)
+                assert np.array_equal(np.sort(allr), np.arange(n)), (n, world)
+                for p in parts:
+                    assert np.all(np.diff(p.astype(np.int64)) > 0)
+
+
+def test_cost_balanced_shards_are_balanced():
+    rng = np.random.default_rng(1)
+    cost = rng.pareto(1.5, 5000) + 0.01
+    world = 4
+    loads = [cost[shard(cost.size, world, r, cost)].sum() for r in range(world)]
+    # LPT: every rank within the largest single cost of the mean
+    assert max(loads) - min(loads) <= cost.max() + 1e-9
+    rr = [cost[shard(cost.size, world, r)].sum() for r in range(world)]
+    assert max(loads) <= max(rr) + 1e-9
+
+
+def test_bad_rank_rejected():
+    with pytest.raises(ValueError):
+        shard(10, 2, 2)
+    with pytest.raises(ValueError):
+        shard(10, 2, 0, cost=np.ones(3))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        import g2aimd
+        import orc
+        from g2aimd.context import Plan
+        from g2aimd.shard import allreduce_counts
+        g = g2aimd.Graph.er(300, 0.08, planted=2, planted_size=9, seed=5).degeneracy_recoded()
+        deg = g.degrees().astype(np.float64)
+        roots = shard(g.n, world, rank, cost=deg * deg)
+        part = orc.mce(g, roots=roots, hist_len=32)
+        c, h = allreduce_counts(part["count"], part["hist"])
+        plan = Plan.preset(24)
+        mc = orc.match(g, plan, roots=shard(g.n, world, rank))["count"]
+        m, _ = allreduce_counts(mc)
+        q.put((rank, c, h.tolist(), m))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_world2_sharded_counts(g2, orc):
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    g = g2.Graph.er(300, 0.08, planted=2, planted_size=9, seed=5).degeneracy_recoded()
+    want = orc.mce(g, hist_len=32)
+    from g2aimd.context import Plan
+    wm = orc.match(g, Plan.preset(24))["count"]
+    for rank, c, h, m in res:
+        assert c == want["count"], rank
+        assert np.array_equal(np.array(h, np.uint64), want["hist"]), rank
+        assert m == wm, rank
