@@ -43,8 +43,9 @@ UNIT = "4-clique matches/s"
 HIST = 256
 K4 = 24
 # DRAM bytes (read + write) of one main-pass launch of the headline kernel on the
-# default graph, from the ncu capture summarised in profiles/ (null until captured).
-TRAFFIC_K4_S20 = None
+# default graph (R-MAT s20 ef16, seed 1), from the ncu capture summarised in
+# profiles/match_kernel_k4_rmat_s20.md (dram__bytes_read.sum + dram__bytes_write.sum).
+TRAFFIC_K4_S20 = 257.954048e6 + 251.607040e6
 
 
 def parse():
@@ -272,7 +273,7 @@ def run_ours(a):
     if a.fixed:
         # the configuration the autotuner settles on for this workload (no splits, 4 warps per CTA)
         plain_ms, tuned, tlog = [float("nan")], {"flags": 1 | 8, "granularity": 64, "warps_per_block": 4,
-                                                 "chunk": 1}, []
+                                                 "chunk": 1, "ctas_per_sm": 6}, []
     else:
         # plain schedule: heuristic order, one task per root (no model, no splits)
         plain_ms, _ = timed(lambda: run(schedule="heuristic", flags=1), a.steps, a.warmup)
@@ -312,6 +313,10 @@ def run_ours(a):
         extras["schedules"]["heuristic_split_ms"] = float(np.mean(hs))
         gs, _ = timed(lambda: run(flags=1), 3, 1)
         extras["schedules"]["given_order_ms"] = float(np.mean(gs))
+        # the plain heuristic order with the tuned launch parameters: the schedule's own effect
+        launch = {k: v for k, v in tuned.items() if k in ("warps_per_block", "chunk", "ctas_per_sm")}
+        ps, _ = timed(lambda: run(schedule="heuristic", flags=1, **launch), 3, 1)
+        extras["schedules"]["plain_heuristic_tuned_launch_ms"] = float(np.mean(ps))
         # ---- triangles on the same graph (heuristic splits)
         ctx.set_plan(Plan.preset(0))
         tri_step = lambda: run(schedule="heuristic", **dict(tuned, flags=1))  # noqa: E731
@@ -402,7 +407,8 @@ def run_ours(a):
                        "k4_matches": k4, "l2": "512 MiB flush before every timed step",
                        "parallelism": f"dp{world} (one graph instance per rank)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": TRAFFIC_K4_S20,
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": TRAFFIC_K4_S20 if (a.scale, a.edge_factor, a.seed) == (20, 16, 1) else None,
                          "kernel": "match_kernel<1,0> (clique bitmap path), main pass", "kernel_ms": kern_ms,
                          "algorithmic_bytes": stream_bytes, "peak_kind": peak_kind,
                          "merge_model_bytes": work_bytes,

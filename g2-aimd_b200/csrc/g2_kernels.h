@@ -64,6 +64,9 @@ struct MceArgs {
 constexpr int kQHead = 0, kQOut = 1;
 
 size_t mce_smem_bytes(int wpl, int warps_per_block);
+// Resident CTAs per SM of the kernel a launch with these parameters runs (0 on error).
+int mce_blocks_per_sm(int wpl, int warps_per_block, bool metrics);
+int match_blocks_per_sm(int wpl, int warps_per_block, bool metrics, int ctas_per_sm);
 cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_block, cudaStream_t st);
 
 // Plan in device-friendly form: everything by POSITION.
@@ -113,7 +116,7 @@ struct MatchArgs {
 
 size_t match_smem_bytes(int wpl, int warps_per_block);
 cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block,
-                         cudaStream_t st, bool clique_path, int wpl);
+                         cudaStream_t st, bool clique_path, int wpl, int ctas_per_sm);
 
 // Learned root-cost model (costmodel.cu).
 size_t model_smem_bytes();

@@ -321,8 +321,11 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
     return true;
 }
 
-template <int WPL, bool METRICS>
-__global__ void __launch_bounds__(256) match_kernel(MatchArgs a, int clique_path) {
+// MINB: CTAs of 256 threads per SM the register budget is set for (4: 64
+// registers; 6: 40 registers and more resident warps, which pays on graphs
+// larger than L2 where the rows' loads wait on memory).
+template <int WPL, bool METRICS, int MINB>
+__global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int clique_path) {
     extern __shared__ uint32_t smem[];
     const uint32_t wib = threadIdx.x >> 5;
     uint32_t *rowbuf = smem + wib * (32u * WPL + 1024u * WPL);
@@ -361,25 +364,54 @@ size_t match_smem_bytes(int wpl, int warps_per_block) {
     return (size_t)warps_per_block * (32u * wpl + 1024u * wpl) * sizeof(uint32_t);
 }
 
-template <int WPL, bool M>
+template <int WPL, bool M, int MINB>
 static void launch_match(const MatchArgs &a, dim3 g, dim3 b, size_t sm, cudaStream_t st, int cp) {
-    cudaFuncSetAttribute(match_kernel<WPL, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    match_kernel<WPL, M><<<g, b, sm, st>>>(a, cp);
+    cudaFuncSetAttribute(match_kernel<WPL, M, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    match_kernel<WPL, M, MINB><<<g, b, sm, st>>>(a, cp);
+}
+
+template <int WPL, bool M, int MINB>
+static int match_occ(int warps_per_block) {
+    const size_t sm = match_smem_bytes(WPL, warps_per_block);
+    cudaFuncSetAttribute(match_kernel<WPL, M, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, match_kernel<WPL, M, MINB>, 32 * warps_per_block, sm) !=
+        cudaSuccess)
+        return 0;
+    return nb;
+}
+
+// The 40-register build exists for the hot case only: WPL 1, no metrics.
+static bool wide_budget(int wpl, bool metrics, int ctas_per_sm) { return ctas_per_sm == 6 && wpl == 1 && !metrics; }
+
+int match_blocks_per_sm(int wpl, int warps_per_block, bool metrics, int ctas_per_sm) {
+    if (wide_budget(wpl, metrics, ctas_per_sm)) return match_occ<1, false, 6>(warps_per_block);
+    switch (wpl) {
+        case 1: return metrics ? match_occ<1, true, 4>(warps_per_block) : match_occ<1, false, 4>(warps_per_block);
+        case 2: return metrics ? match_occ<2, true, 4>(warps_per_block) : match_occ<2, false, 4>(warps_per_block);
+        case 4: return metrics ? match_occ<4, true, 4>(warps_per_block) : match_occ<4, false, 4>(warps_per_block);
+        case 8: return metrics ? match_occ<8, true, 4>(warps_per_block) : match_occ<8, false, 4>(warps_per_block);
+        default: return 0;
+    }
 }
 
 cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block, cudaStream_t st,
-                         bool clique_path, int wpl) {
+                         bool clique_path, int wpl, int ctas_per_sm) {
     cudaError_t e = cudaMemcpyToSymbolAsync(c_plan, &plan, sizeof(DevPlan), 0, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
     size_t sm = match_smem_bytes(wpl, warps_per_block);
     dim3 g(blocks), b(32 * warps_per_block);
     const int cp = clique_path ? 1 : 0;
     const bool m = a.work != nullptr;
+    if (wide_budget(wpl, m, ctas_per_sm)) {
+        launch_match<1, false, 6>(a, g, b, sm, st, cp);
+        return cudaGetLastError();
+    }
     switch (wpl) {
-        case 1: m ? launch_match<1, true>(a, g, b, sm, st, cp) : launch_match<1, false>(a, g, b, sm, st, cp); break;
-        case 2: m ? launch_match<2, true>(a, g, b, sm, st, cp) : launch_match<2, false>(a, g, b, sm, st, cp); break;
-        case 4: m ? launch_match<4, true>(a, g, b, sm, st, cp) : launch_match<4, false>(a, g, b, sm, st, cp); break;
-        case 8: m ? launch_match<8, true>(a, g, b, sm, st, cp) : launch_match<8, false>(a, g, b, sm, st, cp); break;
+        case 1: m ? launch_match<1, true, 4>(a, g, b, sm, st, cp) : launch_match<1, false, 4>(a, g, b, sm, st, cp); break;
+        case 2: m ? launch_match<2, true, 4>(a, g, b, sm, st, cp) : launch_match<2, false, 4>(a, g, b, sm, st, cp); break;
+        case 4: m ? launch_match<4, true, 4>(a, g, b, sm, st, cp) : launch_match<4, false, 4>(a, g, b, sm, st, cp); break;
+        case 8: m ? launch_match<8, true, 4>(a, g, b, sm, st, cp) : launch_match<8, false, 4>(a, g, b, sm, st, cp); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -732,7 +732,7 @@ __device__ __forceinline__ void run_entry(const MceArgs &a, uint32_t entry, uint
 // The wait is bounded by wait_cycles; past that the warp flags the run and
 // leaves (its ticket's record, if one comes, would be lost: an error).
 template <int WPL, bool METRICS>
-__global__ void __launch_bounds__(256) mce_kernel(MceArgs a) {
+__global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
     extern __shared__ uint32_t smem[];
     const uint32_t wib = threadIdx.x >> 5;
     const uint32_t lane = lane_id();
@@ -811,6 +811,27 @@ template <int WPL, bool M>
 static void launch_one(const MceArgs &a, dim3 g, dim3 b, size_t sm, cudaStream_t st) {
     cudaFuncSetAttribute(mce_kernel<WPL, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     mce_kernel<WPL, M><<<g, b, sm, st>>>(a);
+}
+
+template <int WPL, bool M>
+static int mce_occ(int warps_per_block) {
+    const size_t sm = mce_smem_bytes(WPL, warps_per_block);
+    cudaFuncSetAttribute(mce_kernel<WPL, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mce_kernel<WPL, M>, 32 * warps_per_block, sm) !=
+        cudaSuccess)
+        return 0;
+    return nb;
+}
+
+int mce_blocks_per_sm(int wpl, int warps_per_block, bool metrics) {
+    switch (wpl) {
+        case 1: return metrics ? mce_occ<1, true>(warps_per_block) : mce_occ<1, false>(warps_per_block);
+        case 2: return metrics ? mce_occ<2, true>(warps_per_block) : mce_occ<2, false>(warps_per_block);
+        case 4: return metrics ? mce_occ<4, true>(warps_per_block) : mce_occ<4, false>(warps_per_block);
+        case 8: return metrics ? mce_occ<8, true>(warps_per_block) : mce_occ<8, false>(warps_per_block);
+        default: return 0;
+    }
 }
 
 cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_block, cudaStream_t st) {

@@ -156,6 +156,6 @@ extern "C" int g2_match_count_noalloc(const uint64_t *d_row_ptrs, const uint32_t
     a.words_per_warp = wpw;
     a.out = reinterpret_cast<unsigned long long *>(d_count);
     a.status = reinterpret_cast<int *>(S + 2);
-    if (g2::match_launch(dp, a, blocks, wpb, st, clique, 1) != cudaSuccess) return G2_ERR_CUDA;
+    if (g2::match_launch(dp, a, blocks, wpb, st, clique, 1, 0) != cudaSuccess) return G2_ERR_CUDA;
     return G2_OK;
 }

@@ -231,10 +231,11 @@ __global__ void gather_tasks_kernel(const uint64_t *keys_sorted, const uint32_t 
 
 int default_warps(const g2_opts *o) { return (o && o->warps_per_block) ? (int)o->warps_per_block : 8; }
 
-int default_blocks(g2_ctx *ctx, const g2_opts *o, int wpb) {
+// Persistent grid: the CTAs that are resident at once (occupancy of the kernel
+// the launch runs), so that no CTA waits for another to leave.
+int default_blocks(g2_ctx *ctx, const g2_opts *o, int wpb, int resident_per_sm) {
     if (o && o->blocks) return (int)o->blocks;
-    // persistent grid: resident CTAs per SM x SMs
-    int per_sm = std::max(1, 32 / wpb);
+    const int per_sm = resident_per_sm > 0 ? resident_per_sm : std::max(1, 32 / wpb);
     return ctx->sm_count * per_sm;
 }
 
@@ -525,7 +526,7 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     rc = prepare_flags(ctx, flags, st);
     if (rc) return rc;
     const int wpb = default_warps(o);
-    const int blocks = default_blocks(ctx, o, wpb);
+    const int blocks = default_blocks(ctx, o, wpb, g2::mce_blocks_per_sm(1, wpb, (flags & G2_FLAG_WORK_MODEL) != 0));
     // records hold rows of the WPL=1 main pass: at most 32 words
     const uint32_t rec_words = std::min<uint32_t>((ctx->max_fwd + 31u) / 32u, 32u);
     const uint32_t rec_stride = (4u + 3u * std::max<uint32_t>(rec_words, 1u) + 3u) & ~3u;
@@ -603,7 +604,8 @@ void match_geometry(g2_ctx *ctx, const g2_opts *o, int *wpl, int *wpb, int *bloc
     *wpl = wpl_for(ctx->max_fwd);
     *wpb = default_warps(o);
     while (*wpb > 1 && g2::match_smem_bytes(*wpl, *wpb) > 200 * 1024) *wpb /= 2;
-    *blocks = default_blocks(ctx, o, *wpb);
+    const bool metrics = o && (o->flags & G2_FLAG_WORK_MODEL);
+    *blocks = default_blocks(ctx, o, *wpb, g2::match_blocks_per_sm(*wpl, *wpb, metrics, o ? (int)o->ctas_per_sm : 0));
 }
 
 int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long long *d_out,
@@ -640,7 +642,7 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
     a.work = (flags & G2_FLAG_WORK_MODEL) ? ctx->d_work : nullptr;
     const bool clique = ctx->clique_plan && !(o && o->intersect_mode == 1);
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
-    cudaError_t e = g2::match_launch(ctx->plan, a, blocks, wpb, st, clique, wpl);
+    cudaError_t e = g2::match_launch(ctx->plan, a, blocks, wpb, st, clique, wpl, o ? (int)o->ctas_per_sm : 0);
     if (e != cudaSuccess) return fail_cuda(ctx, e, "match_launch");
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[1], st));
     ctx->launches++;
@@ -649,7 +651,8 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
 
 uint64_t mce_warps(g2_ctx *ctx, const g2_opts *o) {
     const int wpb = default_warps(o);
-    return (uint64_t)default_blocks(ctx, o, wpb) * wpb;
+    const bool metrics = o && (o->flags & G2_FLAG_WORK_MODEL);
+    return (uint64_t)default_blocks(ctx, o, wpb, g2::mce_blocks_per_sm(1, wpb, metrics)) * wpb;
 }
 
 uint64_t match_warps(g2_ctx *ctx, const g2_opts *o) {

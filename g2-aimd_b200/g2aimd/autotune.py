@@ -7,6 +7,8 @@ results never depend on:
   * warps per CTA       4 or 8 (the persistent grid keeps 32 warps per SM)
   * queue chunk         tasks taken per atomic on the device queue
   * intersection path   clique plans: bitmap (0) or generic plan interpreter (1)
+  * register budget     GMatch kernel built for 4 or 6 CTAs of 256 threads per SM
+  * MCE hand-off        check interval of walks for idle warps (bench's MCE space)
 Coordinate descent over that grid, one parameter at a time, starting from the
 library defaults; every candidate is run `reps` times and its best time kept.
 """
@@ -53,6 +55,7 @@ DEFAULT_SPACE = {
     "granularity": [4, 16, 64],
     "warps_per_block": [4, 8],
     "chunk": [1, 4, 16],
+    "ctas_per_sm": [4, 6],
 }
 
 

@@ -125,6 +125,10 @@ typedef struct g2_opts {
     uint32_t spill_kcycles;     /* MCE: every this many thousand SM cycles a walk
                                    checks for idle warps and hands them the pending
                                    branches of its shallowest open level (0 = 20)   */
+    uint32_t ctas_per_sm;       /* GMatch register budget, as CTAs of 256 threads per
+                                   SM: 0 or 4 (64 registers), 6 (40 registers, more
+                                   resident warps; pays on graphs larger than L2)   */
+    uint32_t reserved2;
 } g2_opts;
 
 /* g2_opts.flags */

@@ -31,6 +31,9 @@ def test_rmat_s13(g2, orc, ctx, q):
     want = orc.match(g, plan, threads=8)["count"]
     assert ctx.match(plan) == want
     assert ctx.match(plan, schedule="heuristic") == want
+    # the 40-register build of the kernel (6 CTAs of 256 threads per SM)
+    assert ctx.match(plan, schedule="heuristic", ctas_per_sm=6) == want
+    assert ctx.match(plan, ctas_per_sm=6, warps_per_block=4, intersect_mode=1) == want
 
 
 def test_raw_ids_and_sources(g2, orc, ctx):
