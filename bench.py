@@ -141,6 +141,79 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def c4_work_estimate(g):
+    """Host estimate of the plan walk's work for 4-vertex patterns rooted at a
+    vertex's forward neighbourhood: sum over roots v of |N+(v)| / 2 x the degree
+    sum of N+(v) (used to keep the 4-cycle / diamond legs bounded)."""
+    rp = g.row_ptrs.astype(np.int64)
+    deg = np.diff(rp)
+    src = np.repeat(np.arange(g.n), deg)
+    dst = g.cols.astype(np.int64)
+    fw = dst > src
+    pf = np.bincount(src[fw], minlength=g.n)
+    s1 = np.bincount(src[fw], weights=deg[dst[fw]], minlength=g.n)
+    return float((s1 * pf).sum() / 2)
+
+
+def c4_leg(Context, CostModel, Plan, models, local, seed, torch, stream):
+    """64 Chung-Lu graphs (n log-uniform in [1e3, 1e6], exponent in [2.1, 2.8],
+    average degree in [8, 40]): triangles over all of them, maximal cliques over
+    the ones of degeneracy <= 160 (the densest cores hold 5e9 to over 3e10
+    maximal cliques each), 4-cycles and diamonds over the ones whose estimated
+    walk is at most 1e9; each job is one launch over the batch (disjoint union),
+    compared with one run per graph."""
+    from g2aimd.graph import chung_lu_batch
+    t0 = time.perf_counter()
+    gs = chung_lu_batch(count=64, seed=seed)
+    gen_s = time.perf_counter() - t0
+    est = [c4_work_estimate(g) for g in gs]
+    light = [g for g, e in zip(gs, est) if e <= 1e9]
+    mce_set = [g for g in gs if int(g.core.max()) <= 160]
+
+    def ev_ms(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), r
+
+    jobs = [("triangle", 0, gs), ("mce", None, mce_set), ("4-cycle", 1, light), ("diamond", 2, light)]
+    out = {"graphs": len(gs), "vertices": int(sum(g.n for g in gs)), "directed_edges": int(sum(g.m for g in gs)),
+           "generation_s": round(gen_s, 1), "mce_graphs": len(mce_set), "mce_rule": "degeneracy <= 160",
+           "light_graphs": len(light), "light_rule": "estimated 4-vertex walk <= 1e9"}
+    with Context(local) as bc:
+        bc.set_model(CostModel.load(os.path.join(models, "mce.npz")))
+        loaded = None
+        for name, q, members in jobs:
+            if loaded is not members:
+                bc.batch_load(members)
+                bc.reserve()
+                loaded = members
+            run = (lambda: bc.batch_mce(schedule="learned")[0]) if q is None else \
+                (lambda q=q: bc.batch_match(Plan.preset(q), schedule="heuristic"))
+            run()
+            ms, counts = min((ev_ms(run) for _ in range(3)), key=lambda x: x[0])
+            out[name] = {"batched_ms": ms, "total": int(np.sum(counts)), "graphs": len(members)}
+        # one graph at a time: a load, then the same job, device time of the jobs only
+        for name, q, members in jobs:
+            tot, cnt = 0.0, 0
+            for g in members:
+                bc.load(g)
+                if q is None:
+                    bc.load_core(g.core)
+                run = (lambda: bc.mce(schedule="learned")[0]) if q is None else \
+                    (lambda q=q: bc.match(Plan.preset(q), schedule="heuristic"))
+                run()
+                ms, c = ev_ms(run)
+                tot += ms
+                cnt += int(c)
+            assert cnt == out[name]["total"], (name, cnt, out[name]["total"])
+            out[name]["per_graph_loop_ms"] = tot
+            out[name]["batched_vs_loop"] = tot / out[name]["batched_ms"]
+    return out
+
+
 def cpu_sample(g, target_s, threads, what="k4"):
     """The CPU restatement of the reference algorithm (oracle/g2_oracle.c) on a
     bounded random sample of roots, grown until it takes about target_s.
@@ -360,6 +433,8 @@ def run_ours(a):
             cs = cpu_sample(cl, a.cpu_sample_s / 2, os.cpu_count() or 1, what="mce")
             extras["mce_chung_lu"]["cpu_port_per_s"] = cs["value"]
         mctx.close()
+        # ---- a batch of 64 power-law graphs, one launch per job
+        extras["batch_chung_lu_64"] = c4_leg(Context, CostModel, Plan, models, local, a.seed + rank, torch, stream)
         # ---- end to end through the host ABI with pinned host buffers
         prp = torch.from_numpy(g.row_ptrs.view(np.int64)).pin_memory()
         pci = torch.from_numpy(g.cols.view(np.int32)).pin_memory()

@@ -44,6 +44,7 @@ struct MceArgs {
     unsigned long long *ndeferred;
     uint64_t deferred_cap;
     uint64_t *root_nodes;           // optional, per task id
+    uint64_t *root_cliques;         // optional: maximal cliques found per task id
     unsigned long long *work;       // optional: work model W in bytes (metrics kernel)
     int *status;
     // handed-off search-tree nodes (record: task, depth, pool offset / 64, nb,

@@ -696,6 +696,8 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
     if (lane == 0) {
         atomicAdd(a.out, cliques);
         if (a.root_nodes) atomicAdd(reinterpret_cast<unsigned long long *>(a.root_nodes + task), nodes);
+        if (a.root_cliques && cliques)
+            atomicAdd(reinterpret_cast<unsigned long long *>(a.root_cliques + task), cliques);
         if (METRICS) atomicAdd(a.work, work * 4ull);
     }
     for (uint32_t s = lane; s < p + 2; s += 32) {

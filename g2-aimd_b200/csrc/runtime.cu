@@ -82,6 +82,14 @@ struct g2_ctx {
     uint64_t launches = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around the enumeration passes
     uint32_t epoch = 0;  // MCE runs so far (ready word of their records)
+    // batch of graphs loaded as one disjoint union (g2_batch_load)
+    std::vector<uint64_t> batch_off;  // first vertex of each graph, then n
+    uint64_t *d_goff = nullptr;
+    uint64_t goff_cap = 0;
+    uint64_t *d_root_cliques = nullptr;
+    uint64_t root_cliques_cap = 0;
+    unsigned long long *d_gcount = nullptr;
+    uint64_t gcount_cap = 0;
     bool timed = false;
     unsigned long long *d_work = nullptr;
     cudaStream_t last_stream = nullptr;
@@ -227,6 +235,33 @@ __global__ void gather_tasks_kernel(const uint64_t *keys_sorted, const uint32_t 
         tasks[i] = roots[t];
         if (task_part) task_part[i] = parts ? parts[t] : (1u << 16);
     }
+}
+
+// Per-graph sums of per-task counts: graph of a task's root by binary search
+// over the batch's vertex offsets, partial sums in shared memory per CTA.
+constexpr uint32_t kMaxBatchGraphs = 4096;
+__global__ void segment_sum_kernel(const uint32_t *tasks, const uint64_t *per_task, uint64_t cap,
+                                   const unsigned long long *ntask_dev, const uint64_t *goff, uint32_t ngraphs,
+                                   unsigned long long *out) {
+    __shared__ unsigned long long part[kMaxBatchGraphs];
+    for (uint32_t g = threadIdx.x; g < ngraphs; g += blockDim.x) part[g] = 0ull;
+    __syncthreads();
+    const uint64_t n = ntask_dev ? (*ntask_dev < cap ? *ntask_dev : cap) : cap;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = per_task[t];
+        if (!c) continue;
+        const uint64_t v = tasks[t];
+        uint32_t lo = 0, hi = ngraphs;  // last g with goff[g] <= v
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (goff[mid] <= v) lo = mid;
+            else hi = mid;
+        }
+        atomicAdd(part + lo, (unsigned long long)c);
+    }
+    __syncthreads();
+    for (uint32_t g = threadIdx.x; g < ngraphs; g += blockDim.x)
+        if (part[g]) atomicAdd(out + g, part[g]);
 }
 
 int default_warps(const g2_opts *o) { return (o && o->warps_per_block) ? (int)o->warps_per_block : 8; }
@@ -508,7 +543,7 @@ int gather_root_outputs(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, uin
 
 // Enqueue the MCE passes; counters land in d_out.
 int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long long *d_out, uint32_t hist_len,
-                uint64_t *d_root_nodes, uint64_t *d_root_cost, cudaStream_t st) {
+                uint64_t *d_root_nodes, uint64_t *d_root_cost, cudaStream_t st, uint64_t *d_root_cliques = nullptr) {
     int rc = ensure_scratch(ctx);
     if (rc) return rc;
     rc = ensure_counters(ctx);
@@ -546,6 +581,7 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     base.out = d_out;
     base.deferred_cap = ctx->tasks_cap;
     base.root_nodes = d_root_nodes;
+    base.root_cliques = d_root_cliques;
     base.status = ctx->d_status;
     base.work = (flags & G2_FLAG_WORK_MODEL) ? ctx->d_work : nullptr;
     base.records = ctx->d_rec;
@@ -769,7 +805,8 @@ int g2_close(g2_ctx *ctx) {
                     ctx->d_root_cost, ctx->d_ctr,  ctx->d_status,  ctx->d_out,    ctx->d_keys,       ctx->d_keys2,
                     ctx->d_roots,  ctx->d_S,       ctx->d_part,    ctx->d_xroots, ctx->d_xparts,     ctx->d_cost,
                     ctx->d_total,  ctx->d_ntask,   ctx->d_cub,     ctx->d_model,  ctx->d_work,
-                    ctx->d_feat,   ctx->d_rec,     ctx->d_pool,    ctx->d_ready};
+                    ctx->d_feat,   ctx->d_rec,     ctx->d_pool,    ctx->d_ready,  ctx->d_goff,
+                    ctx->d_root_cliques, ctx->d_gcount};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (auto &e : ctx->ev)
@@ -781,6 +818,7 @@ int g2_close(g2_ctx *ctx) {
 static int after_load(g2_ctx *ctx) {
     int rc = grow(ctx, ctx->d_fo, ctx->fo_cap, std::max<uint64_t>(ctx->n, 1), "forward offsets");
     if (rc) return rc;
+    ctx->batch_off.clear();  // a batch load sets it again afterwards
     ctx->feat_valid = false;
     if (ctx->d_core) {  // core numbers belong to the previous graph
         cudaFree(ctx->d_core);
@@ -994,6 +1032,123 @@ int g2_match_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_o
     }
     rc = gather_root_outputs(ctx, sources, nsrc, o2.root_nodes, o2.root_cost);
     if (rc) return rc;
+    return status_to_code(status);
+}
+
+// ---------------------------------------------------------- batches of graphs
+
+int g2_batch_load(g2_ctx *ctx, const g2_batch_graph *graphs, uint32_t ngraphs) {
+    if (!ctx || (!graphs && ngraphs) || ngraphs > kMaxBatchGraphs) return G2_ERR_INVALID;
+    uint64_t n = 0, m = 0;
+    bool cores = ngraphs > 0;
+    for (uint32_t g = 0; g < ngraphs; g++) {
+        const g2_batch_graph &b = graphs[g];
+        if (!b.row_ptrs || (!b.cols && b.m) || b.row_ptrs[b.n] != b.m) return G2_ERR_INVALID;
+        n += b.n;
+        m += b.m;
+        cores = cores && b.core;
+    }
+    if (n >= (1ull << 32)) return G2_ERR_INVALID;
+    // the disjoint union: graph g's vertices are shifted by the vertices before it
+    std::vector<uint64_t> rp(n + 1), off(ngraphs + 1);
+    std::vector<uint32_t> ci(m ? m : 1), core(cores ? n : 0);
+    uint64_t v0 = 0, e0 = 0;
+    for (uint32_t g = 0; g < ngraphs; g++) {
+        const g2_batch_graph &b = graphs[g];
+        off[g] = v0;
+        for (uint64_t i = 0; i < b.n; i++) rp[v0 + i] = e0 + b.row_ptrs[i];
+        for (uint64_t e = 0; e < b.m; e++) ci[e0 + e] = (uint32_t)(v0 + b.cols[e]);
+        if (cores) std::copy(b.core, b.core + b.n, core.begin() + v0);
+        v0 += b.n;
+        e0 += b.m;
+    }
+    rp[n] = m;
+    off[ngraphs] = n;
+    int rc = g2_load_csr(ctx, rp.data(), ci.data(), n, m);
+    if (!rc && cores) rc = g2_load_core(ctx, core.data());
+    if (!rc) rc = grow(ctx, ctx->d_goff, ctx->goff_cap, ngraphs + 1, "batch offsets");
+    if (rc) return rc;
+    G2_TRY(cudaMemcpy(ctx->d_goff, off.data(), sizeof(uint64_t) * (ngraphs + 1), cudaMemcpyHostToDevice));
+    ctx->batch_off = off;
+    return G2_OK;
+}
+
+// Per-graph sums of the per-task counts of the last run into host `counts`.
+static int batch_counts(g2_ctx *ctx, const uint64_t *d_per_task, uint64_t *counts, cudaStream_t st) {
+    const uint32_t ng = (uint32_t)ctx->batch_off.size() - 1;
+    int rc = grow(ctx, ctx->d_gcount, ctx->gcount_cap, ng, "batch counts");
+    if (rc) return rc;
+    G2_TRY(cudaMemsetAsync(ctx->d_gcount, 0, sizeof(unsigned long long) * ng, st));
+    segment_sum_kernel<<<ctx->sm_count * 2, 512, 0, st>>>(ctx->d_tasks, d_per_task, ctx->last_cap,
+                                                          ctx->last_split ? ctx->d_ntask : nullptr, ctx->d_goff, ng,
+                                                          ctx->d_gcount);
+    ctx->launches++;
+    G2_TRY(cudaMemcpyAsync(counts, ctx->d_gcount, sizeof(uint64_t) * ng, cudaMemcpyDeviceToHost, st));
+    G2_TRY(cudaStreamSynchronize(st));
+    return G2_OK;
+}
+
+int g2_batch_mce(g2_ctx *ctx, const g2_opts *opts, uint64_t *counts, uint64_t *hist, uint32_t hist_len) {
+    if (!ctx || !counts || (hist && hist_len == 0)) return G2_ERR_INVALID;
+    if (ctx->batch_off.size() < 2) return G2_ERR_NO_GRAPH;
+    G2_TRY(cudaSetDevice(ctx->device));
+    ctx->launches = 0;
+    const uint32_t hl = hist ? hist_len : 0u;
+    cudaStream_t st = nullptr;
+    g2_opts o2{};
+    if (opts) o2 = *opts;
+    o2.root_nodes = o2.root_cost = nullptr;
+    o2.work_bytes = nullptr;
+    o2.flags &= ~G2_FLAG_WORK_MODEL;
+    TaskList tl;
+    int rc = prepare_tasks(ctx, nullptr, 0, false, &o2, mce_warps(ctx, &o2), st, &tl, true);
+    if (rc) return rc;
+    ctx->last_split = tl.split;
+    ctx->last_cap = tl.cap;
+    rc = grow(ctx, ctx->d_root_cliques, ctx->root_cliques_cap, ctx->tasks_cap, "root cliques");
+    if (!rc) rc = grow(ctx, ctx->d_out, ctx->out_cap, 1 + hl, "out");
+    if (rc) return rc;
+    G2_TRY(cudaMemsetAsync(ctx->d_root_cliques, 0, sizeof(uint64_t) * ctx->tasks_cap, st));
+    rc = mce_enqueue(ctx, tl, &o2, ctx->d_out, hl, nullptr, nullptr, st, ctx->d_root_cliques);
+    if (rc) return rc;
+    rc = batch_counts(ctx, ctx->d_root_cliques, counts, st);
+    if (rc) return rc;
+    std::vector<unsigned long long> h(1 + hl);
+    int status = 0;
+    unsigned long long ndef3 = 0;
+    G2_TRY(cudaMemcpy(h.data(), ctx->d_out, sizeof(unsigned long long) * (1 + hl), cudaMemcpyDeviceToHost));
+    G2_TRY(cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    G2_TRY(cudaMemcpy(&ndef3, ctx->d_ctr + kCtrDefer + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    if (ndef3) return G2_ERR_OVERFLOW;
+    if (hist)
+        for (uint32_t s = 0; s < hist_len; s++) hist[s] = h[1 + s];
+    return status_to_code(status);
+}
+
+int g2_batch_match(g2_ctx *ctx, const g2_opts *opts, uint64_t *counts) {
+    if (!ctx || !counts) return G2_ERR_INVALID;
+    if (ctx->batch_off.size() < 2) return G2_ERR_NO_GRAPH;
+    if (!ctx->has_plan) return G2_ERR_NO_PLAN;
+    G2_TRY(cudaSetDevice(ctx->device));
+    ctx->launches = 0;
+    cudaStream_t st = nullptr;
+    g2_opts o2{};
+    if (opts) o2 = *opts;
+    o2.root_nodes = o2.root_cost = nullptr;
+    o2.work_bytes = nullptr;
+    o2.flags &= ~G2_FLAG_WORK_MODEL;
+    TaskList tl;
+    int rc = prepare_tasks(ctx, nullptr, 0, false, &o2, match_warps(ctx, &o2), st, &tl, false);
+    if (rc) return rc;
+    ctx->last_split = tl.split;
+    ctx->last_cap = tl.cap;
+    rc = prepare_root_outputs(ctx, true, false, st);  // per-task counts
+    if (!rc) rc = grow(ctx, ctx->d_out, ctx->out_cap, 1, "out");
+    if (!rc) rc = match_enqueue(ctx, tl, &o2, ctx->d_out, ctx->d_root_nodes, nullptr, st);
+    if (!rc) rc = batch_counts(ctx, ctx->d_root_nodes, counts, st);
+    if (rc) return rc;
+    int status = 0;
+    G2_TRY(cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     return status_to_code(status);
 }
 

@@ -32,6 +32,10 @@ class G2Plan(C.Structure):
     ]
 
 
+class G2BatchGraph(C.Structure):
+    _fields_ = [("row_ptrs", P(u64)), ("cols", P(u32)), ("n", u64), ("m", u64), ("core", P(u32))]
+
+
 class G2Opts(C.Structure):
     _fields_ = [
         ("blocks", u32), ("warps_per_block", u32), ("schedule", u32),
@@ -71,6 +75,9 @@ def lib():
         "g2_last_work_bytes": (i32, [C.c_void_p, P(u64)]),
         "g2_last_spill_stats": (i32, [C.c_void_p, P(u64), P(u64)]),
         "g2_reserve": (i32, [C.c_void_p, u64]),
+        "g2_batch_load": (i32, [C.c_void_p, C.c_void_p, u32]),
+        "g2_batch_mce": (i32, [C.c_void_p, C.c_void_p, P(u64), P(u64), u32]),
+        "g2_batch_match": (i32, [C.c_void_p, C.c_void_p, P(u64)]),
         "g2_load_core": (i32, [C.c_void_p, C.c_void_p]),
         "g2_root_features": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p]),
         "g2_model_train": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, u32, u32, C.c_float, u64, C.c_void_p,

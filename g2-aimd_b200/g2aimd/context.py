@@ -138,6 +138,52 @@ class Context:
     def launches(self) -> int:
         return int(lib().g2_last_launch_count(self._h))
 
+    def batch_load(self, graphs):
+        """Load several graphs as one disjoint union (g2_batch_load); cores are
+        loaded too when every graph has them (degeneracy_recoded graphs do)."""
+        from ._lib import G2BatchGraph
+        arr = (G2BatchGraph * len(graphs))()
+        keep = []
+        for i, g in enumerate(graphs):
+            rp = np.ascontiguousarray(g.row_ptrs, dtype=np.uint64)
+            ci = np.ascontiguousarray(g.cols, dtype=np.uint32)
+            core = getattr(g, "core", None)
+            keep += [rp, ci]
+            arr[i].row_ptrs = rp.ctypes.data_as(C.POINTER(C.c_uint64))
+            arr[i].cols = ci.ctypes.data_as(C.POINTER(C.c_uint32))
+            arr[i].n, arr[i].m = g.n, g.m
+            if core is not None:
+                core = np.ascontiguousarray(core, dtype=np.uint32)
+                keep.append(core)
+                arr[i].core = core.ctypes.data_as(C.POINTER(C.c_uint32))
+        self._check(lib().g2_batch_load(self._h, arr, len(graphs)), "g2_batch_load")
+        self.graph = None
+        self.n = int(sum(g.n for g in graphs))
+        self.batch = len(graphs)
+        del keep
+        return self
+
+    def batch_mce(self, hist_len=256, **kw):
+        """(maximal cliques per graph, size histogram of all) of the loaded batch."""
+        o, keep = _opts(**kw)
+        counts = np.zeros(self.batch, np.uint64)
+        hist = np.zeros(hist_len, np.uint64)
+        self._check(lib().g2_batch_mce(self._h, C.byref(o), counts.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                       hist.ctypes.data_as(C.POINTER(C.c_uint64)), hist_len), "g2_batch_mce")
+        del keep
+        return counts, hist
+
+    def batch_match(self, plan: Plan = None, **kw):
+        """Matches per graph of the loaded batch."""
+        if plan is not None:
+            self.set_plan(plan)
+        o, keep = _opts(**kw)
+        counts = np.zeros(self.batch, np.uint64)
+        self._check(lib().g2_batch_match(self._h, C.byref(o), counts.ctypes.data_as(C.POINTER(C.c_uint64))),
+                    "g2_batch_match")
+        del keep
+        return counts
+
     def reserve(self, max_sources: int = 0):
         """Allocate the run buffers now (g2_reserve) instead of in the first run."""
         self._check(lib().g2_reserve(self._h, max_sources), "g2_reserve")

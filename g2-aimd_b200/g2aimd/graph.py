@@ -162,3 +162,19 @@ class Graph:
         per = np.where(p > 0, 20 + 24 * deg + 4 * s, 20)
         return int(per.sum())
 
+
+
+def chung_lu_batch(count=64, seed=1, n_range=(10**3, 10**6), gamma_range=(2.1, 2.8), degree_range=(8.0, 40.0)):
+    """A batch of Chung-Lu power-law graphs, degeneracy-ordered: n log-uniform
+    in n_range, exponent uniform in gamma_range, average degree uniform in
+    degree_range, one seed per graph (all drawn from `seed`)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+        gamma = float(rng.uniform(*gamma_range))
+        deg = float(rng.uniform(*degree_range))
+        g = Graph.chung_lu(n, gamma, deg, seed=int(rng.integers(1, 2**31))).degeneracy_recoded()
+        g.spec = {"n": n, "gamma": gamma, "avg_degree": deg}
+        out.append(g)
+    return out

@@ -163,6 +163,28 @@ int g2_close(g2_ctx *ctx);
  * system/pipeline_executor.h:121-147).  The context keeps a device copy. */
 int g2_load_csr(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols,
                 uint64_t n, uint64_t m);
+/*
+ * Batches of small graphs (C4-style workloads).  g2_batch_load loads the
+ * graphs as one disjoint union (graph g's vertex i becomes off[g] + i), so one
+ * launch per job covers every graph: a maximal clique or a connected pattern
+ * lies inside one graph.  Per-graph results are summed on the device from the
+ * per-root counts.  Ids inside each graph should be in degeneracy order.
+ * At most 4096 graphs; the union must have fewer than 2^32 vertices.
+ */
+typedef struct g2_batch_graph {
+    const uint64_t *row_ptrs;  /* n + 1 entries, host memory */
+    const uint32_t *cols;      /* m entries */
+    uint64_t n, m;
+    const uint32_t *core;      /* optional core numbers (learned schedule); NULL in
+                                  any graph means none are loaded */
+} g2_batch_graph;
+
+int g2_batch_load(g2_ctx *ctx, const g2_batch_graph *graphs, uint32_t ngraphs);
+/* Maximal cliques per graph (counts[ngraphs]) and the size histogram of all. */
+int g2_batch_mce(g2_ctx *ctx, const g2_opts *opts, uint64_t *counts, uint64_t *hist, uint32_t hist_len);
+/* Matches of the plan set with g2_set_plan, per graph (counts[ngraphs]). */
+int g2_batch_match(g2_ctx *ctx, const g2_opts *opts, uint64_t *counts);
+
 /* Allocate the working buffers of runs over up to `max_sources` roots (0 = the
  * loaded graph's n): DFS slabs, counters, task lists and the MCE hand-off
  * record queue.  Optional; a run allocates what is missing.  Callers that time
