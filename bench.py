@@ -45,7 +45,7 @@ K4 = 24
 # DRAM bytes (read + write) of one main-pass launch of the headline kernel on the
 # default graph (R-MAT s20 ef16, seed 1), from the ncu capture summarised in
 # profiles/match_kernel_k4_rmat_s20.md (dram__bytes_read.sum + dram__bytes_write.sum).
-TRAFFIC_K4_S20 = 257.954048e6 + 251.607040e6
+TRAFFIC_K4_S20 = 859.611648e6 + 655.506176e6
 
 
 def parse():

@@ -740,9 +740,12 @@ int g2_reserve(g2_ctx *ctx, uint64_t max_sources) {
     if (!rc) rc = ensure_handoff(ctx, nullptr);
     if (rc) return rc;
     if (max_sources) {
-        // tasks of an unsplit run plus the three deferred lists
+        // tasks of a run with heavy-root splits at the default granularity (4)
+        // over the largest resident grid, the three deferred lists, the
+        // schedule's keys, costs and root lists, and the sort's scratch
+        const uint64_t cap = max_sources + 4ull * (uint64_t)ctx->sm_count * 64ull + 64ull;
         uint64_t tc = ctx->tasks_cap;
-        rc = grow(ctx, ctx->d_tasks, tc, max_sources, "tasks");
+        rc = grow(ctx, ctx->d_tasks, tc, cap, "tasks");
         if (rc) return rc;
         if (tc != ctx->tasks_cap || !ctx->d_defer) {
             if (ctx->d_defer) cudaFree(ctx->d_defer);
@@ -750,6 +753,22 @@ int g2_reserve(g2_ctx *ctx, uint64_t max_sources) {
             G2_TRY(cudaMalloc(&ctx->d_defer, sizeof(uint32_t) * 3 * std::max<uint64_t>(tc, 1)));
         }
         ctx->tasks_cap = tc;
+        rc = grow(ctx, ctx->d_roots, ctx->roots_cap, max_sources, "roots");
+        if (!rc) rc = grow(ctx, ctx->d_keys, ctx->keys_cap, cap, "keys");
+        if (!rc) rc = grow(ctx, ctx->d_keys2, ctx->keys2_cap, cap, "keys2");
+        if (!rc) rc = grow(ctx, ctx->d_cost, ctx->cost_cap, max_sources, "cost");
+        if (!rc && !ctx->d_total) rc = grow(ctx, ctx->d_total, ctx->total_cap, 2, "total");
+        if (!rc) rc = grow(ctx, ctx->d_S, ctx->S_cap, 2 * max_sources, "split counts");
+        if (!rc) rc = grow(ctx, ctx->d_part, ctx->part_cap, ctx->tasks_cap, "task parts");
+        if (!rc) rc = grow(ctx, ctx->d_xroots, ctx->xroots_cap, cap, "expanded roots");
+        if (!rc) rc = grow(ctx, ctx->d_xparts, ctx->xparts_cap, cap, "expanded parts");
+        if (!rc && !ctx->d_ntask) rc = grow(ctx, ctx->d_ntask, ctx->ntask_cap, 1, "task count");
+        if (rc) return rc;
+        size_t sort_need = 0, scan_need = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, sort_need, ctx->d_keys, ctx->d_keys2, (int)cap, 0, 64);
+        cub::DeviceScan::ExclusiveSum(nullptr, scan_need, ctx->d_S, ctx->d_S, (int)max_sources);
+        rc = cub_space(ctx, std::max(sort_need, scan_need));
+        if (rc) return rc;
     }
     G2_TRY(cudaDeviceSynchronize());
     return G2_OK;

@@ -10,7 +10,9 @@ results never depend on:
   * register budget     GMatch kernel built for 4 or 6 CTAs of 256 threads per SM
   * MCE hand-off        check interval of walks for idle warps (bench's MCE space)
 Coordinate descent over that grid, one parameter at a time, starting from the
-library defaults; every candidate is run `reps` times and its best time kept.
+library defaults and repeated until a full pass changes nothing (parameters
+interact: whether splitting pays depends on the register budget, for one);
+every candidate is run `reps` times and its best time kept.
 """
 from __future__ import annotations
 
@@ -29,7 +31,7 @@ def _time(torch, stream, fn, reps):
     return best
 
 
-def tune(run, base: dict, space: dict, reps: int = 2):
+def tune(run, base: dict, space: dict, reps: int = 2, max_passes: int = 3):
     """run(**opts) enqueues one enumeration on the current torch stream.
     Returns (best opts, best ms, log of (opts, ms))."""
     import torch
@@ -39,23 +41,30 @@ def tune(run, base: dict, space: dict, reps: int = 2):
     torch.cuda.synchronize()
     best_ms = _time(torch, stream, lambda: run(**cur), reps)
     log = [(dict(cur), best_ms)]
-    for key, values in space.items():
-        for v in values:
-            if cur.get(key) == v:
-                continue
-            cand = dict(cur, **{key: v})
-            ms = _time(torch, stream, lambda: run(**cand), reps)
-            log.append((cand, ms))
-            if ms < best_ms:
-                best_ms, cur = ms, cand
+    seen = {tuple(sorted(cur.items()))}
+    for _ in range(max_passes):
+        changed = False
+        for key, values in space.items():
+            for v in values:
+                cand = dict(cur, **{key: v})
+                sig = tuple(sorted(cand.items()))
+                if sig in seen:
+                    continue
+                seen.add(sig)
+                ms = _time(torch, stream, lambda: run(**cand), reps)
+                log.append((cand, ms))
+                if ms < best_ms:
+                    best_ms, cur, changed = ms, cand, True
+        if not changed:
+            break
     return cur, best_ms, log
 
 
 DEFAULT_SPACE = {
+    "ctas_per_sm": [4, 6],
     "granularity": [4, 16, 64],
     "warps_per_block": [4, 8],
     "chunk": [1, 4, 16],
-    "ctas_per_sm": [4, 6],
 }
 
 
