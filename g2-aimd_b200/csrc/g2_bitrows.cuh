@@ -85,7 +85,13 @@ __device__ __forceinline__ uint32_t smem_lower_bound(const uint32_t *a, uint32_t
     return lo;
 }
 
-constexpr uint32_t kLongList = 96;  // forward lists longer than this are scanned by the whole warp
+// Forward lists longer than this are scanned by the whole warp (coalesced, one
+// row at a time) instead of by their row's lane.  The lane loop runs as long as
+// the warp's longest list, so a lower bound balances lanes better; the walks of
+// clique plans gain from 32 (R-MAT s20 4-cliques 18.3 -> 17.3 ms), while MCE's
+// row builds (more, shorter rows per root) lose below 96.
+constexpr uint32_t kLongList = 96;
+constexpr uint32_t kLongListMatch = 32;
 
 // Adjacency rows of the root's forward neighbourhood.
 //   p0s   : P0 = N(v) ∩ (v, ∞) staged in shared memory (p sorted ids)
@@ -98,7 +104,7 @@ constexpr uint32_t kLongList = 96;  // forward lists longer than this are scanne
 // on, bits j > i) is built: enough for walks that only look above the row.
 __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo,
                                    const uint32_t *p0s, uint32_t p, uint32_t W, uint32_t *A, uint32_t *rowbuf,
-                                   bool symmetric = true) {
+                                   bool symmetric = true, uint32_t long_list = kLongList) {
     const uint32_t lane = lane_id();
     const uint32_t pmax = p0s[p - 1];
     if (symmetric)
@@ -114,7 +120,7 @@ __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const
             const uint32_t u = p0s[i];
             uint64_t e = ldg(rp + u) + ldg(fo + u);
             const uint64_t end = ldg(rp + u + 1);
-            if (end - e > kLongList) big = true;
+            if (end - e > long_list) big = true;
             else {
                 uint32_t *row = A + (uint64_t)i * W;
                 uint32_t j = i + 1;
@@ -177,7 +183,7 @@ __device__ __noinline__ static unsigned long long count_forward_edges(const uint
             const uint32_t u = p0s[i];
             uint64_t e = ldg(rp + u) + ldg(fo + u);
             const uint64_t end = ldg(rp + u + 1);
-            if (end - e > kLongList) big = true;
+            if (end - e > kLongListMatch) big = true;
             else {
                 uint32_t j = i + 1;
                 for (; e < end; e++) {

@@ -63,6 +63,7 @@ struct MceArgs {
     uint64_t wait_cycles;           // longest wait of a warp for its ticket's record
 };
 constexpr int kQHead = 0, kQOut = 1;
+constexpr uint32_t kMatchRecordWords = 32;  // stride of a plan-walk record
 
 size_t mce_smem_bytes(int wpl, int warps_per_block);
 // Resident CTAs per SM of the kernel a launch with these parameters runs (0 on error).
@@ -113,6 +114,17 @@ struct MatchArgs {
     uint64_t deferred_cap;
     uint64_t *root_nodes;           // optional: embeddings counted per task
     int *status;
+    // hand-off of pending plan-walk work to idle warps (g2_handoff.cuh); record:
+    // [task, level, kind, ncand, M[0..7], window pos (2), end (2), candidates (16)]
+    uint32_t *records;
+    uint32_t *ready;
+    unsigned long long *nrec;
+    uint64_t rec_cap;
+    uint32_t rec_stride;
+    unsigned long long *qctl;
+    uint32_t epoch;
+    uint64_t wait_cycles;
+    uint64_t spill_cycles;          // 0: no hand-off
 };
 
 size_t match_smem_bytes(int wpl, int warps_per_block);

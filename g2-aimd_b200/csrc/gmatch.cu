@@ -27,6 +27,7 @@
 
 #include "g2_bitrows.cuh"
 #include "g2_device.cuh"
+#include "g2_handoff.cuh"
 #include "g2_kernels.h"
 
 namespace g2 {
@@ -93,10 +94,104 @@ __device__ __forceinline__ bool cand_ok(const uint64_t *rp, const uint32_t *ci, 
     return true;
 }
 
-// Generic plan-driven walk of one root; returns the number of embeddings and
-// adds the work model (4 x back-neighbour degrees per partial embedding) to work.
-__device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v, uint32_t *S,
-                                                 unsigned long long &work, uint32_t part, uint32_t nparts) {
+// Record layout of a handed-off plan walk (kMatchRecordWords words): the walk
+// resumes at position `level` with M[0..level-1]; kind 0 (prefix) initialises
+// that level from the plan, kind 1 (window) scans only [pos, end) of its
+// parent's list, kind 2 (candidates) takes `ncand` already-filtered candidates.
+constexpr uint32_t kRecKind = 2, kRecN = 3, kRecM = 4, kRecPos = 12, kRecEnd = 14, kRecCand = 16;
+constexpr uint32_t kRecMaxCand = kMatchRecordWords - kRecCand;
+static_assert(kRecMaxCand >= 8, "record layout");
+enum : uint32_t { kRecPrefix = 0, kRecWindow = 1, kRecCandidates = 2 };
+
+__device__ __forceinline__ uint64_t ldcg64(const uint32_t *p) {
+    return (uint64_t)__ldcg(p) | ((uint64_t)__ldcg(p + 1) << 32);
+}
+
+// Write window records for [p0, p1) of position l in `pieces` equal parts.
+__device__ __forceinline__ void put_window(uint32_t *rec, uint32_t task, const uint32_t *M, uint32_t l, uint64_t p0,
+                                           uint64_t p1) {
+    rec[0] = task;
+    rec[1] = l;
+    rec[kRecKind] = kRecWindow;
+    rec[kRecN] = 0;
+    for (uint32_t j = 0; j < l; j++) rec[kRecM + j] = M[j];
+    rec[kRecPos] = (uint32_t)p0;
+    rec[kRecPos + 1] = (uint32_t)(p0 >> 32);
+    rec[kRecEnd] = (uint32_t)p1;
+    rec[kRecEnd + 1] = (uint32_t)(p1 >> 32);
+}
+
+// Hand half of the pending work of the shallowest open level (levels
+// base..i) with enough of it to idle warps and keep walking: the upper half of
+// its scan window (in up to 4 pieces) and the later half of its materialised
+// candidates (kRecMaxCand per record).  Returns false if nothing was handed off;
+// *full is set when the record buffer is exhausted.
+__device__ __noinline__ bool match_donate(const MatchArgs &a, uint32_t task, const uint32_t *M, Level *Ls,
+                                          uint32_t base, uint32_t i, uint32_t *S, uint32_t CH, bool *full) {
+    const uint32_t lane = lane_id();
+    uint32_t l = base;
+    for (; l <= i; l++)
+        if (Ls[l].len - Ls[l].idx >= 2 || Ls[l].end > Ls[l].pos + 64) break;
+    if (l > i) return false;
+    Level &L = Ls[l];
+    const uint64_t span = L.end > L.pos + 64 ? L.end - L.pos : 0;
+    const uint64_t wcut = L.pos + span / 2;  // the donor keeps [pos, wcut)
+    const uint32_t nw = span ? (uint32_t)((span / 2 + 4095u) / 4096u < 4u ? (span / 2 + 4095u) / 4096u : 4u) : 0u;
+    const uint32_t rc = L.len - L.idx;
+    const uint32_t dc = rc >= 2 ? rc / 2 : 0;  // candidates handed off: the last dc
+    const uint32_t nc = (dc + kRecMaxCand - 1) / kRecMaxCand;
+    if (nw + nc == 0) return false;
+    const unsigned long long k0 = reserve_records(a, nw + nc);
+    if (k0 == ~0ull) {
+        *full = true;
+        return false;
+    }
+    const uint32_t *buf = S + (uint64_t)(l - 1) * CH;
+    const uint32_t c0 = L.len - dc;
+    for (uint32_t r = lane; r < nw + nc; r += 32) {
+        uint32_t *rec = a.records + (k0 + r) * a.rec_stride;
+        if (r < nw) {
+            const uint64_t w = L.end - wcut;
+            put_window(rec, task, M, l, wcut + w * r / nw, wcut + w * (r + 1) / nw);
+        } else {
+            const uint32_t q = r - nw, first = c0 + q * kRecMaxCand;
+            const uint32_t cnt = dc - q * kRecMaxCand < kRecMaxCand ? dc - q * kRecMaxCand : kRecMaxCand;
+            rec[0] = task;
+            rec[1] = l;
+            rec[kRecKind] = kRecCandidates;
+            rec[kRecN] = cnt;
+            for (uint32_t j = 0; j < l; j++) rec[kRecM + j] = M[j];
+            for (uint32_t j = 0; j < cnt; j++) rec[kRecCand + j] = buf[first + j];
+        }
+    }
+    publish_records(a, k0, k0 + nw + nc);
+    if (span) L.end = wcut;
+    L.len -= dc;
+    return true;
+}
+
+// The last position's scan: hand the upper half of [e, end) to idle warps.
+__device__ __noinline__ bool match_donate_last(const MatchArgs &a, uint32_t task, const uint32_t *M, uint32_t l,
+                                               uint64_t e, Level &L, bool *full) {
+    if (L.end <= e + 1024) return false;
+    const uint64_t cut = e + (L.end - e) / 2;
+    const unsigned long long k0 = reserve_records(a, 1);
+    if (k0 == ~0ull) {
+        *full = true;
+        return false;
+    }
+    if (lane_id() == 0) put_window(a.records + k0 * a.rec_stride, task, M, l, cut, L.end);
+    publish_records(a, k0, k0 + 1);
+    L.end = cut;
+    return true;
+}
+
+// Generic plan-driven walk of a root (rec == nullptr: M[0] = v) or of a handed-off
+// record; returns the number of embeddings and adds the work model (4 x
+// back-neighbour degrees per partial embedding) to work.
+__device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, uint32_t task, uint32_t v,
+                                                     const uint32_t *rec, uint32_t *S, unsigned long long &work,
+                                                     uint32_t part, uint32_t nparts, long long c0) {
     const DevPlan &pl = c_plan;
     const uint32_t k = pl.k;
     const uint32_t lane = lane_id();
@@ -104,7 +199,6 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
     const uint32_t *ci = a.ci;
     uint32_t M[G2_MAX_QUERY];
     Level Ls[G2_MAX_QUERY];
-    M[0] = v;
     const uint32_t nlists = k > 2 ? k - 2 : 1;
     const uint32_t CH = (uint32_t)((a.words_per_warp / nlists) & ~31ull);
     unsigned long long count = 0;
@@ -112,15 +206,55 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
         if (lane == 0) atomicOr(a.status, kStatusStackOverflow);
         return 0;
     }
-    uint32_t i = 1;
+    uint32_t base = 1;
+    if (!rec) {
+        M[0] = v;
+        const uint64_t w1 = 4ull * level_init(rp, ci, M, 1, Ls[1]);
+        if (part == 0) work += w1;
+    } else {
+        // record words are read past L1 (two records share a cache line)
+        base = __ldcg(rec + 1);
+        const uint32_t kind = __ldcg(rec + kRecKind);
+        for (uint32_t j = 0; j < base; j++) M[j] = __ldcg(rec + kRecM + j);
+        const uint64_t d = level_init(rp, ci, M, base, Ls[base]);
+        if (kind == kRecPrefix) {
+            work += 4ull * d;  // this partial embedding's share is counted where it starts
+        } else if (kind == kRecWindow) {
+            Ls[base].pos = ldcg64(rec + kRecPos);
+            Ls[base].end = ldcg64(rec + kRecEnd);
+        } else {  // candidates already filtered: they are the level's chunk
+            const uint32_t n = __ldcg(rec + kRecN);
+            uint32_t *buf = S + (uint64_t)(base - 1) * CH;
+            for (uint32_t j = lane; j < n; j += 32) buf[j] = __ldcg(rec + kRecCand + j);
+            __syncwarp();
+            Ls[base].pos = Ls[base].end = 0;
+            Ls[base].len = n;
+            Ls[base].idx = 0;
+        }
+    }
+    uint32_t i = base;
     uint32_t ord = 0;  // ordinal of the next position-1 candidate (heavy-root split)
-    const uint64_t w1 = 4ull * level_init(rp, ci, M, 1, Ls[1]);
-    if (part == 0) work += w1;
+    bool may_spill = a.spill_cycles != 0 && nparts == 1;
+    long long next_check = (long long)a.spill_cycles;
     for (;;) {
         Level &L = Ls[i];
         if (i == k - 1) {
-            // last position: count, never materialise
+            // last position: count, never materialise (a long scan hands off its upper half)
+            uint32_t iter = 0;
             for (uint64_t e = L.pos; e < L.end; e += 32) {
+                if (may_spill && (++iter & 63u) == 0) {
+                    long long el = 0;
+                    if (lane == 0) el = clock64() - c0;
+                    el = __shfl_sync(G2_FULL, el, 0);
+                    if (el > next_check) {
+                        if (handoff_wanted(a)) {
+                            bool full = false;
+                            match_donate_last(a, task, M, i, e + 32, L, &full);
+                            if (full) may_spill = false;
+                        }
+                        next_check = el + (long long)a.spill_cycles;
+                    }
+                }
                 uint64_t x = e + lane;
                 bool ok = x < L.end && cand_ok(rp, ci, M, i, L.parent, ldg(ci + x));
                 uint32_t b = __ballot_sync(G2_FULL, ok);
@@ -132,14 +266,14 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
                 }
                 count += __popc(b);
             }
-            if (i == 1) break;
+            if (i == base) break;
             i--;
             continue;
         }
         uint32_t *buf = S + (uint64_t)(i - 1) * CH;
         if (L.idx == L.len) {
             if (L.pos >= L.end) {
-                if (i == 1) break;
+                if (i == base) break;
                 i--;
                 continue;
             }
@@ -163,6 +297,19 @@ __device__ unsigned long long match_root_generic(const MatchArgs &a, uint32_t v,
         M[i] = buf[L.idx];
         L.idx++;
         if (i == 1 && nparts > 1 && (ord++ % nparts) != part) continue;  // another part's candidate
+        if (may_spill) {  // every spill_cycles: hand work to idle warps
+            long long el = 0;
+            if (lane == 0) el = clock64() - c0;
+            el = __shfl_sync(G2_FULL, el, 0);
+            if (el > next_check) {
+                if (handoff_wanted(a)) {
+                    bool full = false;
+                    match_donate(a, task, M, Ls, base, i, S, CH, &full);
+                    if (full) may_spill = false;
+                }
+                next_check = el + (long long)a.spill_cycles;
+            }
+        }
         i++;
         work += 4ull * level_init(rp, ci, M, i, Ls[i]);
     }
@@ -251,12 +398,12 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
         // lane-parallel counting: lane takes the depth-1 vertices x = lane, lane+32, ...
         // (in ordinal order, so the split filter is x % nparts) and counts the
         // (k-2)-cliques above x serially; it reads only the upper part of rows.
-        build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf, false);
+        build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf, false, kLongListMatch);
         __syncwarp();
         count = clique_count_lanes(S + a0, p, W, k, part, nparts);
         return true;
     }
-    build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf);
+    build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf, true, kLongListMatch);
     __syncwarp();
     // C = remaining candidates at the current depth; depth = vertices chosen (v included)
     Row<WPL> C;
@@ -333,27 +480,51 @@ __global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int cliqu
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t *S = a.scratch + gw * a.words_per_warp;
     unsigned long long total = 0, work = 0;
+    const bool handoff = a.spill_cycles != 0;
     const unsigned long long ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
+    auto credit = [&](uint32_t task, unsigned long long c, long long c0) {
+        total += c;
+        if (lane_id() == 0) {
+            if (a.root_nodes && c) atomicAdd(reinterpret_cast<unsigned long long *>(a.root_nodes + task), c);
+            if (a.root_cost)
+                atomicAdd(reinterpret_cast<unsigned long long *>(a.root_cost + task),
+                          (unsigned long long)(clock64() - c0));
+        }
+    };
     for (;;) {
+        outstanding_add(a, handoff, 1);
         unsigned long long t0 = grab(a.head, a.chunk);
-        if (t0 >= ntasks) break;
+        if (t0 >= ntasks) {
+            outstanding_add(a, handoff, -1);
+            break;
+        }
         unsigned long long t1 = t0 + a.chunk < ntasks ? t0 + a.chunk : ntasks;
         for (unsigned long long t = t0; t < t1; t++) {
             const uint64_t task = a.task_index ? a.task_index[t] : t;
             const uint32_t v = a.tasks[task];
             const uint32_t tp = a.task_part ? a.task_part[task] : (1u << 16);
             const uint32_t nparts = tp >> 16, part = tp & 0xffffu;
-            const long long c0 = clock64();
+            long long c0 = 0;
+            if (lane_id() == 0) c0 = clock64();
+            c0 = __shfl_sync(G2_FULL, c0, 0);
             unsigned long long c = 0;
             if (!clique_path || !match_root_clique<WPL, METRICS>(a, v, S, p0s, rowbuf, c, work, part, nparts))
-                c = match_root_generic(a, v, S, work, part, nparts);
-            total += c;
-            if (lane_id() == 0) {
-                if (a.root_nodes) a.root_nodes[task] = c;
-                if (a.root_cost) a.root_cost[task] = (uint64_t)(clock64() - c0);
-            }
+                c = match_walk(a, (uint32_t)task, v, nullptr, S, work, part, nparts, c0);
+            credit((uint32_t)task, c, c0);
         }
+        outstanding_add(a, handoff, -1);
     }
+    if (handoff)
+        run_record_queue(a, [&](unsigned long long h) {
+            const uint32_t *rec = a.records + h * a.rec_stride;
+            if (__ldcg(rec + 1) == kVoidRecord) return;  // slot of a reservation that did not fit
+            long long c0 = 0;
+            if (lane_id() == 0) c0 = clock64();
+            c0 = __shfl_sync(G2_FULL, c0, 0);
+            const uint32_t task = __ldcg(rec);
+            const unsigned long long c = match_walk(a, task, 0u, rec, S, work, 0u, 1u, c0);
+            credit(task, c, c0);
+        });
     if (lane_id() == 0 && total) atomicAdd(a.out, total);
     if (METRICS && lane_id() == 0 && work) atomicAdd(a.work, work);
 }

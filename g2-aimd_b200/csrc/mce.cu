@@ -35,16 +35,13 @@
 
 #include "g2_bitrows.cuh"
 #include "g2_device.cuh"
+#include "g2_handoff.cuh"
 #include "g2_kernels.h"
 
 namespace g2 {
 
 namespace {
 
-__device__ __forceinline__ unsigned long long vload(const unsigned long long *p) {
-    return *reinterpret_cast<const volatile unsigned long long *>(p);
-}
-__device__ __forceinline__ uint32_t vload32(const uint32_t *p) { return *reinterpret_cast<const volatile uint32_t *>(p); }
 
 // slab frame per open level: P, X, Qr rows, list offset, list length, branch taken
 __device__ __forceinline__ uint32_t frame_words(uint32_t W) { return 3u * W + 3u; }
@@ -132,31 +129,6 @@ struct Rows {
 // epochs, whatever the record stride of earlier runs was).
 constexpr uint32_t kRecRows = 4;
 
-// Reserve n consecutive records with one atomic (no retries: many warps hand
-// off work at the same moment).  The slots that exist are added to the
-// outstanding count before any of them is published (the caller is itself
-// outstanding, so the count cannot touch zero meanwhile).  If the slots run
-// past the end of the buffer the ones below the end are published as void
-// (their ticket holders skip them) and ~0 is returned.
-__device__ __forceinline__ unsigned long long reserve_records(const MceArgs &a, uint32_t n) {
-    unsigned long long base = 0;
-    if (lane_id() == 0) {
-        base = atomicAdd(a.nrec, (unsigned long long)n);
-        const unsigned long long end = base + n < a.rec_cap ? base + n : a.rec_cap;
-        if (end > base) atomicAdd(a.qctl + kQOut, end - base);
-    }
-    base = __shfl_sync(G2_FULL, base, 0);
-    if (base + n <= a.rec_cap) return base;
-    for (unsigned long long i = base + lane_id(); i < a.rec_cap && i < base + n; i += 32)
-        a.records[i * a.rec_stride + 1] = kVoidRecord;
-    __syncwarp();
-    __threadfence();
-    for (unsigned long long i = base + lane_id(); i < a.rec_cap && i < base + n; i += 32)
-        *reinterpret_cast<volatile uint32_t *>(a.ready + i) = a.epoch;
-    __syncwarp();
-    return ~0ull;
-}
-
 // Rows of a root task go to the pool before its first records reference them.
 template <bool METRICS>
 __device__ bool ensure_pooled(const MceArgs &a, uint32_t p, uint32_t nb, uint32_t W, Rows &rows) {
@@ -217,15 +189,6 @@ __device__ unsigned long long emit_level(const MceArgs &a, unsigned long long k,
         row_assign_bit(Xl, q, true);
     }
     return k;
-}
-
-// Make records [k0, k1) visible to claimers: data first, then the ready words.
-__device__ __forceinline__ void publish(const MceArgs &a, unsigned long long k0, unsigned long long k1) {
-    __syncwarp();
-    __threadfence();
-    for (unsigned long long i = k0 + lane_id(); i < k1; i += 32)
-        *reinterpret_cast<volatile uint32_t *>(a.ready + i) = a.epoch;
-    __syncwarp();
 }
 
 // Pending-branch count of every frame level below d, as (first level with any, its count).
@@ -298,7 +261,7 @@ __device__ __noinline__ bool donate(const MceArgs &a, uint32_t task, uint32_t d0
         row_assign_bit(Ql, q0, false);
     }
     const unsigned long long k1 = emit_level<WPL>(a, k0, task, d0 + l + 1u, Pl, Xl, Ql, R, rows, nb, W);
-    publish(a, k0, k1);
+    publish_records(a, k0, k1);
     if (l < d) {
         Row<WPL> z;
         row_zero(z);
@@ -344,7 +307,7 @@ __device__ __noinline__ bool spill_all(const MceArgs &a, uint32_t task, uint32_t
             k = emit_level<WPL>(a, k, task, d0 + l + 1u, P, X, Qr, R, rows, nb, W);
         }
     }
-    publish(a, k0, k);
+    publish_records(a, k0, k);
     return true;
 }
 
@@ -484,7 +447,6 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
     bool donated = false;  // some branches went to records: the entry can no longer be re-run
     bool may_spill = a.spill_cycles != 0 && nparts == 1 && W <= a.rec_words;
     long long next_check = (long long)a.spill_cycles;
-    const unsigned long long *qc = a.qctl;
     for (;;) {
         bool want_pop = false;
         if (enter) {
@@ -597,10 +559,7 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
                     if (lane == 0) el = clock64() - c0;
                     el = __shfl_sync(G2_FULL, el, 0);
                     if (el > next_check) {
-                        // idle warps hold tickets past the last reserved record
-                        int want = 0;
-                        if (lane == 0) want = vload(qc + kQHead) > vload(a.nrec);
-                        if (__shfl_sync(G2_FULL, want, 0)) {
+                        if (handoff_wanted(a)) {  // idle warps hold tickets past the last record
                             bool full = false;
                             if (donate<WPL, METRICS>(a, task, d0, d, P, X, Qr, Rb, S + fr0, W, p, nb, rows, &full))
                                 donated = true;
@@ -725,24 +684,16 @@ __device__ __forceinline__ void run_entry(const MceArgs &a, uint32_t entry, uint
 }
 
 // Persistent pass.  Phase 1: entries from the task queue (or a deferred list).
-// Phase 2 (passes that hand off work): a warp takes a ticket (the index of the
-// next record, reserved or not yet) and runs that record once it is published.
-// kQOut counts the work that exists: warps holding queue tasks plus reserved,
-// unfinished records.  It is raised before work is published and lowered when
-// it is done, by warps that are themselves counted, so once it reads zero no
-// record can appear any more and a warp still waiting on a ticket leaves.
-// The wait is bounded by wait_cycles; past that the warp flags the run and
-// leaves (its ticket's record, if one comes, would be lost: an error).
+// Phase 2 (passes that hand off work): records through the ticket queue of
+// g2_handoff.cuh until no work is outstanding.
 template <int WPL, bool METRICS>
 __global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
     extern __shared__ uint32_t smem[];
     const uint32_t wib = threadIdx.x >> 5;
-    const uint32_t lane = lane_id();
     uint32_t *cand = smem + wib * (32u * 32u * WPL + 32u * WPL);
     uint32_t *rowbuf = cand + 32u * 32u * WPL;
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t *S = a.scratch + gw * a.words_per_warp;
-    unsigned long long *qc = a.qctl;
     const bool handoff = a.spill_cycles != 0;
     unsigned long long n = a.ntasks;
     if (a.ntasks_dev) {
@@ -750,57 +701,21 @@ __global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
         if (n > a.deferred_cap) n = a.deferred_cap;
     }
     for (;;) {
-        if (handoff && lane == 0) {
-            atomicAdd(qc + kQOut, 1ull);
-            __threadfence();  // counted before the task is taken
-        }
+        outstanding_add(a, handoff, 1);
         const unsigned long long t0 = grab(a.head, a.chunk);
         if (t0 >= n) {
-            if (handoff && lane == 0) atomicAdd(qc + kQOut, ~0ull);  // -1
+            outstanding_add(a, handoff, -1);
             break;
         }
         const unsigned long long t1 = t0 + a.chunk < n ? t0 + a.chunk : n;
         for (unsigned long long t = t0; t < t1; t++)
             run_entry<WPL, METRICS>(a, a.task_index ? a.task_index[t] : (uint32_t)t, S, cand, rowbuf);
-        if (handoff && lane == 0) atomicAdd(qc + kQOut, ~0ull);
+        outstanding_add(a, handoff, -1);
     }
-    if (!handoff) return;
-    unsigned long long h = 0;
-    if (lane == 0) h = atomicAdd(qc + kQHead, 1ull);
-    h = __shfl_sync(G2_FULL, h, 0);
-    uint32_t sleep_ns = 32;
-    long long w0 = clock64();
-    for (;;) {
-        int action = 0;  // 0 wait, 1 run record h, 2 leave
-        if (lane == 0) {
-            if (h < a.rec_cap && vload32(a.ready + h) == a.epoch) {
-                action = 1;
-            } else {
-                __threadfence();  // whatever this warp saw taken was counted first
-                if (vload(qc + kQOut) == 0) action = 2;
-            }
-        }
-        action = __shfl_sync(G2_FULL, action, 0);
-        if (action == 1) {
-            __threadfence();
+    if (handoff)
+        run_record_queue(a, [&](unsigned long long h) {
             run_entry<WPL, METRICS>(a, kRecordBit | (uint32_t)h, S, cand, rowbuf);
-            if (lane == 0) {
-                atomicAdd(qc + kQOut, ~0ull);
-                h = atomicAdd(qc + kQHead, 1ull);
-            }
-            h = __shfl_sync(G2_FULL, h, 0);
-            sleep_ns = 32;
-            w0 = clock64();
-            continue;
-        }
-        if (action == 2) break;
-        if (clock64() - w0 > (long long)a.wait_cycles) {
-            if (lane == 0) atomicOr(a.status, kStatusWaitLimit);
-            break;
-        }
-        __nanosleep(sleep_ns);
-        sleep_ns = sleep_ns < 2048 ? sleep_ns * 2 : 2048;
-    }
+        });
 }
 
 }  // namespace

@@ -439,7 +439,7 @@ uint32_t next_epoch() {
 }
 
 // MCE hand-off buffers and defaults.
-constexpr uint64_t kRecordBytes = 64ull << 20;  // records
+constexpr uint64_t kRecordBytes = 1ull << 30;   // records (8 M plan-walk records, 16 M+ MCE records)
 constexpr uint64_t kPoolBytes = 64ull << 20;    // rows of roots whose tasks handed off work
 constexpr uint64_t kMaxRecords = kRecordBytes / 32;  // slots at the smallest stride (8 words)
 constexpr uint32_t kSpillKcycles = 20;          // default check interval (x1000 SM cycles)
@@ -677,6 +677,21 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
     a.status = ctx->d_status;
     a.work = (flags & G2_FLAG_WORK_MODEL) ? ctx->d_work : nullptr;
     const bool clique = ctx->clique_plan && !(o && o->intersect_mode == 1);
+    // plan walks (non-clique plans) hand pending work to idle warps
+    if (!clique && !(flags & G2_FLAG_NO_SPILL)) {
+        rc = ensure_handoff(ctx, st);
+        if (rc) return rc;
+        ctx->epoch = next_epoch();
+        a.records = ctx->d_rec;
+        a.ready = ctx->d_ready;
+        a.nrec = ctx->d_ctr + kCtrRec;
+        a.rec_stride = g2::kMatchRecordWords;
+        a.rec_cap = std::min<uint64_t>(kRecordBytes / (4ull * a.rec_stride), g2::kRecordBit - 1u);
+        a.qctl = ctx->d_ctr + kCtrQueue;
+        a.epoch = ctx->epoch;
+        a.wait_cycles = kWaitCycles;
+        a.spill_cycles = 1000ull * ((o && o->spill_kcycles) ? o->spill_kcycles : kSpillKcycles);
+    }
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
     cudaError_t e = g2::match_launch(ctx->plan, a, blocks, wpb, st, clique, wpl, o ? (int)o->ctas_per_sm : 0);
     if (e != cudaSuccess) return fail_cuda(ctx, e, "match_launch");

@@ -122,9 +122,10 @@ typedef struct g2_opts {
     uint64_t *root_cost;        /* optional host out: SM cycles per source (summed
                                    over its split tasks)                            */
     uint32_t chunk;             /* tasks taken per queue atomic (0 = 1 MCE, 4 match) */
-    uint32_t spill_kcycles;     /* MCE: every this many thousand SM cycles a walk
-                                   checks for idle warps and hands them the pending
-                                   branches of its shallowest open level (0 = 20)   */
+    uint32_t spill_kcycles;     /* MCE and plan walks of non-clique plans: every this
+                                   many thousand SM cycles a walk checks for idle
+                                   warps and hands them the pending work of its
+                                   shallowest open level (0 = 20)                   */
     uint32_t ctas_per_sm;       /* GMatch register budget, as CTAs of 256 threads per
                                    SM: 0 or 4 (64 registers), 6 (40 registers, more
                                    resident warps; pays on graphs larger than L2)   */
@@ -143,7 +144,7 @@ typedef struct g2_opts {
 #define G2_FLAG_NO_SPLIT 8u      /* GMatch G2_SCHED_LEARNED without splitting (MCE
                                     splits only with G2_FLAG_SPLIT; its walks hand
                                     branches to idle warps instead)                 */
-#define G2_FLAG_NO_SPILL 16u     /* MCE: no hand-off of branches to idle warps       */
+#define G2_FLAG_NO_SPILL 16u     /* no hand-off of pending work to idle warps        */
 
 typedef struct g2_ctx g2_ctx;
 

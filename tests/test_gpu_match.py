@@ -70,3 +70,25 @@ def test_device_work_model_matches_oracle(g2, orc, ctx, q):
         w2 = np.zeros(1, np.uint64)
         assert ctx.match(plan, intersect_mode=1, work_bytes=w2) == want["count"]
         assert int(w2[0]) == want["work"]
+
+
+@pytest.mark.parametrize("q", [1, 2, 3, 9, 17])
+def test_plan_walk_handoff_keeps_counts(g2, orc, ctx, q):
+    """Plan walks hand pending work (window halves, candidate batches, last-level
+    scan halves) to idle warps; with hand-offs forced early (every 1000 SM
+    cycles) and switched off, per-root counts and the work model stay the
+    oracle's."""
+    from g2aimd.context import Plan
+    plan = Plan.preset(q)
+    g = g2.Graph.rmat(12, 16, seed=6).degeneracy_recoded()
+    ctx.load(g)
+    want = orc.match(g, plan, threads=8, per_root=True)
+    for kw in ({"spill_kcycles": 1}, {"spill_kcycles": 1, "schedule": "heuristic"}, {"flags": 16}):
+        rc = np.zeros(g.n, np.uint64)
+        assert ctx.match(plan, root_counts=rc, intersect_mode=1, **kw) == want["count"], (q, kw)
+        assert np.array_equal(rc, want["root_counts"]), (q, kw)
+        records, _ = ctx.spill_stats()
+        assert (records == 0) == (kw.get("flags") == 16), (q, kw, records)
+        w = np.zeros(1, np.uint64)
+        ctx.match(plan, work_bytes=w, intersect_mode=1, **kw)
+        assert int(w[0]) == want["work"], (q, kw)
