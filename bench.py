@@ -62,7 +62,32 @@ def parse():
     ap.add_argument("--scratch-mb", type=int, default=4096, help="device scratch for the DFS slabs")
     ap.add_argument("--fixed", action="store_true",
                     help="skip the plain-schedule timing and the autotuner (profiling runs)")
+    ap.add_argument("--leg", choices=["all", "mce"], default="all",
+                    help="mce: only the maximal-clique workload (Chung-Lu 2^18), for profiling")
     return ap.parse_args()
+
+
+def run_mce_leg(a):
+    """Maximal cliques on the Chung-Lu graph (n = 2^18, gamma 2.3, average degree
+    16) with hand-off, W warm-up and K timed runs; one JSON line (device times)."""
+    import torch
+
+    import g2aimd
+    from g2aimd.context import Context
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = g2aimd.Graph.chung_lu(1 << 18, 2.3, 16.0, seed=a.seed).degeneracy_recoded()
+    with Context(0, a.scratch_mb << 20) as ctx:
+        ctx.load(g)
+        ctx.reserve()
+        for _ in range(a.warmup):
+            c, _h = ctx.mce(schedule="heuristic", flags=1)
+        times = []
+        for _ in range(a.steps):
+            c, _h = ctx.mce(schedule="heuristic", flags=1)
+            times.append(ctx.pass_times()[0])
+        print(json.dumps({"workload": "mce chung-lu n=2^18 gamma 2.3 avg degree 16", "maximal_cliques": int(c),
+                          "kernel_ms": times, "records": ctx.spill_stats()[0]}), flush=True)
 
 
 def dist_env():
@@ -501,6 +526,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.leg == "mce":
+        run_mce_leg(a)
     else:
         run_ours(a)
 

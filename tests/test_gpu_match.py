@@ -72,15 +72,15 @@ def test_device_work_model_matches_oracle(g2, orc, ctx, q):
         assert int(w2[0]) == want["work"]
 
 
-@pytest.mark.parametrize("q", [1, 2, 3, 9, 17])
-def test_plan_walk_handoff_keeps_counts(g2, orc, ctx, q):
+@pytest.mark.parametrize("q,scale,ef", [(1, 12, 16), (2, 12, 16), (3, 10, 8), (9, 10, 8), (17, 9, 8)])
+def test_plan_walk_handoff_keeps_counts(g2, orc, ctx, q, scale, ef):
     """Plan walks hand pending work (window halves, candidate batches, last-level
     scan halves) to idle warps; with hand-offs forced early (every 1000 SM
     cycles) and switched off, per-root counts and the work model stay the
     oracle's."""
     from g2aimd.context import Plan
     plan = Plan.preset(q)
-    g = g2.Graph.rmat(12, 16, seed=6).degeneracy_recoded()
+    g = g2.Graph.rmat(scale, ef, seed=6).degeneracy_recoded()  # oracle sized to seconds
     ctx.load(g)
     want = orc.match(g, plan, threads=8, per_root=True)
     for kw in ({"spill_kcycles": 1}, {"spill_kcycles": 1, "schedule": "heuristic"}, {"flags": 16}):
