@@ -185,14 +185,14 @@ def c4_leg(Context, CostModel, Plan, models, local, seed, torch, stream):
     average degree in [8, 40]): triangles over all of them, maximal cliques over
     the ones of degeneracy <= 160 (the densest cores hold 5e9 to over 3e10
     maximal cliques each), 4-cycles and diamonds over the ones whose estimated
-    walk is at most 1e9; each job is one launch over the batch (disjoint union),
+    walk is at most 1e10; each job is one launch over the batch (disjoint union),
     compared with one run per graph."""
     from g2aimd.graph import chung_lu_batch
     t0 = time.perf_counter()
     gs = chung_lu_batch(count=64, seed=seed)
     gen_s = time.perf_counter() - t0
     est = [c4_work_estimate(g) for g in gs]
-    light = [g for g, e in zip(gs, est) if e <= 1e9]
+    light = [g for g, e in zip(gs, est) if e <= 1e10]
     mce_set = [g for g in gs if int(g.core.max()) <= 160]
 
     def ev_ms(fn):
@@ -206,7 +206,7 @@ def c4_leg(Context, CostModel, Plan, models, local, seed, torch, stream):
     jobs = [("triangle", 0, gs), ("mce", None, mce_set), ("4-cycle", 1, light), ("diamond", 2, light)]
     out = {"graphs": len(gs), "vertices": int(sum(g.n for g in gs)), "directed_edges": int(sum(g.m for g in gs)),
            "generation_s": round(gen_s, 1), "mce_graphs": len(mce_set), "mce_rule": "degeneracy <= 160",
-           "light_graphs": len(light), "light_rule": "estimated 4-vertex walk <= 1e9"}
+           "light_graphs": len(light), "light_rule": "estimated 4-vertex walk <= 1e10"}
     with Context(local) as bc:
         bc.set_model(CostModel.load(os.path.join(models, "mce.npz")))
         loaded = None
