@@ -302,8 +302,8 @@ def run_ours(a):
 
     import g2aimd
     from g2aimd.autotune import DEFAULT_SPACE, tune
-    # learned schedule search: heavy-root splits on (flags 1) or off (1 | G2_FLAG_NO_SPLIT)
-    LEARNED_SPACE = dict({"flags": [1, 1 | 8]}, **DEFAULT_SPACE)
+    # flags: heavy-root splits on (1) or off (1 | 8), L2 persistence window (| 32)
+    LEARNED_SPACE = dict({"flags": [1, 1 | 8, 1 | 8 | 32, 1 | 32]}, **DEFAULT_SPACE)
     # MCE: hand-off check interval and queue chunk
     FLAG_NO_SPILL = 16
     MCE_SPACE = {"spill_kcycles": [5, 20, 100], "chunk": [1, 2], "warps_per_block": [4, 8]}
@@ -318,6 +318,10 @@ def run_ours(a):
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    # a created stream for everything timed: stream attributes (the L2 window
+    # option) apply to created streams, not to the legacy default stream
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     L = g2aimd.lib()
     models = os.path.join(ROOT, "g2-aimd_b200", "models")
     g, gen_s = make_graph(a.scale, a.edge_factor, a.seed + rank)
@@ -329,7 +333,6 @@ def run_ours(a):
     ctx.set_model(CostModel.load(os.path.join(models, "k4.npz")))
     out = torch.zeros(1 + HIST, dtype=torch.int64, device=dev)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
-    stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
     cur = {"ctx": ctx}
 

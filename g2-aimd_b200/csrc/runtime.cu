@@ -82,6 +82,11 @@ struct g2_ctx {
     uint64_t launches = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around the enumeration passes
     uint32_t epoch = 0;  // MCE runs so far (ready word of their records)
+    g2::MceArgs last_mce{};            // arguments of the last MCE enqueue (host-spill pass)
+    int last_mce_wpl = 1;
+    uint64_t host_spill_bytes = 1ull << 30;  // pinned host slab for roots no device slab holds
+    void *h_spill = nullptr;
+    uint64_t h_spill_bytes = 0;
     // batch of graphs loaded as one disjoint union (g2_batch_load)
     std::vector<uint64_t> batch_off;  // first vertex of each graph, then n
     uint64_t *d_goff = nullptr;
@@ -424,6 +429,7 @@ constexpr int kCtrHead = 0;    // 3 queue heads
 constexpr int kCtrDefer = 16;  // 3 deferred-list sizes
 constexpr int kCtrRec = 19;    // records reserved
 constexpr int kCtrPool = 20;   // pool units (64 words) used
+constexpr int kCtrSpillDefer = 21;  // entries the host-spill pass could not hold
 constexpr int kCtrQueue = 24;  // record queue: claimed, busy warps, idle warps
 constexpr int kCtrWords = 40;
 
@@ -541,6 +547,44 @@ int gather_root_outputs(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, uin
     return G2_OK;
 }
 
+// Optional L2 persistence window over the tail of the column array (the dense
+// core's adjacency: ids are in degeneracy order) for the launches enqueued
+// while it is set on the caller's stream.  The persisting-L2 limit it sets is a
+// resource limit of this process's CUDA context and ends with it.
+struct L2Window {
+    cudaStream_t st = nullptr;
+    bool on = false;
+    L2Window(g2_ctx *ctx, cudaStream_t s, uint32_t flags) : st(s) {
+        if (!(flags & G2_FLAG_L2_PERSIST) || !s || !ctx->m) return;
+        int max_win = 0, max_persist = 0;
+        if (cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, ctx->device) != cudaSuccess ||
+            cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, ctx->device) != cudaSuccess ||
+            max_win <= 0 || max_persist <= 0) {
+            cudaGetLastError();
+            return;
+        }
+        if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)max_persist) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        const uint64_t bytes = std::min<uint64_t>(ctx->m * 4ull, (uint64_t)max_win);
+        cudaStreamAttrValue v{};
+        v.accessPolicyWindow.base_ptr = reinterpret_cast<char *>(ctx->d_ci) + (ctx->m * 4ull - bytes);
+        v.accessPolicyWindow.num_bytes = bytes;
+        v.accessPolicyWindow.hitRatio = std::min(1.0f, (float)max_persist / (float)bytes);
+        v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        on = cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &v) == cudaSuccess;
+        if (!on) cudaGetLastError();
+    }
+    ~L2Window() {
+        if (!on) return;
+        cudaStreamAttrValue v{};
+        v.accessPolicyWindow.num_bytes = 0;
+        cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &v);
+    }
+};
+
 // Enqueue the MCE passes; counters land in d_out.
 int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long long *d_out, uint32_t hist_len,
                 uint64_t *d_root_nodes, uint64_t *d_root_cost, cudaStream_t st, uint64_t *d_root_cliques = nullptr) {
@@ -597,6 +641,7 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     base.epoch = ctx->epoch;
     base.wait_cycles = kWaitCycles;
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
+    L2Window l2(ctx, st, flags);
     {  // main pass: every task, WPL=1, one slab per resident warp; long walks
        // hand branches to idle warps through the record queue
         g2::MceArgs a = base;
@@ -632,7 +677,46 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
         if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[k + 2], st));
         ctx->launches++;
     }
+    ctx->last_mce = base;
+    ctx->last_mce_wpl = wpl_for(ctx->max_fwd);
     return G2_OK;
+}
+
+// After a synchronous MCE run: entries that no device slab held (deferred by the
+// single-warp pass) run once more with one warp whose slab is mapped pinned host
+// memory (g2_set_host_spill), adding to the same outputs.  The host memory is
+// pinned on first need.  Returns G2_ERR_OVERFLOW if entries remain.
+int mce_host_spill(g2_ctx *ctx, cudaStream_t st) {
+    unsigned long long left = 0;
+    G2_TRY(cudaMemcpy(&left, ctx->d_ctr + kCtrDefer + 2, sizeof(left), cudaMemcpyDeviceToHost));
+    if (!left) return G2_OK;
+    if (!ctx->host_spill_bytes || left > ctx->tasks_cap) return G2_ERR_OVERFLOW;
+    if (ctx->h_spill_bytes != ctx->host_spill_bytes) {
+        if (ctx->h_spill) cudaFreeHost(ctx->h_spill);
+        ctx->h_spill = nullptr;
+        ctx->h_spill_bytes = 0;
+        G2_TRY(cudaHostAlloc(&ctx->h_spill, ctx->host_spill_bytes, cudaHostAllocMapped));
+        ctx->h_spill_bytes = ctx->host_spill_bytes;
+    }
+    void *d = nullptr;
+    G2_TRY(cudaHostGetDevicePointer(&d, ctx->h_spill, 0));
+    g2::MceArgs a = ctx->last_mce;
+    a.scratch = static_cast<uint32_t *>(d);
+    a.words_per_warp = (ctx->h_spill_bytes / 4) & ~63ull;
+    a.task_index = ctx->d_defer + 2 * ctx->tasks_cap;
+    a.ntasks_dev = ctx->d_ctr + kCtrDefer + 2;
+    a.head = ctx->d_ctr + kCtrHead + 3;
+    a.chunk = 1;
+    a.deferred = ctx->d_defer;  // list 0 is free again
+    a.ndeferred = ctx->d_ctr + kCtrSpillDefer;
+    a.spill_cycles = 0;
+    G2_TRY(cudaMemsetAsync(a.head, 0, sizeof(unsigned long long), st));
+    G2_TRY(cudaMemsetAsync(a.ndeferred, 0, sizeof(unsigned long long), st));
+    cudaError_t e = g2::mce_launch(ctx->last_mce_wpl, a, 1, 1, st);
+    if (e != cudaSuccess) return fail_cuda(ctx, e, "mce_launch (host spill)");
+    ctx->launches++;
+    G2_TRY(cudaMemcpy(&left, a.ndeferred, sizeof(left), cudaMemcpyDeviceToHost));
+    return left ? G2_ERR_OVERFLOW : G2_OK;
 }
 
 // Persistent-grid geometry of the match kernel.
@@ -693,6 +777,7 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
         a.spill_cycles = 1000ull * ((o && o->spill_kcycles) ? o->spill_kcycles : kSpillKcycles);
     }
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
+    L2Window l2(ctx, st, flags);
     cudaError_t e = g2::match_launch(ctx->plan, a, blocks, wpb, st, clique, wpl, o ? (int)o->ctas_per_sm : 0);
     if (e != cudaSuccess) return fail_cuda(ctx, e, "match_launch");
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[1], st));
@@ -789,6 +874,12 @@ int g2_reserve(g2_ctx *ctx, uint64_t max_sources) {
     return G2_OK;
 }
 
+int g2_set_host_spill(g2_ctx *ctx, uint64_t bytes) {
+    if (!ctx || (bytes && bytes < (1u << 20))) return G2_ERR_INVALID;
+    ctx->host_spill_bytes = bytes;
+    return G2_OK;
+}
+
 int g2_last_spill_stats(g2_ctx *ctx, uint64_t *records, uint64_t *pool_bytes) {
     if (!ctx || !records || !pool_bytes || !ctx->d_ctr) return G2_ERR_INVALID;
     unsigned long long h[2] = {0, 0};
@@ -845,6 +936,7 @@ int g2_close(g2_ctx *ctx) {
         if (b) cudaFree(b);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    if (ctx->h_spill) cudaFreeHost(ctx->h_spill);
     delete ctx;
     return G2_OK;
 }
@@ -998,13 +1090,12 @@ int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opt
     rc = mce_enqueue(ctx, tl, &o2, ctx->d_out, hl, o2.root_nodes ? ctx->d_root_nodes : nullptr,
                      o2.root_cost ? ctx->d_root_cost : nullptr, st);
     if (rc) return rc;
+    rc = mce_host_spill(ctx, st);  // adds to the outputs: read them after it
+    if (rc) return rc;
     std::vector<unsigned long long> h(1 + hl);
     int status = 0;
     G2_TRY(cudaMemcpy(h.data(), ctx->d_out, sizeof(unsigned long long) * (1 + hl), cudaMemcpyDeviceToHost));
     G2_TRY(cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-    unsigned long long ndef3 = 0;
-    G2_TRY(cudaMemcpy(&ndef3, ctx->d_ctr + kCtrDefer + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-    if (ndef3) return G2_ERR_OVERFLOW;
     *count = h[0];
     if (hist)
         for (uint32_t s = 0; s < hist_len; s++) hist[s] = h[1 + s];
@@ -1144,16 +1235,13 @@ int g2_batch_mce(g2_ctx *ctx, const g2_opts *opts, uint64_t *counts, uint64_t *h
     if (rc) return rc;
     G2_TRY(cudaMemsetAsync(ctx->d_root_cliques, 0, sizeof(uint64_t) * ctx->tasks_cap, st));
     rc = mce_enqueue(ctx, tl, &o2, ctx->d_out, hl, nullptr, nullptr, st, ctx->d_root_cliques);
-    if (rc) return rc;
-    rc = batch_counts(ctx, ctx->d_root_cliques, counts, st);
+    if (!rc) rc = mce_host_spill(ctx, st);
+    if (!rc) rc = batch_counts(ctx, ctx->d_root_cliques, counts, st);
     if (rc) return rc;
     std::vector<unsigned long long> h(1 + hl);
     int status = 0;
-    unsigned long long ndef3 = 0;
     G2_TRY(cudaMemcpy(h.data(), ctx->d_out, sizeof(unsigned long long) * (1 + hl), cudaMemcpyDeviceToHost));
     G2_TRY(cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-    G2_TRY(cudaMemcpy(&ndef3, ctx->d_ctr + kCtrDefer + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-    if (ndef3) return G2_ERR_OVERFLOW;
     if (hist)
         for (uint32_t s = 0; s < hist_len; s++) hist[s] = h[1 + s];
     return status_to_code(status);

@@ -16,7 +16,7 @@ import numpy as np
 from ._lib import G2_MAX_QUERY, G2Opts, G2Plan, check, lib
 
 SCHED = {"given": 0, "heuristic": 1, "scores": 2, "learned": 3}
-FLAG_TIME_KERNELS, FLAG_WORK_MODEL, FLAG_SPLIT, FLAG_NO_SPLIT, FLAG_NO_SPILL = 1, 2, 4, 8, 16
+FLAG_TIME_KERNELS, FLAG_WORK_MODEL, FLAG_SPLIT, FLAG_NO_SPLIT, FLAG_NO_SPILL, FLAG_L2_PERSIST = 1, 2, 4, 8, 16, 32
 MODEL_FEATURES, MODEL_PARAMS, MODEL_NORM = 8, 4801, 18
 
 
@@ -183,6 +183,11 @@ class Context:
                     "g2_batch_match")
         del keep
         return counts
+
+    def set_host_spill(self, nbytes: int):
+        """Pinned host slab for MCE roots that no device slab holds (0: none)."""
+        self._check(lib().g2_set_host_spill(self._h, nbytes), "g2_set_host_spill")
+        return self
 
     def reserve(self, max_sources: int = 0):
         """Allocate the run buffers now (g2_reserve) instead of in the first run."""

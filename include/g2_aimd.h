@@ -145,6 +145,9 @@ typedef struct g2_opts {
                                     splits only with G2_FLAG_SPLIT; its walks hand
                                     branches to idle warps instead)                 */
 #define G2_FLAG_NO_SPILL 16u     /* no hand-off of pending work to idle warps        */
+#define G2_FLAG_L2_PERSIST 32u   /* device-stream runs: keep the tail of the column
+                                    array (the dense core's adjacency) persisting in
+                                    L2 during the enumeration launches               */
 
 typedef struct g2_ctx g2_ctx;
 
@@ -254,6 +257,13 @@ int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms);
  * 4 x sum over partial embeddings of the back neighbours' degrees).
  * Synchronises the run's stream. */
 int g2_last_work_bytes(g2_ctx *ctx, uint64_t *bytes);
+
+/* Size of the pinned, device-mapped host slab on which a synchronous MCE run
+ * (g2_mce_run, g2_batch_mce) walks the roots that no device slab holds, after
+ * the deferral passes (default 1 GiB, pinned on first need; 0 = none: such roots
+ * make the run return G2_ERR_OVERFLOW).  The device-stream entry points never
+ * spill to the host and return G2_ERR_OVERFLOW through their status instead. */
+int g2_set_host_spill(g2_ctx *ctx, uint64_t bytes);
 
 /* Search-tree nodes the last MCE run handed from long walks to idle warps
  * (records) and the bytes of root rows it moved to the record row pool.

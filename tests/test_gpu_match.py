@@ -92,3 +92,19 @@ def test_plan_walk_handoff_keeps_counts(g2, orc, ctx, q, scale, ef):
         w = np.zeros(1, np.uint64)
         ctx.match(plan, work_bytes=w, intersect_mode=1, **kw)
         assert int(w[0]) == want["work"], (q, kw)
+
+
+def test_l2_persistence_window_keeps_counts(g2, orc, ctx):
+    """The L2 persistence window (device-stream runs) changes nothing but cache policy."""
+    import torch
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(12, 16, seed=3).degeneracy_recoded()
+    ctx.load(g)
+    out = torch.zeros(1, dtype=torch.int64, device="cuda:0")
+    s = torch.cuda.Stream()  # the window is a stream attribute: not the legacy stream
+    for q in (24, 1):
+        plan = Plan.preset(q)
+        ctx.set_plan(plan)
+        ctx.match_device(out.data_ptr(), stream=s.cuda_stream, flags=32)
+        s.synchronize()
+        assert int(out[0].item()) == orc.match(g, plan, threads=8)["count"], q

@@ -137,3 +137,20 @@ def test_spilled_records_keep_results(g2, orc, ctx, c1_graph):
         got = c.mce(root_nodes=True, spill_kcycles=1)
         _same(got, want, "tiny-scratch-spill")
         assert np.array_equal(got[2], want["root_nodes"])
+
+
+def test_host_spill_pass(g2, orc):
+    """Raw R-MAT ids give roots whose rows and frames exceed a 256 KiB device
+    scratch even for one warp; they run on the pinned host slab and the results
+    stay the oracle's.  Without a host slab the run reports the overflow."""
+    from g2aimd.context import Context
+    g = g2.Graph.rmat(11, 16, seed=21)
+    want = orc.mce(g, threads=8, per_root=True)
+    with Context(0, scratch_bytes=256 << 10) as c:
+        c.load(g)
+        got = c.mce(root_nodes=True, flags=16)
+        _same(got, want, "host-spill")
+        assert np.array_equal(got[2], want["root_nodes"])
+        c.set_host_spill(0)
+        with pytest.raises(g2.G2Error):
+            c.mce(flags=16)
