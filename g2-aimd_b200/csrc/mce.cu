@@ -368,8 +368,11 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
     const uint64_t SW = a.words_per_warp;
     const uint32_t FR = frame_words(W);
     const uint64_t fr0 = SW >= (uint64_t)(p + 1) * FR ? SW - (uint64_t)(p + 1) * FR : 0;
-    unsigned long long *hist_local = reinterpret_cast<unsigned long long *>(S);
+    unsigned long long *hist_local = a.hist_dev ? a.hist_dev : reinterpret_cast<unsigned long long *>(S);
     const uint64_t a0 = 2ull * (p + 2);  // after the histogram
+    // nothing is written before the slab is known to hold the histogram and frames
+    // (a small slab's neighbours are other warps' slabs)
+    if (fr0 < a0 + 64) return kTaskDeferred;
     for (uint32_t s = lane; s < p + 2; s += 32) hist_local[s] = 0ull;
     Rows rows;
     uint32_t nb;

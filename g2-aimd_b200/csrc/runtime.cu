@@ -84,7 +84,7 @@ struct g2_ctx {
     uint32_t epoch = 0;  // MCE runs so far (ready word of their records)
     g2::MceArgs last_mce{};            // arguments of the last MCE enqueue (host-spill pass)
     int last_mce_wpl = 1;
-    uint64_t host_spill_bytes = 1ull << 30;  // pinned host slab for roots no device slab holds
+    uint64_t host_spill_bytes = 1ull << 30;  // managed slab for roots no device slab holds
     void *h_spill = nullptr;
     uint64_t h_spill_bytes = 0;
     // batch of graphs loaded as one disjoint union (g2_batch_load)
@@ -683,25 +683,30 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
 }
 
 // After a synchronous MCE run: entries that no device slab held (deferred by the
-// single-warp pass) run once more with one warp whose slab is mapped pinned host
-// memory (g2_set_host_spill), adding to the same outputs.  The host memory is
-// pinned on first need.  Returns G2_ERR_OVERFLOW if entries remain.
+// single-warp pass) run once more with one warp whose slab is managed memory of
+// g2_set_host_spill's size (allocated on first need; its pages move to the GPU
+// as they are touched and back to the host if device memory runs out), adding
+// to the same outputs.  Returns G2_ERR_OVERFLOW if entries remain.  (A slab in
+// mapped pinned host memory gave wrong results: lanes read rows and lists other
+// lanes wrote, and those host-memory writes were not reliably visible to them.)
 int mce_host_spill(g2_ctx *ctx, cudaStream_t st) {
     unsigned long long left = 0;
     G2_TRY(cudaMemcpy(&left, ctx->d_ctr + kCtrDefer + 2, sizeof(left), cudaMemcpyDeviceToHost));
     if (!left) return G2_OK;
     if (!ctx->host_spill_bytes || left > ctx->tasks_cap) return G2_ERR_OVERFLOW;
+    if (ctx->scratch_words < 2ull * (ctx->max_fwd + 2)) return G2_ERR_OVERFLOW;  // room for the histogram
     if (ctx->h_spill_bytes != ctx->host_spill_bytes) {
-        if (ctx->h_spill) cudaFreeHost(ctx->h_spill);
+        if (ctx->h_spill) cudaFree(ctx->h_spill);
         ctx->h_spill = nullptr;
         ctx->h_spill_bytes = 0;
-        G2_TRY(cudaHostAlloc(&ctx->h_spill, ctx->host_spill_bytes, cudaHostAllocMapped));
+        G2_TRY(cudaMallocManaged(&ctx->h_spill, ctx->host_spill_bytes));
         ctx->h_spill_bytes = ctx->host_spill_bytes;
     }
-    void *d = nullptr;
-    G2_TRY(cudaHostGetDevicePointer(&d, ctx->h_spill, 0));
     g2::MceArgs a = ctx->last_mce;
-    a.scratch = static_cast<uint32_t *>(d);
+    a.scratch = static_cast<uint32_t *>(ctx->h_spill);
+    // the root's clique-size counters stay in device memory (the idle device
+    // scratch): lane 0 counts there and every lane reads them at commit
+    a.hist_dev = reinterpret_cast<unsigned long long *>(ctx->d_scratch);
     a.words_per_warp = (ctx->h_spill_bytes / 4) & ~63ull;
     a.task_index = ctx->d_defer + 2 * ctx->tasks_cap;
     a.ntasks_dev = ctx->d_ctr + kCtrDefer + 2;
@@ -936,7 +941,7 @@ int g2_close(g2_ctx *ctx) {
         if (b) cudaFree(b);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
-    if (ctx->h_spill) cudaFreeHost(ctx->h_spill);
+    if (ctx->h_spill) cudaFree(ctx->h_spill);
     delete ctx;
     return G2_OK;
 }

@@ -185,7 +185,7 @@ class Context:
         return counts
 
     def set_host_spill(self, nbytes: int):
-        """Pinned host slab for MCE roots that no device slab holds (0: none)."""
+        """Managed spill slab for MCE roots no scratch slab holds (0: none)."""
         self._check(lib().g2_set_host_spill(self._h, nbytes), "g2_set_host_spill")
         return self
 

@@ -258,11 +258,12 @@ int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms);
  * Synchronises the run's stream. */
 int g2_last_work_bytes(g2_ctx *ctx, uint64_t *bytes);
 
-/* Size of the pinned, device-mapped host slab on which a synchronous MCE run
- * (g2_mce_run, g2_batch_mce) walks the roots that no device slab holds, after
- * the deferral passes (default 1 GiB, pinned on first need; 0 = none: such roots
- * make the run return G2_ERR_OVERFLOW).  The device-stream entry points never
- * spill to the host and return G2_ERR_OVERFLOW through their status instead. */
+/* Size of the spill slab on which a synchronous MCE run (g2_mce_run,
+ * g2_batch_mce) walks the roots that no slab of the context's scratch holds,
+ * after the deferral passes: managed memory (default 1 GiB, allocated on first
+ * need) whose pages live on the GPU while used and in host memory when device
+ * memory runs out; 0 = none: such roots make the run return G2_ERR_OVERFLOW.
+ * The device-stream entry points never spill and report G2_ERR_OVERFLOW. */
 int g2_set_host_spill(g2_ctx *ctx, uint64_t bytes);
 
 /* Search-tree nodes the last MCE run handed from long walks to idle warps
