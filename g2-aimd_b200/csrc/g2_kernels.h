@@ -45,8 +45,8 @@ struct MceArgs {
     uint64_t deferred_cap;
     uint64_t *root_nodes;           // optional, per task id
     uint64_t *root_cliques;         // optional: maximal cliques found per task id
-    unsigned long long *hist_dev;   // optional: per-root histogram in device memory (one warp
-                                    // whose slab is host memory) instead of the slab's head
+    unsigned long long *hist_dev;   // optional: per-root histogram here (a one-warp pass
+                                    // whose slab is the spill slab) instead of the slab's head
     unsigned long long *work;       // optional: work model W in bytes (metrics kernel)
     int *status;
     // handed-off search-tree nodes (record: task, depth, pool offset / 64, nb,

@@ -686,9 +686,9 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
 // single-warp pass) run once more with one warp whose slab is managed memory of
 // g2_set_host_spill's size (allocated on first need; its pages move to the GPU
 // as they are touched and back to the host if device memory runs out), adding
-// to the same outputs.  Returns G2_ERR_OVERFLOW if entries remain.  (A slab in
-// mapped pinned host memory gave wrong results: lanes read rows and lists other
-// lanes wrote, and those host-memory writes were not reliably visible to them.)
+// to the same outputs.  Returns G2_ERR_OVERFLOW if entries remain.  Managed
+// rather than mapped pinned memory: the walk's many small reads stay in device
+// memory while the slab is in use.
 int mce_host_spill(g2_ctx *ctx, cudaStream_t st) {
     unsigned long long left = 0;
     G2_TRY(cudaMemcpy(&left, ctx->d_ctr + kCtrDefer + 2, sizeof(left), cudaMemcpyDeviceToHost));
@@ -704,8 +704,7 @@ int mce_host_spill(g2_ctx *ctx, cudaStream_t st) {
     }
     g2::MceArgs a = ctx->last_mce;
     a.scratch = static_cast<uint32_t *>(ctx->h_spill);
-    // the root's clique-size counters stay in device memory (the idle device
-    // scratch): lane 0 counts there and every lane reads them at commit
+    // the root's clique-size counters go to the idle device scratch
     a.hist_dev = reinterpret_cast<unsigned long long *>(ctx->d_scratch);
     a.words_per_warp = (ctx->h_spill_bytes / 4) & ~63ull;
     a.task_index = ctx->d_defer + 2 * ctx->tasks_cap;
