@@ -39,6 +39,9 @@ struct g2_ctx {
     uint32_t *d_fo = nullptr;  // forward-list offsets
     uint64_t fo_cap = 0;
     uint32_t *d_core = nullptr;  // optional core numbers (cost-model feature)
+    bool core_loaded = false;    // d_core holds the loaded graph's core numbers
+    uint64_t rp_cap = 0, ci_cap = 0;       // owned CSR buffers (entries), reused by later loads
+    unsigned int *d_fwdmax = nullptr;      // max forward degree of a load
     uint64_t core_cap = 0;
     // work buffers
     uint32_t *d_scratch = nullptr;
@@ -114,6 +117,8 @@ int fail_cuda(g2_ctx *c, cudaError_t e, const char *where) {
         cudaError_t _e = (call);                                 \
         if (_e != cudaSuccess) return fail_cuda(ctx, _e, #call); \
     } while (0)
+
+const uint32_t *core_of(const g2_ctx *ctx) { return ctx->core_loaded ? ctx->d_core : nullptr; }
 
 template <class T>
 int grow(g2_ctx *ctx, T *&p, uint64_t &cap, uint64_t need, const char *what) {
@@ -359,13 +364,13 @@ int prepare_tasks(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, bool on_d
             rc = grow(ctx, ctx->d_feat, ctx->feat_cap, (uint64_t)G2_MODEL_FEATURES * std::max<uint64_t>(ctx->n, 1),
                       "features");
             if (rc) return rc;
-            cudaError_t e = g2::features_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, ctx->d_core, nullptr, ctx->n,
+            cudaError_t e = g2::features_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, core_of(ctx), nullptr, ctx->n,
                                                 ctx->d_feat, ctx->sm_count, st);
             if (e != cudaSuccess) return fail_cuda(ctx, e, "features_launch");
             ctx->launches++;
             ctx->feat_valid = true;
         }
-        cudaError_t e = g2::score_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, ctx->d_core, roots, nsrc, ctx->d_feat,
+        cudaError_t e = g2::score_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, core_of(ctx), roots, nsrc, ctx->d_feat,
                                          ctx->d_model, ctx->d_model + G2_MODEL_PARAMS, nullptr, ctx->d_cost,
                                          ctx->d_total, ctx->sm_count, st);
         if (e != cudaSuccess) return fail_cuda(ctx, e, "score_launch");
@@ -934,7 +939,7 @@ int g2_close(g2_ctx *ctx) {
                     ctx->d_root_cost, ctx->d_ctr,  ctx->d_status,  ctx->d_out,    ctx->d_keys,       ctx->d_keys2,
                     ctx->d_roots,  ctx->d_S,       ctx->d_part,    ctx->d_xroots, ctx->d_xparts,     ctx->d_cost,
                     ctx->d_total,  ctx->d_ntask,   ctx->d_cub,     ctx->d_model,  ctx->d_work,
-                    ctx->d_feat,   ctx->d_rec,     ctx->d_pool,    ctx->d_ready,  ctx->d_goff,
+                    ctx->d_feat,   ctx->d_rec,     ctx->d_pool,    ctx->d_ready,  ctx->d_goff,    ctx->d_fwdmax,
                     ctx->d_root_cliques, ctx->d_gcount};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -950,19 +955,14 @@ static int after_load(g2_ctx *ctx) {
     if (rc) return rc;
     ctx->batch_off.clear();  // a batch load sets it again afterwards
     ctx->feat_valid = false;
-    if (ctx->d_core) {  // core numbers belong to the previous graph
-        cudaFree(ctx->d_core);
-        ctx->d_core = nullptr;
-        ctx->core_cap = 0;
-    }
-    unsigned int *d_max = nullptr;
-    G2_TRY(cudaMalloc(&d_max, sizeof(unsigned int)));
+    ctx->core_loaded = false;  // core numbers belong to the previous graph (buffer kept)
+    if (!ctx->d_fwdmax) G2_TRY(cudaMalloc(&ctx->d_fwdmax, sizeof(unsigned int)));
+    unsigned int *d_max = ctx->d_fwdmax;
     G2_TRY(cudaMemset(d_max, 0, sizeof(unsigned int)));
     if (ctx->n) forward_offsets_kernel<<<ctx->sm_count * 4, 256>>>(ctx->d_rp, ctx->d_ci, ctx->n, ctx->d_fo, d_max);
     ctx->launches++;
     unsigned int h = 0;
     cudaError_t e = cudaMemcpy(&h, d_max, sizeof(unsigned int), cudaMemcpyDeviceToHost);
-    cudaFree(d_max);
     if (e != cudaSuccess) return fail_cuda(ctx, e, "fwd_max");
     ctx->max_fwd = h;
     return G2_OK;
@@ -972,15 +972,28 @@ int g2_load_csr(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, uin
     if (!ctx || !row_ptrs || (!cols && m) || n >= (1ull << 32)) return G2_ERR_INVALID;
     if (row_ptrs[n] != m) return G2_ERR_INVALID;
     G2_TRY(cudaSetDevice(ctx->device));
-    if (ctx->owns_csr) {
-        cudaFree(ctx->d_rp);
-        cudaFree(ctx->d_ci);
+    // owned CSR buffers are kept and reused while large enough (no free/alloc,
+    // which synchronise the device, on a reload of a graph of the same size)
+    if (!ctx->owns_csr) {
+        ctx->d_rp = nullptr;
+        ctx->d_ci = nullptr;
+        ctx->rp_cap = ctx->ci_cap = 0;
     }
-    ctx->d_rp = nullptr;
-    ctx->d_ci = nullptr;
     ctx->owns_csr = true;
-    G2_TRY(cudaMalloc(&ctx->d_rp, sizeof(uint64_t) * (n + 1)));
-    G2_TRY(cudaMalloc(&ctx->d_ci, sizeof(uint32_t) * (m ? m : 1)));
+    if (ctx->rp_cap < n + 1) {
+        if (ctx->d_rp) cudaFree(ctx->d_rp);
+        ctx->d_rp = nullptr;
+        ctx->rp_cap = 0;
+        G2_TRY(cudaMalloc(&ctx->d_rp, sizeof(uint64_t) * (n + 1)));
+        ctx->rp_cap = n + 1;
+    }
+    if (ctx->ci_cap < std::max<uint64_t>(m, 1)) {
+        if (ctx->d_ci) cudaFree(ctx->d_ci);
+        ctx->d_ci = nullptr;
+        ctx->ci_cap = 0;
+        G2_TRY(cudaMalloc(&ctx->d_ci, sizeof(uint32_t) * std::max<uint64_t>(m, 1)));
+        ctx->ci_cap = std::max<uint64_t>(m, 1);
+    }
     G2_TRY(cudaMemcpy(ctx->d_rp, row_ptrs, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice));
     if (m) G2_TRY(cudaMemcpy(ctx->d_ci, cols, sizeof(uint32_t) * m, cudaMemcpyHostToDevice));
     ctx->n = n;
@@ -994,6 +1007,7 @@ int g2_load_csr_device(g2_ctx *ctx, const uint64_t *d_row_ptrs, const uint32_t *
     if (ctx->owns_csr) {
         cudaFree(ctx->d_rp);
         cudaFree(ctx->d_ci);
+        ctx->rp_cap = ctx->ci_cap = 0;
     }
     ctx->d_rp = const_cast<uint64_t *>(d_row_ptrs);
     ctx->d_ci = const_cast<uint32_t *>(d_cols);
@@ -1011,6 +1025,7 @@ int g2_load_core(g2_ctx *ctx, const uint32_t *core) {
     if (rc) return rc;
     ctx->feat_valid = false;
     if (ctx->n) G2_TRY(cudaMemcpy(ctx->d_core, core, sizeof(uint32_t) * ctx->n, cudaMemcpyHostToDevice));
+    ctx->core_loaded = true;
     return G2_OK;
 }
 
@@ -1292,7 +1307,7 @@ int g2_root_features(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, float 
     if (e == cudaSuccess && sources)
         e = cudaMemcpy(d_src, sources, sizeof(uint32_t) * nsrc, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && nsrc)
-        e = g2::features_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, ctx->d_core, d_src, nsrc, d_f, ctx->sm_count, 0);
+        e = g2::features_launch(ctx->d_rp, ctx->d_ci, ctx->d_fo, core_of(ctx), d_src, nsrc, d_f, ctx->sm_count, 0);
     if (e == cudaSuccess)
         e = cudaMemcpy(out, d_f, sizeof(float) * G2_MODEL_FEATURES * nsrc, cudaMemcpyDeviceToHost);
     cudaFree(d_src);
