@@ -461,6 +461,18 @@ def run_ours(a):
             cs = cpu_sample(cl, a.cpu_sample_s / 2, os.cpu_count() or 1, what="mce")
             extras["mce_chung_lu"]["cpu_port_per_s"] = cs["value"]
         mctx.close()
+        # ---- degeneracy order of the benchmark graph: host peeling vs device peeling
+        t0 = time.perf_counter()
+        perm_h, core_h = g.degeneracy_order()
+        host_s = time.perf_counter() - t0
+        with Context(local) as oc:
+            oc.load(g)
+            oc.degeneracy_order()  # warm-up (module load)
+            t0 = time.perf_counter()
+            perm_d, core_d = oc.degeneracy_order()
+            dev_s = time.perf_counter() - t0
+        extras["degeneracy_order"] = {"host_s": host_s, "device_s": dev_s, "speedup": host_s / dev_s,
+                                      "equal": bool(np.array_equal(perm_h, perm_d) and np.array_equal(core_h, core_d))}
         # ---- a batch of 64 power-law graphs, one launch per job
         extras["batch_chung_lu_64"] = c4_leg(Context, CostModel, Plan, models, local, a.seed + rank, torch, stream)
         # ---- end to end through the host ABI with pinned host buffers

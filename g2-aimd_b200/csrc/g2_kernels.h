@@ -133,6 +133,10 @@ size_t match_smem_bytes(int wpl, int warps_per_block);
 cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block,
                          cudaStream_t st, bool clique_path, int wpl, int ctas_per_sm);
 
+// Degeneracy order of a CSR on the device (kcore.cu); synchronous.
+cudaError_t degeneracy_order_device(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint32_t *perm,
+                                    uint32_t *core, int sms, uint64_t *rounds);
+
 // Learned root-cost model (costmodel.cu).
 size_t model_smem_bytes();
 cudaError_t features_launch(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, const uint32_t *core,

@@ -883,6 +883,26 @@ int g2_reserve(g2_ctx *ctx, uint64_t max_sources) {
     return G2_OK;
 }
 
+int g2_degeneracy_order_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core) {
+    if (!ctx || !perm) return G2_ERR_INVALID;
+    if (!ctx->d_rp) return G2_ERR_NO_GRAPH;
+    G2_TRY(cudaSetDevice(ctx->device));
+    const uint64_t n = ctx->n;
+    if (n == 0) return G2_OK;
+    uint32_t *d_perm = nullptr, *d_core = nullptr;
+    G2_TRY(cudaMalloc(&d_perm, n * 4));
+    cudaError_t e = cudaMalloc(&d_core, n * 4);
+    uint64_t rounds = 0;
+    if (e == cudaSuccess) e = g2::degeneracy_order_device(ctx->d_rp, ctx->d_ci, n, d_perm, d_core, ctx->sm_count, &rounds);
+    if (e == cudaSuccess) e = cudaMemcpy(perm, d_perm, n * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && core) e = cudaMemcpy(core, d_core, n * 4, cudaMemcpyDeviceToHost);
+    cudaFree(d_perm);
+    cudaFree(d_core);
+    if (e != cudaSuccess) return fail_cuda(ctx, e, "degeneracy_order_device");
+    ctx->launches = 2 * rounds + 4;
+    return G2_OK;
+}
+
 int g2_set_host_spill(g2_ctx *ctx, uint64_t bytes) {
     if (!ctx || (bytes && bytes < (1u << 20))) return G2_ERR_INVALID;
     ctx->host_spill_bytes = bytes;

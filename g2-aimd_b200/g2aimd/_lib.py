@@ -76,6 +76,7 @@ def lib():
         "g2_last_spill_stats": (i32, [C.c_void_p, P(u64), P(u64)]),
         "g2_reserve": (i32, [C.c_void_p, u64]),
         "g2_set_host_spill": (i32, [C.c_void_p, u64]),
+        "g2_degeneracy_order_device": (i32, [C.c_void_p, P(u32), P(u32)]),
         "g2_batch_load": (i32, [C.c_void_p, C.c_void_p, u32]),
         "g2_batch_mce": (i32, [C.c_void_p, C.c_void_p, P(u64), P(u64), u32]),
         "g2_batch_match": (i32, [C.c_void_p, C.c_void_p, P(u64)]),

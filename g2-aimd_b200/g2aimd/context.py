@@ -184,6 +184,15 @@ class Context:
         del keep
         return counts
 
+    def degeneracy_order(self):
+        """(perm, core) of the loaded graph computed on the device."""
+        perm = np.zeros(self.n, np.uint32)
+        core = np.zeros(self.n, np.uint32)
+        self._check(lib().g2_degeneracy_order_device(self._h, perm.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                     core.ctypes.data_as(C.POINTER(C.c_uint32))),
+                    "g2_degeneracy_order_device")
+        return perm, core
+
     def set_host_spill(self, nbytes: int):
         """Managed spill slab for MCE roots no scratch slab holds (0: none)."""
         self._check(lib().g2_set_host_spill(self._h, nbytes), "g2_set_host_spill")

@@ -258,6 +258,11 @@ int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms);
  * Synchronises the run's stream. */
 int g2_last_work_bytes(g2_ctx *ctx, uint64_t *bytes);
 
+/* Degeneracy order of the loaded graph computed on the device (replaces the
+ * host peeling of kmeans/kcore.cpp:39-191): perm[v] = new id of v, core[v] =
+ * core number (optional).  Equal to g2_degeneracy_order's output. */
+int g2_degeneracy_order_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core);
+
 /* Size of the spill slab on which a synchronous MCE run (g2_mce_run,
  * g2_batch_mce) walks the roots that no slab of the context's scratch holds,
  * after the deferral passes: managed memory (default 1 GiB, allocated on first
