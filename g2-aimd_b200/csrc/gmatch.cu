@@ -14,7 +14,10 @@
 //    scan, which removes only candidates the filter rejects.  Candidate lists
 //    live in the warp's HBM slab and are generated in chunks (the reference's
 //    TEMPSIZE chunking, :617-622), so any degree fits.  The last position is
-//    counted, never materialised (:602-609).
+//    counted, never materialised (:602-609).  Long walks hand half of their
+//    shallowest pending level (window half, candidate batches) or half of a long
+//    last-position scan to idle warps through the record queue of
+//    g2_handoff.cuh; records resume from a matched prefix.
 //  * clique (plans whose every position is adjacent to all earlier ones with
 //    images strictly increasing - presets 0, 23-27): every candidate lies in
 //    P0 = N(v) ∩ (v, ∞), so the root's P0 adjacency is built once as bitmap

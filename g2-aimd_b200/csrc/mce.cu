@@ -17,20 +17,25 @@
 // (app_BK/BK.h:314; X0 ids < v < P0 ids and both are kept sorted), so the tree
 // is exactly the reference's and per-root node counts match the oracle.
 //
-// Spilling (load balance inside a root): once the pass's task queue is empty,
-// a task that has run for more than spill_cycles SM cycles stops and writes one
-// record per pending branch of every open level of its walk (node depth, P, X
-// and the path R as P0 bitmaps); its rows go once to a shared row pool.  The
-// next pass (a wave) runs those records on the whole grid, each rebuilding its
-// B list as the root's kept rows that contain R.  Every node is still visited
-// exactly once, in the same tree, so counts, histograms and per-root node
-// counts do not change.  Search trees of the dense cores of power-law graphs are
-// chains at the top (one branch per node for many levels), which is why the
-// split is taken where the walk is, not at a fixed depth.
+// Hand-off (load balance inside a root): every spill_cycles SM cycles a walk
+// checks whether idle warps hold tickets beyond the published records
+// (g2_handoff.cuh); if so it writes the pending branches of its shallowest open
+// level as records (node depth, P, X and the path R as P0 bitmaps; at its own
+// level it keeps the first branch) and keeps walking.  A root's rows go once to
+// a shared row pool.  Idle warps run the records, each rebuilding its B list as
+// the root's kept rows that contain R.  Every node is still visited exactly
+// once, in the same tree, so counts, histograms and per-root node counts do not
+// change.  Search trees of the dense cores of power-law graphs are chains at the
+// top (one branch per node for many levels), which is why the split is taken
+// where the walk is, not at a fixed depth.
 //
 // A root whose rows or frames do not fit in the warp's slab (or whose p needs
-// more than 32*WPL words) is deferred: the host re-runs deferred roots with a
-// larger slab per warp (fewer warps) or a wider WPL.  No spin waits exist.
+// more than 32*WPL words) is deferred whole, before anything is written or
+// counted: the host re-runs deferred entries with a larger slab per warp (fewer
+// warps), then with one warp owning the whole scratch, then (synchronous runs)
+// on a managed spill slab.  An entry that has handed work off is never deferred:
+// on slab overflow it hands off everything instead.  The only waits are the
+// bounded ones of the record queue.
 #include <cstdint>
 
 #include "g2_bitrows.cuh"
