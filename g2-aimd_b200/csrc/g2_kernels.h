@@ -61,7 +61,8 @@ struct MceArgs {
     uint64_t pool_cap;              // words
     uint64_t spill_cycles;          // 0: no hand-off in this pass
     unsigned long long *qctl;       // record queue: [kQHead] tickets taken, [kQOut] outstanding work
-    uint32_t epoch;                 // ready word of records published in this run
+    uint32_t epoch;                 // ready word of records published in this run (read from epoch_dev)
+    const uint32_t *epoch_dev;      // the run's epoch, bumped on the device at the run's start
     uint64_t wait_cycles;           // longest wait of a warp for its ticket's record
 };
 constexpr int kQHead = 0, kQOut = 1;
@@ -72,6 +73,10 @@ size_t mce_smem_bytes(int wpl, int warps_per_block);
 int mce_blocks_per_sm(int wpl, int warps_per_block, bool metrics);
 int match_blocks_per_sm(int wpl, int warps_per_block, bool metrics, int ctas_per_sm);
 cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_block, cudaStream_t st);
+// Advance a run's hand-off epoch in stream order (skipping 0, the value of a
+// never-published ready word), so runs captured in a CUDA graph stay distinct
+// when the graph is replayed.
+cudaError_t epoch_bump(uint32_t *epoch_dev, cudaStream_t st);
 
 // Plan in device-friendly form: everything by POSITION.
 struct DevPlan {
@@ -124,7 +129,8 @@ struct MatchArgs {
     uint64_t rec_cap;
     uint32_t rec_stride;
     unsigned long long *qctl;
-    uint32_t epoch;
+    uint32_t epoch;                 // ready word of records published in this run (read from epoch_dev)
+    const uint32_t *epoch_dev;      // the run's epoch, bumped on the device at the run's start
     uint64_t wait_cycles;
     uint64_t spill_cycles;          // 0: no hand-off
 };

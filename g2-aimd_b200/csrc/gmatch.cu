@@ -477,6 +477,7 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
 template <int WPL, bool METRICS, int MINB>
 __global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int clique_path) {
     extern __shared__ uint32_t smem[];
+    if (a.epoch_dev) a.epoch = *a.epoch_dev;
     const uint32_t wib = threadIdx.x >> 5;
     uint32_t *rowbuf = smem + wib * (32u * WPL + 1024u * WPL);
     uint32_t *p0s = rowbuf + 32u * WPL;

@@ -697,6 +697,7 @@ __device__ __forceinline__ void run_entry(const MceArgs &a, uint32_t entry, uint
 template <int WPL, bool METRICS>
 __global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
     extern __shared__ uint32_t smem[];
+    if (a.epoch_dev) a.epoch = *a.epoch_dev;
     const uint32_t wib = threadIdx.x >> 5;
     uint32_t *cand = smem + wib * (32u * 32u * WPL + 32u * WPL);
     uint32_t *rowbuf = cand + 32u * 32u * WPL;
@@ -757,6 +758,16 @@ int mce_blocks_per_sm(int wpl, int warps_per_block, bool metrics) {
         case 8: return metrics ? mce_occ<8, true>(warps_per_block) : mce_occ<8, false>(warps_per_block);
         default: return 0;
     }
+}
+
+__global__ void epoch_bump_kernel(uint32_t *e) {
+    uint32_t v = *e + 1u;
+    *e = v ? v : 1u;
+}
+
+cudaError_t epoch_bump(uint32_t *epoch_dev, cudaStream_t st) {
+    epoch_bump_kernel<<<1, 1, 0, st>>>(epoch_dev);
+    return cudaGetLastError();
 }
 
 cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_block, cudaStream_t st) {

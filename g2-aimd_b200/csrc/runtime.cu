@@ -17,7 +17,6 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
-#include <atomic>
 #include <random>
 #include <string>
 #include <unordered_map>
@@ -54,6 +53,7 @@ struct g2_ctx {
     unsigned long long *d_ctr = nullptr;  // kCtr* layout below
     uint32_t *d_rec = nullptr;            // MCE hand-off records
     uint32_t *d_ready = nullptr;          // their ready words
+    uint32_t *d_epoch = nullptr;          // epoch of the current run (bumped on the device)
     uint32_t *d_pool = nullptr;           // MCE spill row pool
     int *d_status = nullptr;
     unsigned long long *d_out = nullptr;  // counters for the host entry points
@@ -84,7 +84,6 @@ struct g2_ctx {
     std::string cuda_err;
     uint64_t launches = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around the enumeration passes
-    uint32_t epoch = 0;  // MCE runs so far (ready word of their records)
     g2::MceArgs last_mce{};            // arguments of the last MCE enqueue (host-spill pass)
     int last_mce_wpl = 1;
     uint64_t host_spill_bytes = 1ull << 30;  // managed slab for roots no device slab holds
@@ -438,17 +437,6 @@ constexpr int kCtrSpillDefer = 21;  // entries the host-spill pass could not hol
 constexpr int kCtrQueue = 24;  // record queue: claimed, busy warps, idle warps
 constexpr int kCtrWords = 40;
 
-// Epoch of an MCE run: unique in the process and never 0, so a ready word left
-// in memory by an earlier run or context (buffers are reused by the allocator)
-// cannot match.
-uint32_t next_epoch() {
-    static std::atomic<uint32_t> counter{0};
-    uint32_t e;
-    do e = counter.fetch_add(1) + 1;
-    while (e == 0);
-    return e;
-}
-
 // MCE hand-off buffers and defaults.
 constexpr uint64_t kRecordBytes = 1ull << 30;   // records (8 M plan-walk records, 16 M+ MCE records)
 constexpr uint64_t kPoolBytes = 64ull << 20;    // rows of roots whose tasks handed off work
@@ -461,9 +449,12 @@ int ensure_handoff(g2_ctx *ctx, cudaStream_t st) {
     G2_TRY(cudaMalloc(&ctx->d_rec, kRecordBytes));
     G2_TRY(cudaMalloc(&ctx->d_pool, kPoolBytes));
     G2_TRY(cudaMalloc(&ctx->d_ready, sizeof(uint32_t) * kMaxRecords));
-    // a ready word must never match a run's epoch by accident: a waiting warp
-    // polls the ready word of a slot before it is reserved
+    G2_TRY(cudaMalloc(&ctx->d_epoch, sizeof(uint32_t)));
+    // a ready word must never match a run's epoch by accident (a waiting warp
+    // polls the ready word of a slot before it is reserved): ready words start
+    // at 0, and every run bumps the device epoch, which skips 0, in stream order
     G2_TRY(cudaMemsetAsync(ctx->d_ready, 0, sizeof(uint32_t) * kMaxRecords, st));
+    G2_TRY(cudaMemsetAsync(ctx->d_epoch, 0, sizeof(uint32_t), st));
     return G2_OK;
 }
 
@@ -616,7 +607,11 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     const uint32_t rec_stride = (4u + 3u * std::max<uint32_t>(rec_words, 1u) + 3u) & ~3u;
     const uint64_t spill_cycles =
         spill ? 1000ull * ((o && o->spill_kcycles) ? o->spill_kcycles : kSpillKcycles) : 0ull;
-    ctx->epoch = next_epoch();
+    if (spill) {
+        cudaError_t e = g2::epoch_bump(ctx->d_epoch, st);
+        if (e != cudaSuccess) return fail_cuda(ctx, e, "epoch_bump");
+        ctx->launches++;
+    }
     g2::MceArgs base{};
     base.rp = ctx->d_rp;
     base.ci = ctx->d_ci;
@@ -643,7 +638,7 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     base.npool = ctx->d_ctr + kCtrPool;
     base.pool_cap = spill ? kPoolBytes / 4 : 0;
     base.qctl = ctx->d_ctr + kCtrQueue;
-    base.epoch = ctx->epoch;
+    base.epoch_dev = spill ? ctx->d_epoch : nullptr;
     base.wait_cycles = kWaitCycles;
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
     L2Window l2(ctx, st, flags);
@@ -774,14 +769,16 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
     if (!clique && !(flags & G2_FLAG_NO_SPILL)) {
         rc = ensure_handoff(ctx, st);
         if (rc) return rc;
-        ctx->epoch = next_epoch();
+        cudaError_t eb = g2::epoch_bump(ctx->d_epoch, st);
+        if (eb != cudaSuccess) return fail_cuda(ctx, eb, "epoch_bump");
+        ctx->launches++;
         a.records = ctx->d_rec;
         a.ready = ctx->d_ready;
         a.nrec = ctx->d_ctr + kCtrRec;
         a.rec_stride = g2::kMatchRecordWords;
         a.rec_cap = std::min<uint64_t>(kRecordBytes / (4ull * a.rec_stride), g2::kRecordBit - 1u);
         a.qctl = ctx->d_ctr + kCtrQueue;
-        a.epoch = ctx->epoch;
+        a.epoch_dev = ctx->d_epoch;
         a.wait_cycles = kWaitCycles;
         a.spill_cycles = 1000ull * ((o && o->spill_kcycles) ? o->spill_kcycles : kSpillKcycles);
     }
@@ -960,6 +957,7 @@ int g2_close(g2_ctx *ctx) {
                     ctx->d_roots,  ctx->d_S,       ctx->d_part,    ctx->d_xroots, ctx->d_xparts,     ctx->d_cost,
                     ctx->d_total,  ctx->d_ntask,   ctx->d_cub,     ctx->d_model,  ctx->d_work,
                     ctx->d_feat,   ctx->d_rec,     ctx->d_pool,    ctx->d_ready,  ctx->d_goff,    ctx->d_fwdmax,
+                    ctx->d_epoch,
                     ctx->d_root_cliques, ctx->d_gcount};
     for (void *b : bufs)
         if (b) cudaFree(b);
