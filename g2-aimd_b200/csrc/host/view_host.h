@@ -1,0 +1,79 @@
+// view_host.h - views of a host CSR around a set of roots (internal C++ API).
+//
+// A view holds everything that the searches rooted at a set of sources read:
+// the ball B of radius `radius` around the sources (every vertex an embedding
+// rooted there can reach), with ids renumbered 0..|B|-1 in ascending global
+// order, so that id comparisons (symmetry-breaking conditions, P/X split of a
+// Bron-Kerbosch root, forward lists) give the same answers as in the whole
+// graph.  Vertices within `row_radius` of a source keep their adjacency
+// restricted to B; the others keep an empty row (their neighbours are never
+// scanned).  Replaces the materialisation of view/view_bin.h:61-159, which
+// keeps global ids and copies the full rows of the vertices within hop-1 of
+// the sources.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace g2view {
+
+constexpr uint32_t kNone = 0xffffffffu;
+
+struct Sizes {
+    uint64_t n = 0;         // view vertices |B|
+    uint64_t m = 0;         // view column entries
+    uint64_t nsrc = 0;      // sources kept (degree >= min_root_degree)
+    uint32_t max_fwd = 0;   // max |N(v) ∩ (v, ∞)| inside the view
+};
+
+// Byte layout of a view in one buffer (host slot or device slot):
+//   rp u64[n+1] | fo u32[n] | ci u32[m] | src u32[nsrc], each part 16-byte aligned.
+struct Layout {
+    uint64_t fo = 0, ci = 0, src = 0, bytes = 0;
+    explicit Layout(const Sizes &s);
+};
+
+// One builder per thread; it keeps an n-entry mark array (4 bytes per vertex of
+// the whole graph) between views and clears only what a view touched.
+class Builder {
+  public:
+    Builder(const uint64_t *rp, const uint32_t *ci, uint64_t n) : rp_(rp), ci_(ci), n_(n) {}
+    // Collect the view of `src` (sources of degree < min_root_degree are
+    // dropped: no embedding is rooted there).  Sources must be < n.
+    Sizes plan(const uint32_t *src, uint64_t nsrc, uint32_t radius, uint32_t row_radius, uint32_t min_root_degree);
+    // Write the planned view: rp[n+1], fo[n] (per vertex, neighbours <= v),
+    // ci[m], src[nsrc] (local ids of the kept sources, in the given order),
+    // ids[n] (global id of each view vertex; may be null).  Releases the marks.
+    void fill(uint64_t *rp, uint32_t *fo, uint32_t *ci, uint32_t *src, uint32_t *ids);
+    // Same, into one buffer laid out as Layout(sizes).
+    void fill_packed(void *buf, const Sizes &s);
+
+  private:
+    void release();
+    const uint64_t *rp_;
+    const uint32_t *ci_;
+    uint64_t n_;
+    std::vector<uint32_t> mark_;    // BFS depth, then the local id; kNone outside the view
+    std::vector<uint64_t> ball_;    // (global << 4 | depth) while planning, then sorted
+    std::vector<uint32_t> src_;     // kept sources (global ids)
+    std::vector<uint32_t> deg_;     // view degree of each view vertex
+    uint32_t row_radius_ = 0;
+};
+
+// Greedy partition of the roots 0..n-1 into bins in id order: a bin is closed
+// when its view would exceed max_bytes (estimated from full degrees, an upper
+// bound of the view's size; a bin holds at least one source).  bin_of[v] for
+// every vertex; returns the number of bins.
+uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint32_t radius, uint32_t row_radius,
+                   uint32_t min_root_degree, uint64_t max_bytes, uint32_t *bin_of);
+
+// Radii of a query plan given by positions: k positions, bn_count[i] back
+// neighbours of position i at positions bn_pos[i][j] (< i).  radius = largest
+// distance from position 0 (every embedding vertex lies within it of the
+// root's image); row_radius = largest distance of a position that some later
+// position lists as back neighbour (only those vertices' rows are scanned);
+// root_degree = query degree of position 0.
+void plan_radii(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[8], uint32_t *radius,
+                uint32_t *row_radius, uint32_t *root_degree);
+
+}  // namespace g2view

@@ -46,6 +46,26 @@ class G2Opts(C.Structure):
     ]
 
 
+class G2View(C.Structure):
+    _fields_ = [("row_ptrs", P(u64)), ("cols", P(u32)), ("fwd_offsets", P(u32)), ("sources", P(u32)),
+                ("ids", P(u32)), ("n", u64), ("m", u64), ("nsrc", u64), ("max_fwd", u32)]
+
+
+class G2ViewOpts(C.Structure):
+    _fields_ = [("producers", u32), ("radius", u32), ("row_radius", u32), ("reserved", u32)]
+
+
+class G2ViewStats(C.Structure):
+    _fields_ = [("bins", u64), ("view_vertices", u64), ("view_edges", u64), ("h2d_bytes", u64),
+                ("max_view_bytes", u64), ("build_ms", C.c_double), ("wait_ms", C.c_double),
+                ("total_ms", C.c_double)]
+
+    def to_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+G2_VIEW_NO_BIN = 0xFFFFFFFF
+
 _lib = None
 
 
@@ -80,6 +100,14 @@ def lib():
         "g2_batch_load": (i32, [C.c_void_p, C.c_void_p, u32]),
         "g2_batch_mce": (i32, [C.c_void_p, C.c_void_p, P(u64), P(u64), u32]),
         "g2_batch_match": (i32, [C.c_void_p, C.c_void_p, P(u64)]),
+        "g2_view_mce": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, C.c_void_p, u32, P(G2ViewOpts), P(G2Opts),
+                              P(u64), C.c_void_p, u32, C.c_void_p, P(G2ViewStats)]),
+        "g2_view_match": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, C.c_void_p, u32, P(G2ViewOpts),
+                                P(G2Opts), P(u64), C.c_void_p, P(G2ViewStats)]),
+        "g2_view_materialize": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p, u64, u32, u32, u32, P(G2View)]),
+        "g2_view_free": (None, [P(G2View)]),
+        "g2_plan_view_radius": (i32, [P(G2Plan), P(u32), P(u32), P(u32)]),
+        "g2_view_bins": (i32, [C.c_void_p, C.c_void_p, u64, u32, u32, u32, u64, C.c_void_p, P(u32)]),
         "g2_load_core": (i32, [C.c_void_p, C.c_void_p]),
         "g2_root_features": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p]),
         "g2_model_train": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, u32, u32, C.c_float, u64, C.c_void_p,

@@ -43,6 +43,14 @@ class Plan:
     def k(self) -> int:
         return self.raw.k
 
+    def view_radius(self):
+        """(radius, row_radius, root_degree) a view of this plan's roots needs
+        (g2_plan_view_radius)."""
+        r, rr, d = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib().g2_plan_view_radius(C.byref(self.raw), C.byref(r), C.byref(rr), C.byref(d)),
+              "g2_plan_view_radius")
+        return r.value, rr.value, d.value
+
     def to_dict(self) -> dict:
         """Same field layout as the reference-planner fixtures."""
         r, k = self.raw, self.raw.k
@@ -271,6 +279,55 @@ class Context:
                                        0 if src is None else src.size, C.byref(o), C.byref(count)), "g2_match_run")
         del keep
         return count.value
+
+    # out-of-core runs over view bins: the graph stays in host memory
+    def _view_args(self, graph, bin_of, nbins, producers, radius, row_radius):
+        from ._lib import G2ViewOpts
+        bins = np.ascontiguousarray(bin_of, dtype=np.uint32)
+        if nbins is None:
+            valid = bins[bins != 0xFFFFFFFF]
+            nbins = int(valid.max()) + 1 if valid.size else 0
+        vo = G2ViewOpts(producers, radius, row_radius, 0)
+        return bins, nbins, vo
+
+    def view_mce(self, graph, bin_of, nbins=None, hist_len=256, producers=0, radius=0, row_radius=0, **kw):
+        """(count, hist, per-bin counts, stats) of maximal cliques of a host graph
+        enumerated view bin by view bin (g2_view_mce)."""
+        from ._lib import G2ViewStats
+        bins, nbins, vo = self._view_args(graph, bin_of, nbins, producers, radius, row_radius)
+        o, keep = _opts(**kw)
+        count = C.c_uint64()
+        hist = np.zeros(hist_len, np.uint64)
+        per_bin = np.zeros(max(nbins, 1), np.uint64)
+        st = G2ViewStats()
+        self._check(lib().g2_view_mce(self._h, graph.row_ptrs.ctypes.data_as(C.c_void_p),
+                                      graph.cols.ctypes.data_as(C.c_void_p), graph.n,
+                                      bins.ctypes.data_as(C.c_void_p), nbins, C.byref(vo), C.byref(o),
+                                      C.byref(count), hist.ctypes.data_as(C.c_void_p), hist_len,
+                                      per_bin.ctypes.data_as(C.c_void_p), C.byref(st)), "g2_view_mce")
+        del keep
+        self.graph, self.n = None, 0
+        return count.value, hist, per_bin[:nbins], st.to_dict()
+
+    def view_match(self, graph, bin_of, plan: Plan = None, nbins=None, producers=0, radius=0, row_radius=0, **kw):
+        """(count, per-bin counts, stats) of the plan's matches in a host graph,
+        view bin by view bin (g2_view_match)."""
+        from ._lib import G2ViewStats
+        if plan is not None:
+            self.set_plan(plan)
+        bins, nbins, vo = self._view_args(graph, bin_of, nbins, producers, radius, row_radius)
+        o, keep = _opts(**kw)
+        count = C.c_uint64()
+        per_bin = np.zeros(max(nbins, 1), np.uint64)
+        st = G2ViewStats()
+        self._check(lib().g2_view_match(self._h, graph.row_ptrs.ctypes.data_as(C.c_void_p),
+                                        graph.cols.ctypes.data_as(C.c_void_p), graph.n,
+                                        bins.ctypes.data_as(C.c_void_p), nbins, C.byref(vo), C.byref(o),
+                                        C.byref(count), per_bin.ctypes.data_as(C.c_void_p), C.byref(st)),
+                    "g2_view_match")
+        del keep
+        self.graph, self.n = None, 0
+        return count.value, per_bin[:nbins], st.to_dict()
 
     # device-resident entry points (timing): pointers are raw device addresses
     def mce_device(self, d_out: int, hist_len: int, d_sources: int = 0, nsrc: int = 0, stream: int = 0, **kw):

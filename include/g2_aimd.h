@@ -263,6 +263,49 @@ int g2_last_work_bytes(g2_ctx *ctx, uint64_t *bytes);
  * core number (optional).  Equal to g2_degeneracy_order's output. */
 int g2_degeneracy_order_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core);
 
+/*
+ * Out-of-core enumeration over view bins, for graphs whose CSR exceeds device
+ * memory (replaces Worker::run's producer/consumer loop, system/worker.h:165-279,
+ * with ViewBin::Materialize, view/view_bin.h:61-159, and
+ * PipelineExecutor::Transfer, system/pipeline_executor.h:121-147).  The CSR
+ * stays in host memory.  bin_of[v] is the bin of root v (G2_VIEW_NO_BIN: not a
+ * root), as g2_read_vbmap or g2_view_bins give it.  Host threads build each
+ * bin's view (g2_view_materialize) into pinned buffers; the context uploads
+ * views into two device slots, the upload of the next view overlapping the
+ * enumeration of the current one, and sums the per-bin results.  Every
+ * maximal clique / match is found from exactly one root, so the totals equal
+ * g2_mce_run / g2_match_run over the whole graph.  The context's loaded graph
+ * is released (load again before other runs).  Per-root outputs, work model
+ * and caller scores (G2_SCHED_SCORES) are not available here.
+ */
+#define G2_VIEW_NO_BIN 0xffffffffu
+typedef struct g2_view_opts {
+    uint32_t producers;   /* host threads building views (0 = min(8, cores))    */
+    uint32_t radius;      /* ball radius (0 = from the query: 1 for MCE)         */
+    uint32_t row_radius;  /* rows kept up to this distance (0 = from the query)  */
+    uint32_t reserved;
+} g2_view_opts;
+typedef struct g2_view_stats {
+    uint64_t bins;            /* views enumerated (bins with a root of enough degree) */
+    uint64_t view_vertices;   /* sum over views                                   */
+    uint64_t view_edges;      /* column entries, summed over views                */
+    uint64_t h2d_bytes;       /* bytes uploaded                                   */
+    uint64_t max_view_bytes;  /* largest view                                     */
+    double build_ms;          /* host time building views, summed over threads    */
+    double wait_ms;           /* time the device side waited for a view           */
+    double total_ms;          /* wall time of the call                            */
+} g2_view_stats;
+int g2_view_mce(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n,
+                const uint32_t *bin_of, uint32_t nbins, const g2_view_opts *vopts,
+                const g2_opts *opts, uint64_t *count, uint64_t *hist, uint32_t hist_len,
+                uint64_t *bin_counts, g2_view_stats *stats);
+/* Matches of the plan set with g2_set_plan (radius and row radius from its
+ * query; roots of degree below the query root's degree are skipped). */
+int g2_view_match(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n,
+                  const uint32_t *bin_of, uint32_t nbins, const g2_view_opts *vopts,
+                  const g2_opts *opts, uint64_t *count, uint64_t *bin_counts,
+                  g2_view_stats *stats);
+
 /* Size of the spill slab on which a synchronous MCE run (g2_mce_run,
  * g2_batch_mce) walks the roots that no slab of the context's scratch holds,
  * after the deferral passes: managed memory (default 1 GiB, allocated on first
@@ -357,6 +400,41 @@ int g2_write_vbmap(const char *path, uint32_t nbins, const uint32_t *bins,
                    uint64_t n);
 int g2_read_vbmap(const char *path, uint64_t n, uint32_t *nbins,
                   uint32_t *bins);
+
+/*
+ * Views (host only).  The view of a root set S is the ball B of radius `radius`
+ * around S, ids renumbered 0..|B|-1 in ascending global order (so id
+ * comparisons agree with the whole graph); vertices within `row_radius` of S
+ * keep their neighbours inside B, the others an empty row.  Every embedding
+ * rooted in S lies in B and uses only rows of vertices within the query's
+ * back-neighbour distance, so a search over the view from S's local ids finds
+ * exactly what it finds in the whole graph (view/view_bin.h:40-159 keeps
+ * global ids and whole rows instead).  Sources of degree < min_root_degree are
+ * dropped.  Arrays are malloc'd; release them with g2_view_free.
+ */
+typedef struct g2_view {
+    uint64_t *row_ptrs;     /* n + 1                                          */
+    uint32_t *cols;         /* m                                              */
+    uint32_t *fwd_offsets;  /* n: neighbours <= v in row v                     */
+    uint32_t *sources;      /* nsrc local ids, in the given order             */
+    uint32_t *ids;          /* n: global id of each view vertex               */
+    uint64_t n, m, nsrc;
+    uint32_t max_fwd;       /* max forward degree inside the view             */
+} g2_view;
+int g2_view_materialize(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n,
+                        const uint32_t *sources, uint64_t nsrc, uint32_t radius,
+                        uint32_t row_radius, uint32_t min_root_degree, g2_view *out);
+void g2_view_free(g2_view *view);
+/* Radius, row radius and root degree a plan needs (system/plan.h:51-73 derives
+ * the reference's single hop count the same way). */
+int g2_plan_view_radius(const g2_plan *plan, uint32_t *radius, uint32_t *row_radius,
+                        uint32_t *root_degree);
+/* Greedy bins over the roots 0..n-1 in id order: a bin closes when its view
+ * would exceed max_bytes (an estimate from full degrees, so an upper bound; a
+ * bin holds at least one root).  bin_of: n entries (a .vbmap body). */
+int g2_view_bins(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uint32_t radius,
+                 uint32_t row_radius, uint32_t min_root_degree, uint64_t max_bytes,
+                 uint32_t *bin_of, uint32_t *nbins);
 
 /*
  * Degeneracy order (kmeans/kcore.cpp:103-191): k-core shells in increasing core

@@ -1,0 +1,104 @@
+"""Out-of-core runs over view bins on the GPU (g2_view_mce / g2_view_match):
+the CSR stays in host memory, host threads build each bin's view, the device
+enumerates view after view with the next upload overlapping the current run.
+Totals, histograms and per-bin counts equal the oracle over the whole graph."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def vctx(g2):
+    from g2aimd.context import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def per_bin_oracle_mce(orc, g, bin_of, nbins, hist_len=64):
+    out = np.zeros(nbins, np.uint64)
+    for b in range(nbins):
+        src = np.flatnonzero(bin_of == b).astype(np.uint32)
+        if src.size:
+            out[b] = orc.mce(g, roots=src, hist_len=hist_len)["count"]
+    return out
+
+
+@pytest.mark.parametrize("nbins,producers", [(1, 1), (7, 1), (7, 3), (64, 4)])
+def test_view_mce_equals_oracle(vctx, orc, c1_graph, nbins, producers):
+    g = c1_graph
+    want = orc.mce(g, hist_len=64)
+    bin_of = np.random.default_rng(nbins).integers(0, nbins, g.n).astype(np.uint32)
+    count, hist, per_bin, st = vctx.view_mce(g, bin_of, nbins=nbins, hist_len=64, producers=producers)
+    assert count == want["count"]
+    assert np.array_equal(hist, want["hist"])
+    assert int(per_bin.sum()) == count
+    assert np.array_equal(per_bin, per_bin_oracle_mce(orc, g, bin_of, nbins))
+    assert 1 <= st["bins"] <= nbins and st["h2d_bytes"] > 0 and st["view_edges"] > 0
+
+
+def test_view_mce_many_bins_rmat(vctx, orc, g2):
+    g = g2.Graph.rmat(11, 8, seed=2).degeneracy_recoded()
+    want = orc.mce(g, hist_len=64)
+    nb, bin_of = g.view_bins(max_bytes=96 << 10, radius=1, row_radius=1, min_root_degree=1)
+    assert nb > 4
+    count, hist, per_bin, st = vctx.view_mce(g, bin_of, hist_len=64, producers=2)
+    assert count == want["count"] and np.array_equal(hist, want["hist"])
+    assert 4 < st["bins"] <= nb
+
+
+def test_view_mce_schedules_and_no_graph_after(vctx, orc, c1_graph):
+    g = c1_graph
+    want = orc.mce(g, hist_len=64)["count"]
+    bin_of = (np.arange(g.n) % 5).astype(np.uint32)
+    c, _, _, _ = vctx.view_mce(g, bin_of, hist_len=64, schedule="heuristic")
+    assert c == want
+    # the view run released the context's graph: a run needs a load first
+    with pytest.raises(Exception):
+        vctx.mce(hist_len=64)
+    vctx.load(g)
+    assert vctx.mce(hist_len=64)[0] == want
+
+
+def test_view_roots_subset(vctx, orc, c1_graph):
+    g = c1_graph
+    bin_of = np.full(g.n, 0xFFFFFFFF, np.uint32)  # only even roots, in 3 bins
+    bin_of[::2] = (np.arange(0, g.n, 2) // 700).astype(np.uint32)
+    src = np.arange(0, g.n, 2, dtype=np.uint32)
+    want = orc.mce(g, roots=src, hist_len=64)
+    count, hist, per_bin, _ = vctx.view_mce(g, bin_of, hist_len=64)
+    assert count == want["count"] and np.array_equal(hist, want["hist"])
+
+
+@pytest.mark.parametrize("q", [0, 1, 2, 24])
+def test_view_match_equals_oracle(vctx, orc, g2, q):
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(11, 8, seed=4).degeneracy_recoded()
+    plan = Plan.preset(q)
+    want = orc.match(g, plan, threads=4)["count"]
+    radius, row_radius, root_degree = plan.view_radius()
+    nb, bin_of = g.view_bins(max_bytes=64 << 10, radius=radius, row_radius=row_radius,
+                             min_root_degree=root_degree)
+    assert nb > 8
+    count, per_bin, st = vctx.view_match(g, bin_of, plan, producers=3)
+    assert count == want, (q, count, want)
+    assert int(per_bin.sum()) == count
+    assert st["bins"] >= 1
+
+
+def test_view_match_plan_walk_handoff(vctx, orc, g2):
+    """4-cycles with frequent hand-offs inside each view."""
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(10, 12, seed=6).degeneracy_recoded()
+    plan = Plan.preset(1)
+    want = orc.match(g, plan, threads=4)["count"]
+    bin_of = (np.arange(g.n) % 3).astype(np.uint32)
+    count, _, _ = vctx.view_match(g, bin_of, plan, spill_kcycles=1)
+    assert count == want
+
+
+def test_view_rejects_scores(vctx, c1_graph):
+    bin_of = np.zeros(c1_graph.n, np.uint32)
+    with pytest.raises(Exception):
+        vctx.view_mce(c1_graph, bin_of, schedule="scores", scores=np.ones(c1_graph.n, np.float32))
