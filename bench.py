@@ -62,8 +62,11 @@ def parse():
     ap.add_argument("--scratch-mb", type=int, default=4096, help="device scratch for the DFS slabs")
     ap.add_argument("--fixed", action="store_true",
                     help="skip the plain-schedule timing and the autotuner (profiling runs)")
-    ap.add_argument("--leg", choices=["all", "mce"], default="all",
-                    help="mce: only the maximal-clique workload (Chung-Lu 2^18), for profiling")
+    ap.add_argument("--leg", choices=["all", "mce", "view"], default="all",
+                    help="mce: only the maximal-clique workload (Chung-Lu 2^18), for profiling; "
+                         "view: out-of-core runs over view bins against in-core runs")
+    ap.add_argument("--view-split", type=int, default=2,
+                    help="view leg: bin budget = CSR bytes / this")
     return ap.parse_args()
 
 
@@ -88,6 +91,72 @@ def run_mce_leg(a):
             times.append(ctx.pass_times()[0])
         print(json.dumps({"workload": "mce chung-lu n=2^18 gamma 2.3 avg degree 16", "maximal_cliques": int(c),
                           "kernel_ms": times, "records": ctx.spill_stats()[0]}), flush=True)
+
+
+def run_view_leg(a):
+    """Out-of-core enumeration (g2_view_match / g2_view_mce: CSR in pinned host
+    memory, views built by host threads, uploads overlapping the runs) against
+    the in-core path (upload the whole CSR, then run) on the same host graph,
+    both timed end to end on the host.  One JSON line."""
+    import torch
+
+    import g2aimd
+    from g2aimd.context import Context, Plan
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    producers = min(16, os.cpu_count() or 1)
+    launch = {"warps_per_block": 8, "chunk": 1, "ctas_per_sm": 6}
+    out = {"workload": "out-of-core view bins vs in-core, host CSR in pinned memory", "producers": producers}
+
+    def pinned(g):
+        prp = torch.from_numpy(g.row_ptrs.view(np.int64)).pin_memory()
+        pci = torch.from_numpy(g.cols.view(np.int32)).pin_memory()
+        return g2aimd.Graph(prp.numpy().view(np.uint64), pci.numpy().view(np.uint32)), (prp, pci)
+
+    def leg(name, g, shape, view_fn, core_fn):
+        csr = g.row_ptrs.nbytes + g.cols.nbytes
+        budget = csr // a.view_split
+        t0 = time.perf_counter()
+        nb, bins = g.view_bins(budget, **shape)
+        bin_s = time.perf_counter() - t0
+        pg, keep = pinned(g)
+        with Context(0, a.scratch_mb << 20) as ctx:
+            for _ in range(a.warmup):
+                c_view, st = view_fn(ctx, pg, bins, nb)
+            vt = []
+            for _ in range(a.steps):
+                t0 = time.perf_counter()
+                c_view, st = view_fn(ctx, pg, bins, nb)
+                vt.append((time.perf_counter() - t0) * 1e3)
+            for _ in range(a.warmup):
+                ctx.load(pg)
+                c_core = core_fn(ctx)
+            ct = []
+            for _ in range(a.steps):
+                t0 = time.perf_counter()
+                ctx.load(pg)
+                c_core = core_fn(ctx)
+                ct.append((time.perf_counter() - t0) * 1e3)
+        assert c_view == c_core, (name, c_view, c_core)
+        del keep
+        out[name] = {"graph": {"n": g.n, "m": g.m}, "shape": shape, "csr_bytes": int(csr),
+                     "bin_budget_bytes": int(budget),
+                     "bins": nb, "bin_plan_s": round(bin_s, 3), "count": int(c_view),
+                     "view_ms": float(np.mean(vt)), "in_core_ms": float(np.mean(ct)),
+                     "view_vs_in_core": float(np.mean(ct)) / float(np.mean(vt)), "stats": st}
+
+    g, _ = make_graph(a.scale, a.edge_factor, a.seed)
+    k4 = Plan.preset(K4)
+    leg(f"k4_rmat_s{a.scale}", g, k4.view_shape(),
+        lambda ctx, pg, bins, nb: (lambda c, _pb, st: (c, st))(
+            *ctx.view_match(pg, bins, k4, nbins=nb, producers=producers, schedule="heuristic", **launch)),
+        lambda ctx: ctx.match(k4, schedule="heuristic", **launch))
+    cl = g2aimd.Graph.chung_lu(1 << 18, 2.3, 16.0, seed=a.seed).degeneracy_recoded()
+    leg("mce_chung_lu_2^18", cl, {"radius": 1, "row_radius": 1, "min_root_degree": 1, "upper": False},
+        lambda ctx, pg, bins, nb: (lambda c, _h, _pb, st: (c, st))(
+            *ctx.view_mce(pg, bins, nbins=nb, hist_len=HIST, producers=producers, schedule="heuristic")),
+        lambda ctx: ctx.mce(hist_len=HIST, schedule="heuristic")[0])
+    print(json.dumps(out), flush=True)
 
 
 def dist_env():
@@ -543,6 +612,8 @@ def main():
         run_reference(a)
     elif a.leg == "mce":
         run_mce_leg(a)
+    elif a.leg == "view":
+        run_view_leg(a)
     else:
         run_ours(a)
 

@@ -1,5 +1,5 @@
 // view_host.cpp - views of a host CSR around a set of roots, the greedy bin
-// partition that sizes them, and the radii a query plan needs.
+// partition that sizes them, and what a query plan needs of a view.
 //
 // Replaces the host side of the reference's out-of-core path:
 // ViewBin::Materialize / ExtendFromSource (view/view_bin.h:40-159) and the
@@ -8,6 +8,7 @@
 #include "view_host.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "g2_aimd.h"
@@ -26,52 +27,72 @@ Layout::Layout(const Sizes &s) {
 }
 
 void Builder::release() {
-    for (uint64_t e : ball_) mark_[e >> 4] = kNone;
+    for (uint32_t g : ball_) mark_[g] = kNone;
     ball_.clear();
+    row_.clear();
     src_.clear();
     deg_.clear();
 }
 
-Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, uint32_t radius, uint32_t row_radius,
-                    uint32_t min_root_degree) {
+// Lower x's depth to d (a vertex is walked again only when its depth drops).
+bool Builder::relax(uint32_t x, uint32_t d) {
+    const uint32_t old = mark_[x];
+    if (old != kNone && old <= d) return false;
+    if (old == kNone) ball_.push_back(x);
+    mark_[x] = d;
+    return true;
+}
+
+Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
     if (mark_.size() != n_) mark_.assign(n_, kNone);
     release();
-    row_radius_ = row_radius;
-    // multi-source BFS: depth of every vertex within `radius` of a kept source
-    std::vector<uint32_t> frontier, next;
-    for (uint64_t i = 0; i < nsrc; i++) {
-        const uint32_t s = src[i];
-        if (rp_[s + 1] - rp_[s] < min_root_degree) continue;
-        src_.push_back(s);
-        if (mark_[s] == kNone) {
-            mark_[s] = 0;
-            ball_.push_back((uint64_t)s << 4);
-            frontier.push_back(s);
+    for (uint64_t i = 0; i < nsrc; i++)
+        if (rp_[src[i] + 1] - rp_[src[i]] >= sh.min_deg) src_.push_back(src[i]);
+    auto walk = [&](uint32_t lo_excl, bool upper) {
+        for (uint32_t d = 0; d < sh.radius && !frontier_.empty(); d++) {
+            next_.clear();
+            for (uint32_t x : frontier_)
+                for (uint64_t e = rp_[x]; e < rp_[x + 1]; e++) {
+                    const uint32_t u = ci_[e];
+                    if ((!upper || u > lo_excl) && relax(u, d + 1)) next_.push_back(u);
+                }
+            frontier_.swap(next_);
+        }
+    };
+    if (!sh.upper) {
+        // one multi-source BFS: the depth of a vertex is its distance to the set
+        frontier_.clear();
+        for (uint32_t s : src_)
+            if (relax(s, 0)) frontier_.push_back(s);
+        walk(0, false);
+    } else {
+        // source by source in ascending order, through vertices above the
+        // source: a vertex already reached at depth <= d from a smaller source
+        // was walked from there through a superset of what this source allows
+        std::vector<uint32_t> order(src_);
+        std::sort(order.begin(), order.end());
+        order.erase(std::unique(order.begin(), order.end()), order.end());
+        for (uint32_t s : order) {
+            if (!relax(s, 0)) continue;
+            frontier_.assign(1, s);
+            walk(s, true);
         }
     }
-    for (uint32_t d = 0; d < radius && !frontier.empty(); d++) {
-        next.clear();
-        for (uint32_t x : frontier)
-            for (uint64_t e = rp_[x]; e < rp_[x + 1]; e++) {
-                const uint32_t u = ci_[e];
-                if (mark_[u] != kNone) continue;
-                mark_[u] = d + 1;
-                ball_.push_back(((uint64_t)u << 4) | std::min<uint32_t>(d + 1, 15u));
-                next.push_back(u);
-            }
-        frontier.swap(next);
-    }
-    // ascending global order = local ids; marks become local ids
+    // ascending global order = local ids; rows where the depth allows; marks become local ids
     std::sort(ball_.begin(), ball_.end());
-    for (uint64_t i = 0; i < ball_.size(); i++) mark_[ball_[i] >> 4] = (uint32_t)i;
-    // view degrees and forward degrees
+    const uint64_t nv = ball_.size();
+    row_.resize(nv);
+    for (uint64_t i = 0; i < nv; i++) {
+        row_[i] = mark_[ball_[i]] <= sh.row_radius;
+        mark_[ball_[i]] = (uint32_t)i;
+    }
     Sizes s;
-    s.n = ball_.size();
+    s.n = nv;
     s.nsrc = src_.size();
-    deg_.assign(s.n, 0u);
-    for (uint64_t i = 0; i < s.n; i++) {
-        if ((ball_[i] & 15u) > row_radius) continue;
-        const uint32_t g = (uint32_t)(ball_[i] >> 4);
+    deg_.assign(nv, 0u);
+    for (uint64_t i = 0; i < nv; i++) {
+        if (!row_[i]) continue;
+        const uint32_t g = ball_[i];
         uint32_t d = 0, back = 0;
         for (uint64_t e = rp_[g]; e < rp_[g + 1]; e++) {
             const uint32_t l = mark_[ci_[e]];
@@ -90,7 +111,7 @@ void Builder::fill(uint64_t *rp, uint32_t *fo, uint32_t *ci, uint32_t *src, uint
     uint64_t off = 0;
     for (uint64_t i = 0; i < ball_.size(); i++) {
         rp[i] = off;
-        const uint32_t g = (uint32_t)(ball_[i] >> 4);
+        const uint32_t g = ball_[i];
         if (ids) ids[i] = g;
         uint32_t back = 0;
         if (deg_[i]) {
@@ -115,41 +136,53 @@ void Builder::fill_packed(void *buf, const Sizes &s) {
          reinterpret_cast<uint32_t *>(b + L.src), nullptr);
 }
 
-uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint32_t radius, uint32_t row_radius,
-                   uint32_t min_root_degree, uint64_t max_bytes, uint32_t *bin_of) {
+uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Shape &sh, uint64_t max_bytes,
+                   uint32_t *bin_of) {
     if (n == 0) return 0;
-    // depth[x] = smallest distance from a source of the open bin; a vertex is
-    // expanded again only when its depth drops (decrease-key BFS), so adding a
-    // source costs what its ball adds to the bin
+    // The open bin's view is tracked exactly: depth[x] = smallest depth from a
+    // source of the bin (walked again only when it drops; sources come in
+    // ascending order, which the upper walks need), and a vertex that enters
+    // the ball or gains its row adds its column entries towards the ball.
     std::vector<uint32_t> depth(n, kNone), touched, frontier, next;
     uint64_t bytes = 8, delta = 0;
     uint32_t bin = 0, nsrc = 0;
     auto relax = [&](uint32_t x, uint32_t d) {
         const uint32_t old = depth[x];
         if (old != kNone && old <= d) return false;
-        if (old == kNone) {
+        const bool fresh = old == kNone;
+        const bool gains_row = d <= sh.row_radius && (fresh || old > sh.row_radius);
+        depth[x] = d;
+        if (fresh) {
             delta += 12;  // row pointer + forward offset
             touched.push_back(x);
         }
-        if (d <= row_radius && (old == kNone || old > row_radius)) delta += 4ull * (rp[x + 1] - rp[x]);
-        depth[x] = d;
+        if (fresh || gains_row) {
+            for (uint64_t e = rp[x]; e < rp[x + 1]; e++) {
+                const uint32_t y = ci[e];
+                if (y == x || depth[y] == kNone) continue;
+                if (gains_row) delta += 4;                             // x -> y
+                if (fresh && y != x && depth[y] <= sh.row_radius) delta += 4;  // y -> x
+            }
+        }
         return true;
     };
     auto add = [&](uint32_t s) {
         delta = 4;  // the source entry
         frontier.clear();
         if (relax(s, 0)) frontier.push_back(s);
-        for (uint32_t d = 0; d < radius && !frontier.empty(); d++) {
+        for (uint32_t d = 0; d < sh.radius && !frontier.empty(); d++) {
             next.clear();
             for (uint32_t x : frontier)
-                for (uint64_t e = rp[x]; e < rp[x + 1]; e++)
-                    if (relax(ci[e], d + 1)) next.push_back(ci[e]);
+                for (uint64_t e = rp[x]; e < rp[x + 1]; e++) {
+                    const uint32_t u = ci[e];
+                    if ((!sh.upper || u > s) && relax(u, d + 1)) next.push_back(u);
+                }
             frontier.swap(next);
         }
         return delta;
     };
     for (uint64_t v = 0; v < n; v++) {
-        if (rp[v + 1] - rp[v] < min_root_degree) {
+        if (rp[v + 1] - rp[v] < sh.min_deg) {
             bin_of[v] = bin;  // no embedding is rooted here: no size
             continue;
         }
@@ -169,11 +202,13 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint32_t 
     return bin + 1;
 }
 
-void plan_radii(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[8], uint32_t *radius,
-                uint32_t *row_radius, uint32_t *root_degree) {
+Shape plan_shape(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[8], const uint32_t *cond_count,
+                 const uint32_t (*cond_op)[8], const uint32_t (*cond_pos)[8]) {
+    k = std::min<uint32_t>(k, 8u);
     uint32_t adj[8] = {0};  // bit j of adj[i]: positions i and j adjacent
+    uint32_t gt[8] = {0};   // bit j of gt[i]: the conditions imply M(i) > M(j)
     bool is_bn[8] = {false};
-    for (uint32_t i = 0; i < k && i < 8; i++)
+    for (uint32_t i = 0; i < k; i++) {
         for (uint32_t j = 0; j < bn_count[i] && j < 8; j++) {
             const uint32_t p = bn_pos[i][j];
             if (p >= k) continue;
@@ -181,6 +216,17 @@ void plan_radii(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[8
             adj[p] |= 1u << i;
             is_bn[p] = true;
         }
+        for (uint32_t j = 0; j < cond_count[i] && j < 8; j++) {
+            const uint32_t p = cond_pos[i][j];
+            if (p >= k) continue;
+            if (cond_op[i][j] == G2_COND_LARGER_THAN) gt[i] |= 1u << p;
+            if (cond_op[i][j] == G2_COND_LESS_THAN) gt[p] |= 1u << i;
+        }
+    }
+    for (uint32_t it = 0; it < k; it++)  // transitive closure
+        for (uint32_t a = 0; a < k; a++)
+            for (uint32_t b = 0; b < k; b++)
+                if (gt[a] >> b & 1u) gt[a] |= gt[b];
     uint32_t dist[8];
     for (auto &d : dist) d = kNone;
     dist[0] = 0;
@@ -195,41 +241,60 @@ void plan_radii(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[8
         seen |= nxt;
         cur = nxt;
     }
-    uint32_t r = 0, rr = 0;
+    Shape sh;
+    sh.radius = 0;
+    sh.row_radius = 0;
+    sh.upper = k > 1;
     for (uint32_t i = 0; i < k; i++) {
+        if (i > 0 && !(gt[i] & 1u)) sh.upper = false;
         if (dist[i] == kNone) continue;
-        r = std::max(r, dist[i]);
-        if (is_bn[i]) rr = std::max(rr, dist[i]);
+        sh.radius = std::max(sh.radius, dist[i]);
+        if (is_bn[i]) sh.row_radius = std::max(sh.row_radius, dist[i]);
     }
-    *radius = r;
-    *row_radius = rr;
-    *root_degree = (uint32_t)__builtin_popcount(adj[0]);
+    sh.min_deg = (uint32_t)__builtin_popcount(adj[0]);
+    return sh;
 }
 
 }  // namespace g2view
 
+namespace {
+
+bool shape_from(uint32_t radius, uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
+                g2view::Shape *sh) {
+    if (row_radius > radius || radius > 15 || (flags & ~(uint32_t)G2_VIEW_UPPER)) return false;
+    sh->radius = radius;
+    sh->row_radius = row_radius;
+    sh->min_deg = min_root_degree;
+    sh->upper = (flags & G2_VIEW_UPPER) != 0;
+    return true;
+}
+
+}  // namespace
+
 extern "C" {
 
 int g2_view_bins(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uint32_t radius, uint32_t row_radius,
-                 uint32_t min_root_degree, uint64_t max_bytes, uint32_t *bin_of, uint32_t *nbins) {
-    if (!row_ptrs || !bin_of || !nbins || (!cols && row_ptrs[n]) || n >= (1ull << 32) || row_radius > radius ||
-        radius > 15)
+                 uint32_t min_root_degree, uint32_t flags, uint64_t max_bytes, uint32_t *bin_of, uint32_t *nbins) {
+    g2view::Shape sh;
+    if (!row_ptrs || !bin_of || !nbins || (!cols && row_ptrs[n]) || n >= (1ull << 32) ||
+        !shape_from(radius, row_radius, min_root_degree, flags, &sh))
         return G2_ERR_INVALID;
-    *nbins = g2view::plan_bins(row_ptrs, cols, n, radius, row_radius, min_root_degree, max_bytes, bin_of);
+    *nbins = g2view::plan_bins(row_ptrs, cols, n, sh, max_bytes, bin_of);
     return G2_OK;
 }
 
 int g2_view_materialize(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, const uint32_t *sources,
-                        uint64_t nsrc, uint32_t radius, uint32_t row_radius, uint32_t min_root_degree,
+                        uint64_t nsrc, uint32_t radius, uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
                         g2_view *out) {
+    g2view::Shape sh;
     if (!row_ptrs || !out || (!sources && nsrc) || (!cols && row_ptrs[n]) || n >= (1ull << 32) ||
-        row_radius > radius || radius > 15)
+        !shape_from(radius, row_radius, min_root_degree, flags, &sh))
         return G2_ERR_INVALID;
     for (uint64_t i = 0; i < nsrc; i++)
         if (sources[i] >= n) return G2_ERR_INVALID;
     memset(out, 0, sizeof(*out));
     g2view::Builder b(row_ptrs, cols, n);
-    const g2view::Sizes s = b.plan(sources, nsrc, radius, row_radius, min_root_degree);
+    const g2view::Sizes s = b.plan(sources, nsrc, sh);
     auto *rp = static_cast<uint64_t *>(malloc(8 * (s.n + 1)));
     auto *fo = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.n, 1)));
     auto *ci = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.m, 1)));
@@ -258,19 +323,32 @@ void g2_view_free(g2_view *v) {
     memset(v, 0, sizeof(*v));
 }
 
-int g2_plan_view_radius(const g2_plan *p, uint32_t *radius, uint32_t *row_radius, uint32_t *root_degree) {
-    if (!p || !radius || !row_radius || !root_degree || p->k < 2 || p->k > G2_MAX_QUERY) return G2_ERR_INVALID;
-    uint32_t pos[G2_MAX_QUERY][8] = {{0}};
-    uint32_t cnt[G2_MAX_QUERY] = {0};
+int g2_plan_view_radius(const g2_plan *p, uint32_t *radius, uint32_t *row_radius, uint32_t *root_degree,
+                        uint32_t *flags) {
+    if (!p || !radius || !row_radius || !root_degree || !flags || p->k < 2 || p->k > G2_MAX_QUERY)
+        return G2_ERR_INVALID;
+    uint32_t bn[8][8] = {{0}}, cop[8][8] = {{0}}, cpos[8][8] = {{0}};
+    uint32_t bnc[8] = {0}, cc[8] = {0};
     for (uint32_t i = 0; i < p->k; i++) {
-        if (p->bn_count[i] > p->k) return G2_ERR_INVALID;
-        cnt[i] = p->bn_count[i];
-        for (uint32_t j = 0; j < cnt[i]; j++) {
+        const uint32_t u = p->order[i];  // query vertex at position i
+        if (u >= p->k || p->bn_count[i] > p->k || p->cond_count[u] > p->k) return G2_ERR_INVALID;
+        bnc[i] = p->bn_count[i];
+        for (uint32_t j = 0; j < bnc[i]; j++) {
             if (p->bn[i][j] >= p->k) return G2_ERR_INVALID;
-            pos[i][j] = p->id2order[p->bn[i][j]];
+            bn[i][j] = p->id2order[p->bn[i][j]];
+        }
+        cc[i] = p->cond_count[u];
+        for (uint32_t j = 0; j < cc[i]; j++) {
+            if (p->cond[u][j][1] >= p->k) return G2_ERR_INVALID;
+            cop[i][j] = p->cond[u][j][0];
+            cpos[i][j] = p->id2order[p->cond[u][j][1]];
         }
     }
-    g2view::plan_radii(p->k, cnt, pos, radius, row_radius, root_degree);
+    const g2view::Shape sh = g2view::plan_shape(p->k, bnc, bn, cc, cop, cpos);
+    *radius = sh.radius;
+    *row_radius = sh.row_radius;
+    *root_degree = sh.min_deg;
+    *flags = sh.upper ? G2_VIEW_UPPER : 0u;
     return G2_OK;
 }
 

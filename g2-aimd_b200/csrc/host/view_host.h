@@ -7,9 +7,11 @@
 // Bron-Kerbosch root, forward lists) give the same answers as in the whole
 // graph.  Vertices within `row_radius` of a source keep their adjacency
 // restricted to B; the others keep an empty row (their neighbours are never
-// scanned).  Replaces the materialisation of view/view_bin.h:61-159, which
-// keeps global ids and copies the full rows of the vertices within hop-1 of
-// the sources.
+// scanned).  With `upper` (queries whose conditions put every matched vertex
+// above the root's image) the ball of source s is walked through vertices
+// larger than s only.  Replaces the materialisation of view/view_bin.h:61-159,
+// which keeps global ids and copies the full rows of the vertices within hop-1
+// of the sources.
 #pragma once
 
 #include <cstdint>
@@ -33,14 +35,21 @@ struct Layout {
     explicit Layout(const Sizes &s);
 };
 
+// How a view is cut.
+struct Shape {
+    uint32_t radius = 1;      // ball radius
+    uint32_t row_radius = 1;  // rows kept up to this depth
+    uint32_t min_deg = 0;     // sources of smaller degree are dropped
+    bool upper = false;       // balls walked through vertices above their source
+};
+
 // One builder per thread; it keeps an n-entry mark array (4 bytes per vertex of
 // the whole graph) between views and clears only what a view touched.
 class Builder {
   public:
     Builder(const uint64_t *rp, const uint32_t *ci, uint64_t n) : rp_(rp), ci_(ci), n_(n) {}
-    // Collect the view of `src` (sources of degree < min_root_degree are
-    // dropped: no embedding is rooted there).  Sources must be < n.
-    Sizes plan(const uint32_t *src, uint64_t nsrc, uint32_t radius, uint32_t row_radius, uint32_t min_root_degree);
+    // Collect the view of `src` (sources must be < n).
+    Sizes plan(const uint32_t *src, uint64_t nsrc, const Shape &shape);
     // Write the planned view: rp[n+1], fo[n] (per vertex, neighbours <= v),
     // ci[m], src[nsrc] (local ids of the kept sources, in the given order),
     // ids[n] (global id of each view vertex; may be null).  Releases the marks.
@@ -50,30 +59,34 @@ class Builder {
 
   private:
     void release();
+    bool relax(uint32_t x, uint32_t d);
     const uint64_t *rp_;
     const uint32_t *ci_;
     uint64_t n_;
-    std::vector<uint32_t> mark_;    // BFS depth, then the local id; kNone outside the view
-    std::vector<uint64_t> ball_;    // (global << 4 | depth) while planning, then sorted
-    std::vector<uint32_t> src_;     // kept sources (global ids)
-    std::vector<uint32_t> deg_;     // view degree of each view vertex
-    uint32_t row_radius_ = 0;
+    std::vector<uint32_t> mark_;   // BFS depth, then the local id; kNone outside the view
+    std::vector<uint32_t> ball_;   // view vertices (global ids), sorted after the walk
+    std::vector<uint8_t> row_;     // view vertex i keeps its row
+    std::vector<uint32_t> src_;    // kept sources (global ids), given order
+    std::vector<uint32_t> deg_;    // view degree of each view vertex
+    std::vector<uint32_t> frontier_, next_;
 };
 
 // Greedy partition of the roots 0..n-1 into bins in id order: a bin is closed
-// when its view would exceed max_bytes (estimated from full degrees, an upper
-// bound of the view's size; a bin holds at least one source).  bin_of[v] for
-// every vertex; returns the number of bins.
-uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint32_t radius, uint32_t row_radius,
-                   uint32_t min_root_degree, uint64_t max_bytes, uint32_t *bin_of);
+// when its view would exceed max_bytes (the view's exact size, counted while
+// the bin grows, up to 48 bytes of alignment; a bin holds at least one source).
+// bin_of[v] for every vertex; returns the number of bins.
+uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Shape &shape, uint64_t max_bytes,
+                   uint32_t *bin_of);
 
-// Radii of a query plan given by positions: k positions, bn_count[i] back
-// neighbours of position i at positions bn_pos[i][j] (< i).  radius = largest
-// distance from position 0 (every embedding vertex lies within it of the
-// root's image); row_radius = largest distance of a position that some later
-// position lists as back neighbour (only those vertices' rows are scanned);
-// root_degree = query degree of position 0.
-void plan_radii(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[8], uint32_t *radius,
-                uint32_t *row_radius, uint32_t *root_degree);
+// What a query plan given by positions needs: k positions, bn_count[i] back
+// neighbours of position i at positions bn_pos[i][j] (< i), cond_count[i]
+// conditions {cond_op[i][j], cond_pos[i][j]} (LESS_THAN: M(i) < M(pos)).
+// radius = largest distance from position 0 (every embedding vertex lies
+// within it of the root's image); row_radius = largest distance of a position
+// that some later position lists as back neighbour (only those vertices' rows
+// are scanned); min_deg = query degree of position 0; upper = the conditions
+// imply M(i) > M(0) for every position i > 0.
+Shape plan_shape(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[8], const uint32_t *cond_count,
+                 const uint32_t (*cond_op)[8], const uint32_t (*cond_pos)[8]);
 
 }  // namespace g2view

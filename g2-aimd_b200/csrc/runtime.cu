@@ -1347,7 +1347,8 @@ struct ViewProducers {
     uint64_t n = 0;
     const uint64_t *bin_start = nullptr;  // roots of bin b: roots[bin_start[b] .. bin_start[b+1])
     const uint32_t *roots = nullptr;
-    uint32_t nbins = 0, radius = 1, row_radius = 1, min_deg = 1;
+    uint32_t nbins = 0;
+    g2view::Shape shape;
     int device = 0;
 
     struct Slot {
@@ -1394,8 +1395,7 @@ struct ViewProducers {
                 const auto t0 = std::chrono::steady_clock::now();
                 ReadyView v;
                 v.bin = bin;
-                v.sizes = b.plan(roots + bin_start[bin], bin_start[bin + 1] - bin_start[bin], radius, row_radius,
-                                 min_deg);
+                v.sizes = b.plan(roots + bin_start[bin], bin_start[bin + 1] - bin_start[bin], shape);
                 if (v.sizes.nsrc) {
                     const g2view::Layout L(v.sizes);
                     {
@@ -1575,12 +1575,18 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
     if (opts && (opts->root_nodes || opts->root_cost || opts->work_bytes || opts->schedule == G2_SCHED_SCORES))
         return G2_ERR_INVALID;
     if (!mce && !ctx->has_plan) return G2_ERR_NO_PLAN;
-    // radii: the query's (MCE: cliques around the root, rows of its neighbours)
-    uint32_t radius = 1, row_radius = 1, min_deg = 1;
-    if (!mce) g2view::plan_radii(ctx->plan.k, ctx->plan.bn_count, ctx->plan.bn_pos, &radius, &row_radius, &min_deg);
-    if (vo && vo->radius) radius = vo->radius;
-    if (vo && vo->row_radius) row_radius = vo->row_radius;
-    if (row_radius > radius || radius > 15) return G2_ERR_INVALID;
+    // view shape: the query's (MCE: cliques around the root, rows of its
+    // neighbours, full balls: X holds the root's smaller neighbours)
+    g2view::Shape shape;
+    shape.min_deg = 1;
+    if (!mce)
+        shape = g2view::plan_shape(ctx->plan.k, ctx->plan.bn_count, ctx->plan.bn_pos, ctx->plan.cond_count,
+                                   ctx->plan.cond_op, ctx->plan.cond_pos);
+    if (vo && vo->radius) shape.radius = vo->radius;
+    if (vo && vo->row_radius) shape.row_radius = vo->row_radius;
+    if (vo && (vo->flags & G2_VIEW_NO_UPPER)) shape.upper = false;
+    if (vo && (vo->flags & ~(uint32_t)G2_VIEW_NO_UPPER)) return G2_ERR_INVALID;
+    if (shape.row_radius > shape.radius || shape.radius > 15) return G2_ERR_INVALID;
     // roots grouped by bin, ascending inside a bin
     std::vector<uint64_t> start((uint64_t)nbins + 1, 0);
     for (uint64_t v = 0; v < n; v++) {
@@ -1633,9 +1639,7 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
         prod.bin_start = start.data();
         prod.roots = roots.data();
         prod.nbins = nbins;
-        prod.radius = radius;
-        prod.row_radius = row_radius;
-        prod.min_deg = min_deg;
+        prod.shape = shape;
         prod.device = ctx->device;
         uint32_t np = vo && vo->producers ? vo->producers : std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
         np = std::min<uint32_t>(np, std::max<uint32_t>(nbins, 1u));

@@ -52,7 +52,7 @@ class G2View(C.Structure):
 
 
 class G2ViewOpts(C.Structure):
-    _fields_ = [("producers", u32), ("radius", u32), ("row_radius", u32), ("reserved", u32)]
+    _fields_ = [("producers", u32), ("radius", u32), ("row_radius", u32), ("flags", u32)]
 
 
 class G2ViewStats(C.Structure):
@@ -65,6 +65,7 @@ class G2ViewStats(C.Structure):
 
 
 G2_VIEW_NO_BIN = 0xFFFFFFFF
+G2_VIEW_UPPER, G2_VIEW_NO_UPPER = 1, 2
 
 _lib = None
 
@@ -104,10 +105,11 @@ def lib():
                               P(u64), C.c_void_p, u32, C.c_void_p, P(G2ViewStats)]),
         "g2_view_match": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, C.c_void_p, u32, P(G2ViewOpts),
                                 P(G2Opts), P(u64), C.c_void_p, P(G2ViewStats)]),
-        "g2_view_materialize": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p, u64, u32, u32, u32, P(G2View)]),
+        "g2_view_materialize": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p, u64, u32, u32, u32, u32,
+                                      P(G2View)]),
         "g2_view_free": (None, [P(G2View)]),
-        "g2_plan_view_radius": (i32, [P(G2Plan), P(u32), P(u32), P(u32)]),
-        "g2_view_bins": (i32, [C.c_void_p, C.c_void_p, u64, u32, u32, u32, u64, C.c_void_p, P(u32)]),
+        "g2_plan_view_radius": (i32, [P(G2Plan), P(u32), P(u32), P(u32), P(u32)]),
+        "g2_view_bins": (i32, [C.c_void_p, C.c_void_p, u64, u32, u32, u32, u32, u64, C.c_void_p, P(u32)]),
         "g2_load_core": (i32, [C.c_void_p, C.c_void_p]),
         "g2_root_features": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p]),
         "g2_model_train": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, u32, u32, C.c_float, u64, C.c_void_p,

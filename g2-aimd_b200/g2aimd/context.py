@@ -43,13 +43,13 @@ class Plan:
     def k(self) -> int:
         return self.raw.k
 
-    def view_radius(self):
-        """(radius, row_radius, root_degree) a view of this plan's roots needs
-        (g2_plan_view_radius)."""
-        r, rr, d = C.c_uint32(), C.c_uint32(), C.c_uint32()
-        check(lib().g2_plan_view_radius(C.byref(self.raw), C.byref(r), C.byref(rr), C.byref(d)),
+    def view_shape(self):
+        """dict(radius, row_radius, min_root_degree, upper): the view this plan's
+        roots need (g2_plan_view_radius); keyword arguments of Graph.view."""
+        r, rr, d, f = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib().g2_plan_view_radius(C.byref(self.raw), C.byref(r), C.byref(rr), C.byref(d), C.byref(f)),
               "g2_plan_view_radius")
-        return r.value, rr.value, d.value
+        return {"radius": r.value, "row_radius": rr.value, "min_root_degree": d.value, "upper": bool(f.value & 1)}
 
     def to_dict(self) -> dict:
         """Same field layout as the reference-planner fixtures."""
@@ -281,20 +281,20 @@ class Context:
         return count.value
 
     # out-of-core runs over view bins: the graph stays in host memory
-    def _view_args(self, graph, bin_of, nbins, producers, radius, row_radius):
-        from ._lib import G2ViewOpts
+    def _view_args(self, graph, bin_of, nbins, producers, radius, row_radius, no_upper):
+        from ._lib import G2_VIEW_NO_UPPER, G2ViewOpts
         bins = np.ascontiguousarray(bin_of, dtype=np.uint32)
         if nbins is None:
             valid = bins[bins != 0xFFFFFFFF]
             nbins = int(valid.max()) + 1 if valid.size else 0
-        vo = G2ViewOpts(producers, radius, row_radius, 0)
+        vo = G2ViewOpts(producers, radius, row_radius, G2_VIEW_NO_UPPER if no_upper else 0)
         return bins, nbins, vo
 
     def view_mce(self, graph, bin_of, nbins=None, hist_len=256, producers=0, radius=0, row_radius=0, **kw):
         """(count, hist, per-bin counts, stats) of maximal cliques of a host graph
         enumerated view bin by view bin (g2_view_mce)."""
         from ._lib import G2ViewStats
-        bins, nbins, vo = self._view_args(graph, bin_of, nbins, producers, radius, row_radius)
+        bins, nbins, vo = self._view_args(graph, bin_of, nbins, producers, radius, row_radius, False)
         o, keep = _opts(**kw)
         count = C.c_uint64()
         hist = np.zeros(hist_len, np.uint64)
@@ -309,13 +309,14 @@ class Context:
         self.graph, self.n = None, 0
         return count.value, hist, per_bin[:nbins], st.to_dict()
 
-    def view_match(self, graph, bin_of, plan: Plan = None, nbins=None, producers=0, radius=0, row_radius=0, **kw):
+    def view_match(self, graph, bin_of, plan: Plan = None, nbins=None, producers=0, radius=0, row_radius=0,
+                   no_upper=False, **kw):
         """(count, per-bin counts, stats) of the plan's matches in a host graph,
         view bin by view bin (g2_view_match)."""
         from ._lib import G2ViewStats
         if plan is not None:
             self.set_plan(plan)
-        bins, nbins, vo = self._view_args(graph, bin_of, nbins, producers, radius, row_radius)
+        bins, nbins, vo = self._view_args(graph, bin_of, nbins, producers, radius, row_radius, no_upper)
         o, keep = _opts(**kw)
         count = C.c_uint64()
         per_bin = np.zeros(max(nbins, 1), np.uint64)

@@ -109,16 +109,18 @@ class Graph:
         return nb.value, bins
 
     # ----------------------------------------------------- views (out of core)
-    def view(self, sources, radius=1, row_radius=None, min_root_degree=0):
+    def view(self, sources, radius=1, row_radius=None, min_root_degree=0, upper=False):
         """(view graph, local sources, global ids) of the ball of `radius` around
         `sources` (g2_view_materialize): ids ascending in global order, rows kept
-        for vertices within row_radius (default: radius), restricted to the ball."""
+        for vertices within row_radius (default: radius), restricted to the ball;
+        upper: each source's ball walked through vertices above it."""
         from ._lib import G2View
         src = np.ascontiguousarray(sources, dtype=np.uint32)
         v = G2View()
         rr = radius if row_radius is None else row_radius
         check(lib().g2_view_materialize(_ptr(self.row_ptrs), _ptr(self.cols), self.n, _ptr(src), src.size,
-                                        radius, rr, min_root_degree, C.byref(v)), "g2_view_materialize")
+                                        radius, rr, min_root_degree, int(bool(upper)), C.byref(v)),
+              "g2_view_materialize")
         try:
             n, m, ns = v.n, v.m, v.nsrc
             rp = np.ctypeslib.as_array(v.row_ptrs, shape=(n + 1,)).copy()
@@ -134,14 +136,14 @@ class Graph:
         g.max_fwd = max_fwd
         return g, lsrc, ids
 
-    def view_bins(self, max_bytes, radius=1, row_radius=None, min_root_degree=0):
+    def view_bins(self, max_bytes, radius=1, row_radius=None, min_root_degree=0, upper=False):
         """(nbins, bin_of) from g2_view_bins: roots in id order, a bin closes when
         its view would exceed max_bytes."""
         bins = np.zeros(self.n, np.uint32)
         nb = C.c_uint32()
         rr = radius if row_radius is None else row_radius
         check(lib().g2_view_bins(_ptr(self.row_ptrs), _ptr(self.cols), self.n, radius, rr, min_root_degree,
-                                 int(max_bytes), _ptr(bins), C.byref(nb)), "g2_view_bins")
+                                 int(bool(upper)), int(max_bytes), _ptr(bins), C.byref(nb)), "g2_view_bins")
         return nb.value, bins
 
     # ----------------------------------------------------- degeneracy order

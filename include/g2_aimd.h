@@ -279,11 +279,13 @@ int g2_degeneracy_order_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core);
  * and caller scores (G2_SCHED_SCORES) are not available here.
  */
 #define G2_VIEW_NO_BIN 0xffffffffu
+#define G2_VIEW_UPPER 1u     /* balls walked through vertices above their source */
+#define G2_VIEW_NO_UPPER 2u  /* g2_view_opts: full balls even where the query allows upper ones */
 typedef struct g2_view_opts {
     uint32_t producers;   /* host threads building views (0 = min(8, cores))    */
     uint32_t radius;      /* ball radius (0 = from the query: 1 for MCE)         */
     uint32_t row_radius;  /* rows kept up to this distance (0 = from the query)  */
-    uint32_t reserved;
+    uint32_t flags;       /* G2_VIEW_NO_UPPER                                    */
 } g2_view_opts;
 typedef struct g2_view_stats {
     uint64_t bins;            /* views enumerated (bins with a root of enough degree) */
@@ -299,8 +301,9 @@ int g2_view_mce(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, uin
                 const uint32_t *bin_of, uint32_t nbins, const g2_view_opts *vopts,
                 const g2_opts *opts, uint64_t *count, uint64_t *hist, uint32_t hist_len,
                 uint64_t *bin_counts, g2_view_stats *stats);
-/* Matches of the plan set with g2_set_plan (radius and row radius from its
- * query; roots of degree below the query root's degree are skipped). */
+/* Matches of the plan set with g2_set_plan (view shape from its query, as
+ * g2_plan_view_radius gives it; roots of degree below the query root's degree
+ * are skipped). */
 int g2_view_match(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n,
                   const uint32_t *bin_of, uint32_t nbins, const g2_view_opts *vopts,
                   const g2_opts *opts, uint64_t *count, uint64_t *bin_counts,
@@ -405,12 +408,15 @@ int g2_read_vbmap(const char *path, uint64_t n, uint32_t *nbins,
  * Views (host only).  The view of a root set S is the ball B of radius `radius`
  * around S, ids renumbered 0..|B|-1 in ascending global order (so id
  * comparisons agree with the whole graph); vertices within `row_radius` of S
- * keep their neighbours inside B, the others an empty row.  Every embedding
- * rooted in S lies in B and uses only rows of vertices within the query's
- * back-neighbour distance, so a search over the view from S's local ids finds
- * exactly what it finds in the whole graph (view/view_bin.h:40-159 keeps
- * global ids and whole rows instead).  Sources of degree < min_root_degree are
- * dropped.  Arrays are malloc'd; release them with g2_view_free.
+ * keep their neighbours inside B, the others an empty row.  With G2_VIEW_UPPER
+ * the ball of each source s is walked through vertices larger than s only
+ * (queries whose conditions place every matched vertex above the root's
+ * image: cliques, cycles).  Every embedding rooted in S lies in B and uses only
+ * rows of vertices within the query's back-neighbour distance, so a search
+ * over the view from S's local ids finds exactly what it finds in the whole
+ * graph (view/view_bin.h:40-159 keeps global ids and whole rows instead).
+ * Sources of degree < min_root_degree are dropped.  Arrays are malloc'd;
+ * release them with g2_view_free.
  */
 typedef struct g2_view {
     uint64_t *row_ptrs;     /* n + 1                                          */
@@ -423,18 +429,21 @@ typedef struct g2_view {
 } g2_view;
 int g2_view_materialize(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n,
                         const uint32_t *sources, uint64_t nsrc, uint32_t radius,
-                        uint32_t row_radius, uint32_t min_root_degree, g2_view *out);
+                        uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
+                        g2_view *out);
 void g2_view_free(g2_view *view);
-/* Radius, row radius and root degree a plan needs (system/plan.h:51-73 derives
- * the reference's single hop count the same way). */
+/* Radius, row radius, root degree and flags (G2_VIEW_UPPER) a plan's views
+ * need (system/plan.h:51-73 derives the reference's single hop count from the
+ * same query distances). */
 int g2_plan_view_radius(const g2_plan *plan, uint32_t *radius, uint32_t *row_radius,
-                        uint32_t *root_degree);
+                        uint32_t *root_degree, uint32_t *flags);
 /* Greedy bins over the roots 0..n-1 in id order: a bin closes when its view
- * would exceed max_bytes (an estimate from full degrees, so an upper bound; a
- * bin holds at least one root).  bin_of: n entries (a .vbmap body). */
+ * would exceed max_bytes (its exact size, counted as the bin grows, up to 48
+ * bytes of alignment; a bin holds at least one root).  bin_of: n entries (a
+ * .vbmap body). */
 int g2_view_bins(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uint32_t radius,
-                 uint32_t row_radius, uint32_t min_root_degree, uint64_t max_bytes,
-                 uint32_t *bin_of, uint32_t *nbins);
+                 uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
+                 uint64_t max_bytes, uint32_t *bin_of, uint32_t *nbins);
 
 /*
  * Degeneracy order (kmeans/kcore.cpp:103-191): k-core shells in increasing core

@@ -77,14 +77,14 @@ def test_view_match_equals_oracle(vctx, orc, g2, q):
     g = g2.Graph.rmat(11, 8, seed=4).degeneracy_recoded()
     plan = Plan.preset(q)
     want = orc.match(g, plan, threads=4)["count"]
-    radius, row_radius, root_degree = plan.view_radius()
-    nb, bin_of = g.view_bins(max_bytes=64 << 10, radius=radius, row_radius=row_radius,
-                             min_root_degree=root_degree)
-    assert nb > 8
-    count, per_bin, st = vctx.view_match(g, bin_of, plan, producers=3)
-    assert count == want, (q, count, want)
-    assert int(per_bin.sum()) == count
-    assert st["bins"] >= 1
+    sh = plan.view_shape()
+    for no_upper in sorted({True, not sh["upper"]}):
+        nb, bin_of = g.view_bins(max_bytes=32 << 10, **dict(sh, upper=sh["upper"] and not no_upper))
+        assert nb > 8
+        count, per_bin, st = vctx.view_match(g, bin_of, plan, producers=3, no_upper=no_upper)
+        assert count == want, (q, no_upper, count, want)
+        assert int(per_bin.sum()) == count
+        assert st["bins"] >= 1
 
 
 def test_view_match_plan_walk_handoff(vctx, orc, g2):

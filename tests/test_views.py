@@ -10,26 +10,27 @@ import pytest
 from helpers import random_graph, small_graphs
 
 
-def py_view(g, sources, radius, row_radius, min_deg):
-    """Direct construction: BFS depths from the kept sources, ascending ids,
+def py_view(g, sources, radius, row_radius, min_deg, upper=False):
+    """Direct construction: per kept source, BFS depths (through vertices above
+    the source when upper); a vertex's depth is its smallest; ascending ids;
     rows of vertices within row_radius restricted to the ball."""
     rp, ci = g.row_ptrs, g.cols
     deg = np.diff(rp)
     kept = [int(s) for s in sources if deg[s] >= min_deg]
     depth = {}
-    frontier = []
-    for s in kept:
-        if s not in depth:
-            depth[s] = 0
-            frontier.append(s)
-    for d in range(radius):
-        nxt = []
-        for x in frontier:
-            for u in ci[rp[x]:rp[x + 1]].tolist():
-                if u not in depth:
-                    depth[u] = d + 1
-                    nxt.append(u)
-        frontier = nxt
+    for s in set(kept):
+        seen = {s: 0}
+        frontier = [s]
+        for d in range(radius):
+            nxt = []
+            for x in frontier:
+                for u in ci[rp[x]:rp[x + 1]].tolist():
+                    if u not in seen and (not upper or u > s):
+                        seen[u] = d + 1
+                        nxt.append(u)
+            frontier = nxt
+        for x, d in seen.items():
+            depth[x] = min(depth.get(x, d), d)
     ids = sorted(depth)
     local = {g_: i for i, g_ in enumerate(ids)}
     rows = []
@@ -41,9 +42,9 @@ def py_view(g, sources, radius, row_radius, min_deg):
     return ids, rows, [local[s] for s in kept]
 
 
-def check_view(g, sources, radius, row_radius, min_deg=0):
-    v, lsrc, ids = g.view(sources, radius=radius, row_radius=row_radius, min_root_degree=min_deg)
-    want_ids, want_rows, want_src = py_view(g, sources, radius, row_radius, min_deg)
+def check_view(g, sources, radius, row_radius, min_deg=0, upper=False):
+    v, lsrc, ids = g.view(sources, radius=radius, row_radius=row_radius, min_root_degree=min_deg, upper=upper)
+    want_ids, want_rows, want_src = py_view(g, sources, radius, row_radius, min_deg, upper)
     assert ids.tolist() == want_ids
     assert lsrc.tolist() == want_src
     assert v.n == len(want_ids) and v.row_ptrs[0] == 0
@@ -64,15 +65,17 @@ def test_view_structure_small_graphs(g2):
             for trial in range(3):
                 k = int(rng.integers(0, max(1, g.n) + 1))
                 src = rng.choice(g.n, size=min(k, g.n), replace=False) if g.n else np.zeros(0, np.uint32)
-                check_view(g, src, radius, row_radius, min_deg=int(trial == 2) * 2)
+                for upper in (False, True):
+                    check_view(g, src, radius, row_radius, min_deg=int(trial == 2) * 2, upper=upper)
 
 
 def test_view_structure_rmat(g2):
     g = g2.Graph.rmat(10, 8, seed=5)
     rng = np.random.default_rng(11)
     for radius, row_radius in ((1, 1), (2, 1), (2, 2)):
-        src = np.sort(rng.choice(g.n, size=40, replace=False))
-        check_view(g, src, radius, row_radius)
+        for upper in (False, True):
+            src = rng.choice(g.n, size=40, replace=False)  # unsorted: upper walks sort them
+            check_view(g, src, radius, row_radius, upper=upper)
 
 
 def test_view_duplicates_and_empty(g2):
@@ -93,23 +96,42 @@ def test_view_rejects_bad_arguments(g2):
     v = G2View()
     lib = g2.lib()
     rp, ci = g.row_ptrs.ctypes.data_as(C.c_void_p), g.cols.ctypes.data_as(C.c_void_p)
-    assert lib.g2_view_materialize(rp, ci, g.n, src.ctypes.data_as(C.c_void_p), 1, 1, 1, 0, C.byref(v)) == -1
+    assert lib.g2_view_materialize(rp, ci, g.n, src.ctypes.data_as(C.c_void_p), 1, 1, 1, 0, 0, C.byref(v)) == -1
     src = np.array([0], np.uint32)
-    assert lib.g2_view_materialize(rp, ci, g.n, src.ctypes.data_as(C.c_void_p), 1, 1, 2, 0, C.byref(v)) == -1
+    sp = src.ctypes.data_as(C.c_void_p)
+    assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 2, 0, 0, C.byref(v)) == -1  # row radius > radius
+    assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 1, 0, 4, C.byref(v)) == -1  # unknown flag
+    assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 1, 0, 1, C.byref(v)) == 0
+    lib.g2_view_free(C.byref(v))
 
 
-def plan_radii_py(plan):
-    """Distances from position 0 in the query graph of the plan's back neighbours."""
+def plan_shape_py(plan):
+    """Distances from position 0 in the query graph of the plan's back
+    neighbours; upper = every position provably above position 0."""
     r = plan.raw
     k = r.k
     adj = [set() for _ in range(k)]
     is_bn = [False] * k
+    gt = set()  # (a, b): M(a) > M(b), positions
     for i in range(k):
         for j in range(r.bn_count[i]):
             p = r.id2order[r.bn[i][j]]
             adj[i].add(p)
             adj[p].add(i)
             is_bn[p] = True
+        u = r.order[i]
+        for j in range(r.cond_count[u]):
+            op, w = r.cond[u][j][0], r.id2order[r.cond[u][j][1]]
+            if op == 1:
+                gt.add((i, w))
+            elif op == 0:
+                gt.add((w, i))
+    changed = True
+    while changed:
+        extra = {(a, c) for (a, b) in gt for (b2, c) in gt if b == b2} - gt
+        changed = bool(extra)
+        gt |= extra
+    upper = all((i, 0) in gt for i in range(1, k))
     dist = {0: 0}
     fr = [0]
     while fr:
@@ -120,25 +142,28 @@ def plan_radii_py(plan):
                     dist[y] = dist[x] + 1
                     nxt.append(y)
         fr = nxt
-    return max(dist.values()), max(dist[i] for i in range(k) if is_bn[i]), len(adj[0])
+    return {"radius": max(dist.values()), "row_radius": max(dist[i] for i in range(k) if is_bn[i]),
+            "min_root_degree": len(adj[0]), "upper": upper}
 
 
 @pytest.mark.parametrize("q", [0, 1, 2, 3, 4, 5, 6, 23, 24, 25])
-def test_plan_view_radius(q):
+def test_plan_view_shape(q):
     from g2aimd.context import Plan
     p = Plan.preset(q)
-    assert p.view_radius() == plan_radii_py(p)
+    sh = p.view_shape()
+    assert sh == plan_shape_py(p)
     # the reference's single hop count covers the view's rows
-    radius, row_radius, root_degree = p.view_radius()
-    assert row_radius <= p.raw.hop - 1 <= radius
-    assert root_degree == p.raw.root_degree
+    assert sh["row_radius"] <= p.raw.hop - 1 <= sh["radius"]
+    assert sh["min_root_degree"] == p.raw.root_degree
 
 
-def test_known_radii():
+def test_known_shapes():
     from g2aimd.context import Plan
-    assert Plan.preset(0).view_radius() == (1, 1, 2)   # triangle
-    assert Plan.preset(1).view_radius() == (2, 1, 2)   # 4-cycle: opposite corner at distance 2
-    assert Plan.preset(24).view_radius() == (1, 1, 3)  # 4-clique
+    tri, c4, diamond, k4 = (Plan.preset(q).view_shape() for q in (0, 1, 2, 24))
+    assert (tri["radius"], tri["row_radius"], tri["upper"]) == (1, 1, True)
+    assert (c4["radius"], c4["row_radius"], c4["upper"]) == (2, 1, True)  # opposite corner at distance 2
+    assert (diamond["radius"], diamond["upper"]) == (1, False)  # conditions only "!=" against the root
+    assert (k4["radius"], k4["min_root_degree"], k4["upper"]) == (1, 3, True)
 
 
 def bins_from_bounds(n, bounds):
@@ -191,15 +216,27 @@ def test_views_sum_to_whole_graph_match(g2, orc, q):
     g = random_graph(g2.Graph, 300, 0.05, 21, planted=[tuple(range(0, 24, 2))]).degeneracy_recoded()
     plan = Plan.preset(q)
     want = orc.match(g, plan)["count"]
-    radius, row_radius, root_degree = plan.view_radius()
+    sh = plan.view_shape()
     for nbins in (1, 5, 40):
         bin_of = np.random.default_rng(q * 100 + nbins).integers(0, nbins, g.n).astype(np.uint32)
-        total = 0
-        for src in by_bin(bin_of, nbins):
-            v, lsrc, _ = g.view(src, radius=radius, row_radius=row_radius, min_root_degree=root_degree)
-            if lsrc.size:
-                total += orc.match(v, plan, roots=lsrc)["count"]
-        assert total == want, (q, nbins, total, want)
+        for upper in sorted({False, sh["upper"]}):
+            total = 0
+            for src in by_bin(bin_of, nbins):
+                v, lsrc, _ = g.view(src, **dict(sh, upper=upper))
+                if lsrc.size:
+                    total += orc.match(v, plan, roots=lsrc)["count"]
+            assert total == want, (q, nbins, upper, total, want)
+
+
+def test_upper_views_are_smaller(g2):
+    """Where the query allows it, upper views skip everything below each source."""
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(11, 8, seed=3).degeneracy_recoded()
+    sh = Plan.preset(24).view_shape()
+    src = np.arange(0, g.n, 7, dtype=np.uint32)
+    full, _, _ = g.view(src, **dict(sh, upper=False))
+    up, _, _ = g.view(src, **sh)
+    assert up.m < full.m and up.n < full.n
 
 
 def test_view_too_small_radius_misses_matches(g2, orc):
@@ -225,20 +262,27 @@ def view_bytes(v, nsrc):
     return a16(src + 4 * nsrc)
 
 
-@pytest.mark.parametrize("radius,row_radius", [(1, 1), (2, 1)])
-def test_view_bins_respect_budget(g2, radius, row_radius):
+@pytest.mark.parametrize("radius,row_radius,upper", [(1, 1, False), (2, 1, False), (1, 1, True), (2, 1, True),
+                                                    (2, 2, True)])
+def test_view_bins_respect_budget(g2, radius, row_radius, upper):
     g = g2.Graph.rmat(10, 8, seed=9)
     budget = 48 << 10
-    nb, bin_of = g.view_bins(max_bytes=budget, radius=radius, row_radius=row_radius)
+    nb, bin_of = g.view_bins(max_bytes=budget, radius=radius, row_radius=row_radius, upper=upper)
     assert nb >= 2
     assert bin_of.max() == nb - 1
     assert np.all(np.diff(bin_of.astype(np.int64)) >= 0)  # ranges of ids, in order
-    for src in by_bin(bin_of, nb):
+    bins = by_bin(bin_of, nb)
+    for b, src in enumerate(bins):
         assert src.size > 0
-        v, lsrc, _ = g.view(src, radius=radius, row_radius=row_radius)
-        # the estimate bounds the view (up to the layout's alignment padding)
-        assert src.size == 1 or view_bytes(v, lsrc.size) <= budget + 48
-    nb_big, _ = g.view_bins(max_bytes=1 << 40, radius=radius, row_radius=row_radius)
+        v, lsrc, _ = g.view(src, radius=radius, row_radius=row_radius, upper=upper)
+        size = view_bytes(v, lsrc.size)
+        # the bin's view is counted exactly (up to the layout's alignment padding) ...
+        assert src.size == 1 or size <= budget + 48
+        # ... so the bin was closed because the next root did not fit
+        if b + 1 < nb:
+            v2, l2, _ = g.view(np.append(src, bins[b + 1][0]), radius=radius, row_radius=row_radius, upper=upper)
+            assert view_bytes(v2, l2.size) > budget - 48
+    nb_big, _ = g.view_bins(max_bytes=1 << 40, radius=radius, row_radius=row_radius, upper=upper)
     assert nb_big == 1
 
 
