@@ -17,6 +17,12 @@ namespace g2view {
 
 namespace {
 inline uint64_t align16(uint64_t x) { return (x + 15u) & ~15ull; }
+
+// First entry of row x that is >= lo (rows are sorted).
+inline uint64_t row_from(const uint64_t *rp, const uint32_t *ci, uint32_t x, uint32_t lo) {
+    if (lo == 0) return rp[x];
+    return (uint64_t)(std::lower_bound(ci + rp[x], ci + rp[x + 1], lo) - ci);
+}
 }  // namespace
 
 Layout::Layout(const Sizes &s) {
@@ -52,9 +58,9 @@ Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
         for (uint32_t d = 0; d < sh.radius && !frontier_.empty(); d++) {
             next_.clear();
             for (uint32_t x : frontier_)
-                for (uint64_t e = rp_[x]; e < rp_[x + 1]; e++) {
+                for (uint64_t e = upper ? row_from(rp_, ci_, x, lo_excl + 1) : rp_[x]; e < rp_[x + 1]; e++) {
                     const uint32_t u = ci_[e];
-                    if ((!upper || u > lo_excl) && relax(u, d + 1)) next_.push_back(u);
+                    if (relax(u, d + 1)) next_.push_back(u);
                 }
             frontier_.swap(next_);
         }
@@ -81,29 +87,37 @@ Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
     // ascending global order = local ids; rows where the depth allows; marks become local ids
     std::sort(ball_.begin(), ball_.end());
     const uint64_t nv = ball_.size();
+    // nothing below the smallest view vertex is in the view: rows are read from there
+    lo_ = nv ? ball_[0] : 0u;
     row_.resize(nv);
     for (uint64_t i = 0; i < nv; i++) {
         row_[i] = mark_[ball_[i]] <= sh.row_radius;
         mark_[ball_[i]] = (uint32_t)i;
     }
+    // one pass over the kept rows: local columns staged here, copied out by fill
     Sizes s;
     s.n = nv;
     s.nsrc = src_.size();
     deg_.assign(nv, 0u);
+    fo_.assign(nv, 0u);
+    cols_.clear();
     for (uint64_t i = 0; i < nv; i++) {
         if (!row_[i]) continue;
         const uint32_t g = ball_[i];
-        uint32_t d = 0, back = 0;
-        for (uint64_t e = rp_[g]; e < rp_[g + 1]; e++) {
+        const uint64_t before = cols_.size();
+        uint32_t back = 0;
+        for (uint64_t e = row_from(rp_, ci_, g, lo_); e < rp_[g + 1]; e++) {
             const uint32_t l = mark_[ci_[e]];
             if (l == kNone) continue;
-            d++;
+            cols_.push_back(l);
             back += l <= i;
         }
+        const uint32_t d = (uint32_t)(cols_.size() - before);
         deg_[i] = d;
-        s.m += d;
+        fo_[i] = back;
         s.max_fwd = std::max(s.max_fwd, d - back);
     }
+    s.m = cols_.size();
     return s;
 }
 
@@ -111,20 +125,12 @@ void Builder::fill(uint64_t *rp, uint32_t *fo, uint32_t *ci, uint32_t *src, uint
     uint64_t off = 0;
     for (uint64_t i = 0; i < ball_.size(); i++) {
         rp[i] = off;
-        const uint32_t g = ball_[i];
-        if (ids) ids[i] = g;
-        uint32_t back = 0;
-        if (deg_[i]) {
-            for (uint64_t e = rp_[g]; e < rp_[g + 1]; e++) {
-                const uint32_t l = mark_[ci_[e]];
-                if (l == kNone) continue;
-                ci[off++] = l;
-                back += l <= i;
-            }
-        }
-        fo[i] = back;
+        off += deg_[i];
+        if (ids) ids[i] = ball_[i];
     }
     rp[ball_.size()] = off;
+    if (!fo_.empty()) memcpy(fo, fo_.data(), 4 * fo_.size());
+    if (!cols_.empty()) memcpy(ci, cols_.data(), 4 * cols_.size());
     for (uint64_t i = 0; i < src_.size(); i++) src[i] = mark_[src_[i]];
     release();
 }
@@ -146,6 +152,7 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
     std::vector<uint32_t> depth(n, kNone), touched, frontier, next;
     uint64_t bytes = 8, delta = 0;
     uint32_t bin = 0, nsrc = 0;
+    uint32_t lo = 0;  // upper walks: no vertex below the bin's first source is in its ball
     auto relax = [&](uint32_t x, uint32_t d) {
         const uint32_t old = depth[x];
         if (old != kNone && old <= d) return false;
@@ -157,7 +164,7 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
             touched.push_back(x);
         }
         if (fresh || gains_row) {
-            for (uint64_t e = rp[x]; e < rp[x + 1]; e++) {
+            for (uint64_t e = row_from(rp, ci, x, lo); e < rp[x + 1]; e++) {
                 const uint32_t y = ci[e];
                 if (y == x || depth[y] == kNone) continue;
                 if (gains_row) delta += 4;                             // x -> y
@@ -173,9 +180,9 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
         for (uint32_t d = 0; d < sh.radius && !frontier.empty(); d++) {
             next.clear();
             for (uint32_t x : frontier)
-                for (uint64_t e = rp[x]; e < rp[x + 1]; e++) {
+                for (uint64_t e = sh.upper ? row_from(rp, ci, x, s + 1) : rp[x]; e < rp[x + 1]; e++) {
                     const uint32_t u = ci[e];
-                    if ((!sh.upper || u > s) && relax(u, d + 1)) next.push_back(u);
+                    if (relax(u, d + 1)) next.push_back(u);
                 }
             frontier.swap(next);
         }
@@ -186,6 +193,7 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
             bin_of[v] = bin;  // no embedding is rooted here: no size
             continue;
         }
+        if (sh.upper && nsrc == 0) lo = (uint32_t)v;
         uint64_t d = add((uint32_t)v);
         if (nsrc > 0 && bytes + d > max_bytes) {
             for (uint32_t x : touched) depth[x] = kNone;
@@ -193,6 +201,7 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
             bin++;
             bytes = 8;
             nsrc = 0;
+            if (sh.upper) lo = (uint32_t)v;
             d = add((uint32_t)v);
         }
         bytes += d;

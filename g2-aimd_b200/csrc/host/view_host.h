@@ -68,7 +68,10 @@ class Builder {
     std::vector<uint8_t> row_;     // view vertex i keeps its row
     std::vector<uint32_t> src_;    // kept sources (global ids), given order
     std::vector<uint32_t> deg_;    // view degree of each view vertex
+    std::vector<uint32_t> fo_;     // view neighbours <= v of each view vertex
+    std::vector<uint32_t> cols_;   // the view's columns, staged between plan and fill
     std::vector<uint32_t> frontier_, next_;
+    uint32_t lo_ = 0;  // smallest view vertex: row scans start at the first entry >= it
 };
 
 // Greedy partition of the roots 0..n-1 into bins in id order: a bin is closed

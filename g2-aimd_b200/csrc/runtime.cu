@@ -104,7 +104,13 @@ struct g2_ctx {
     uint64_t root_cliques_cap = 0;
     unsigned long long *d_gcount = nullptr;
     uint64_t gcount_cap = 0;
+    // out-of-core view runs: pinned host slots and the two device slots, kept
+    // between calls (pinning and device allocation stall other CUDA calls)
+    std::vector<std::pair<void *, uint64_t>> view_host;
+    void *view_dev[2] = {nullptr, nullptr};
+    uint64_t view_dev_cap[2] = {0, 0};
     bool timed = false;
+    int timed_passes = 0;  // enumeration passes the last timed run recorded (MCE 3, match 1)
     unsigned long long *d_work = nullptr;
     cudaStream_t last_stream = nullptr;
 };
@@ -485,6 +491,7 @@ int status_to_code(int st) {
 // Events for pass timing and the device work counter, as the flags ask.
 int prepare_flags(g2_ctx *ctx, uint32_t flags, cudaStream_t st) {
     ctx->timed = (flags & G2_FLAG_TIME_KERNELS) != 0;
+    ctx->timed_passes = 0;
     ctx->last_stream = st;
     if (ctx->timed && !ctx->ev[0]) {
         for (auto &e : ctx->ev) G2_TRY(cudaEventCreate(&e));
@@ -688,6 +695,7 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     }
     ctx->last_mce = base;
     ctx->last_mce_wpl = wpl_for(ctx->max_fwd);
+    if (ctx->timed) ctx->timed_passes = 3;
     return G2_OK;
 }
 
@@ -797,6 +805,7 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
     if (e != cudaSuccess) return fail_cuda(ctx, e, "match_launch");
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[1], st));
     ctx->launches++;
+    if (ctx->timed) ctx->timed_passes = 1;
     return G2_OK;
 }
 
@@ -840,7 +849,7 @@ const char *g2_last_cuda_error(const g2_ctx *ctx) { return ctx ? ctx->cuda_err.c
 uint64_t g2_last_launch_count(const g2_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
 int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms) {
-    if (!ctx || !ms || pass < 0 || pass > 2 || !ctx->timed) return G2_ERR_INVALID;
+    if (!ctx || !ms || pass < 0 || pass >= ctx->timed_passes || !ctx->timed) return G2_ERR_INVALID;
     G2_TRY(cudaEventSynchronize(ctx->ev[pass + 1]));
     G2_TRY(cudaEventElapsedTime(ms, ctx->ev[pass], ctx->ev[pass + 1]));
     return G2_OK;
@@ -973,6 +982,10 @@ int g2_close(g2_ctx *ctx) {
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->h_spill) cudaFree(ctx->h_spill);
+    for (auto &h : ctx->view_host)
+        if (h.first) cudaFreeHost(h.first);
+    for (void *b : ctx->view_dev)
+        if (b) cudaFree(b);
     delete ctx;
     return G2_OK;
 }
@@ -1351,11 +1364,7 @@ struct ViewProducers {
     g2view::Shape shape;
     int device = 0;
 
-    struct Slot {
-        void *buf = nullptr;
-        uint64_t cap = 0;
-    };
-    std::vector<Slot> slots;
+    std::vector<std::pair<void *, uint64_t>> *slots = nullptr;  // pinned, owned by the context
     std::mutex mu;
     std::condition_variable cv;
     std::vector<int> free_slots;
@@ -1368,7 +1377,7 @@ struct ViewProducers {
     std::vector<std::thread> threads;
 
     void start(uint32_t producers, uint32_t nslots) {
-        slots.resize(nslots);
+        if (slots->size() < nslots) slots->resize(nslots, {nullptr, 0});
         for (uint32_t i = 0; i < nslots; i++) free_slots.push_back((int)i);
         running = producers;
         for (uint32_t t = 0; t < producers; t++) threads.emplace_back([this] { produce(); });
@@ -1405,21 +1414,30 @@ struct ViewProducers {
                         v.slot = free_slots.back();
                         free_slots.pop_back();
                     }
-                    Slot &s = slots[v.slot];
-                    if (s.cap < L.bytes) {
-                        const uint64_t want = std::max<uint64_t>(L.bytes, s.cap + s.cap / 2);
-                        if (s.buf) cudaFreeHost(s.buf);
-                        s.buf = nullptr;
-                        s.cap = 0;
-                        if (cudaHostAlloc(&s.buf, want, cudaHostAllocPortable) != cudaSuccess) {
+                    void *buf = nullptr;
+                    uint64_t want = 0;
+                    {
+                        std::lock_guard<std::mutex> g(mu);  // slot sizes are read by every producer
+                        buf = (*slots)[v.slot].first;
+                        if ((*slots)[v.slot].second < L.bytes) {
+                            // straight to the largest slot so far: slots settle after one call
+                            want = std::max<uint64_t>(L.bytes, (*slots)[v.slot].second * 3 / 2);
+                            for (const auto &o : *slots) want = std::max(want, o.second);
+                            (*slots)[v.slot] = {nullptr, 0};
+                        }
+                    }
+                    if (want) {
+                        if (buf) cudaFreeHost(buf);
+                        buf = nullptr;
+                        if (cudaHostAlloc(&buf, want, cudaHostAllocPortable) != cudaSuccess) {
                             cudaGetLastError();
-                            s.buf = nullptr;
                             fail(G2_ERR_OOM);
                             break;
                         }
-                        s.cap = want;
+                        std::lock_guard<std::mutex> g(mu);
+                        (*slots)[v.slot] = {buf, want};
                     }
-                    b.fill_packed(s.buf, v.sizes);
+                    b.fill_packed(buf, v.sizes);
                 }
                 const double ms = ms_between(t0, std::chrono::steady_clock::now());
                 std::lock_guard<std::mutex> g(mu);
@@ -1461,8 +1479,6 @@ struct ViewProducers {
             cv.notify_all();
         }
         for (auto &t : threads) t.join();
-        for (auto &s : slots)
-            if (s.buf) cudaFreeHost(s.buf);
     }
 };
 
@@ -1470,19 +1486,34 @@ struct ViewProducers {
 // that order uploads against the enumeration on the legacy stream.
 struct ViewDevice {
     g2_ctx *ctx;
-    void *buf[2] = {nullptr, nullptr};
-    uint64_t cap[2] = {0, 0};
+    void **buf;       // the context's two device slots
+    uint64_t *cap;
     cudaStream_t copy = nullptr;
     cudaEvent_t copied[2] = {nullptr, nullptr}, done[2] = {nullptr, nullptr};
-    explicit ViewDevice(g2_ctx *c) : ctx(c) {}
+    cudaEvent_t t_copy[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // around each slot's upload
+    cudaEvent_t t_run[2] = {nullptr, nullptr};                             // around the current run
+    explicit ViewDevice(g2_ctx *c) : ctx(c), buf(c->view_dev), cap(c->view_dev_cap) {}
 
     int init() {
         G2_TRY(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
         for (int d = 0; d < 2; d++) {
             G2_TRY(cudaEventCreateWithFlags(&copied[d], cudaEventDisableTiming));
             G2_TRY(cudaEventCreateWithFlags(&done[d], cudaEventDisableTiming));
+            G2_TRY(cudaEventCreate(&t_copy[d][0]));
+            G2_TRY(cudaEventCreate(&t_copy[d][1]));
+            G2_TRY(cudaEventCreate(&t_run[d]));
         }
         return G2_OK;
+    }
+
+    // Device milliseconds of slot d's last upload and of the last run (both ended).
+    float copy_ms(int d) const {
+        float ms = 0.f;
+        return cudaEventElapsedTime(&ms, t_copy[d][0], t_copy[d][1]) == cudaSuccess ? ms : 0.f;
+    }
+    float run_ms() const {
+        float ms = 0.f;
+        return cudaEventElapsedTime(&ms, t_run[0], t_run[1]) == cudaSuccess ? ms : 0.f;
     }
 
     // Upload a built view into device slot d once that slot's last run is done.
@@ -1497,7 +1528,9 @@ struct ViewDevice {
             cap[d] = want;
         }
         G2_TRY(cudaStreamWaitEvent(copy, done[d], 0));
+        G2_TRY(cudaEventRecord(t_copy[d][0], copy));
         G2_TRY(cudaMemcpyAsync(buf[d], host, L.bytes, cudaMemcpyHostToDevice, copy));
+        G2_TRY(cudaEventRecord(t_copy[d][1], copy));
         G2_TRY(cudaEventRecord(copied[d], copy));
         return G2_OK;
     }
@@ -1524,9 +1557,13 @@ struct ViewDevice {
         if (copy) cudaStreamSynchronize(copy);
         cudaDeviceSynchronize();
         for (int d = 0; d < 2; d++) {
-            if (buf[d]) cudaFree(buf[d]);
             if (copied[d]) cudaEventDestroy(copied[d]);
             if (done[d]) cudaEventDestroy(done[d]);
+        }
+        for (int d = 0; d < 2; d++) {
+            for (auto e : t_copy[d])
+                if (e) cudaEventDestroy(e);
+            if (t_run[d]) cudaEventDestroy(t_run[d]);
         }
         if (copy) cudaStreamDestroy(copy);
     }
@@ -1638,6 +1675,7 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
         prod.n = n;
         prod.bin_start = start.data();
         prod.roots = roots.data();
+        prod.slots = &ctx->view_host;
         prod.nbins = nbins;
         prod.shape = shape;
         prod.device = ctx->device;
@@ -1655,18 +1693,20 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
         ReadyView cur, nxt;
         int d = 0;
         bool have = !rc && nbins && take(&cur);
-        if (have) rc = dev.upload(cur, prod.slots[cur.slot].buf, d);
+        if (have) rc = dev.upload(cur, (*prod.slots)[cur.slot].first, d);
         while (have && !rc) {
             // the run of this view, on the legacy stream after its upload
             rc = fail_cuda_if(ctx, cudaStreamWaitEvent(nullptr, dev.copied[d], 0), "view wait");
             if (rc) break;
             const uint32_t *d_src = dev.bind(cur, d);
-            rc = job.enqueue(ctx, d_src, cur.sizes.nsrc);
+            rc = fail_cuda_if(ctx, cudaEventRecord(dev.t_run[0], nullptr), "view record");
+            if (!rc) rc = job.enqueue(ctx, d_src, cur.sizes.nsrc);
+            if (!rc) rc = fail_cuda_if(ctx, cudaEventRecord(dev.t_run[1], nullptr), "view record");
             if (!rc) rc = fail_cuda_if(ctx, cudaEventRecord(dev.done[d], nullptr), "view record");
             if (rc) break;
             // the next view's upload overlaps this run
             const bool more = take(&nxt);
-            if (more) rc = dev.upload(nxt, prod.slots[nxt.slot].buf, d ^ 1);
+            if (more) rc = dev.upload(nxt, (*prod.slots)[nxt.slot].first, d ^ 1);
             if (!rc) rc = job.finish(ctx);
             if (rc) break;
             total += job.h[0];
@@ -1678,6 +1718,8 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
             st.view_edges += cur.sizes.m;
             st.h2d_bytes += L.bytes;
             st.max_view_bytes = std::max(st.max_view_bytes, L.bytes);
+            st.copy_ms += dev.copy_ms(d);
+            st.run_ms += dev.run_ms();
             prod.release(cur.slot);
             cur = nxt;
             have = more;

@@ -58,7 +58,7 @@ class G2ViewOpts(C.Structure):
 class G2ViewStats(C.Structure):
     _fields_ = [("bins", u64), ("view_vertices", u64), ("view_edges", u64), ("h2d_bytes", u64),
                 ("max_view_bytes", u64), ("build_ms", C.c_double), ("wait_ms", C.c_double),
-                ("total_ms", C.c_double)]
+                ("total_ms", C.c_double), ("copy_ms", C.c_double), ("run_ms", C.c_double)]
 
     def to_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

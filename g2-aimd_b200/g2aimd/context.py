@@ -218,11 +218,15 @@ class Context:
         return r.value, b.value
 
     def pass_times(self):
-        """Device ms of the last run's passes (after a run with flags=1)."""
+        """Device ms of the last run's passes (after a run with flags=1): three
+        for MCE (main, two deferred), one for a match run."""
         out = []
         for k in range(3):
             ms = C.c_float()
-            self._check(lib().g2_pass_time_ms(self._h, k, C.byref(ms)), "g2_pass_time_ms")
+            rc = lib().g2_pass_time_ms(self._h, k, C.byref(ms))
+            if rc == -1 and k > 0:
+                break
+            self._check(rc, "g2_pass_time_ms")
             out.append(ms.value)
         return out
 

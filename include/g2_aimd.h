@@ -248,8 +248,9 @@ int g2_match_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc,
 uint64_t g2_last_launch_count(const g2_ctx *ctx);
 
 /* After a run with G2_FLAG_TIME_KERNELS: device milliseconds of enumeration
- * pass `pass` (0 = main pass, 1-2 = deferred passes) of the last run, measured
- * with CUDA events on the run's stream.  Synchronises on the events. */
+ * pass `pass` of the last run (MCE: 0 = main pass, 1-2 = deferred passes;
+ * match: pass 0 only, G2_ERR_INVALID beyond), measured with CUDA events on the
+ * run's stream.  Synchronises on the events. */
 int g2_pass_time_ms(g2_ctx *ctx, int pass, float *ms);
 
 /* After a run with G2_FLAG_WORK_MODEL: the work model W of the last run in
@@ -296,6 +297,8 @@ typedef struct g2_view_stats {
     double build_ms;          /* host time building views, summed over threads    */
     double wait_ms;           /* time the device side waited for a view           */
     double total_ms;          /* wall time of the call                            */
+    double copy_ms;           /* device time of the uploads (CUDA events)         */
+    double run_ms;            /* device time of the runs, task set-up included    */
 } g2_view_stats;
 int g2_view_mce(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n,
                 const uint32_t *bin_of, uint32_t nbins, const g2_view_opts *vopts,
