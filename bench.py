@@ -93,20 +93,20 @@ def run_mce_leg(a):
                           "kernel_ms": times, "records": ctx.spill_stats()[0]}), flush=True)
 
 
-def run_view_leg(a):
+def view_legs(a, g, steps, warmup):
     """Out-of-core enumeration (g2_view_match / g2_view_mce: CSR in pinned host
     memory, views built by host threads, uploads overlapping the runs) against
     the in-core path (upload the whole CSR, then run) on the same host graph,
-    both timed end to end on the host.  One JSON line."""
+    both timed end to end on the host: 4-cliques on `g` and maximal cliques on
+    the Chung-Lu graph (n = 2^18, gamma 2.3, average degree 16)."""
     import torch
 
     import g2aimd
     from g2aimd.context import Context, Plan
-    dev = torch.device("cuda", 0)
-    torch.cuda.set_device(dev)
     producers = min(16, os.cpu_count() or 1)
     launch = {"warps_per_block": 8, "chunk": 1, "ctas_per_sm": 6}
-    out = {"workload": "out-of-core view bins vs in-core, host CSR in pinned memory", "producers": producers}
+    out = {"workload": "out-of-core view bins vs in-core, host CSR in pinned memory, bins of CSR bytes / "
+                       f"{a.view_split}", "producers": producers}
 
     def pinned(g):
         prp = torch.from_numpy(g.row_ptrs.view(np.int64)).pin_memory()
@@ -121,18 +121,18 @@ def run_view_leg(a):
         bin_s = time.perf_counter() - t0
         pg, keep = pinned(g)
         with Context(0, a.scratch_mb << 20) as ctx:
-            for _ in range(a.warmup):
+            for _ in range(warmup):
                 c_view, st = view_fn(ctx, pg, bins, nb)
             vt = []
-            for _ in range(a.steps):
+            for _ in range(steps):
                 t0 = time.perf_counter()
                 c_view, st = view_fn(ctx, pg, bins, nb)
                 vt.append((time.perf_counter() - t0) * 1e3)
-            for _ in range(a.warmup):
+            for _ in range(warmup):
                 ctx.load(pg)
                 c_core = core_fn(ctx)
             ct = []
-            for _ in range(a.steps):
+            for _ in range(steps):
                 t0 = time.perf_counter()
                 ctx.load(pg)
                 c_core = core_fn(ctx)
@@ -140,12 +140,10 @@ def run_view_leg(a):
         assert c_view == c_core, (name, c_view, c_core)
         del keep
         out[name] = {"graph": {"n": g.n, "m": g.m}, "shape": shape, "csr_bytes": int(csr),
-                     "bin_budget_bytes": int(budget),
-                     "bins": nb, "bin_plan_s": round(bin_s, 3), "count": int(c_view),
-                     "view_ms": float(np.mean(vt)), "in_core_ms": float(np.mean(ct)),
+                     "bin_budget_bytes": int(budget), "bins": nb, "bin_plan_s": round(bin_s, 3),
+                     "count": int(c_view), "view_ms": float(np.mean(vt)), "in_core_ms": float(np.mean(ct)),
                      "view_vs_in_core": float(np.mean(ct)) / float(np.mean(vt)), "stats": st}
 
-    g, _ = make_graph(a.scale, a.edge_factor, a.seed)
     k4 = Plan.preset(K4)
     leg(f"k4_rmat_s{a.scale}", g, k4.view_shape(),
         lambda ctx, pg, bins, nb: (lambda c, _pb, st: (c, st))(
@@ -156,7 +154,15 @@ def run_view_leg(a):
         lambda ctx, pg, bins, nb: (lambda c, _h, _pb, st: (c, st))(
             *ctx.view_mce(pg, bins, nbins=nb, hist_len=HIST, producers=producers, schedule="heuristic")),
         lambda ctx: ctx.mce(hist_len=HIST, schedule="heuristic")[0])
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_view_leg(a):
+    """The view legs alone (one JSON line)."""
+    import torch
+    torch.cuda.set_device(torch.device("cuda", 0))
+    g, _ = make_graph(a.scale, a.edge_factor, a.seed)
+    print(json.dumps(view_legs(a, g, a.steps, a.warmup)), flush=True)
 
 
 def dist_env():
@@ -571,6 +577,9 @@ def run_ours(a):
         e2e = {"value": k4 / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(g.row_ptrs.nbytes + g.cols.nbytes + g.core.nbytes),
                "d2h_bytes_per_step": 8}
+        # ---- the same graph out of core: view bins against in-core runs
+        if world == 1:
+            extras["view_bins"] = view_legs(a, g, 2, 1)
         if rank == 0 and world == 1:
             cs = cpu_sample(g, a.cpu_sample_s, os.cpu_count() or 1)
             cpu = {"value": cs["value"], "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",

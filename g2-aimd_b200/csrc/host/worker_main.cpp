@@ -8,16 +8,23 @@
 //   -h  <hop>         view-bin hop for BK (GMatch takes the plan's hop; must be unset)
 //   -cn <n>           consumers = GPUs 0..n-1
 //   -ss <0|1>         sort the sources of each bin
+//   -ooc <0|1>        out of core: the CSR stays in host memory and each bin's view
+//                     is built by -pn host threads and uploaded (g2_view_mce /
+//                     g2_view_match); without a .vbmap, bins of at most -m GB
+//                     (default 10, the reference's view-bin budget) come from
+//                     g2_view_bins
 //   -m, -t, -qs, -pn, -dr, -ds, -dst  accepted for compatibility (see below)
 // Bins come from "<graph.bin>.<hop>.hop.vbmap" (view/view_bin_manager.h:34-94); a
 // missing file means one bin holding every vertex.  BK prints one
 // "Total No. of Cliques: N" line per bin (app_BK/BK.h:72-76), GMatch one final
 // "Total counts: N" (system/worker.h:273-279).
 //
-// What changes: each GPU holds the whole CSR (loaded once) instead of a k-hop view
-// per bin, so there is no producer-side materialisation (-pn, -t, -qs, -m have no
-// work to size); the view of a bin is a subset of the full graph that contains every
-// adjacency list the bin's roots read, so the counts are the same.  Bins go to GPUs
+// What changes: by default each GPU holds the whole CSR (loaded once) instead of a
+// k-hop view per bin, so there is no producer-side materialisation (-pn, -t, -qs, -m
+// have no work to size); the view of a bin is a subset of the full graph that
+// contains every adjacency list the bin's roots read, so the counts are the same.
+// With -ooc 1 the views are materialised as in the reference (a compact induced
+// ball per bin, system/worker.h:165-279), for graphs larger than device memory.  Bins go to GPUs
 // through an atomic counter instead of the MPMC queues.  -dr (reorder bins by
 // sum of degrees, largest first) and -ds/-dst (split) are honoured as orderings of the
 // bin list; they do not change results.
@@ -56,8 +63,11 @@ int main(int argc, char **argv) {
     const int consumers = std::max(1, atoi(opt(argc, argv, "-cn", "1")));
     const int sort_sources = atoi(opt(argc, argv, "-ss", "0"));
     const int reorder = atoi(opt(argc, argv, "-dr", "0"));
+    const int ooc = atoi(opt(argc, argv, "-ooc", "0"));
+    const int producers = std::max(1, atoi(opt(argc, argv, "-pn", "1")));
+    const double mem_gb = atof(opt(argc, argv, "-m", "10"));
     if (data.empty()) {
-        fprintf(stderr, "usage: g2_worker -dg graph.bin [-q id] [-h hop] [-cn gpus] [-ss 0|1]\n");
+        fprintf(stderr, "usage: g2_worker -dg graph.bin [-q id] [-h hop] [-cn gpus] [-ss 0|1] [-ooc 0|1 -pn threads -m GB]\n");
         return 2;
     }
     const bool bk = query == 1000;
@@ -88,6 +98,71 @@ int main(int argc, char **argv) {
     if (g2_read_vbmap(vb.c_str(), n, &nbins, bins.data()) != G2_OK) {
         nbins = 1;
         std::fill(bins.begin(), bins.end(), 0u);
+        if (ooc) {
+            uint32_t radius = 1, row_radius = 1, root_degree = 1, flags = 0;
+            if (!bk) {
+                rc = g2_plan_view_radius(&plan, &radius, &row_radius, &root_degree, &flags);
+                if (rc) return die("view shape", rc);
+            }
+            rc = g2_view_bins(rp, ci, n, radius, row_radius, root_degree, flags, (uint64_t)(mem_gb * 1e9),
+                              bins.data(), &nbins);
+            if (rc) return die("view bins", rc);
+            printf("view bins: %u (budget %.3f GB)\n", nbins, mem_gb);
+        }
+    }
+    if (ooc) {
+        // consumer c runs bins c, c + cn, ...: its bin_of maps them to 0, 1, ...
+        std::atomic<int> failed{0};
+        std::atomic<unsigned long long> total{0};
+        std::mutex out_mu;
+        std::vector<std::thread> th;
+        for (int c = 0; c < consumers; c++) {
+            th.emplace_back([&, c] {
+                std::vector<uint32_t> mine(n, G2_VIEW_NO_BIN);
+                uint32_t nb = 0;
+                for (uint32_t b = (uint32_t)c; b < nbins; b += (uint32_t)consumers) nb++;
+                for (uint64_t v = 0; v < n; v++)
+                    if (bins[v] % (uint32_t)consumers == (uint32_t)c) mine[v] = bins[v] / (uint32_t)consumers;
+                std::vector<uint64_t> per(std::max<uint32_t>(nb, 1), 0);
+                g2_ctx *ctx = nullptr;
+                int r = g2_open(c, 0, &ctx);
+                if (!r && !bk) r = g2_set_plan(ctx, &plan);
+                g2_opts o;
+                memset(&o, 0, sizeof(o));
+                o.schedule = G2_SCHED_HEURISTIC;
+                g2_view_opts vo;
+                memset(&vo, 0, sizeof(vo));
+                vo.producers = (uint32_t)producers;
+                g2_view_stats st;
+                memset(&st, 0, sizeof(st));
+                uint64_t count = 0;
+                if (!r && nb)
+                    r = bk ? g2_view_mce(ctx, rp, ci, n, mine.data(), nb, &vo, &o, &count, nullptr, 0, per.data(), &st)
+                           : g2_view_match(ctx, rp, ci, n, mine.data(), nb, &vo, &o, &count, per.data(), &st);
+                std::lock_guard<std::mutex> lk(out_mu);
+                if (r) {
+                    fprintf(stderr, "g2_worker: device %d: %s (%d) %s\n", c, g2_strerror(r), r,
+                            ctx ? g2_last_cuda_error(ctx) : "");
+                    failed = 1;
+                } else {
+                    total += count;
+                    for (uint32_t i = 0; i < nb; i++) {
+                        printf("consumer %d completes bin %u\n", c, c + i * (uint32_t)consumers);
+                        if (bk) printf("Total No. of Cliques: %llu\n", (unsigned long long)per[i]);
+                    }
+                    printf("consumer %d: %llu views, %.1f MB uploaded, %.3f ms\n", c, (unsigned long long)st.bins,
+                           st.h2d_bytes / 1e6, st.total_ms);
+                }
+                if (ctx) g2_close(ctx);
+            });
+        }
+        for (auto &t : th) t.join();
+        double total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        printf("finish total time, elapsed_time=%.3fms\n", total_ms);
+        if (!bk) printf("Total counts: %llu\n", (unsigned long long)total.load());
+        g2_free(rp);
+        g2_free(ci);
+        return failed ? 1 : 0;
     }
     std::vector<std::vector<uint32_t>> sources(nbins);
     for (uint64_t v = 0; v < n; v++) sources[bins[v]].push_back((uint32_t)v);
