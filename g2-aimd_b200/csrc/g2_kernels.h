@@ -142,6 +142,11 @@ cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, in
 // Degeneracy order of a CSR on the device (kcore.cu); synchronous.
 cudaError_t degeneracy_order_device(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint32_t *perm,
                                     uint32_t *core, int sms, uint64_t *rounds);
+// The CSR with vertex v renamed perm[v], rows sorted (kcore.cu); synchronous.
+// new_rp (n+1) and new_ci (m) are allocated here (cudaMalloc); rows are sorted
+// in calls of at most max_chunk entries (a row longer than that: NotSupported).
+cudaError_t recode_device(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint64_t m, const uint32_t *perm,
+                          uint64_t max_chunk, int sms, uint64_t **new_rp, uint32_t **new_ci);
 
 // Learned root-cost model (costmodel.cu).
 size_t model_smem_bytes();

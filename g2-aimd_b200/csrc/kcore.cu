@@ -1,4 +1,5 @@
-// kcore.cu - degeneracy order of the loaded graph on the device.
+// kcore.cu - degeneracy order of the loaded graph on the device, and the
+// recode that renames vertices by it.
 //
 // Replaces the host preprocessing of kmeans/kcore.cpp:39-191 (k-core peeling,
 // then a degree sort inside each shell and a recode): core numbers by
@@ -9,7 +10,10 @@
 // result equals g2_degeneracy_order's (csrc/host/graph_host.cpp) exactly.
 #include <cub/cub.cuh>
 
+#include <algorithm>
+#include <climits>
 #include <cstdint>
+#include <vector>
 
 #include "g2_kernels.h"
 
@@ -78,7 +82,133 @@ __global__ void scatter_perm_kernel(const uint32_t *ord, uint64_t n, uint32_t *p
         perm[ord[i]] = (uint32_t)i;
 }
 
+// Row length of each vertex under its new name (entry n stays 0 for the scan).
+__global__ void recode_degrees_kernel(const uint64_t *rp, const uint32_t *perm, uint64_t n, uint64_t *deg) {
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+        deg[perm[v]] = rp[v + 1] - rp[v];
+}
+
+// Row of v, renamed, written unsorted at its new place (a warp per row).
+__global__ void recode_scatter_kernel(const uint64_t *rp, const uint32_t *ci, const uint32_t *perm,
+                                      const uint64_t *new_rp, uint64_t n, uint32_t *out) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = w0; v < n; v += nw) {
+        const uint64_t lo = rp[v], len = rp[v + 1] - lo, base = new_rp[perm[v]];
+        for (uint64_t i = lane; i < len; i += 32) out[base + i] = perm[ci[lo + i]];
+    }
+}
+
+// Offsets of rows [r0, r0 + rows] relative to row r0 (segmented sort of one chunk).
+__global__ void chunk_offsets_kernel(const uint64_t *new_rp, uint64_t r0, uint64_t rows, int *off) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= rows; i += (uint64_t)gridDim.x * blockDim.x)
+        off[i] = (int)(new_rp[r0 + i] - new_rp[r0]);
+}
+
 }  // namespace
+
+cudaError_t recode_device(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint64_t m, const uint32_t *perm,
+                          uint64_t max_chunk, int sms, uint64_t **new_rp, uint32_t **new_ci) {
+    *new_rp = nullptr;
+    *new_ci = nullptr;
+    if (n + 1 > (uint64_t)INT_MAX) return cudaErrorNotSupported;  // the scan counts items in int
+    max_chunk = std::min<uint64_t>(std::max<uint64_t>(max_chunk, 1), (uint64_t)INT_MAX);
+    uint64_t *nrp = nullptr, *deg = nullptr;
+    uint32_t *tmp = nullptr, *nci = nullptr;
+    int *off = nullptr;
+    void *cub_tmp = nullptr;
+    size_t cub_bytes = 0, need = 0;
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+        return e == cudaSuccess;
+    };
+    const int G = sms * 8;
+    std::vector<uint64_t> cuts;  // row boundaries of the sort calls
+    if (!ok(cudaMalloc(&nrp, 8 * (n + 1))) || !ok(cudaMalloc(&deg, 8 * (n + 1))) ||
+        !ok(cudaMalloc(&tmp, 4 * std::max<uint64_t>(m, 1))) || !ok(cudaMalloc(&nci, 4 * std::max<uint64_t>(m, 1))) ||
+        !ok(cudaMemset(deg, 0, 8 * (n + 1))))
+        goto done;
+    recode_degrees_kernel<<<G, 256>>>(rp, perm, n, deg);
+    // exclusive scan: row pointers of the renamed rows (entry n = m)
+    if (!ok(cub::DeviceScan::ExclusiveSum(nullptr, need, deg, nrp, (int)(n + 1)))) goto done;
+    cub_bytes = need;
+    if (!ok(cudaMalloc(&cub_tmp, cub_bytes ? cub_bytes : 16)) ||
+        !ok(cub::DeviceScan::ExclusiveSum(cub_tmp, need, deg, nrp, (int)(n + 1))))
+        goto done;
+    recode_scatter_kernel<<<G, 256>>>(rp, ci, perm, nrp, n, tmp);
+    if (!ok(cudaGetLastError())) goto done;
+    // sort the rows, in calls of at most max_chunk entries
+    if (m <= max_chunk) {
+        cuts = {0, n};
+    } else {
+        std::vector<uint64_t> h(n + 1);
+        if (!ok(cudaMemcpy(h.data(), nrp, 8 * (n + 1), cudaMemcpyDeviceToHost))) goto done;
+        cuts.push_back(0);
+        uint64_t r = 0;
+        while (r < n) {
+            if (h[r + 1] - h[r] > max_chunk) {
+                e = cudaErrorNotSupported;
+                goto done;
+            }
+            // the last row r1 with h[r1] - h[r] <= max_chunk
+            const uint64_t r1 =
+                (uint64_t)(std::upper_bound(h.begin() + r, h.end(), h[r] + max_chunk) - h.begin()) - 1;
+            r = std::min<uint64_t>(r1, n);
+            cuts.push_back(r);
+        }
+    }
+    if (!ok(cudaMalloc(&off, sizeof(int) * (std::min<uint64_t>(n, max_chunk) + 2)))) goto done;
+    for (size_t k = 0; k + 1 < cuts.size(); k++) {
+        const uint64_t r0 = cuts[k], rows = cuts[k + 1] - r0;
+        if (!rows) continue;
+        uint64_t base = 0, items = 0;
+        if (!ok(cudaMemcpy(&base, nrp + r0, 8, cudaMemcpyDeviceToHost)) ||
+            !ok(cudaMemcpy(&items, nrp + r0 + rows, 8, cudaMemcpyDeviceToHost)))
+            goto done;
+        items -= base;
+        if (!items) continue;
+        if (rows + 1 > (uint64_t)INT_MAX) {
+            e = cudaErrorNotSupported;
+            goto done;
+        }
+        if (rows + 2 > std::min<uint64_t>(n, max_chunk) + 2) {  // more rows than the offsets buffer holds
+            cudaFree(off);
+            off = nullptr;
+            if (!ok(cudaMalloc(&off, sizeof(int) * (rows + 1)))) goto done;
+        }
+        chunk_offsets_kernel<<<G, 256>>>(nrp, r0, rows, off);
+        need = 0;
+        if (!ok(cub::DeviceSegmentedSort::SortKeys(nullptr, need, tmp + base, nci + base, (int)items, (int)rows, off,
+                                                    off + 1)))
+            goto done;
+        if (need > cub_bytes) {
+            cudaFree(cub_tmp);
+            cub_tmp = nullptr;
+            cub_bytes = need;
+            if (!ok(cudaMalloc(&cub_tmp, cub_bytes))) goto done;
+        }
+        if (!ok(cub::DeviceSegmentedSort::SortKeys(cub_tmp, need, tmp + base, nci + base, (int)items, (int)rows, off,
+                                                    off + 1)))
+            goto done;
+    }
+    ok(cudaGetLastError());
+    ok(cudaDeviceSynchronize());
+done:
+    cudaFree(deg);
+    cudaFree(tmp);
+    cudaFree(off);
+    cudaFree(cub_tmp);
+    if (e != cudaSuccess) {
+        cudaFree(nrp);
+        cudaFree(nci);
+        return e;
+    }
+    *new_rp = nrp;
+    *new_ci = nci;
+    return cudaSuccess;
+}
 
 // perm (new id of each vertex) and core numbers of the CSR (rp, ci) with n
 // vertices; device buffers.  Synchronous (the level loop reads counts back).

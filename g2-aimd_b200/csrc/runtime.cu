@@ -15,7 +15,9 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -178,6 +180,12 @@ __global__ void forward_offsets_kernel(const uint64_t *rp, const uint32_t *ci, u
         best = y > best ? y : best;
     }
     if ((threadIdx.x & 31) == 0) atomicMax(out, best);
+}
+
+// out[perm[v]] = in[v].
+__global__ void rename_kernel(const uint32_t *in, const uint32_t *perm, uint64_t n, uint32_t *out) {
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+        out[perm[v]] = in[v];
 }
 
 __global__ void iota_kernel(uint32_t *t, uint64_t n) {
@@ -915,6 +923,70 @@ int g2_degeneracy_order_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core) {
     cudaFree(d_core);
     if (e != cudaSuccess) return fail_cuda(ctx, e, "degeneracy_order_device");
     ctx->launches = 2 * rounds + 4;
+    return G2_OK;
+}
+
+static int after_load(g2_ctx *ctx);
+
+int g2_degeneracy_recode_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core) {
+    if (!ctx) return G2_ERR_INVALID;
+    if (!ctx->d_rp) return G2_ERR_NO_GRAPH;
+    G2_TRY(cudaSetDevice(ctx->device));
+    const uint64_t n = ctx->n, m = ctx->m;
+    if (n == 0) return G2_OK;
+    if (n + 1 > (uint64_t)INT_MAX) return G2_ERR_UNSUPPORTED;
+    uint64_t max_chunk = 1ull << 30;  // entries per segmented-sort call (CUB counts items in int)
+    if (const char *env = getenv("G2_RECODE_CHUNK")) max_chunk = std::max<uint64_t>(strtoull(env, nullptr, 10), 1);
+    uint32_t *d_perm = nullptr, *d_core = nullptr;
+    uint64_t *nrp = nullptr;
+    uint32_t *nci = nullptr;
+    uint64_t rounds = 0;
+    cudaError_t e = cudaMalloc(&d_perm, n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&d_core, n * 4);
+    if (e == cudaSuccess)
+        e = g2::degeneracy_order_device(ctx->d_rp, ctx->d_ci, n, d_perm, d_core, ctx->sm_count, &rounds);
+    if (e == cudaSuccess) e = g2::recode_device(ctx->d_rp, ctx->d_ci, n, m, d_perm, max_chunk, ctx->sm_count, &nrp, &nci);
+    if (e == cudaSuccess && perm) e = cudaMemcpy(perm, d_perm, n * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && core) e = cudaMemcpy(core, d_core, n * 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cudaFree(d_perm);
+        cudaFree(d_core);
+        cudaFree(nrp);
+        cudaFree(nci);
+        return e == cudaErrorNotSupported ? G2_ERR_UNSUPPORTED : fail_cuda(ctx, e, "degeneracy recode");
+    }
+    // the recoded CSR becomes the context's graph
+    if (ctx->owns_csr) {
+        cudaFree(ctx->d_rp);
+        cudaFree(ctx->d_ci);
+    }
+    ctx->d_rp = nrp;
+    ctx->d_ci = nci;
+    ctx->owns_csr = true;
+    ctx->rp_cap = n + 1;
+    ctx->ci_cap = std::max<uint64_t>(m, 1);
+    int rc = after_load(ctx);
+    // core numbers under the new names, for the learned schedule's features
+    if (!rc) rc = grow(ctx, ctx->d_core, ctx->core_cap, n, "core");
+    if (!rc) {
+        rename_kernel<<<ctx->sm_count * 4, 256>>>(d_core, d_perm, n, ctx->d_core);
+        e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) rc = fail_cuda(ctx, e, "core rename");
+    }
+    cudaFree(d_perm);
+    cudaFree(d_core);
+    if (rc) return rc;
+    ctx->core_loaded = true;
+    ctx->launches = 2 * rounds + 12;
+    return G2_OK;
+}
+
+int g2_copy_csr(g2_ctx *ctx, uint64_t *row_ptrs, uint32_t *cols) {
+    if (!ctx || !row_ptrs || (!cols && ctx->m)) return G2_ERR_INVALID;
+    if (!ctx->d_rp) return G2_ERR_NO_GRAPH;
+    G2_TRY(cudaSetDevice(ctx->device));
+    G2_TRY(cudaMemcpy(row_ptrs, ctx->d_rp, 8 * (ctx->n + 1), cudaMemcpyDeviceToHost));
+    if (ctx->m) G2_TRY(cudaMemcpy(cols, ctx->d_ci, 4 * ctx->m, cudaMemcpyDeviceToHost));
     return G2_OK;
 }
 

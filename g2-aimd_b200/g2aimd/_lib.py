@@ -98,6 +98,8 @@ def lib():
         "g2_reserve": (i32, [C.c_void_p, u64]),
         "g2_set_host_spill": (i32, [C.c_void_p, u64]),
         "g2_degeneracy_order_device": (i32, [C.c_void_p, P(u32), P(u32)]),
+        "g2_degeneracy_recode_device": (i32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+        "g2_copy_csr": (i32, [C.c_void_p, C.c_void_p, C.c_void_p]),
         "g2_batch_load": (i32, [C.c_void_p, C.c_void_p, u32]),
         "g2_batch_mce": (i32, [C.c_void_p, C.c_void_p, P(u64), P(u64), u32]),
         "g2_batch_match": (i32, [C.c_void_p, C.c_void_p, P(u64)]),

@@ -201,6 +201,27 @@ class Context:
                     "g2_degeneracy_order_device")
         return perm, core
 
+    def degeneracy_recode(self):
+        """Rename the loaded graph by its degeneracy order on the device
+        (g2_degeneracy_recode_device); core numbers are loaded under the new
+        names.  Returns (perm, core) by old id."""
+        perm = np.zeros(self.n, np.uint32)
+        core = np.zeros(self.n, np.uint32)
+        self._check(lib().g2_degeneracy_recode_device(self._h, perm.ctypes.data_as(C.c_void_p),
+                                                      core.ctypes.data_as(C.c_void_p)),
+                    "g2_degeneracy_recode_device")
+        self.graph = None
+        return perm, core
+
+    def copy_csr(self, m: int):
+        """The loaded CSR copied back to host memory (m column entries)."""
+        from .graph import Graph
+        rp = np.zeros(self.n + 1, np.uint64)
+        ci = np.zeros(max(m, 1), np.uint32)
+        self._check(lib().g2_copy_csr(self._h, rp.ctypes.data_as(C.c_void_p), ci.ctypes.data_as(C.c_void_p)),
+                    "g2_copy_csr")
+        return Graph(rp, ci[:m].copy())
+
     def set_host_spill(self, nbytes: int):
         """Managed spill slab for MCE roots no scratch slab holds (0: none)."""
         self._check(lib().g2_set_host_spill(self._h, nbytes), "g2_set_host_spill")

@@ -312,6 +312,18 @@ int g2_view_match(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, u
                   const g2_opts *opts, uint64_t *count, uint64_t *bin_counts,
                   g2_view_stats *stats);
 
+/* Rename the loaded graph by its degeneracy order on the device (replaces
+ * kmeans/kcore.cpp:39-191: peeling, degree sort inside each shell, recode):
+ * afterwards the context holds the recoded CSR (rows sorted; equal to
+ * g2_recode(g2_degeneracy_order)) and its core numbers under the new names, as
+ * g2_load_core would load them.  perm[old] = new id and core[old] (optional host
+ * outputs, n entries).  Rows are sorted in device calls of at most 2^30 entries
+ * (environment G2_RECODE_CHUNK overrides); a longer row, or n >= 2^31 - 1, gives
+ * G2_ERR_UNSUPPORTED.  Needs about twice the CSR's device memory meanwhile. */
+int g2_degeneracy_recode_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core);
+/* Copy the loaded CSR back to host memory (row_ptrs: n + 1, cols: m entries). */
+int g2_copy_csr(g2_ctx *ctx, uint64_t *row_ptrs, uint32_t *cols);
+
 /* Size of the spill slab on which a synchronous MCE run (g2_mce_run,
  * g2_batch_mce) walks the roots that no slab of the context's scratch holds,
  * after the deferral passes: managed memory (default 1 GiB, allocated on first
