@@ -106,7 +106,7 @@ Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
         const uint32_t g = ball_[i];
         const uint64_t before = cols_.size();
         uint32_t back = 0;
-        for (uint64_t e = row_from(rp_, ci_, g, lo_); e < rp_[g + 1]; e++) {
+        for (uint64_t e = row_from(rp_, ci_, g, sh.forward ? g + 1 : lo_); e < rp_[g + 1]; e++) {
             const uint32_t l = mark_[ci_[e]];
             if (l == kNone) continue;
             cols_.push_back(l);
@@ -167,8 +167,9 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
             for (uint64_t e = row_from(rp, ci, x, lo); e < rp[x + 1]; e++) {
                 const uint32_t y = ci[e];
                 if (y == x || depth[y] == kNone) continue;
-                if (gains_row) delta += 4;                             // x -> y
-                if (fresh && y != x && depth[y] <= sh.row_radius) delta += 4;  // y -> x
+                // forward rows keep only entries above their own vertex
+                if (gains_row && (!sh.forward || y > x)) delta += 4;                            // x -> y
+                if (fresh && depth[y] <= sh.row_radius && (!sh.forward || x > y)) delta += 4;  // y -> x
             }
         }
         return true;
@@ -254,8 +255,10 @@ Shape plan_shape(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[
     sh.radius = 0;
     sh.row_radius = 0;
     sh.upper = k > 1;
+    sh.forward = k > 1;
     for (uint32_t i = 0; i < k; i++) {
         if (i > 0 && !(gt[i] & 1u)) sh.upper = false;
+        if ((gt[i] & ((1u << i) - 1u)) != ((1u << i) - 1u)) sh.forward = false;  // above every earlier position
         if (dist[i] == kNone) continue;
         sh.radius = std::max(sh.radius, dist[i]);
         if (is_bn[i]) sh.row_radius = std::max(sh.row_radius, dist[i]);
@@ -270,11 +273,12 @@ namespace {
 
 bool shape_from(uint32_t radius, uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
                 g2view::Shape *sh) {
-    if (row_radius > radius || radius > 15 || (flags & ~(uint32_t)G2_VIEW_UPPER)) return false;
+    if (row_radius > radius || radius > 15 || (flags & ~(uint32_t)(G2_VIEW_UPPER | G2_VIEW_FORWARD))) return false;
     sh->radius = radius;
     sh->row_radius = row_radius;
     sh->min_deg = min_root_degree;
     sh->upper = (flags & G2_VIEW_UPPER) != 0;
+    sh->forward = (flags & G2_VIEW_FORWARD) != 0;
     return true;
 }
 
@@ -357,7 +361,7 @@ int g2_plan_view_radius(const g2_plan *p, uint32_t *radius, uint32_t *row_radius
     *radius = sh.radius;
     *row_radius = sh.row_radius;
     *root_degree = sh.min_deg;
-    *flags = sh.upper ? G2_VIEW_UPPER : 0u;
+    *flags = (sh.upper ? G2_VIEW_UPPER : 0u) | (sh.forward ? G2_VIEW_FORWARD : 0u);
     return G2_OK;
 }
 

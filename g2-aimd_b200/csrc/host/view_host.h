@@ -9,7 +9,9 @@
 // restricted to B; the others keep an empty row (their neighbours are never
 // scanned).  With `upper` (queries whose conditions put every matched vertex
 // above the root's image) the ball of source s is walked through vertices
-// larger than s only.  Replaces the materialisation of view/view_bin.h:61-159,
+// larger than s only, and with `forward` (queries that order every position
+// above all earlier ones) rows keep only their entries above their own vertex.
+// Replaces the materialisation of view/view_bin.h:61-159,
 // which keeps global ids and copies the full rows of the vertices within hop-1
 // of the sources.
 #pragma once
@@ -41,6 +43,7 @@ struct Shape {
     uint32_t row_radius = 1;  // rows kept up to this depth
     uint32_t min_deg = 0;     // sources of smaller degree are dropped
     bool upper = false;       // balls walked through vertices above their source
+    bool forward = false;     // rows keep only neighbours above their own vertex
 };
 
 // One builder per thread; it keeps an n-entry mark array (4 bytes per vertex of
@@ -88,7 +91,9 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
 // within it of the root's image); row_radius = largest distance of a position
 // that some later position lists as back neighbour (only those vertices' rows
 // are scanned); min_deg = query degree of position 0; upper = the conditions
-// imply M(i) > M(0) for every position i > 0.
+// imply M(i) > M(0) for every position i > 0; forward = they imply M(i) > M(j)
+// for every j < i (cliques): every candidate lies above its parent's image, so
+// rows need only their entries above their own vertex.
 Shape plan_shape(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[8], const uint32_t *cond_count,
                  const uint32_t (*cond_op)[8], const uint32_t (*cond_pos)[8]);
 

@@ -1693,7 +1693,7 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
                                    ctx->plan.cond_op, ctx->plan.cond_pos);
     if (vo && vo->radius) shape.radius = vo->radius;
     if (vo && vo->row_radius) shape.row_radius = vo->row_radius;
-    if (vo && (vo->flags & G2_VIEW_NO_UPPER)) shape.upper = false;
+    if (vo && (vo->flags & G2_VIEW_NO_UPPER)) shape.upper = shape.forward = false;
     if (vo && (vo->flags & ~(uint32_t)G2_VIEW_NO_UPPER)) return G2_ERR_INVALID;
     if (shape.row_radius > shape.radius || shape.radius > 15) return G2_ERR_INVALID;
     // roots grouped by bin, ascending inside a bin

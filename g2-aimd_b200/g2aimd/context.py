@@ -44,12 +44,13 @@ class Plan:
         return self.raw.k
 
     def view_shape(self):
-        """dict(radius, row_radius, min_root_degree, upper): the view this plan's
+        """dict(radius, row_radius, min_root_degree, upper, forward): the view this plan's
         roots need (g2_plan_view_radius); keyword arguments of Graph.view."""
         r, rr, d, f = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
         check(lib().g2_plan_view_radius(C.byref(self.raw), C.byref(r), C.byref(rr), C.byref(d), C.byref(f)),
               "g2_plan_view_radius")
-        return {"radius": r.value, "row_radius": rr.value, "min_root_degree": d.value, "upper": bool(f.value & 1)}
+        return {"radius": r.value, "row_radius": rr.value, "min_root_degree": d.value, "upper": bool(f.value & 1),
+                "forward": bool(f.value & 4)}
 
     def to_dict(self) -> dict:
         """Same field layout as the reference-planner fixtures."""

@@ -281,7 +281,9 @@ int g2_degeneracy_order_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core);
  */
 #define G2_VIEW_NO_BIN 0xffffffffu
 #define G2_VIEW_UPPER 1u     /* balls walked through vertices above their source */
-#define G2_VIEW_NO_UPPER 2u  /* g2_view_opts: full balls even where the query allows upper ones */
+#define G2_VIEW_FORWARD 4u   /* rows keep only neighbours above their own vertex */
+#define G2_VIEW_NO_UPPER 2u  /* g2_view_opts: full balls and rows even where the query
+                                allows upper balls and forward rows */
 typedef struct g2_view_opts {
     uint32_t producers;   /* host threads building views (0 = min(8, cores))    */
     uint32_t radius;      /* ball radius (0 = from the query: 1 for MCE)         */
@@ -426,7 +428,10 @@ int g2_read_vbmap(const char *path, uint64_t n, uint32_t *nbins,
  * keep their neighbours inside B, the others an empty row.  With G2_VIEW_UPPER
  * the ball of each source s is walked through vertices larger than s only
  * (queries whose conditions place every matched vertex above the root's
- * image: cliques, cycles).  Every embedding rooted in S lies in B and uses only
+ * image: cliques, cycles); with G2_VIEW_FORWARD rows keep only their entries
+ * above their own vertex (queries whose conditions order every position above
+ * all earlier ones: cliques; every candidate then lies above its parent's
+ * image).  Every embedding rooted in S lies in B and uses only
  * rows of vertices within the query's back-neighbour distance, so a search
  * over the view from S's local ids finds exactly what it finds in the whole
  * graph (view/view_bin.h:40-159 keeps global ids and whole rows instead).
@@ -447,7 +452,7 @@ int g2_view_materialize(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t
                         uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
                         g2_view *out);
 void g2_view_free(g2_view *view);
-/* Radius, row radius, root degree and flags (G2_VIEW_UPPER) a plan's views
+/* Radius, row radius, root degree and flags (G2_VIEW_UPPER, G2_VIEW_FORWARD) a plan's views
  * need (system/plan.h:51-73 derives the reference's single hop count from the
  * same query distances). */
 int g2_plan_view_radius(const g2_plan *plan, uint32_t *radius, uint32_t *row_radius,

@@ -79,7 +79,8 @@ def test_view_match_equals_oracle(vctx, orc, g2, q):
     want = orc.match(g, plan, threads=4)["count"]
     sh = plan.view_shape()
     for no_upper in sorted({True, not sh["upper"]}):
-        nb, bin_of = g.view_bins(max_bytes=32 << 10, **dict(sh, upper=sh["upper"] and not no_upper))
+        kw = dict(sh, upper=sh["upper"] and not no_upper, forward=sh["forward"] and not no_upper)
+        nb, bin_of = g.view_bins(max_bytes=(8 << 10) if kw["forward"] else (32 << 10), **kw)
         assert nb > 8
         count, per_bin, st = vctx.view_match(g, bin_of, plan, producers=3, no_upper=no_upper)
         assert count == want, (q, no_upper, count, want)

@@ -54,6 +54,6 @@ def test_worker_match_in_core_and_out_of_core(tmp_path, orc, g2, q):
     g.write_bin(path)
     want = orc.match(g, Plan.preset(q), threads=4)["count"]
     assert total_counts(run_worker("-dg", path, "-q", q)) == want
-    out = run_worker("-dg", path, "-q", q, "-ooc", 1, "-pn", 4, "-m", 0.00005)
+    out = run_worker("-dg", path, "-q", q, "-ooc", 1, "-pn", 4, "-m", 0.00001)  # 10 KB bins
     assert int(re.search(r"view bins: (\d+)", out).group(1)) > 1
     assert total_counts(out) == want

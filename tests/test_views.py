@@ -10,10 +10,11 @@ import pytest
 from helpers import random_graph, small_graphs
 
 
-def py_view(g, sources, radius, row_radius, min_deg, upper=False):
+def py_view(g, sources, radius, row_radius, min_deg, upper=False, forward=False):
     """Direct construction: per kept source, BFS depths (through vertices above
     the source when upper); a vertex's depth is its smallest; ascending ids;
-    rows of vertices within row_radius restricted to the ball."""
+    rows of vertices within row_radius restricted to the ball (and to entries
+    above the row's vertex when forward)."""
     rp, ci = g.row_ptrs, g.cols
     deg = np.diff(rp)
     kept = [int(s) for s in sources if deg[s] >= min_deg]
@@ -36,15 +37,16 @@ def py_view(g, sources, radius, row_radius, min_deg, upper=False):
     rows = []
     for g_ in ids:
         if depth[g_] <= row_radius:
-            rows.append([local[u] for u in ci[rp[g_]:rp[g_ + 1]].tolist() if u in local])
+            rows.append([local[u] for u in ci[rp[g_]:rp[g_ + 1]].tolist() if u in local and (not forward or u > g_)])
         else:
             rows.append([])
     return ids, rows, [local[s] for s in kept]
 
 
-def check_view(g, sources, radius, row_radius, min_deg=0, upper=False):
-    v, lsrc, ids = g.view(sources, radius=radius, row_radius=row_radius, min_root_degree=min_deg, upper=upper)
-    want_ids, want_rows, want_src = py_view(g, sources, radius, row_radius, min_deg, upper)
+def check_view(g, sources, radius, row_radius, min_deg=0, upper=False, forward=False):
+    v, lsrc, ids = g.view(sources, radius=radius, row_radius=row_radius, min_root_degree=min_deg, upper=upper,
+                          forward=forward)
+    want_ids, want_rows, want_src = py_view(g, sources, radius, row_radius, min_deg, upper, forward)
     assert ids.tolist() == want_ids
     assert lsrc.tolist() == want_src
     assert v.n == len(want_ids) and v.row_ptrs[0] == 0
@@ -65,17 +67,18 @@ def test_view_structure_small_graphs(g2):
             for trial in range(3):
                 k = int(rng.integers(0, max(1, g.n) + 1))
                 src = rng.choice(g.n, size=min(k, g.n), replace=False) if g.n else np.zeros(0, np.uint32)
-                for upper in (False, True):
-                    check_view(g, src, radius, row_radius, min_deg=int(trial == 2) * 2, upper=upper)
+                for upper, forward in ((False, False), (True, False), (True, True), (False, True)):
+                    check_view(g, src, radius, row_radius, min_deg=int(trial == 2) * 2, upper=upper,
+                               forward=forward)
 
 
 def test_view_structure_rmat(g2):
     g = g2.Graph.rmat(10, 8, seed=5)
     rng = np.random.default_rng(11)
     for radius, row_radius in ((1, 1), (2, 1), (2, 2)):
-        for upper in (False, True):
+        for upper, forward in ((False, False), (True, False), (True, True)):
             src = rng.choice(g.n, size=40, replace=False)  # unsorted: upper walks sort them
-            check_view(g, src, radius, row_radius, upper=upper)
+            check_view(g, src, radius, row_radius, upper=upper, forward=forward)
 
 
 def test_view_duplicates_and_empty(g2):
@@ -100,7 +103,7 @@ def test_view_rejects_bad_arguments(g2):
     src = np.array([0], np.uint32)
     sp = src.ctypes.data_as(C.c_void_p)
     assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 2, 0, 0, C.byref(v)) == -1  # row radius > radius
-    assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 1, 0, 4, C.byref(v)) == -1  # unknown flag
+    assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 1, 0, 8, C.byref(v)) == -1  # unknown flag
     assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 1, 0, 1, C.byref(v)) == 0
     lib.g2_view_free(C.byref(v))
 
@@ -132,6 +135,7 @@ def plan_shape_py(plan):
         changed = bool(extra)
         gt |= extra
     upper = all((i, 0) in gt for i in range(1, k))
+    forward = all((i, j) in gt for i in range(1, k) for j in range(i))
     dist = {0: 0}
     fr = [0]
     while fr:
@@ -143,7 +147,7 @@ def plan_shape_py(plan):
                     nxt.append(y)
         fr = nxt
     return {"radius": max(dist.values()), "row_radius": max(dist[i] for i in range(k) if is_bn[i]),
-            "min_root_degree": len(adj[0]), "upper": upper}
+            "min_root_degree": len(adj[0]), "upper": upper, "forward": forward}
 
 
 @pytest.mark.parametrize("q", [0, 1, 2, 3, 4, 5, 6, 23, 24, 25])
@@ -164,6 +168,7 @@ def test_known_shapes():
     assert (c4["radius"], c4["row_radius"], c4["upper"]) == (2, 1, True)  # opposite corner at distance 2
     assert (diamond["radius"], diamond["upper"]) == (1, False)  # conditions only "!=" against the root
     assert (k4["radius"], k4["min_root_degree"], k4["upper"]) == (1, 3, True)
+    assert tri["forward"] and k4["forward"] and not c4["forward"] and not diamond["forward"]
 
 
 def bins_from_bounds(n, bounds):
@@ -219,13 +224,13 @@ def test_views_sum_to_whole_graph_match(g2, orc, q):
     sh = plan.view_shape()
     for nbins in (1, 5, 40):
         bin_of = np.random.default_rng(q * 100 + nbins).integers(0, nbins, g.n).astype(np.uint32)
-        for upper in sorted({False, sh["upper"]}):
+        for upper, forward in sorted({(False, False), (sh["upper"], False), (sh["upper"], sh["forward"])}):
             total = 0
             for src in by_bin(bin_of, nbins):
-                v, lsrc, _ = g.view(src, **dict(sh, upper=upper))
+                v, lsrc, _ = g.view(src, **dict(sh, upper=upper, forward=forward))
                 if lsrc.size:
                     total += orc.match(v, plan, roots=lsrc)["count"]
-            assert total == want, (q, nbins, upper, total, want)
+            assert total == want, (q, nbins, upper, forward, total, want)
 
 
 def test_upper_views_are_smaller(g2):
@@ -234,9 +239,11 @@ def test_upper_views_are_smaller(g2):
     g = g2.Graph.rmat(11, 8, seed=3).degeneracy_recoded()
     sh = Plan.preset(24).view_shape()
     src = np.arange(0, g.n, 7, dtype=np.uint32)
-    full, _, _ = g.view(src, **dict(sh, upper=False))
-    up, _, _ = g.view(src, **sh)
+    full, _, _ = g.view(src, **dict(sh, upper=False, forward=False))
+    up, _, _ = g.view(src, **dict(sh, forward=False))
+    fwd, _, _ = g.view(src, **sh)
     assert up.m < full.m and up.n < full.n
+    assert fwd.n == up.n and 2 * fwd.m <= up.m  # each kept edge at most once
 
 
 def test_view_too_small_radius_misses_matches(g2, orc):
@@ -262,27 +269,30 @@ def view_bytes(v, nsrc):
     return a16(src + 4 * nsrc)
 
 
-@pytest.mark.parametrize("radius,row_radius,upper", [(1, 1, False), (2, 1, False), (1, 1, True), (2, 1, True),
-                                                    (2, 2, True)])
-def test_view_bins_respect_budget(g2, radius, row_radius, upper):
+@pytest.mark.parametrize("radius,row_radius,upper,forward", [(1, 1, False, False), (2, 1, False, False),
+                                                            (1, 1, True, False), (2, 1, True, False),
+                                                            (2, 2, True, False), (1, 1, True, True),
+                                                            (2, 2, False, True)])
+def test_view_bins_respect_budget(g2, radius, row_radius, upper, forward):
     g = g2.Graph.rmat(10, 8, seed=9)
-    budget = 48 << 10
-    nb, bin_of = g.view_bins(max_bytes=budget, radius=radius, row_radius=row_radius, upper=upper)
+    budget = 48 << 10 if not forward else 24 << 10
+    kw = dict(radius=radius, row_radius=row_radius, upper=upper, forward=forward)
+    nb, bin_of = g.view_bins(max_bytes=budget, **kw)
     assert nb >= 2
     assert bin_of.max() == nb - 1
     assert np.all(np.diff(bin_of.astype(np.int64)) >= 0)  # ranges of ids, in order
     bins = by_bin(bin_of, nb)
     for b, src in enumerate(bins):
         assert src.size > 0
-        v, lsrc, _ = g.view(src, radius=radius, row_radius=row_radius, upper=upper)
+        v, lsrc, _ = g.view(src, **kw)
         size = view_bytes(v, lsrc.size)
         # the bin's view is counted exactly (up to the layout's alignment padding) ...
         assert src.size == 1 or size <= budget + 48
         # ... so the bin was closed because the next root did not fit
         if b + 1 < nb:
-            v2, l2, _ = g.view(np.append(src, bins[b + 1][0]), radius=radius, row_radius=row_radius, upper=upper)
+            v2, l2, _ = g.view(np.append(src, bins[b + 1][0]), **kw)
             assert view_bytes(v2, l2.size) > budget - 48
-    nb_big, _ = g.view_bins(max_bytes=1 << 40, radius=radius, row_radius=row_radius, upper=upper)
+    nb_big, _ = g.view_bins(max_bytes=1 << 40, **kw)
     assert nb_big == 1
 
 
