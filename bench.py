@@ -62,9 +62,10 @@ def parse():
     ap.add_argument("--scratch-mb", type=int, default=4096, help="device scratch for the DFS slabs")
     ap.add_argument("--fixed", action="store_true",
                     help="skip the plain-schedule timing and the autotuner (profiling runs)")
-    ap.add_argument("--leg", choices=["all", "mce", "view"], default="all",
+    ap.add_argument("--leg", choices=["all", "mce", "view", "view-host"], default="all",
                     help="mce: only the maximal-clique workload (Chung-Lu 2^18), for profiling; "
-                         "view: out-of-core runs over view bins against in-core runs")
+                         "view: out-of-core runs over view bins against in-core runs; "
+                         "view-host: the views' sizes and host build time alone (no GPU)")
     ap.add_argument("--view-split", type=int, default=2,
                     help="view leg: bin budget = CSR bytes / this")
     return ap.parse_args()
@@ -155,6 +156,39 @@ def view_legs(a, g, steps, warmup):
             *ctx.view_mce(pg, bins, nbins=nb, hist_len=HIST, producers=producers, schedule="heuristic")),
         lambda ctx: ctx.mce(hist_len=HIST, schedule="heuristic")[0])
     return out
+
+
+def run_view_host_leg(a):
+    """Bins and view sizes of the view legs' workloads, built on the host through
+    g2_view_bins / g2_view_materialize (one thread), for each view shape the
+    query allows (full balls and rows, upper balls, upper balls + forward rows)."""
+    import g2aimd
+    from g2aimd.context import Plan
+    g, _ = make_graph(a.scale, a.edge_factor, a.seed)
+    cl = g2aimd.Graph.chung_lu(1 << 18, 2.3, 16.0, seed=a.seed).degeneracy_recoded()
+    k4 = Plan.preset(K4).view_shape()
+    mce = {"radius": 1, "row_radius": 1, "min_root_degree": 1, "upper": False, "forward": False}
+    out = {"workload": f"view bins of CSR bytes / {a.view_split}, built on the host (no GPU)"}
+    cases = [(f"k4_rmat_s{a.scale}", g, dict(k4, upper=False, forward=False)),
+             (f"k4_rmat_s{a.scale}", g, dict(k4, forward=False)), (f"k4_rmat_s{a.scale}", g, k4),
+             ("mce_chung_lu_2^18", cl, mce)]
+    for name, gr, shape in cases:
+        budget = (gr.row_ptrs.nbytes + gr.cols.nbytes) // a.view_split
+        t0 = time.perf_counter()
+        nb, bins = gr.view_bins(budget, **shape)
+        plan_s = time.perf_counter() - t0
+        order = np.argsort(bins, kind="stable")
+        cuts = np.searchsorted(bins[order], np.arange(nb + 1))
+        vn = vm = 0
+        t0 = time.perf_counter()
+        for b in range(nb):
+            v, _src, _ids = gr.view(order[cuts[b]:cuts[b + 1]].astype(np.uint32), **shape)
+            vn += v.n
+            vm += v.m
+        key = name + ("/forward" if shape["forward"] else "/upper" if shape["upper"] else "/full")
+        out[key] = {"bins": nb, "plan_s": round(plan_s, 2), "view_vertices": int(vn), "view_entries": int(vm),
+                    "entries_vs_m": round(vm / gr.m, 3), "build_s": round(time.perf_counter() - t0, 2)}
+    print(json.dumps(out), flush=True)
 
 
 def run_view_leg(a):
@@ -640,6 +674,8 @@ def main():
         run_mce_leg(a)
     elif a.leg == "view":
         run_view_leg(a)
+    elif a.leg == "view-host":
+        run_view_host_leg(a)
     else:
         run_ours(a)
 
