@@ -91,3 +91,91 @@ def test_gloo_world2_sharded_counts(g2, orc):
         assert c == want["count"], rank
         assert np.array_equal(np.array(h, np.uint64), want["hist"]), rank
         assert m == wm, rank
+
+
+def test_bin_shards_partition_the_bins():
+    from g2aimd.shard import NO_BIN, shard_bins
+    rng = np.random.default_rng(4)
+    n, nbins = 500, 13
+    bin_of = rng.integers(0, nbins, n).astype(np.uint32)
+    bin_of[::17] = NO_BIN  # not roots
+    for world in (1, 2, 3, 5):
+        for cost in (None, rng.random(nbins)):
+            seen = np.zeros(nbins, np.int64)
+            for r in range(world):
+                local, k, ids = shard_bins(bin_of, nbins, world, r, cost)
+                assert ids.size == k
+                seen[ids] += 1
+                mine = local != NO_BIN
+                # a root is this rank's exactly when its bin is, renumbered in order
+                assert np.array_equal(mine, np.isin(bin_of, ids))
+                assert np.array_equal(ids[local[mine]], bin_of[mine])
+            assert np.all(seen == 1)
+    with pytest.raises(ValueError):
+        shard_bins(np.array([0, 5], np.uint32), 3, 1, 0)
+
+
+def _view_rank_main(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        import g2aimd
+        import orc
+        from g2aimd.context import Plan
+        from g2aimd.shard import view_sharded
+        g = g2aimd.Graph.er(300, 0.08, planted=2, planted_size=9, seed=5).degeneracy_recoded()
+        nbins = 7
+        bin_of = (np.arange(g.n) * 5 % nbins).astype(np.uint32)
+
+        def oracle_over_views(shape, plan=None):
+            # the oracle over each view stands in for this rank's device run
+            def run(local, k):
+                count, hist, per = 0, np.zeros(32, np.uint64), np.zeros(k, np.uint64)
+                for b in range(k):
+                    v, src, _ = g.view(np.flatnonzero(local == b).astype(np.uint32), **shape)
+                    if not src.size:
+                        continue
+                    r = orc.mce(v, roots=src, hist_len=32) if plan is None else orc.match(v, plan, roots=src)
+                    per[b] = r["count"]
+                    count += r["count"]
+                    if plan is None:
+                        hist += r["hist"]
+                return count, (hist if plan is None else None), per
+            return run
+
+        mce_shape = {"radius": 1, "row_radius": 1, "min_root_degree": 1}
+        c, h, per = view_sharded(oracle_over_views(mce_shape), bin_of, nbins, world, rank, hist_len=32)
+        plan = Plan.preset(24)
+        m, _, mper = view_sharded(oracle_over_views(plan.view_shape(), plan), bin_of, nbins, world, rank,
+                                  cost=np.arange(nbins, dtype=np.float64))
+        q.put((rank, c, h.tolist(), per.tolist(), m, mper.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_world2_view_bins(g2, orc):
+    """View bins dealt over two ranks: totals, histogram and per-bin counts."""
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_view_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    g = g2.Graph.er(300, 0.08, planted=2, planted_size=9, seed=5).degeneracy_recoded()
+    from g2aimd.context import Plan
+    want = orc.mce(g, hist_len=32)
+    wm = orc.match(g, Plan.preset(24))["count"]
+    nbins = 7
+    bin_of = (np.arange(g.n) * 5 % nbins).astype(np.uint32)
+    want_per = [orc.mce(g, roots=np.flatnonzero(bin_of == b).astype(np.uint32), hist_len=32)["count"]
+                for b in range(nbins)]
+    for rank, c, h, per, m, mper in res:
+        assert c == want["count"] and np.array_equal(np.array(h, np.uint64), want["hist"]), rank
+        assert per == want_per, rank
+        assert m == wm and sum(mper) == wm, rank
