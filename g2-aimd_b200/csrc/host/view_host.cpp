@@ -4,7 +4,7 @@
 // Replaces the host side of the reference's out-of-core path:
 // ViewBin::Materialize / ExtendFromSource (view/view_bin.h:40-159) and the
 // per-query hop of Plan::FindRoot (system/plan.h:51-73).  The pipeline that
-// uploads views and runs the enumeration over them is in runtime.cu.
+// uploads views and runs the enumeration over them is in view_run.cu.
 #include "view_host.h"
 
 #include <algorithm>

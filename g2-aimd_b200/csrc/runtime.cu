@@ -13,113 +13,22 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
-#include <atomic>
-#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdlib>
-#include <condition_variable>
 #include <cstdio>
 #include <cstring>
-#include <deque>
-#include <mutex>
 #include <numeric>
 #include <random>
 #include <string>
-#include <thread>
 #include <unordered_map>
 #include <vector>
 
 #include "g2_aimd.h"
 #include "g2_kernels.h"
-#include "host/view_host.h"
+#include "runtime_internal.h"
 
-struct g2_ctx {
-    int device = 0;
-    int sm_count = 148;
-    uint64_t scratch_bytes = 0;
-    // graph
-    uint64_t *d_rp = nullptr;
-    uint32_t *d_ci = nullptr;
-    bool owns_csr = false;
-    uint64_t n = 0, m = 0;
-    uint32_t max_fwd = 0;      // max |N(v) ∩ (v, ∞)|
-    uint32_t *d_fo = nullptr;  // forward-list offsets
-    uint64_t fo_cap = 0;
-    uint32_t *d_core = nullptr;  // optional core numbers (cost-model feature)
-    bool core_loaded = false;    // d_core holds the loaded graph's core numbers
-    uint64_t rp_cap = 0, ci_cap = 0;       // owned CSR buffers (entries), reused by later loads
-    unsigned int *d_fwdmax = nullptr;      // max forward degree of a load
-    uint64_t core_cap = 0;
-    // work buffers
-    uint32_t *d_scratch = nullptr;
-    uint64_t scratch_words = 0;
-    uint32_t *d_tasks = nullptr;  // root vertex per task (schedule order)
-    uint32_t *d_defer = nullptr;  // 3 deferred lists of tasks_cap each
-    uint64_t tasks_cap = 0;
-    uint64_t *d_root_nodes = nullptr, *d_root_cost = nullptr;
-    uint64_t root_nodes_cap = 0, root_cost_cap = 0;
-    unsigned long long *d_ctr = nullptr;  // kCtr* layout below
-    uint32_t *d_rec = nullptr;            // MCE hand-off records
-    uint32_t *d_ready = nullptr;          // their ready words
-    uint32_t *d_epoch = nullptr;          // epoch of the current run (bumped on the device)
-    uint32_t *d_pool = nullptr;           // MCE spill row pool
-    int *d_status = nullptr;
-    unsigned long long *d_out = nullptr;  // counters for the host entry points
-    uint64_t out_cap = 0;
-    // schedule
-    uint64_t *d_keys = nullptr, *d_keys2 = nullptr;
-    uint64_t keys_cap = 0, keys2_cap = 0;
-    uint32_t *d_roots = nullptr, *d_S = nullptr, *d_part = nullptr, *d_xroots = nullptr, *d_xparts = nullptr;
-    uint64_t roots_cap = 0, S_cap = 0, part_cap = 0, xroots_cap = 0, xparts_cap = 0;
-    float *d_cost = nullptr, *d_total = nullptr;
-    uint64_t cost_cap = 0, total_cap = 0;
-    unsigned long long *d_ntask = nullptr;
-    uint64_t ntask_cap = 0;
-    void *d_cub = nullptr;
-    size_t cub_bytes = 0;
-    bool last_split = false;  // the last run's tasks carry parts
-    uint64_t last_cap = 0;    // tasks buffer entries used by the last run
-    // learned cost model: params (G2_MODEL_PARAMS) followed by norm (G2_MODEL_NORM)
-    float *d_model = nullptr;
-    float *d_feat = nullptr;  // per-vertex features of the loaded graph (n x 8), cached
-    uint64_t feat_cap = 0;
-    bool feat_valid = false;
-    // plan
-    g2::DevPlan plan{};
-    bool has_plan = false;
-    bool clique_plan = false;
-    // diagnostics
-    std::string cuda_err;
-    uint64_t launches = 0;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around the enumeration passes
-    g2::MceArgs last_mce{};            // arguments of the last MCE enqueue (host-spill pass)
-    int last_mce_wpl = 1;
-    uint64_t host_spill_bytes = 1ull << 30;  // managed slab for roots no device slab holds
-    void *h_spill = nullptr;
-    uint64_t h_spill_bytes = 0;
-    // batch of graphs loaded as one disjoint union (g2_batch_load)
-    std::vector<uint64_t> batch_off;  // first vertex of each graph, then n
-    uint64_t *d_goff = nullptr;
-    uint64_t goff_cap = 0;
-    uint64_t *d_root_cliques = nullptr;
-    uint64_t root_cliques_cap = 0;
-    unsigned long long *d_gcount = nullptr;
-    uint64_t gcount_cap = 0;
-    // out-of-core view runs: pinned host slots and the two device slots, kept
-    // between calls (pinning and device allocation stall other CUDA calls)
-    std::vector<std::pair<void *, uint64_t>> view_host;
-    void *view_dev[2] = {nullptr, nullptr};
-    uint64_t view_dev_cap[2] = {0, 0};
-    bool timed = false;
-    int timed_passes = 0;  // enumeration passes the last timed run recorded (MCE 3, match 1)
-    unsigned long long *d_work = nullptr;
-    cudaStream_t last_stream = nullptr;
-};
-
-namespace {
-
-const char *kVersion = "g2aimd-b200 0.2 (sm_100a)";
+namespace g2rt {
 
 int fail_cuda(g2_ctx *c, cudaError_t e, const char *where) {
     if (c) c->cuda_err = std::string(where) + ": " + cudaGetErrorString(e);
@@ -128,25 +37,15 @@ int fail_cuda(g2_ctx *c, cudaError_t e, const char *where) {
 
 int fail_cuda_if(g2_ctx *c, cudaError_t e, const char *where) { return e == cudaSuccess ? G2_OK : fail_cuda(c, e, where); }
 
-#define G2_TRY(call)                                             \
-    do {                                                         \
-        cudaError_t _e = (call);                                 \
-        if (_e != cudaSuccess) return fail_cuda(ctx, _e, #call); \
-    } while (0)
+}  // namespace g2rt
+
+using namespace g2rt;
+
+namespace {
+
+const char *kVersion = "g2aimd-b200 0.2 (sm_100a)";
 
 const uint32_t *core_of(const g2_ctx *ctx) { return ctx->core_loaded ? ctx->d_core : nullptr; }
-
-template <class T>
-int grow(g2_ctx *ctx, T *&p, uint64_t &cap, uint64_t need, const char *what) {
-    if (need <= cap && p) return G2_OK;
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-    cudaError_t e = cudaMalloc(&p, sizeof(T) * (need ? need : 1));
-    if (e != cudaSuccess) return fail_cuda(ctx, e, what);
-    cap = need;
-    return G2_OK;
-}
 
 int cub_space(g2_ctx *ctx, size_t need) {
     if (need <= ctx->cub_bytes && ctx->d_cub) return G2_OK;
@@ -307,11 +206,6 @@ int default_blocks(g2_ctx *ctx, const g2_opts *o, int wpb, int resident_per_sm) 
 }
 
 // Result of task generation.
-struct TaskList {
-    uint64_t cap = 0;    // d_tasks entries in use (upper bound of the task count)
-    bool split = false;  // d_part valid; the task count is in d_ntask
-};
-
 int sort_keys(g2_ctx *ctx, uint64_t n, cudaStream_t st) {
     size_t need = 0;
     cub::DeviceRadixSort::SortKeys(nullptr, need, ctx->d_keys, ctx->d_keys2, (int)n, 0, 64, st);
@@ -325,6 +219,10 @@ int sort_keys(g2_ctx *ctx, uint64_t n, cudaStream_t st) {
 // Task generation: upload the roots, compute the schedule's cost per root (the
 // learned model's features + MLP run here, in one kernel), optionally split
 // heavy roots, sort the tasks by descending cost.  No host synchronisation.
+}  // namespace
+
+namespace g2rt {
+
 int prepare_tasks(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, bool on_device, const g2_opts *o,
                   uint64_t nwarps, cudaStream_t st, TaskList *tl, bool mce) {
     if (!sources) nsrc = ctx->n;
@@ -441,6 +339,10 @@ int prepare_tasks(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, bool on_d
     return G2_OK;
 }
 
+}  // namespace g2rt
+
+namespace {
+
 int ensure_scratch(g2_ctx *ctx) {
     if (ctx->d_scratch) return G2_OK;
     uint64_t words = ctx->scratch_bytes / 4;
@@ -487,6 +389,10 @@ int ensure_counters(g2_ctx *ctx) {
     return G2_OK;
 }
 
+}  // namespace
+
+namespace g2rt {
+
 int status_to_code(int st) {
     if (st & g2::kStatusDeferOverflow) return G2_ERR_OVERFLOW;
     if (st & g2::kStatusStackOverflow) return G2_ERR_OVERFLOW;
@@ -495,6 +401,10 @@ int status_to_code(int st) {
     if (st & g2::kStatusWaitLimit) return G2_ERR_TIMEOUT;
     return G2_OK;
 }
+
+}  // namespace g2rt
+
+namespace {
 
 // Events for pass timing and the device work counter, as the flags ask.
 int prepare_flags(g2_ctx *ctx, uint32_t flags, cudaStream_t st) {
@@ -606,8 +516,12 @@ struct L2Window {
 };
 
 // Enqueue the MCE passes; counters land in d_out.
+}  // namespace
+
+namespace g2rt {
+
 int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long long *d_out, uint32_t hist_len,
-                uint64_t *d_root_nodes, uint64_t *d_root_cost, cudaStream_t st, uint64_t *d_root_cliques = nullptr) {
+                uint64_t *d_root_nodes, uint64_t *d_root_cost, cudaStream_t st, uint64_t *d_root_cliques) {
     int rc = ensure_scratch(ctx);
     if (rc) return rc;
     rc = ensure_counters(ctx);
@@ -707,6 +621,10 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     return G2_OK;
 }
 
+}  // namespace g2rt
+
+namespace {
+
 // After a synchronous MCE run: entries that no device slab held (deferred by the
 // single-warp pass) run once more with one warp whose slab is managed memory of
 // g2_set_host_spill's size (allocated on first need; its pages move to the GPU
@@ -714,6 +632,10 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
 // to the same outputs.  Returns G2_ERR_OVERFLOW if entries remain.  Managed
 // rather than mapped pinned memory: the walk's many small reads stay in device
 // memory while the slab is in use.
+}  // namespace
+
+namespace g2rt {
+
 int mce_host_spill(g2_ctx *ctx, cudaStream_t st) {
     unsigned long long left = 0;
     G2_TRY(cudaMemcpy(&left, ctx->d_ctr + kCtrDefer + 2, sizeof(left), cudaMemcpyDeviceToHost));
@@ -748,6 +670,10 @@ int mce_host_spill(g2_ctx *ctx, cudaStream_t st) {
     return left ? G2_ERR_OVERFLOW : G2_OK;
 }
 
+}  // namespace g2rt
+
+namespace {
+
 // Persistent-grid geometry of the match kernel.
 void match_geometry(g2_ctx *ctx, const g2_opts *o, int *wpl, int *wpb, int *blocks) {
     *wpl = wpl_for(ctx->max_fwd);
@@ -756,6 +682,10 @@ void match_geometry(g2_ctx *ctx, const g2_opts *o, int *wpl, int *wpb, int *bloc
     const bool metrics = o && (o->flags & G2_FLAG_WORK_MODEL);
     *blocks = default_blocks(ctx, o, *wpb, g2::match_blocks_per_sm(*wpl, *wpb, metrics, o ? (int)o->ctas_per_sm : 0));
 }
+
+}  // namespace
+
+namespace g2rt {
 
 int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long long *d_out,
                   uint64_t *d_root_nodes, uint64_t *d_root_cost, cudaStream_t st) {
@@ -817,17 +747,37 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
     return G2_OK;
 }
 
+}  // namespace g2rt
+
+namespace {
+
+}  // namespace
+
+namespace g2rt {
+
 uint64_t mce_warps(g2_ctx *ctx, const g2_opts *o) {
     const int wpb = default_warps(o);
     const bool metrics = o && (o->flags & G2_FLAG_WORK_MODEL);
     return (uint64_t)default_blocks(ctx, o, wpb, g2::mce_blocks_per_sm(1, wpb, metrics)) * wpb;
 }
 
+}  // namespace g2rt
+
+namespace {
+
+}  // namespace
+
+namespace g2rt {
+
 uint64_t match_warps(g2_ctx *ctx, const g2_opts *o) {
     int wpl, wpb, blocks;
     match_geometry(ctx, o, &wpl, &wpb, &blocks);
     return (uint64_t)blocks * wpb;
 }
+
+}  // namespace g2rt
+
+namespace {
 
 }  // namespace
 
@@ -1403,438 +1353,6 @@ int g2_batch_match(g2_ctx *ctx, const g2_opts *opts, uint64_t *counts) {
     int status = 0;
     G2_TRY(cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     return status_to_code(status);
-}
-
-// ---------------------------------------------------------- out-of-core view bins
-
-}  // extern "C"
-
-namespace {
-
-double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
-    return std::chrono::duration<double, std::milli>(b - a).count();
-}
-
-// A view that a producer thread built in a pinned host slot (slot < 0: the bin
-// kept no root; nothing to run).
-struct ReadyView {
-    uint32_t bin = 0;
-    int slot = -1;
-    g2view::Sizes sizes;
-};
-
-// Producers build the views of the bins, in bin order as threads free up, into
-// pinned host slots; the calling thread takes them in the order they are done
-// (replaces the MPMC holder queues of system/worker.h:179-236).
-struct ViewProducers {
-    const uint64_t *rp = nullptr;
-    const uint32_t *ci = nullptr;
-    uint64_t n = 0;
-    const uint64_t *bin_start = nullptr;  // roots of bin b: roots[bin_start[b] .. bin_start[b+1])
-    const uint32_t *roots = nullptr;
-    uint32_t nbins = 0;
-    g2view::Shape shape;
-    int device = 0;
-
-    std::vector<std::pair<void *, uint64_t>> *slots = nullptr;  // pinned, owned by the context
-    std::mutex mu;
-    std::condition_variable cv;
-    std::vector<int> free_slots;
-    std::deque<ReadyView> ready;
-    std::atomic<uint32_t> next_bin{0};
-    uint32_t running = 0;
-    bool stop = false;
-    int error = G2_OK;
-    double build_ms = 0;
-    std::vector<std::thread> threads;
-
-    void start(uint32_t producers, uint32_t nslots) {
-        if (slots->size() < nslots) slots->resize(nslots, {nullptr, 0});
-        for (uint32_t i = 0; i < nslots; i++) free_slots.push_back((int)i);
-        running = producers;
-        for (uint32_t t = 0; t < producers; t++) threads.emplace_back([this] { produce(); });
-    }
-
-    void fail(int rc) {
-        std::lock_guard<std::mutex> g(mu);
-        if (error == G2_OK) error = rc;
-        stop = true;
-        cv.notify_all();
-    }
-
-    void produce() {
-        try {
-            cudaSetDevice(device);  // pinned allocations are made by this thread
-            g2view::Builder b(rp, ci, n);
-            for (;;) {
-                const uint32_t bin = next_bin.fetch_add(1);
-                if (bin >= nbins) break;
-                {
-                    std::lock_guard<std::mutex> g(mu);
-                    if (stop) break;
-                }
-                const auto t0 = std::chrono::steady_clock::now();
-                ReadyView v;
-                v.bin = bin;
-                v.sizes = b.plan(roots + bin_start[bin], bin_start[bin + 1] - bin_start[bin], shape);
-                if (v.sizes.nsrc) {
-                    const g2view::Layout L(v.sizes);
-                    {
-                        std::unique_lock<std::mutex> g(mu);
-                        cv.wait(g, [&] { return stop || !free_slots.empty(); });
-                        if (stop) break;
-                        v.slot = free_slots.back();
-                        free_slots.pop_back();
-                    }
-                    void *buf = nullptr;
-                    uint64_t want = 0;
-                    {
-                        std::lock_guard<std::mutex> g(mu);  // slot sizes are read by every producer
-                        buf = (*slots)[v.slot].first;
-                        if ((*slots)[v.slot].second < L.bytes) {
-                            // straight to the largest slot so far: slots settle after one call
-                            want = std::max<uint64_t>(L.bytes, (*slots)[v.slot].second * 3 / 2);
-                            for (const auto &o : *slots) want = std::max(want, o.second);
-                            (*slots)[v.slot] = {nullptr, 0};
-                        }
-                    }
-                    if (want) {
-                        if (buf) cudaFreeHost(buf);
-                        buf = nullptr;
-                        if (cudaHostAlloc(&buf, want, cudaHostAllocPortable) != cudaSuccess) {
-                            cudaGetLastError();
-                            fail(G2_ERR_OOM);
-                            break;
-                        }
-                        std::lock_guard<std::mutex> g(mu);
-                        (*slots)[v.slot] = {buf, want};
-                    }
-                    b.fill_packed(buf, v.sizes);
-                }
-                const double ms = ms_between(t0, std::chrono::steady_clock::now());
-                std::lock_guard<std::mutex> g(mu);
-                build_ms += ms;
-                ready.push_back(v);
-                cv.notify_all();
-            }
-        } catch (...) {
-            fail(G2_ERR_OOM);
-        }
-        std::lock_guard<std::mutex> g(mu);
-        running--;
-        cv.notify_all();
-    }
-
-    // Next built view, in completion order; false when every bin is done (or on error).
-    bool take(ReadyView *v, double *wait_ms) {
-        const auto t0 = std::chrono::steady_clock::now();
-        std::unique_lock<std::mutex> g(mu);
-        cv.wait(g, [&] { return stop || !ready.empty() || running == 0; });
-        *wait_ms += ms_between(t0, std::chrono::steady_clock::now());
-        if (stop || ready.empty()) return false;
-        *v = ready.front();
-        ready.pop_front();
-        return true;
-    }
-
-    void release(int slot) {
-        if (slot < 0) return;
-        std::lock_guard<std::mutex> g(mu);
-        free_slots.push_back(slot);
-        cv.notify_all();
-    }
-
-    ~ViewProducers() {
-        {
-            std::lock_guard<std::mutex> g(mu);
-            stop = true;
-            cv.notify_all();
-        }
-        for (auto &t : threads) t.join();
-    }
-};
-
-// Device side of a view run: two device slots, a copy stream, and the events
-// that order uploads against the enumeration on the legacy stream.
-struct ViewDevice {
-    g2_ctx *ctx;
-    void **buf;       // the context's two device slots
-    uint64_t *cap;
-    cudaStream_t copy = nullptr;
-    cudaEvent_t copied[2] = {nullptr, nullptr}, done[2] = {nullptr, nullptr};
-    cudaEvent_t t_copy[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // around each slot's upload
-    cudaEvent_t t_run[2] = {nullptr, nullptr};                             // around the current run
-    explicit ViewDevice(g2_ctx *c) : ctx(c), buf(c->view_dev), cap(c->view_dev_cap) {}
-
-    int init() {
-        G2_TRY(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
-        for (int d = 0; d < 2; d++) {
-            G2_TRY(cudaEventCreateWithFlags(&copied[d], cudaEventDisableTiming));
-            G2_TRY(cudaEventCreateWithFlags(&done[d], cudaEventDisableTiming));
-            G2_TRY(cudaEventCreate(&t_copy[d][0]));
-            G2_TRY(cudaEventCreate(&t_copy[d][1]));
-            G2_TRY(cudaEventCreate(&t_run[d]));
-        }
-        return G2_OK;
-    }
-
-    // Device milliseconds of slot d's last upload and of the last run (both ended).
-    float copy_ms(int d) const {
-        float ms = 0.f;
-        return cudaEventElapsedTime(&ms, t_copy[d][0], t_copy[d][1]) == cudaSuccess ? ms : 0.f;
-    }
-    float run_ms() const {
-        float ms = 0.f;
-        return cudaEventElapsedTime(&ms, t_run[0], t_run[1]) == cudaSuccess ? ms : 0.f;
-    }
-
-    // Upload a built view into device slot d once that slot's last run is done.
-    int upload(const ReadyView &v, const void *host, int d) {
-        const g2view::Layout L(v.sizes);
-        if (cap[d] < L.bytes) {
-            const uint64_t want = std::max<uint64_t>(L.bytes, cap[d] + cap[d] / 2);
-            if (buf[d]) cudaFree(buf[d]);  // synchronises: the slot's last run has ended anyway
-            buf[d] = nullptr;
-            cap[d] = 0;
-            G2_TRY(cudaMalloc(&buf[d], want));
-            cap[d] = want;
-        }
-        G2_TRY(cudaStreamWaitEvent(copy, done[d], 0));
-        G2_TRY(cudaEventRecord(t_copy[d][0], copy));
-        G2_TRY(cudaMemcpyAsync(buf[d], host, L.bytes, cudaMemcpyHostToDevice, copy));
-        G2_TRY(cudaEventRecord(t_copy[d][1], copy));
-        G2_TRY(cudaEventRecord(copied[d], copy));
-        return G2_OK;
-    }
-
-    // Point the context's graph at device slot d (after its upload) and return
-    // the view's sources there.
-    uint32_t *bind(const ReadyView &v, int d) {
-        const g2view::Layout L(v.sizes);
-        char *b = static_cast<char *>(buf[d]);
-        ctx->d_rp = reinterpret_cast<uint64_t *>(b);
-        ctx->d_fo = reinterpret_cast<uint32_t *>(b + L.fo);
-        ctx->d_ci = reinterpret_cast<uint32_t *>(b + L.ci);
-        ctx->owns_csr = false;
-        ctx->n = v.sizes.n;
-        ctx->m = v.sizes.m;
-        ctx->max_fwd = v.sizes.max_fwd;
-        ctx->batch_off.clear();
-        ctx->feat_valid = false;
-        ctx->core_loaded = false;
-        return reinterpret_cast<uint32_t *>(b + L.src);
-    }
-
-    ~ViewDevice() {
-        if (copy) cudaStreamSynchronize(copy);
-        cudaDeviceSynchronize();
-        for (int d = 0; d < 2; d++) {
-            if (copied[d]) cudaEventDestroy(copied[d]);
-            if (done[d]) cudaEventDestroy(done[d]);
-        }
-        for (int d = 0; d < 2; d++) {
-            for (auto e : t_copy[d])
-                if (e) cudaEventDestroy(e);
-            if (t_run[d]) cudaEventDestroy(t_run[d]);
-        }
-        if (copy) cudaStreamDestroy(copy);
-    }
-};
-
-// One run over a view bound to the context: enqueue (returns before the
-// enumeration ends) and finish (waits, spills, reads the results).
-struct ViewJob {
-    bool mce;
-    uint32_t hist_len;  // MCE histogram entries read per view (0: count only)
-    g2_opts o{};
-    std::vector<unsigned long long> h;
-
-    int enqueue(g2_ctx *ctx, const uint32_t *d_src, uint64_t nsrc) {
-        TaskList tl;
-        const uint64_t warps = mce ? mce_warps(ctx, &o) : match_warps(ctx, &o);
-        int rc = prepare_tasks(ctx, d_src, nsrc, true, &o, warps, nullptr, &tl, mce);
-        if (rc) return rc;
-        ctx->last_split = tl.split;
-        ctx->last_cap = tl.cap;
-        rc = grow(ctx, ctx->d_out, ctx->out_cap, 1 + (mce ? hist_len : 0u), "out");
-        if (rc) return rc;
-        return mce ? mce_enqueue(ctx, tl, &o, ctx->d_out, hist_len, nullptr, nullptr, nullptr)
-                   : match_enqueue(ctx, tl, &o, ctx->d_out, nullptr, nullptr, nullptr);
-    }
-
-    int finish(g2_ctx *ctx) {
-        if (mce) {
-            const int rc = mce_host_spill(ctx, nullptr);
-            if (rc) return rc;
-        }
-        h.assign(1 + (mce ? hist_len : 0u), 0ull);
-        int status = 0;
-        G2_TRY(cudaMemcpy(h.data(), ctx->d_out, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost));
-        G2_TRY(cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-        return status_to_code(status);
-    }
-};
-
-int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint64_t n, const uint32_t *bin_of,
-             uint32_t nbins, const g2_view_opts *vo, const g2_opts *opts, uint64_t *count, uint64_t *hist,
-             uint32_t hist_len, uint64_t *bin_counts, g2_view_stats *stats) {
-    const auto t_start = std::chrono::steady_clock::now();
-    if (!ctx || !rp || !bin_of || !count || (hist && !hist_len) || n >= (1ull << 32) || (!ci && rp[n]))
-        return G2_ERR_INVALID;
-    if (opts && (opts->root_nodes || opts->root_cost || opts->work_bytes || opts->schedule == G2_SCHED_SCORES))
-        return G2_ERR_INVALID;
-    if (!mce && !ctx->has_plan) return G2_ERR_NO_PLAN;
-    // view shape: the query's (MCE: cliques around the root, rows of its
-    // neighbours, full balls: X holds the root's smaller neighbours)
-    g2view::Shape shape;
-    shape.min_deg = 1;
-    if (!mce)
-        shape = g2view::plan_shape(ctx->plan.k, ctx->plan.bn_count, ctx->plan.bn_pos, ctx->plan.cond_count,
-                                   ctx->plan.cond_op, ctx->plan.cond_pos);
-    if (vo && vo->radius) shape.radius = vo->radius;
-    if (vo && vo->row_radius) shape.row_radius = vo->row_radius;
-    if (vo && (vo->flags & G2_VIEW_NO_UPPER)) shape.upper = shape.forward = false;
-    if (vo && (vo->flags & ~(uint32_t)G2_VIEW_NO_UPPER)) return G2_ERR_INVALID;
-    if (shape.row_radius > shape.radius || shape.radius > 15) return G2_ERR_INVALID;
-    // roots grouped by bin, ascending inside a bin
-    std::vector<uint64_t> start((uint64_t)nbins + 1, 0);
-    for (uint64_t v = 0; v < n; v++) {
-        if (bin_of[v] == G2_VIEW_NO_BIN) continue;
-        if (bin_of[v] >= nbins) return G2_ERR_INVALID;
-        start[bin_of[v] + 1]++;
-    }
-    uint64_t max_roots = 0;
-    for (uint32_t b = 0; b < nbins; b++) {
-        max_roots = std::max(max_roots, start[b + 1]);
-        start[b + 1] += start[b];
-    }
-    std::vector<uint32_t> roots(start[nbins]);
-    {
-        std::vector<uint64_t> pos(start.begin(), start.end() - 1);
-        for (uint64_t v = 0; v < n; v++)
-            if (bin_of[v] != G2_VIEW_NO_BIN) roots[pos[bin_of[v]]++] = (uint32_t)v;
-    }
-    G2_TRY(cudaSetDevice(ctx->device));
-    // the context's own CSR gives way to the view slots
-    if (ctx->owns_csr) {
-        cudaFree(ctx->d_rp);
-        cudaFree(ctx->d_ci);
-        ctx->rp_cap = ctx->ci_cap = 0;
-    }
-    ctx->d_rp = nullptr;
-    ctx->d_ci = nullptr;
-    ctx->owns_csr = false;
-    ctx->n = ctx->m = 0;
-    ctx->launches = 0;
-    int rc = g2_reserve(ctx, std::max<uint64_t>(max_roots, 1));
-    if (rc) return rc;
-
-    ViewJob job;
-    job.mce = mce;
-    job.hist_len = hist ? hist_len : 0u;
-    if (opts) job.o = *opts;
-    std::vector<uint64_t> hsum(job.hist_len, 0ull);
-    uint64_t total = 0;
-    if (bin_counts) memset(bin_counts, 0, sizeof(uint64_t) * nbins);
-    g2_view_stats st{};
-    uint32_t *saved_fo = ctx->d_fo;
-    {
-        ViewProducers prod;  // destroyed after dev, whose destructor waits for uploads from its slots
-        ViewDevice dev(ctx);
-        rc = dev.init();
-        prod.rp = rp;
-        prod.ci = ci;
-        prod.n = n;
-        prod.bin_start = start.data();
-        prod.roots = roots.data();
-        prod.slots = &ctx->view_host;
-        prod.nbins = nbins;
-        prod.shape = shape;
-        prod.device = ctx->device;
-        uint32_t np = vo && vo->producers ? vo->producers : std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
-        np = std::min<uint32_t>(np, std::max<uint32_t>(nbins, 1u));
-        if (!rc && nbins) prod.start(np, np + 2);
-        double wait_ms = 0;
-        // next view with roots (bins that kept none count 0)
-        auto take = [&](ReadyView *v) {
-            while (prod.take(v, &wait_ms)) {
-                if (v->slot >= 0) return true;
-            }
-            return false;
-        };
-        ReadyView cur, nxt;
-        int d = 0;
-        bool have = !rc && nbins && take(&cur);
-        if (have) rc = dev.upload(cur, (*prod.slots)[cur.slot].first, d);
-        while (have && !rc) {
-            // the run of this view, on the legacy stream after its upload
-            rc = fail_cuda_if(ctx, cudaStreamWaitEvent(nullptr, dev.copied[d], 0), "view wait");
-            if (rc) break;
-            const uint32_t *d_src = dev.bind(cur, d);
-            rc = fail_cuda_if(ctx, cudaEventRecord(dev.t_run[0], nullptr), "view record");
-            if (!rc) rc = job.enqueue(ctx, d_src, cur.sizes.nsrc);
-            if (!rc) rc = fail_cuda_if(ctx, cudaEventRecord(dev.t_run[1], nullptr), "view record");
-            if (!rc) rc = fail_cuda_if(ctx, cudaEventRecord(dev.done[d], nullptr), "view record");
-            if (rc) break;
-            // the next view's upload overlaps this run
-            const bool more = take(&nxt);
-            if (more) rc = dev.upload(nxt, (*prod.slots)[nxt.slot].first, d ^ 1);
-            if (!rc) rc = job.finish(ctx);
-            if (rc) break;
-            total += job.h[0];
-            for (uint32_t s = 0; s < job.hist_len; s++) hsum[s] += job.h[1 + s];
-            if (bin_counts) bin_counts[cur.bin] = job.h[0];
-            const g2view::Layout L(cur.sizes);
-            st.bins++;
-            st.view_vertices += cur.sizes.n;
-            st.view_edges += cur.sizes.m;
-            st.h2d_bytes += L.bytes;
-            st.max_view_bytes = std::max(st.max_view_bytes, L.bytes);
-            st.copy_ms += dev.copy_ms(d);
-            st.run_ms += dev.run_ms();
-            prod.release(cur.slot);
-            cur = nxt;
-            have = more;
-            d ^= 1;
-        }
-        if (!rc) {
-            std::lock_guard<std::mutex> g(prod.mu);
-            rc = prod.error;
-        }
-        if (rc) prod.fail(rc);
-        for (auto &t : prod.threads) t.join();
-        prod.threads.clear();
-        st.build_ms = prod.build_ms;
-        st.wait_ms = wait_ms;
-    }
-    ctx->d_fo = saved_fo;
-    ctx->d_rp = nullptr;
-    ctx->d_ci = nullptr;
-    ctx->n = ctx->m = 0;
-    if (rc) return rc;
-    *count = total;
-    if (hist)
-        for (uint32_t s = 0; s < hist_len; s++) hist[s] = hsum[s];
-    st.total_ms = ms_between(t_start, std::chrono::steady_clock::now());
-    if (stats) *stats = st;
-    return G2_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-int g2_view_mce(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, const uint32_t *bin_of,
-                uint32_t nbins, const g2_view_opts *vopts, const g2_opts *opts, uint64_t *count, uint64_t *hist,
-                uint32_t hist_len, uint64_t *bin_counts, g2_view_stats *stats) {
-    return view_run(ctx, true, row_ptrs, cols, n, bin_of, nbins, vopts, opts, count, hist, hist_len, bin_counts,
-                    stats);
-}
-
-int g2_view_match(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, const uint32_t *bin_of,
-                  uint32_t nbins, const g2_view_opts *vopts, const g2_opts *opts, uint64_t *count,
-                  uint64_t *bin_counts, g2_view_stats *stats) {
-    return view_run(ctx, false, row_ptrs, cols, n, bin_of, nbins, vopts, opts, count, nullptr, 0, bin_counts, stats);
 }
 
 // ---------------------------------------------------------- cost model
