@@ -8,8 +8,10 @@
 #include "view_host.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 
 #include "g2_aimd.h"
 
@@ -94,19 +96,43 @@ Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
         row_[i] = mark_[ball_[i]] <= sh.row_radius;
         mark_[ball_[i]] = (uint32_t)i;
     }
-    // one pass over the kept rows: local columns staged here, copied out by fill
     Sizes s;
     s.n = nv;
     s.nsrc = src_.size();
     deg_.assign(nv, 0u);
     fo_.assign(nv, 0u);
     cols_.clear();
+    row_start_ = sh.forward ? 1u : 0u;
+    staged_ = threads_ <= 1 || nv < kParallelRows;
+    if (!staged_) {
+        // large view, several threads: count the rows here, write them in fill
+        std::vector<uint32_t> mf(threads_, 0u);
+        parallel_rows(nv, [&](unsigned t, uint64_t i0, uint64_t i1) {
+            for (uint64_t i = i0; i < i1; i++) {
+                if (!row_[i]) continue;
+                uint32_t d = 0, back = 0;
+                for (uint64_t e = row_begin(i); e < rp_[ball_[i] + 1]; e++) {
+                    const uint32_t l = mark_[ci_[e]];
+                    if (l == kNone) continue;
+                    d++;
+                    back += l <= i;
+                }
+                deg_[i] = d;
+                fo_[i] = back;
+                mf[t] = std::max(mf[t], d - back);
+            }
+        });
+        for (uint32_t v : mf) s.max_fwd = std::max(s.max_fwd, v);
+        for (uint64_t i = 0; i < nv; i++) s.m += deg_[i];
+        return s;
+    }
+    // one pass over the kept rows: local columns staged here, copied out by fill
     for (uint64_t i = 0; i < nv; i++) {
         if (!row_[i]) continue;
         const uint32_t g = ball_[i];
         const uint64_t before = cols_.size();
         uint32_t back = 0;
-        for (uint64_t e = row_from(rp_, ci_, g, sh.forward ? g + 1 : lo_); e < rp_[g + 1]; e++) {
+        for (uint64_t e = row_begin(i); e < rp_[g + 1]; e++) {
             const uint32_t l = mark_[ci_[e]];
             if (l == kNone) continue;
             cols_.push_back(l);
@@ -121,16 +147,50 @@ Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
     return s;
 }
 
+// First entry of view row i's source row that can be in the view.
+uint64_t Builder::row_begin(uint64_t i) const {
+    const uint32_t g = ball_[i];
+    return row_from(rp_, ci_, g, row_start_ ? g + 1 : lo_);
+}
+
+// f(thread, i0, i1) over [0, nv) in blocks of kParallelRows / 8 rows taken in turn.
+template <class F>
+void Builder::parallel_rows(uint64_t nv, F f) {
+    const uint64_t block = kParallelRows / 8;
+    std::atomic<uint64_t> next{0};
+    auto work = [&](unsigned t) {
+        for (uint64_t i0; (i0 = next.fetch_add(block)) < nv;) f(t, i0, std::min(nv, i0 + block));
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < threads_; t++) th.emplace_back(work, t);
+    work(0);
+    for (auto &x : th) x.join();
+}
+
 void Builder::fill(uint64_t *rp, uint32_t *fo, uint32_t *ci, uint32_t *src, uint32_t *ids) {
+    const uint64_t nv = ball_.size();
     uint64_t off = 0;
-    for (uint64_t i = 0; i < ball_.size(); i++) {
+    for (uint64_t i = 0; i < nv; i++) {
         rp[i] = off;
         off += deg_[i];
         if (ids) ids[i] = ball_[i];
     }
-    rp[ball_.size()] = off;
+    rp[nv] = off;
     if (!fo_.empty()) memcpy(fo, fo_.data(), 4 * fo_.size());
-    if (!cols_.empty()) memcpy(ci, cols_.data(), 4 * cols_.size());
+    if (staged_) {
+        if (!cols_.empty()) memcpy(ci, cols_.data(), 4 * cols_.size());
+    } else {
+        parallel_rows(nv, [&](unsigned, uint64_t i0, uint64_t i1) {
+            for (uint64_t i = i0; i < i1; i++) {
+                if (!deg_[i]) continue;
+                uint32_t *out = ci + rp[i];
+                for (uint64_t e = row_begin(i); e < rp_[ball_[i] + 1]; e++) {
+                    const uint32_t l = mark_[ci_[e]];
+                    if (l != kNone) *out++ = l;
+                }
+            }
+        });
+    }
     for (uint64_t i = 0; i < src_.size(); i++) src[i] = mark_[src_[i]];
     release();
 }
@@ -306,7 +366,9 @@ int g2_view_materialize(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t
     for (uint64_t i = 0; i < nsrc; i++)
         if (sources[i] >= n) return G2_ERR_INVALID;
     memset(out, 0, sizeof(*out));
-    g2view::Builder b(row_ptrs, cols, n);
+    unsigned threads = std::thread::hardware_concurrency();
+    if (const char *e = getenv("G2_HOST_THREADS")) threads = (unsigned)atoi(e);
+    g2view::Builder b(row_ptrs, cols, n, threads ? threads : 1u);
     const g2view::Sizes s = b.plan(sources, nsrc, sh);
     auto *rp = static_cast<uint64_t *>(malloc(8 * (s.n + 1)));
     auto *fo = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.n, 1)));

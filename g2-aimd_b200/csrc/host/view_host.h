@@ -46,11 +46,15 @@ struct Shape {
     bool forward = false;     // rows keep only neighbours above their own vertex
 };
 
-// One builder per thread; it keeps an n-entry mark array (4 bytes per vertex of
-// the whole graph) between views and clears only what a view touched.
+// One builder per producer; it keeps an n-entry mark array (4 bytes per vertex
+// of the whole graph) between views and clears only what a view touched.  A
+// view of at least kParallelRows vertices has its rows counted and written by
+// `threads` threads (the walk itself runs on the calling thread).
 class Builder {
   public:
-    Builder(const uint64_t *rp, const uint32_t *ci, uint64_t n) : rp_(rp), ci_(ci), n_(n) {}
+    static constexpr uint64_t kParallelRows = 1u << 14;
+    Builder(const uint64_t *rp, const uint32_t *ci, uint64_t n, unsigned threads = 1)
+        : rp_(rp), ci_(ci), n_(n), threads_(threads ? threads : 1u) {}
     // Collect the view of `src` (sources must be < n).
     Sizes plan(const uint32_t *src, uint64_t nsrc, const Shape &shape);
     // Write the planned view: rp[n+1], fo[n] (per vertex, neighbours <= v),
@@ -63,9 +67,15 @@ class Builder {
   private:
     void release();
     bool relax(uint32_t x, uint32_t d);
+    uint64_t row_begin(uint64_t i) const;
+    template <class F>
+    void parallel_rows(uint64_t nv, F f);
     const uint64_t *rp_;
     const uint32_t *ci_;
     uint64_t n_;
+    unsigned threads_;
+    bool staged_ = true;       // columns staged in cols_ by plan (else written by fill)
+    uint32_t row_start_ = 0;   // 1: rows start above their own vertex (forward rows)
     std::vector<uint32_t> mark_;   // BFS depth, then the local id; kNone outside the view
     std::vector<uint32_t> ball_;   // view vertices (global ids), sorted after the walk
     std::vector<uint8_t> row_;     // view vertex i keeps its row

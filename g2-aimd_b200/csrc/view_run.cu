@@ -47,6 +47,7 @@ struct ViewProducers {
     const uint64_t *bin_start = nullptr;  // roots of bin b: roots[bin_start[b] .. bin_start[b+1])
     const uint32_t *roots = nullptr;
     uint32_t nbins = 0;
+    unsigned build_threads = 1;  // threads of each producer's builder (large views)
     g2view::Shape shape;
     int device = 0;
 
@@ -79,7 +80,7 @@ struct ViewProducers {
     void produce() {
         try {
             cudaSetDevice(device);  // pinned allocations are made by this thread
-            g2view::Builder b(rp, ci, n);
+            g2view::Builder b(rp, ci, n, build_threads);
             for (;;) {
                 const uint32_t bin = next_bin.fetch_add(1);
                 if (bin >= nbins) break;
@@ -367,6 +368,8 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
         prod.device = ctx->device;
         uint32_t np = vo && vo->producers ? vo->producers : std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
         np = std::min<uint32_t>(np, std::max<uint32_t>(nbins, 1u));
+        // the host's threads are shared out: few bins get several threads each
+        prod.build_threads = std::max(1u, std::thread::hardware_concurrency() / np);
         if (!rc && nbins) prod.start(np, np + 2);
         double wait_ms = 0;
         // next view with roots (bins that kept none count 0)

@@ -305,3 +305,20 @@ def test_view_bins_isolated_and_rejects(g2):
     g = g2.Graph.from_edges(3, [(0, 1)])
     with pytest.raises(Exception):
         g.view_bins(1 << 20, radius=1, row_radius=2)
+
+
+@pytest.mark.parametrize("upper,forward", [(False, False), (True, False), (True, True)])
+def test_large_views_built_by_threads_equal_one_thread(g2, monkeypatch, upper, forward):
+    """Views of at least 2^14 vertices have their rows counted and written by
+    several threads; the result is the one-thread view."""
+    g = g2.Graph.rmat(15, 8, seed=12).degeneracy_recoded()
+    src = np.arange(0, g.n, 2, dtype=np.uint32)
+    kw = dict(radius=1, row_radius=1, upper=upper, forward=forward)
+    monkeypatch.setenv("G2_HOST_THREADS", "1")
+    one, s1, i1 = g.view(src, **kw)
+    monkeypatch.setenv("G2_HOST_THREADS", "6")
+    many, s6, i6 = g.view(src, **kw)
+    assert one.n >= 1 << 14
+    assert np.array_equal(one.row_ptrs, many.row_ptrs) and np.array_equal(one.cols, many.cols)
+    assert np.array_equal(one.fwd_offsets, many.fwd_offsets) and one.max_fwd == many.max_fwd
+    assert np.array_equal(s1, s6) and np.array_equal(i1, i6)
