@@ -36,6 +36,8 @@ Layout::Layout(const Sizes &s) {
 
 void Builder::release() {
     for (uint32_t g : ball_) mark_[g] = kNone;
+    if (!bits_.empty())
+        for (uint32_t g : ball_) bits_[g >> 6] = 0;
     ball_.clear();
     row_.clear();
     src_.clear();
@@ -67,7 +69,9 @@ Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
             frontier_.swap(next_);
         }
     };
-    if (!sh.upper) {
+    if (sh.radius == 1 && threads_ > 1 && src_.size() >= kParallelRows) {
+        walk_radius1(sh);  // ball_ sorted, marks = local ids, rows flagged
+    } else if (!sh.upper) {
         // one multi-source BFS: the depth of a vertex is its distance to the set
         frontier_.clear();
         for (uint32_t s : src_)
@@ -86,16 +90,19 @@ Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
             walk(s, true);
         }
     }
-    // ascending global order = local ids; rows where the depth allows; marks become local ids
-    std::sort(ball_.begin(), ball_.end());
+    if (!walked_sorted_) {
+        // ascending global order = local ids; rows where the depth allows; marks become local ids
+        std::sort(ball_.begin(), ball_.end());
+        row_.resize(ball_.size());
+        for (uint64_t i = 0; i < ball_.size(); i++) {
+            row_[i] = mark_[ball_[i]] <= sh.row_radius;
+            mark_[ball_[i]] = (uint32_t)i;
+        }
+    }
+    walked_sorted_ = false;
     const uint64_t nv = ball_.size();
     // nothing below the smallest view vertex is in the view: rows are read from there
     lo_ = nv ? ball_[0] : 0u;
-    row_.resize(nv);
-    for (uint64_t i = 0; i < nv; i++) {
-        row_[i] = mark_[ball_[i]] <= sh.row_radius;
-        mark_[ball_[i]] = (uint32_t)i;
-    }
     Sizes s;
     s.n = nv;
     s.nsrc = src_.size();
@@ -145,6 +152,75 @@ Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
     }
     s.m = cols_.size();
     return s;
+}
+
+// Ball of radius 1 on several threads: the sources and their neighbours (above
+// the source for upper balls) are marked in a bitmap with atomics, depth 0 for
+// sources and 1 for the rest; the bitmap's words, read in order, give the ball
+// sorted, so each thread writes its part of ball_ and of the local ids directly.
+void Builder::walk_radius1(const Shape &sh) {
+    if (bits_.size() != (n_ + 63) / 64) bits_.assign((n_ + 63) / 64, 0ull);
+    const uint64_t ns = src_.size();
+    auto set_bit = [&](uint32_t x) { __atomic_fetch_or(&bits_[x >> 6], 1ull << (x & 63u), __ATOMIC_RELAXED); };
+    parallel_range(ns, [&](uint64_t a, uint64_t b) {
+        for (uint64_t i = a; i < b; i++) {
+            __atomic_store_n(&mark_[src_[i]], 0u, __ATOMIC_RELAXED);
+            set_bit(src_[i]);
+        }
+    });
+    parallel_range(ns, [&](uint64_t a, uint64_t b) {
+        for (uint64_t i = a; i < b; i++) {
+            const uint32_t s = src_[i];
+            for (uint64_t e = sh.upper ? row_from(rp_, ci_, s, s + 1) : rp_[s]; e < rp_[s + 1]; e++) {
+                const uint32_t u = ci_[e];
+                uint32_t none = kNone;  // sources keep depth 0
+                __atomic_compare_exchange_n(&mark_[u], &none, 1u, false, __ATOMIC_RELAXED, __ATOMIC_RELAXED);
+                set_bit(u);
+            }
+        }
+    });
+    // blocks of bitmap words: population per block, prefix, then each block its entries
+    const uint64_t words = bits_.size(), block = 1u << 12;
+    const uint64_t nblk = (words + block - 1) / block;
+    std::vector<uint64_t> cnt(nblk + 1, 0);
+    parallel_range(nblk, [&](uint64_t a, uint64_t b) {
+        for (uint64_t k = a; k < b; k++) {
+            uint64_t c = 0;
+            for (uint64_t w = k * block; w < std::min(words, (k + 1) * block); w++) c += __builtin_popcountll(bits_[w]);
+            cnt[k + 1] = c;
+        }
+    });
+    for (uint64_t k = 0; k < nblk; k++) cnt[k + 1] += cnt[k];
+    ball_.resize(cnt[nblk]);
+    row_.resize(cnt[nblk]);
+    parallel_range(nblk, [&](uint64_t a, uint64_t b) {
+        for (uint64_t k = a; k < b; k++) {
+            uint64_t i = cnt[k];
+            for (uint64_t w = k * block; w < std::min(words, (k + 1) * block); w++)
+                for (uint64_t x = bits_[w]; x; x &= x - 1) {
+                    const uint32_t g = (uint32_t)(w * 64 + (uint64_t)__builtin_ctzll(x));
+                    ball_[i] = g;
+                    row_[i] = mark_[g] <= sh.row_radius;
+                    mark_[g] = (uint32_t)i;
+                    i++;
+                }
+        }
+    });
+    walked_sorted_ = true;
+}
+
+// f(a, b) over [0, n) in blocks taken in turn by the builder's threads.
+template <class F>
+void Builder::parallel_range(uint64_t n, F f) {
+    const uint64_t blk = std::max<uint64_t>(1, std::min<uint64_t>(kParallelRows / 8, n / (4ull * threads_) + 1));
+    std::atomic<uint64_t> next{0};
+    auto work = [&]() {
+        for (uint64_t a; (a = next.fetch_add(blk)) < n;) f(a, std::min(n, a + blk));
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < threads_; t++) th.emplace_back(work);
+    work();
+    for (auto &x : th) x.join();
 }
 
 // First entry of view row i's source row that can be in the view.

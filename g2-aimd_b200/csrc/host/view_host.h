@@ -49,7 +49,8 @@ struct Shape {
 // One builder per producer; it keeps an n-entry mark array (4 bytes per vertex
 // of the whole graph) between views and clears only what a view touched.  A
 // view of at least kParallelRows vertices has its rows counted and written by
-// `threads` threads (the walk itself runs on the calling thread).
+// `threads` threads; a radius-1 ball of at least kParallelRows sources is
+// walked by them too (bitmap of n bits per builder).
 class Builder {
   public:
     static constexpr uint64_t kParallelRows = 1u << 14;
@@ -70,6 +71,11 @@ class Builder {
     uint64_t row_begin(uint64_t i) const;
     template <class F>
     void parallel_rows(uint64_t nv, F f);
+    template <class F>
+    void parallel_range(uint64_t n, F f);
+    void walk_radius1(const Shape &sh);
+    std::vector<uint64_t> bits_;  // radius-1 walks on several threads: view membership
+    bool walked_sorted_ = false;  // the walk left ball_ sorted and the marks as local ids
     const uint64_t *rp_;
     const uint32_t *ci_;
     uint64_t n_;

@@ -308,11 +308,13 @@ def test_view_bins_isolated_and_rejects(g2):
 
 
 @pytest.mark.parametrize("upper,forward", [(False, False), (True, False), (True, True)])
-def test_large_views_built_by_threads_equal_one_thread(g2, monkeypatch, upper, forward):
+@pytest.mark.parametrize("step", [1, 2])
+def test_large_views_built_by_threads_equal_one_thread(g2, monkeypatch, upper, forward, step):
     """Views of at least 2^14 vertices have their rows counted and written by
-    several threads; the result is the one-thread view."""
+    several threads, and radius-1 balls of at least 2^14 roots are walked by
+    them; the result is the one-thread view."""
     g = g2.Graph.rmat(15, 8, seed=12).degeneracy_recoded()
-    src = np.arange(0, g.n, 2, dtype=np.uint32)
+    src = np.arange(0, g.n, step, dtype=np.uint32)
     kw = dict(radius=1, row_radius=1, upper=upper, forward=forward)
     monkeypatch.setenv("G2_HOST_THREADS", "1")
     one, s1, i1 = g.view(src, **kw)
