@@ -168,10 +168,12 @@ def run_view_host_leg(a):
     cl = g2aimd.Graph.chung_lu(1 << 18, 2.3, 16.0, seed=a.seed).degeneracy_recoded()
     k4 = Plan.preset(K4).view_shape()
     mce = {"radius": 1, "row_radius": 1, "min_root_degree": 1, "upper": False, "forward": False}
-    out = {"workload": f"view bins of CSR bytes / {a.view_split}, built on the host (no GPU)"}
+    out = {"workload": f"view bins of CSR bytes / {a.view_split}, built on the host (no GPU); ego rows on "
+                       "the bins planned without them"}
     cases = [(f"k4_rmat_s{a.scale}", g, dict(k4, upper=False, forward=False)),
              (f"k4_rmat_s{a.scale}", g, dict(k4, forward=False)), (f"k4_rmat_s{a.scale}", g, k4),
-             ("mce_chung_lu_2^18", cl, mce)]
+             (f"k4_rmat_s{a.scale}", g, dict(k4, ego=True)),
+             ("mce_chung_lu_2^18", cl, mce), ("mce_chung_lu_2^18", cl, dict(mce, ego=True))]
     for name, gr, shape in cases:
         budget = (gr.row_ptrs.nbytes + gr.cols.nbytes) // a.view_split
         t0 = time.perf_counter()
@@ -185,7 +187,8 @@ def run_view_host_leg(a):
             v, _src, _ids = gr.view(order[cuts[b]:cuts[b + 1]].astype(np.uint32), **shape)
             vn += v.n
             vm += v.m
-        key = name + ("/forward" if shape["forward"] else "/upper" if shape["upper"] else "/full")
+        key = name + ("/forward" if shape["forward"] else "/upper" if shape["upper"] else "/full") + \
+            ("+ego" if shape.get("ego") else "")
         out[key] = {"bins": nb, "plan_s": round(plan_s, 2), "view_vertices": int(vn), "view_entries": int(vm),
                     "entries_vs_m": round(vm / gr.m, 3), "build_s": round(time.perf_counter() - t0, 2)}
     print(json.dumps(out), flush=True)

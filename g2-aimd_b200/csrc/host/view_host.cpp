@@ -110,7 +110,7 @@ Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
     fo_.assign(nv, 0u);
     cols_.clear();
     row_start_ = sh.forward ? 1u : 0u;
-    staged_ = threads_ <= 1 || nv < kParallelRows;
+    staged_ = threads_ <= 1 || nv < kParallelRows || sh.ego;  // ego rows filter staged columns
     if (!staged_) {
         // large view, several threads: count the rows here, write them in fill
         std::vector<uint32_t> mf(threads_, 0u);
@@ -151,7 +151,76 @@ Sizes Builder::plan(const uint32_t *src, uint64_t nsrc, const Shape &sh) {
         s.max_fwd = std::max(s.max_fwd, d - back);
     }
     s.m = cols_.size();
+    if (sh.ego) ego_filter(&s);
     return s;
+}
+
+// Keep only the entries (u, y) with a kept source s in N[u] ∩ N[y] (the edges of
+// the sources' ego networks): a root's search reads rows of its neighbours
+// restricted to its own neighbourhood, nothing else.  Per source s (on the
+// builder's threads): s's row is kept whole, and in the row of each neighbour u
+// the entries in N[s] are marked, by scanning u's row against a stamp of N(s)
+// or, for a row much longer than s's, by binary searches of N[s] in it.
+void Builder::ego_filter(Sizes *s) {
+    const uint64_t nv = ball_.size();
+    std::vector<uint64_t> off(nv + 1, 0);
+    for (uint64_t i = 0; i < nv; i++) off[i + 1] = off[i] + deg_[i];
+    std::vector<uint8_t> keep(cols_.size(), 0);
+    std::vector<uint32_t> ls;
+    ls.reserve(src_.size());
+    for (uint32_t g : src_) ls.push_back(mark_[g]);
+    std::sort(ls.begin(), ls.end());
+    ls.erase(std::unique(ls.begin(), ls.end()), ls.end());
+    auto keep_at = [&](uint64_t p) { __atomic_store_n(&keep[p], (uint8_t)1, __ATOMIC_RELAXED); };
+    std::vector<std::vector<uint32_t>> stamps(threads_);
+    const uint32_t *c = cols_.data();
+    parallel_rows(ls.size(), [&](unsigned t, uint64_t a, uint64_t b) {
+        std::vector<uint32_t> &stamp = stamps[t];
+        if (stamp.size() != nv) stamp.assign(nv, kNone);
+        for (uint64_t k = a; k < b; k++) {
+            const uint32_t src = ls[k];
+            const uint32_t *rs = c + off[src];
+            const uint64_t ns = deg_[src];
+            for (uint64_t j = 0; j < ns; j++) {
+                keep_at(off[src] + j);
+                stamp[rs[j]] = src;
+            }
+            for (uint64_t j = 0; j < ns; j++) {
+                const uint32_t u = rs[j];
+                const uint32_t *ru = c + off[u];
+                const uint64_t nu = deg_[u];
+                if (nu <= 8 * ns) {
+                    for (uint64_t q = 0; q < nu; q++)
+                        if (ru[q] == src || stamp[ru[q]] == src) keep_at(off[u] + q);
+                } else {
+                    auto find = [&](uint32_t x) {
+                        const uint32_t *p = std::lower_bound(ru, ru + nu, x);
+                        if (p != ru + nu && *p == x) keep_at(off[u] + (uint64_t)(p - ru));
+                    };
+                    find(src);
+                    for (uint64_t q = 0; q < ns; q++) find(rs[q]);
+                }
+            }
+        }
+    });
+    // compact in place (kept entries move left), recount forward lists
+    uint64_t w = 0;
+    s->max_fwd = 0;
+    for (uint64_t i = 0; i < nv; i++) {
+        uint32_t d = 0, back = 0;
+        for (uint64_t p = off[i]; p < off[i + 1]; p++) {
+            if (!keep[p]) continue;
+            const uint32_t y = cols_[p];
+            cols_[w++] = y;
+            d++;
+            back += y <= i;
+        }
+        deg_[i] = d;
+        fo_[i] = back;
+        s->max_fwd = std::max(s->max_fwd, d - back);
+    }
+    cols_.resize(w);
+    s->m = w;
 }
 
 // Ball of radius 1 on several threads: the sources and their neighbours (above
@@ -409,12 +478,15 @@ namespace {
 
 bool shape_from(uint32_t radius, uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
                 g2view::Shape *sh) {
-    if (row_radius > radius || radius > 15 || (flags & ~(uint32_t)(G2_VIEW_UPPER | G2_VIEW_FORWARD))) return false;
+    if (row_radius > radius || radius > 15 || (flags & ~(uint32_t)(G2_VIEW_UPPER | G2_VIEW_FORWARD | G2_VIEW_EGO)))
+        return false;
+    if ((flags & G2_VIEW_EGO) && (radius != 1 || row_radius != 1)) return false;  // ego networks: radius 1
     sh->radius = radius;
     sh->row_radius = row_radius;
     sh->min_deg = min_root_degree;
     sh->upper = (flags & G2_VIEW_UPPER) != 0;
     sh->forward = (flags & G2_VIEW_FORWARD) != 0;
+    sh->ego = (flags & G2_VIEW_EGO) != 0;
     return true;
 }
 

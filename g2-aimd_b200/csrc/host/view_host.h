@@ -44,6 +44,7 @@ struct Shape {
     uint32_t min_deg = 0;     // sources of smaller degree are dropped
     bool upper = false;       // balls walked through vertices above their source
     bool forward = false;     // rows keep only neighbours above their own vertex
+    bool ego = false;         // rows keep only edges of the sources' ego networks (radius 1)
 };
 
 // One builder per producer; it keeps an n-entry mark array (4 bytes per vertex
@@ -74,6 +75,7 @@ class Builder {
     template <class F>
     void parallel_range(uint64_t n, F f);
     void walk_radius1(const Shape &sh);
+    void ego_filter(Sizes *s);
     std::vector<uint64_t> bits_;  // radius-1 walks on several threads: view membership
     bool walked_sorted_ = false;  // the walk left ball_ sorted and the marks as local ids
     const uint64_t *rp_;

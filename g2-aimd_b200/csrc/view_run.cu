@@ -309,8 +309,10 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
     if (vo && vo->radius) shape.radius = vo->radius;
     if (vo && vo->row_radius) shape.row_radius = vo->row_radius;
     if (vo && (vo->flags & G2_VIEW_NO_UPPER)) shape.upper = shape.forward = false;
-    if (vo && (vo->flags & ~(uint32_t)G2_VIEW_NO_UPPER)) return G2_ERR_INVALID;
+    if (vo && (vo->flags & G2_VIEW_EGO)) shape.ego = true;
+    if (vo && (vo->flags & ~(uint32_t)(G2_VIEW_NO_UPPER | G2_VIEW_EGO))) return G2_ERR_INVALID;
     if (shape.row_radius > shape.radius || shape.radius > 15) return G2_ERR_INVALID;
+    if (shape.ego && (shape.radius != 1 || shape.row_radius != 1)) return G2_ERR_INVALID;
     // roots grouped by bin, ascending inside a bin
     std::vector<uint64_t> start((uint64_t)nbins + 1, 0);
     for (uint64_t v = 0; v < n; v++) {

@@ -109,18 +109,20 @@ class Graph:
         return nb.value, bins
 
     # ----------------------------------------------------- views (out of core)
-    def view(self, sources, radius=1, row_radius=None, min_root_degree=0, upper=False, forward=False):
+    def view(self, sources, radius=1, row_radius=None, min_root_degree=0, upper=False, forward=False, ego=False):
         """(view graph, local sources, global ids) of the ball of `radius` around
         `sources` (g2_view_materialize): ids ascending in global order, rows kept
         for vertices within row_radius (default: radius), restricted to the ball;
         upper: each source's ball walked through vertices above it; forward: rows
-        keep only their entries above their own vertex."""
+        keep only their entries above their own vertex; ego (radius 1): rows keep
+        only edges inside some source's closed neighbourhood."""
         from ._lib import G2View
         src = np.ascontiguousarray(sources, dtype=np.uint32)
         v = G2View()
         rr = radius if row_radius is None else row_radius
         check(lib().g2_view_materialize(_ptr(self.row_ptrs), _ptr(self.cols), self.n, _ptr(src), src.size,
-                                        radius, rr, min_root_degree, int(bool(upper)) | 4 * int(bool(forward)),
+                                        radius, rr, min_root_degree,
+                                        int(bool(upper)) | 4 * int(bool(forward)) | 8 * int(bool(ego)),
                                         C.byref(v)),
               "g2_view_materialize")
         try:
@@ -138,14 +140,16 @@ class Graph:
         g.max_fwd = max_fwd
         return g, lsrc, ids
 
-    def view_bins(self, max_bytes, radius=1, row_radius=None, min_root_degree=0, upper=False, forward=False):
+    def view_bins(self, max_bytes, radius=1, row_radius=None, min_root_degree=0, upper=False, forward=False,
+                  ego=False):
         """(nbins, bin_of) from g2_view_bins: roots in id order, a bin closes when
         its view would exceed max_bytes."""
         bins = np.zeros(self.n, np.uint32)
         nb = C.c_uint32()
         rr = radius if row_radius is None else row_radius
         check(lib().g2_view_bins(_ptr(self.row_ptrs), _ptr(self.cols), self.n, radius, rr, min_root_degree,
-                                 int(bool(upper)) | 4 * int(bool(forward)), int(max_bytes), _ptr(bins),
+                                 int(bool(upper)) | 4 * int(bool(forward)) | 8 * int(bool(ego)), int(max_bytes),
+                                 _ptr(bins),
                                  C.byref(nb)), "g2_view_bins")
         return nb.value, bins
 

@@ -282,8 +282,11 @@ int g2_degeneracy_order_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core);
 #define G2_VIEW_NO_BIN 0xffffffffu
 #define G2_VIEW_UPPER 1u     /* balls walked through vertices above their source */
 #define G2_VIEW_FORWARD 4u   /* rows keep only neighbours above their own vertex */
+#define G2_VIEW_EGO 8u       /* radius-1 views: rows keep only edges inside the ego network
+                                N[s] of some root s of the bin (also a g2_view_opts flag) */
 #define G2_VIEW_NO_UPPER 2u  /* g2_view_opts: full balls and rows even where the query
-                                allows upper balls and forward rows */
+                                allows upper balls and forward rows; G2_VIEW_EGO there asks
+                                for ego rows (radius-1 views only) */
 typedef struct g2_view_opts {
     uint32_t producers;   /* host threads building views (0 = min(8, cores))    */
     uint32_t radius;      /* ball radius (0 = from the query: 1 for MCE)         */
@@ -431,7 +434,10 @@ int g2_read_vbmap(const char *path, uint64_t n, uint32_t *nbins,
  * image: cliques, cycles); with G2_VIEW_FORWARD rows keep only their entries
  * above their own vertex (queries whose conditions order every position above
  * all earlier ones: cliques; every candidate then lies above its parent's
- * image).  Every embedding rooted in S lies in B and uses only
+ * image); with G2_VIEW_EGO (radius 1 only) rows keep only the entries (u, y)
+ * for which some root s of S has u and y in N[s]: a radius-1 search from s
+ * reads nothing outside N[s] (maximal cliques: P, X and their rows; matches:
+ * every query vertex is adjacent to the root).  Every embedding rooted in S lies in B and uses only
  * rows of vertices within the query's back-neighbour distance, so a search
  * over the view from S's local ids finds exactly what it finds in the whole
  * graph (view/view_bin.h:40-159 keeps global ids and whole rows instead).

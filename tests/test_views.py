@@ -10,7 +10,7 @@ import pytest
 from helpers import random_graph, small_graphs
 
 
-def py_view(g, sources, radius, row_radius, min_deg, upper=False, forward=False):
+def py_view(g, sources, radius, row_radius, min_deg, upper=False, forward=False, ego=False):
     """Direct construction: per kept source, BFS depths (through vertices above
     the source when upper); a vertex's depth is its smallest; ascending ids;
     rows of vertices within row_radius restricted to the ball (and to entries
@@ -34,19 +34,27 @@ def py_view(g, sources, radius, row_radius, min_deg, upper=False, forward=False)
             depth[x] = min(depth.get(x, d), d)
     ids = sorted(depth)
     local = {g_: i for i, g_ in enumerate(ids)}
+    # ego: the sources' closed neighbourhoods as seen in the (forward) rows
+    hoods = []
+    if ego:
+        for s in set(kept):
+            hoods.append({s} | {u for u in ci[rp[s]:rp[s + 1]].tolist() if u in local and (not forward or u > s)})
     rows = []
     for g_ in ids:
         if depth[g_] <= row_radius:
-            rows.append([local[u] for u in ci[rp[g_]:rp[g_ + 1]].tolist() if u in local and (not forward or u > g_)])
+            row = [u for u in ci[rp[g_]:rp[g_ + 1]].tolist() if u in local and (not forward or u > g_)]
+            if ego:
+                row = [u for u in row if any(g_ in h and u in h for h in hoods)]
+            rows.append([local[u] for u in row])
         else:
             rows.append([])
     return ids, rows, [local[s] for s in kept]
 
 
-def check_view(g, sources, radius, row_radius, min_deg=0, upper=False, forward=False):
+def check_view(g, sources, radius, row_radius, min_deg=0, upper=False, forward=False, ego=False):
     v, lsrc, ids = g.view(sources, radius=radius, row_radius=row_radius, min_root_degree=min_deg, upper=upper,
-                          forward=forward)
-    want_ids, want_rows, want_src = py_view(g, sources, radius, row_radius, min_deg, upper, forward)
+                          forward=forward, ego=ego)
+    want_ids, want_rows, want_src = py_view(g, sources, radius, row_radius, min_deg, upper, forward, ego)
     assert ids.tolist() == want_ids
     assert lsrc.tolist() == want_src
     assert v.n == len(want_ids) and v.row_ptrs[0] == 0
@@ -103,7 +111,7 @@ def test_view_rejects_bad_arguments(g2):
     src = np.array([0], np.uint32)
     sp = src.ctypes.data_as(C.c_void_p)
     assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 2, 0, 0, C.byref(v)) == -1  # row radius > radius
-    assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 1, 0, 8, C.byref(v)) == -1  # unknown flag
+    assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 1, 0, 16, C.byref(v)) == -1  # unknown flag
     assert lib.g2_view_materialize(rp, ci, g.n, sp, 1, 1, 1, 0, 1, C.byref(v)) == 0
     lib.g2_view_free(C.byref(v))
 
@@ -324,3 +332,71 @@ def test_large_views_built_by_threads_equal_one_thread(g2, monkeypatch, upper, f
     assert np.array_equal(one.row_ptrs, many.row_ptrs) and np.array_equal(one.cols, many.cols)
     assert np.array_equal(one.fwd_offsets, many.fwd_offsets) and one.max_fwd == many.max_fwd
     assert np.array_equal(s1, s6) and np.array_equal(i1, i6)
+
+
+def test_ego_view_structure(g2):
+    """Ego rows: an entry (u, y) stays when some kept source s has u and y in N[s]
+    (within the rows the other flags keep)."""
+    rng = np.random.default_rng(8)
+    graphs = small_graphs(g2.Graph) + [g2.Graph.rmat(9, 8, seed=2)]
+    for g in graphs:
+        for trial in range(3):
+            k = int(rng.integers(0, max(1, g.n) + 1))
+            src = rng.choice(g.n, size=min(k, g.n), replace=False) if g.n else np.zeros(0, np.uint32)
+            for upper, forward in ((False, False), (True, False), (True, True)):
+                check_view(g, src, 1, 1, min_deg=int(trial == 2), upper=upper, forward=forward, ego=True)
+
+
+def test_ego_needs_radius_one(g2):
+    g = g2.Graph.from_edges(3, [(0, 1), (1, 2)])
+    with pytest.raises(Exception):
+        g.view([0], radius=2, row_radius=1, ego=True)
+
+
+@pytest.mark.parametrize("nbins", [1, 5, 23])
+def test_ego_views_sum_to_whole_graph_mce(g2, orc, nbins):
+    g = random_graph(g2.Graph, 400, 0.04, 31, planted=[tuple(range(0, 30, 3))]).degeneracy_recoded()
+    want = orc.mce(g, hist_len=64)
+    bin_of = np.random.default_rng(nbins).integers(0, nbins, g.n).astype(np.uint32)
+    count, hist, induced, ego = 0, np.zeros(64, np.uint64), 0, 0
+    for src in by_bin(bin_of, nbins):
+        full, _, _ = g.view(src, radius=1, row_radius=1, min_root_degree=1)
+        v, lsrc, _ = g.view(src, radius=1, row_radius=1, min_root_degree=1, ego=True)
+        induced += full.m
+        ego += v.m
+        if lsrc.size:
+            got = orc.mce(v, roots=lsrc, hist_len=64)
+            count += got["count"]
+            hist += got["hist"]
+    assert count == want["count"] and np.array_equal(hist, want["hist"])
+    if nbins > 1:
+        assert ego < induced
+
+
+@pytest.mark.parametrize("q", [0, 2, 24, 25])
+def test_ego_views_sum_to_whole_graph_match(g2, orc, q):
+    from g2aimd.context import Plan
+    g = random_graph(g2.Graph, 300, 0.05, 21, planted=[tuple(range(0, 24, 2))]).degeneracy_recoded()
+    plan = Plan.preset(q)
+    sh = plan.view_shape()
+    assert sh["radius"] == 1
+    want = orc.match(g, plan)["count"]
+    for nbins in (1, 7):
+        bin_of = np.random.default_rng(nbins).integers(0, nbins, g.n).astype(np.uint32)
+        total = 0
+        for src in by_bin(bin_of, nbins):
+            v, lsrc, _ = g.view(src, ego=True, **sh)
+            if lsrc.size:
+                total += orc.match(v, plan, roots=lsrc)["count"]
+        assert total == want, (q, nbins)
+
+
+def test_large_ego_views_threads_equal_one_thread(g2, monkeypatch):
+    g = g2.Graph.chung_lu(1 << 15, 2.3, 12.0, seed=4).degeneracy_recoded()
+    src = np.arange(0, g.n, 3, dtype=np.uint32)
+    monkeypatch.setenv("G2_HOST_THREADS", "1")
+    one, _, _ = g.view(src, radius=1, row_radius=1, min_root_degree=1, ego=True)
+    monkeypatch.setenv("G2_HOST_THREADS", "6")
+    many, _, _ = g.view(src, radius=1, row_radius=1, min_root_degree=1, ego=True)
+    assert np.array_equal(one.row_ptrs, many.row_ptrs) and np.array_equal(one.cols, many.cols)
+    assert np.array_equal(one.fwd_offsets, many.fwd_offsets) and one.max_fwd == many.max_fwd
