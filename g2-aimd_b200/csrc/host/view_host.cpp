@@ -347,23 +347,26 @@ void Builder::fill_packed(void *buf, const Sizes &s) {
          reinterpret_cast<uint32_t *>(b + L.src), nullptr);
 }
 
-uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Shape &sh, uint64_t max_bytes,
-                   uint32_t *bin_of) {
-    if (n == 0) return 0;
-    // The open bin's view is tracked exactly: depth[x] = smallest depth from a
-    // source of the bin (walked again only when it drops; sources come in
-    // ascending order, which the upper walks need), and a vertex that enters
-    // the ball or gains its row adds its column entries towards the ball.
-    std::vector<uint32_t> depth(n, kNone), touched, frontier, next;
+namespace {
+
+// Greedy bins over the roots [v0, v1) (bin ids from 0; returns how many).  The
+// open bin's view is tracked exactly: depth[x] = smallest depth from a source
+// of the bin (walked again only when it drops; sources come in ascending order,
+// which the upper walks need), and a vertex that enters the ball or gains its
+// row adds its column entries towards the ball.  depth: n bytes, all 0xff.
+uint32_t plan_range(const uint64_t *rp, const uint32_t *ci, const Shape &sh, uint64_t max_bytes, uint64_t v0,
+                    uint64_t v1, std::vector<uint8_t> &depth, uint32_t *bin_of) {
+    constexpr uint8_t kOut = 0xff;
+    std::vector<uint32_t> touched, frontier, next;
     uint64_t bytes = 8, delta = 0;
     uint32_t bin = 0, nsrc = 0;
     uint32_t lo = 0;  // upper walks: no vertex below the bin's first source is in its ball
     auto relax = [&](uint32_t x, uint32_t d) {
-        const uint32_t old = depth[x];
-        if (old != kNone && old <= d) return false;
-        const bool fresh = old == kNone;
+        const uint8_t old = depth[x];
+        if (old != kOut && old <= d) return false;
+        const bool fresh = old == kOut;
         const bool gains_row = d <= sh.row_radius && (fresh || old > sh.row_radius);
-        depth[x] = d;
+        depth[x] = (uint8_t)d;
         if (fresh) {
             delta += 12;  // row pointer + forward offset
             touched.push_back(x);
@@ -371,7 +374,7 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
         if (fresh || gains_row) {
             for (uint64_t e = row_from(rp, ci, x, lo); e < rp[x + 1]; e++) {
                 const uint32_t y = ci[e];
-                if (y == x || depth[y] == kNone) continue;
+                if (y == x || depth[y] == kOut) continue;
                 // forward rows keep only entries above their own vertex
                 if (gains_row && (!sh.forward || y > x)) delta += 4;                            // x -> y
                 if (fresh && depth[y] <= sh.row_radius && (!sh.forward || x > y)) delta += 4;  // y -> x
@@ -394,7 +397,7 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
         }
         return delta;
     };
-    for (uint64_t v = 0; v < n; v++) {
+    for (uint64_t v = v0; v < v1; v++) {
         if (rp[v + 1] - rp[v] < sh.min_deg) {
             bin_of[v] = bin;  // no embedding is rooted here: no size
             continue;
@@ -402,7 +405,7 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
         if (sh.upper && nsrc == 0) lo = (uint32_t)v;
         uint64_t d = add((uint32_t)v);
         if (nsrc > 0 && bytes + d > max_bytes) {
-            for (uint32_t x : touched) depth[x] = kNone;
+            for (uint32_t x : touched) depth[x] = kOut;
             touched.clear();
             bin++;
             bytes = 8;
@@ -414,9 +417,42 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
         nsrc++;
         bin_of[v] = bin;
     }
+    for (uint32_t x : touched) depth[x] = kOut;
     return bin + 1;
 }
 
+}  // namespace
+
+uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Shape &sh, uint64_t max_bytes,
+                   uint32_t *bin_of, unsigned threads) {
+    if (n == 0) return 0;
+    // large graphs: contiguous root ranges of about equal edge counts, planned
+    // on threads of their own (a bin never spans two ranges)
+    const unsigned T = n >= kParallelBinRoots ? std::max(1u, threads) : 1u;
+    std::vector<uint64_t> cut(T + 1, n);
+    cut[0] = 0;
+    for (unsigned t = 1; t < T; t++) {
+        const uint64_t target = rp[n] / T * t;
+        cut[t] = std::max<uint64_t>(cut[t - 1], (uint64_t)(std::upper_bound(rp, rp + n + 1, target) - rp) - 1);
+    }
+    std::vector<uint32_t> count(T, 0);
+    auto run = [&](unsigned t) {
+        if (cut[t] >= cut[t + 1]) return;
+        std::vector<uint8_t> depth(n, 0xff);
+        count[t] = plan_range(rp, ci, sh, max_bytes, cut[t], cut[t + 1], depth, bin_of);
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < T; t++) th.emplace_back(run, t);
+    run(0);
+    for (auto &x : th) x.join();
+    uint32_t base = 0;
+    for (unsigned t = 0; t < T; t++) {
+        if (base)
+            for (uint64_t v = cut[t]; v < cut[t + 1]; v++) bin_of[v] += base;
+        base += count[t];
+    }
+    return base;
+}
 Shape plan_shape(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[8], const uint32_t *cond_count,
                  const uint32_t (*cond_op)[8], const uint32_t (*cond_pos)[8]) {
     k = std::min<uint32_t>(k, 8u);
@@ -500,7 +536,9 @@ int g2_view_bins(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uin
     if (!row_ptrs || !bin_of || !nbins || (!cols && row_ptrs[n]) || n >= (1ull << 32) ||
         !shape_from(radius, row_radius, min_root_degree, flags, &sh))
         return G2_ERR_INVALID;
-    *nbins = g2view::plan_bins(row_ptrs, cols, n, sh, max_bytes, bin_of);
+    unsigned threads = std::thread::hardware_concurrency();
+    if (const char *e = getenv("G2_HOST_THREADS")) threads = (unsigned)atoi(e);
+    *nbins = g2view::plan_bins(row_ptrs, cols, n, sh, max_bytes, bin_of, threads ? threads : 1u);
     return G2_OK;
 }
 

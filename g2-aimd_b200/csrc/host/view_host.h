@@ -98,9 +98,12 @@ class Builder {
 // Greedy partition of the roots 0..n-1 into bins in id order: a bin is closed
 // when its view would exceed max_bytes (the view's exact size, counted while
 // the bin grows, up to 48 bytes of alignment; a bin holds at least one source).
-// bin_of[v] for every vertex; returns the number of bins.
+// Graphs of at least kParallelBinRoots vertices are cut into `threads`
+// contiguous root ranges of about equal edge counts, planned in parallel (a bin
+// never spans two ranges).  bin_of[v] for every vertex; returns the number of bins.
+constexpr uint64_t kParallelBinRoots = 1u << 16;
 uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Shape &shape, uint64_t max_bytes,
-                   uint32_t *bin_of);
+                   uint32_t *bin_of, unsigned threads = 1);
 
 // What a query plan given by positions needs: k positions, bn_count[i] back
 // neighbours of position i at positions bn_pos[i][j] (< i), cond_count[i]

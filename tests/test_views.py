@@ -400,3 +400,24 @@ def test_large_ego_views_threads_equal_one_thread(g2, monkeypatch):
     many, _, _ = g.view(src, radius=1, row_radius=1, min_root_degree=1, ego=True)
     assert np.array_equal(one.row_ptrs, many.row_ptrs) and np.array_equal(one.cols, many.cols)
     assert np.array_equal(one.fwd_offsets, many.fwd_offsets) and one.max_fwd == many.max_fwd
+
+
+@pytest.mark.parametrize("upper,forward", [(False, False), (True, True)])
+def test_parallel_bin_plan(g2, monkeypatch, upper, forward):
+    """Graphs of >= 2^16 vertices are planned in contiguous root ranges on
+    several threads: bins stay contiguous and within budget, and each range
+    boundary costs at most one bin."""
+    g = g2.Graph.chung_lu(1 << 17, 2.3, 10.0, seed=6).degeneracy_recoded()
+    kw = dict(radius=1, row_radius=1, min_root_degree=1, upper=upper, forward=forward)
+    budget = (g.row_ptrs.nbytes + g.cols.nbytes) // 40
+    monkeypatch.setenv("G2_HOST_THREADS", "1")
+    n1, b1 = g.view_bins(budget, **kw)
+    monkeypatch.setenv("G2_HOST_THREADS", "6")
+    n6, b6 = g.view_bins(budget, **kw)
+    assert n1 <= n6 <= n1 + 5
+    for bins, nb in ((b1, n1), (b6, n6)):
+        assert bins.max() == nb - 1 and np.all(np.diff(bins.astype(np.int64)) >= 0)
+        for b in sorted(set(np.linspace(0, nb - 1, 12).astype(int).tolist())):
+            src = np.flatnonzero(bins == b).astype(np.uint32)
+            v, lsrc, _ = g.view(src, **kw)
+            assert lsrc.size <= 1 or view_bytes(v, lsrc.size) <= budget + 48
