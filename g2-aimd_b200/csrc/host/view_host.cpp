@@ -423,12 +423,12 @@ uint32_t plan_range(const uint64_t *rp, const uint32_t *ci, const Shape &sh, uin
 
 }  // namespace
 
-uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Shape &sh, uint64_t max_bytes,
-                   uint32_t *bin_of, unsigned threads) {
-    if (n == 0) return 0;
-    // large graphs: contiguous root ranges of about equal edge counts, planned
-    // on threads of their own (a bin never spans two ranges)
-    const unsigned T = n >= kParallelBinRoots ? std::max(1u, threads) : 1u;
+namespace {
+
+// Bins over T contiguous root ranges of about equal edge counts, each planned
+// on a thread of its own (a bin never spans two ranges).
+uint32_t plan_in_ranges(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Shape &sh, uint64_t max_bytes,
+                        uint32_t *bin_of, unsigned T) {
     std::vector<uint64_t> cut(T + 1, n);
     cut[0] = 0;
     for (unsigned t = 1; t < T; t++) {
@@ -452,6 +452,23 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
         base += count[t];
     }
     return base;
+}
+
+}  // namespace
+
+uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Shape &sh, uint64_t max_bytes,
+                   uint32_t *bin_of, unsigned threads) {
+    if (n == 0) return 0;
+    unsigned T = n >= kParallelBinRoots ? std::max(1u, threads) : 1u;
+    if (T == 1) return plan_in_ranges(rp, ci, n, sh, max_bytes, bin_of, 1);
+    // each range boundary adds at most one bin, so a first plan on T ranges
+    // bounds the serial bin count from below; ranges are then sized to hold at
+    // least 8 bins each (at most 1 bin in 8 added), down to one range for a
+    // graph of few bins
+    const uint32_t first = plan_in_ranges(rp, ci, n, sh, max_bytes, bin_of, T);
+    const uint64_t lower = first > T - 1 ? first - (T - 1) : 1;
+    const unsigned T2 = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(T, lower / 8));
+    return T2 == T ? first : plan_in_ranges(rp, ci, n, sh, max_bytes, bin_of, T2);
 }
 Shape plan_shape(uint32_t k, const uint32_t *bn_count, const uint32_t (*bn_pos)[8], const uint32_t *cond_count,
                  const uint32_t (*cond_op)[8], const uint32_t (*cond_pos)[8]) {

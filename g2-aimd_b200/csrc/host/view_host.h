@@ -98,9 +98,10 @@ class Builder {
 // Greedy partition of the roots 0..n-1 into bins in id order: a bin is closed
 // when its view would exceed max_bytes (the view's exact size, counted while
 // the bin grows, up to 48 bytes of alignment; a bin holds at least one source).
-// Graphs of at least kParallelBinRoots vertices are cut into `threads`
-// contiguous root ranges of about equal edge counts, planned in parallel (a bin
-// never spans two ranges).  bin_of[v] for every vertex; returns the number of bins.
+// Graphs of at least kParallelBinRoots vertices are cut into contiguous root
+// ranges of about equal edge counts, planned in parallel (a bin never spans two
+// ranges), as many as keep at least 8 bins per range (up to `threads`; one for
+// a graph of few bins).  bin_of[v] for every vertex; returns the number of bins.
 constexpr uint64_t kParallelBinRoots = 1u << 16;
 uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Shape &shape, uint64_t max_bytes,
                    uint32_t *bin_of, unsigned threads = 1);
