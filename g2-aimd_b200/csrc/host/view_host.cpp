@@ -27,6 +27,12 @@ inline uint64_t row_from(const uint64_t *rp, const uint32_t *ci, uint32_t x, uin
 }
 }  // namespace
 
+unsigned host_threads() {
+    unsigned t = std::thread::hardware_concurrency();
+    if (const char *e = getenv("G2_HOST_THREADS")) t = (unsigned)atoi(e);
+    return t ? t : 1u;
+}
+
 Layout::Layout(const Sizes &s) {
     fo = align16(8ull * (s.n + 1));
     ci = align16(fo + 4ull * s.n);
@@ -553,9 +559,7 @@ int g2_view_bins(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uin
     if (!row_ptrs || !bin_of || !nbins || (!cols && row_ptrs[n]) || n >= (1ull << 32) ||
         !shape_from(radius, row_radius, min_root_degree, flags, &sh))
         return G2_ERR_INVALID;
-    unsigned threads = std::thread::hardware_concurrency();
-    if (const char *e = getenv("G2_HOST_THREADS")) threads = (unsigned)atoi(e);
-    *nbins = g2view::plan_bins(row_ptrs, cols, n, sh, max_bytes, bin_of, threads ? threads : 1u);
+    *nbins = g2view::plan_bins(row_ptrs, cols, n, sh, max_bytes, bin_of, g2view::host_threads());
     return G2_OK;
 }
 
@@ -569,9 +573,7 @@ int g2_view_materialize(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t
     for (uint64_t i = 0; i < nsrc; i++)
         if (sources[i] >= n) return G2_ERR_INVALID;
     memset(out, 0, sizeof(*out));
-    unsigned threads = std::thread::hardware_concurrency();
-    if (const char *e = getenv("G2_HOST_THREADS")) threads = (unsigned)atoi(e);
-    g2view::Builder b(row_ptrs, cols, n, threads ? threads : 1u);
+    g2view::Builder b(row_ptrs, cols, n, g2view::host_threads());
     const g2view::Sizes s = b.plan(sources, nsrc, sh);
     auto *rp = static_cast<uint64_t *>(malloc(8 * (s.n + 1)));
     auto *fo = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.n, 1)));

@@ -23,6 +23,10 @@ namespace g2view {
 
 constexpr uint32_t kNone = 0xffffffffu;
 
+// Host threads the view code may use: G2_HOST_THREADS if set, else the
+// hardware's (at least 1).
+unsigned host_threads();
+
 struct Sizes {
     uint64_t n = 0;         // view vertices |B|
     uint64_t m = 0;         // view column entries

@@ -368,10 +368,11 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
         prod.nbins = nbins;
         prod.shape = shape;
         prod.device = ctx->device;
-        uint32_t np = vo && vo->producers ? vo->producers : std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
+        const unsigned cores = g2view::host_threads();
+        uint32_t np = vo && vo->producers ? vo->producers : std::min(8u, cores);
         np = std::min<uint32_t>(np, std::max<uint32_t>(nbins, 1u));
         // the host's threads are shared out: few bins get several threads each
-        prod.build_threads = std::max(1u, std::thread::hardware_concurrency() / np);
+        prod.build_threads = std::max(1u, cores / np);
         if (!rc && nbins) prod.start(np, np + 2);
         double wait_ms = 0;
         // next view with roots (bins that kept none count 0)

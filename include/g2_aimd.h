@@ -288,7 +288,9 @@ int g2_degeneracy_order_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core);
                                 allows upper balls and forward rows; G2_VIEW_EGO there asks
                                 for ego rows (radius-1 views only) */
 typedef struct g2_view_opts {
-    uint32_t producers;   /* host threads building views (0 = min(8, cores))    */
+    uint32_t producers;   /* host threads building views (0 = min(8, cores); the
+                             host's threads, or G2_HOST_THREADS, are shared out over
+                             the producers for large views)                      */
     uint32_t radius;      /* ball radius (0 = from the query: 1 for MCE)         */
     uint32_t row_radius;  /* rows kept up to this distance (0 = from the query)  */
     uint32_t flags;       /* G2_VIEW_NO_UPPER                                    */
