@@ -563,6 +563,63 @@ int g2_view_bins(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uin
     return G2_OK;
 }
 
+int g2_view_bins_rebalance(const uint64_t *row_ptrs, uint64_t n, uint32_t *bin_of, uint32_t nbins,
+                           uint32_t devices, uint32_t split_times, int reorder, uint32_t *out_nbins) {
+    if (!row_ptrs || !bin_of || !out_nbins || (split_times && !devices) || n >= (1ull << 32)) return G2_ERR_INVALID;
+    // bins as root lists; a bin's factor is the degree sum of its roots
+    // (ViewBin::GetComputationFactors, view/view_bin.h:27-39)
+    std::vector<std::vector<uint32_t>> bins(nbins);
+    for (uint64_t v = 0; v < n; v++) {
+        if (bin_of[v] == G2_VIEW_NO_BIN) continue;
+        if (bin_of[v] >= nbins) return G2_ERR_INVALID;
+        bins[bin_of[v]].push_back((uint32_t)v);
+    }
+    auto deg = [&](uint32_t v) { return row_ptrs[v + 1] - row_ptrs[v]; };
+    std::vector<uint64_t> factor(nbins, 0);
+    for (uint32_t b = 0; b < nbins; b++)
+        for (uint32_t v : bins[b]) factor[b] += deg(v);
+    if (split_times && nbins) {
+        // ViewBinManager::Split (view/view_bin_manager.h:95-175): until there are
+        // (nbins / devices + times) * devices bins, the bin furthest above the
+        // mean factor is cut in two, its roots dealt alternately in descending
+        // degree order (odd positions to the first half); halves go last
+        const uint64_t target = ((uint64_t)nbins / devices + split_times) * devices;
+        while (bins.size() < target) {
+            uint64_t sum = 0;
+            for (uint64_t f : factor) sum += f;
+            const uint64_t avg = sum / bins.size();
+            size_t pick = 0;
+            uint64_t best = 0;
+            for (size_t i = 0; i < bins.size(); i++)
+                if (factor[i] >= avg && factor[i] - avg > best) best = factor[i] - avg, pick = i;
+            std::vector<uint32_t> src = std::move(bins[pick]);
+            std::stable_sort(src.begin(), src.end(), [&](uint32_t a, uint32_t b) { return deg(a) > deg(b); });
+            std::vector<uint32_t> a, b;
+            uint64_t fa = 0, fb = 0;
+            for (size_t i = 0; i < src.size(); i++) {
+                if (i % 2) a.push_back(src[i]), fa += deg(src[i]);
+                else b.push_back(src[i]), fb += deg(src[i]);
+            }
+            bins.erase(bins.begin() + (ptrdiff_t)pick);
+            factor.erase(factor.begin() + (ptrdiff_t)pick);
+            bins.push_back(std::move(a));
+            factor.push_back(fa);
+            bins.push_back(std::move(b));
+            factor.push_back(fb);
+        }
+    }
+    // ViewBinManager::Reorder (view/view_bin_manager.h:176-184), also the end of
+    // Split: descending factor (ties keep their order)
+    std::vector<uint32_t> order(bins.size());
+    for (uint32_t i = 0; i < order.size(); i++) order[i] = i;
+    if (reorder || split_times)
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return factor[a] > factor[b]; });
+    for (uint32_t k = 0; k < order.size(); k++)
+        for (uint32_t v : bins[order[k]]) bin_of[v] = k;
+    *out_nbins = (uint32_t)bins.size();
+    return G2_OK;
+}
+
 int g2_view_materialize(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, const uint32_t *sources,
                         uint64_t nsrc, uint32_t radius, uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
                         g2_view *out) {

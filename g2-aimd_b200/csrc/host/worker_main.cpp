@@ -25,9 +25,10 @@
 // contains every adjacency list the bin's roots read, so the counts are the same.
 // With -ooc 1 the views are materialised as in the reference (a compact induced
 // ball per bin, system/worker.h:165-279), for graphs larger than device memory.  Bins go to GPUs
-// through an atomic counter instead of the MPMC queues.  -dr (reorder bins by
-// sum of degrees, largest first) and -ds/-dst (split) are honoured as orderings of the
-// bin list; they do not change results.
+// through an atomic counter instead of the MPMC queues.  -dr (bins by degree sum
+// of their roots, largest first) and -ds/-dst (heavy bins cut in two until each
+// consumer has -dst more) are applied as the reference applies them
+// (g2_view_bins_rebalance); they change the bins, not the totals.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -63,6 +64,8 @@ int main(int argc, char **argv) {
     const int consumers = std::max(1, atoi(opt(argc, argv, "-cn", "1")));
     const int sort_sources = atoi(opt(argc, argv, "-ss", "0"));
     const int reorder = atoi(opt(argc, argv, "-dr", "0"));
+    const int do_split = atoi(opt(argc, argv, "-ds", "0"));
+    const int split_times = atoi(opt(argc, argv, "-dst", "1"));
     const int ooc = atoi(opt(argc, argv, "-ooc", "0"));
     const int producers = std::max(1, atoi(opt(argc, argv, "-pn", "1")));
     const double mem_gb = atof(opt(argc, argv, "-m", "10"));
@@ -109,6 +112,13 @@ int main(int argc, char **argv) {
             if (rc) return die("view bins", rc);
             printf("view bins: %u (budget %.3f GB)\n", nbins, mem_gb);
         }
+    }
+    // -ds / -dst / -dr: the reference's split of heavy bins over the consumers
+    // and heaviest-first order (view/view_bin_manager.h:95-184)
+    if (do_split || reorder) {
+        rc = g2_view_bins_rebalance(rp, n, bins.data(), nbins, (uint32_t)consumers,
+                                    do_split ? (uint32_t)std::max(1, split_times) : 0u, reorder, &nbins);
+        if (rc) return die("bin split", rc);
     }
     if (ooc) {
         // consumer c runs bins c, c + cn, ...: its bin_of maps them to 0, 1, ...
@@ -168,14 +178,8 @@ int main(int argc, char **argv) {
     for (uint64_t v = 0; v < n; v++) sources[bins[v]].push_back((uint32_t)v);
     if (sort_sources)
         for (auto &s : sources) std::sort(s.begin(), s.end());
-    std::vector<uint32_t> order(nbins);
+    std::vector<uint32_t> order(nbins);  // bins are already numbered heaviest first under -dr / -ds
     for (uint32_t b = 0; b < nbins; b++) order[b] = b;
-    if (reorder) {
-        std::vector<uint64_t> f(nbins, 0);
-        for (uint32_t b = 0; b < nbins; b++)
-            for (uint32_t v : sources[b]) f[b] += rp[v + 1] - rp[v];
-        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return f[a] > f[b]; });
-    }
     std::atomic<uint32_t> next{0};
     std::atomic<int> failed{0};
     std::atomic<unsigned long long> total{0};

@@ -153,6 +153,15 @@ class Graph:
                                  C.byref(nb)), "g2_view_bins")
         return nb.value, bins
 
+    def rebalance_bins(self, bin_of, nbins, devices=1, split_times=0, reorder=False):
+        """(nbins, bin_of) after the reference's split / reorder of view bins
+        (g2_view_bins_rebalance)."""
+        bins = np.array(bin_of, dtype=np.uint32, copy=True)
+        nb = C.c_uint32()
+        check(lib().g2_view_bins_rebalance(_ptr(self.row_ptrs), self.n, _ptr(bins), nbins, devices, split_times,
+                                           int(bool(reorder)), C.byref(nb)), "g2_view_bins_rebalance")
+        return nb.value, bins
+
     # ----------------------------------------------------- degeneracy order
     def degeneracy_order(self):
         """(perm, core): perm[old] = new id (core shells ascending, degree

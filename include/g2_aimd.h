@@ -473,6 +473,16 @@ int g2_view_bins(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uin
                  uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
                  uint64_t max_bytes, uint32_t *bin_of, uint32_t *nbins);
 
+/* The reference's bin balancing for several devices (view/view_bin_manager.h:
+ * 95-184, flags -ds / -dst / -dr): with split_times > 0 the bin whose factor
+ * (degree sum of its roots) is furthest above the mean is cut in two until
+ * there are (nbins / devices + split_times) * devices bins, its roots dealt
+ * alternately in descending degree order; with split_times > 0 or reorder the
+ * bins are then numbered by descending factor.  bin_of (n entries,
+ * G2_VIEW_NO_BIN for non-roots) is rewritten; *out_nbins receives the count. */
+int g2_view_bins_rebalance(const uint64_t *row_ptrs, uint64_t n, uint32_t *bin_of, uint32_t nbins,
+                           uint32_t devices, uint32_t split_times, int reorder, uint32_t *out_nbins);
+
 /*
  * Degeneracy order (kmeans/kcore.cpp:103-191): k-core shells in increasing core
  * number, vertices of a shell by increasing degree (ties: lower old id), then

@@ -421,3 +421,42 @@ def test_parallel_bin_plan(g2, monkeypatch, upper, forward):
             src = np.flatnonzero(bins == b).astype(np.uint32)
             v, lsrc, _ = g.view(src, **kw)
             assert lsrc.size <= 1 or view_bytes(v, lsrc.size) <= budget + 48
+
+
+def py_rebalance(g, bin_of, nbins, devices, times, reorder):
+    """view/view_bin_manager.h:95-184 restated: Split (cut the bin furthest above
+    the mean factor, roots alternately by descending degree, halves appended)
+    then, as after Split or with Reorder, bins by descending factor."""
+    deg = np.diff(g.row_ptrs).astype(np.int64)
+    bins = [[v for v in range(g.n) if bin_of[v] == b] for b in range(nbins)]
+    fac = lambda b: int(sum(deg[v] for v in b))  # noqa: E731
+    if times:
+        target = (nbins // devices + times) * devices
+        while len(bins) < target:
+            avg = sum(fac(b) for b in bins) // len(bins)
+            pick, best = 0, 0
+            for i, b in enumerate(bins):
+                if fac(b) >= avg and fac(b) - avg > best:
+                    pick, best = i, fac(b) - avg
+            src = sorted(bins.pop(pick), key=lambda v: -deg[v])  # stable: ties by id
+            bins += [src[1::2], src[0::2]]
+    if times or reorder:
+        bins = sorted(bins, key=lambda b: -fac(b))  # stable
+    out = np.full(g.n, 0xFFFFFFFF, np.uint32)
+    for k, b in enumerate(bins):
+        out[b] = k
+    return len(bins), out
+
+
+@pytest.mark.parametrize("devices,times,reorder", [(1, 0, True), (4, 1, False), (3, 2, True), (8, 1, False)])
+def test_rebalance_bins_follows_the_reference(g2, devices, times, reorder):
+    g = g2.Graph.chung_lu(3000, 2.2, 10.0, seed=3).degeneracy_recoded()
+    nb, bins = g.view_bins(40 << 10, radius=1, row_radius=1, min_root_degree=1)
+    bins[::13] = 0xFFFFFFFF  # some vertices are no roots
+    got = g.rebalance_bins(bins, nb, devices, times, reorder)
+    want = py_rebalance(g, bins, nb, devices, times, reorder)
+    assert got[0] == want[0] and np.array_equal(got[1], want[1])
+    if times:
+        assert got[0] == (nb // devices + times) * devices
+    # the roots and their partition into bins are kept, only relabelled or cut
+    assert np.array_equal(got[1] == 0xFFFFFFFF, bins == 0xFFFFFFFF)
