@@ -134,3 +134,25 @@ def test_degeneracy_order_matches_reference_kcore(g2, tmp_path):
     assert np.array_equal(ref.degrees(), mine.degrees())
     nb, bins = g.read_vbmap(str(p) + ".2.hop.vbmap")
     assert nb == 1 and not bins.any()
+
+
+NULL_CTX_CALLS = {
+    "g2_close": (None,), "g2_load_csr": (None, None, None, 0, 0), "g2_load_csr_device": (None, None, None, 0, 0),
+    "g2_reserve": (None, 0), "g2_set_plan": (None, None), "g2_mce_run": (None, None, 0, None, None, None, 0),
+    "g2_match_run": (None, None, 0, None, None), "g2_mce_run_device": (None, None, 0, None, None, 0, None),
+    "g2_match_run_device": (None, None, 0, None, None, None), "g2_batch_load": (None, None, 0),
+    "g2_batch_mce": (None, None, None, None, 0), "g2_batch_match": (None, None, None),
+    "g2_degeneracy_order_device": (None, None, None), "g2_degeneracy_recode_device": (None, None, None),
+    "g2_copy_csr": (None, None, None), "g2_set_host_spill": (None, 0), "g2_last_spill_stats": (None, None, None),
+    "g2_last_work_bytes": (None, None), "g2_pass_time_ms": (None, 0, None), "g2_load_core": (None, None),
+    "g2_root_features": (None, None, 0, None), "g2_set_model": (None, None, None),
+    "g2_view_mce": (None, None, None, 0, None, 0, None, None, None, None, 0, None, None),
+    "g2_view_match": (None, None, None, 0, None, 0, None, None, None, None, None),
+}
+
+
+@pytest.mark.parametrize("name", sorted(NULL_CTX_CALLS))
+def test_entry_points_reject_a_null_context(g2, name):
+    """Every context call checks its arguments before touching a device:
+    G2_ERR_INVALID, no crash, no CUDA call (this runs without a GPU)."""
+    assert getattr(g2.lib(), name)(*NULL_CTX_CALLS[name]) == -1
