@@ -577,7 +577,7 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     base.pool_cap = spill ? kPoolBytes / 4 : 0;
     base.qctl = ctx->d_ctr + kCtrQueue;
     base.epoch_dev = spill ? ctx->d_epoch : nullptr;
-    base.wait_cycles = kWaitCycles;
+    base.wait_cycles = (o && o->wait_cycles) ? o->wait_cycles : kWaitCycles;
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
     L2Window l2(ctx, st, flags);
     {  // main pass: every task, WPL=1, one slab per resident warp; long walks
@@ -734,7 +734,7 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
         a.rec_cap = std::min<uint64_t>(kRecordBytes / (4ull * a.rec_stride), g2::kRecordBit - 1u);
         a.qctl = ctx->d_ctr + kCtrQueue;
         a.epoch_dev = ctx->d_epoch;
-        a.wait_cycles = kWaitCycles;
+        a.wait_cycles = (o && o->wait_cycles) ? o->wait_cycles : kWaitCycles;
         a.spill_cycles = 1000ull * ((o && o->spill_kcycles) ? o->spill_kcycles : kSpillKcycles);
     }
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));

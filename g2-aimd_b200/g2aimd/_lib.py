@@ -42,7 +42,7 @@ class G2Opts(C.Structure):
         ("split_granularity", u32), ("scores", P(C.c_float)),
         ("root_nodes", P(u64)), ("work_bytes", P(u64)),
         ("intersect_mode", u32), ("flags", u32), ("split_depth", u32), ("root_cost", P(u64)),
-        ("chunk", u32), ("spill_kcycles", u32), ("ctas_per_sm", u32), ("reserved2", u32),
+        ("chunk", u32), ("spill_kcycles", u32), ("ctas_per_sm", u32), ("wait_cycles", u32),
     ]
 
 

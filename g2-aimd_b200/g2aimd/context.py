@@ -85,8 +85,9 @@ class Plan:
 
 def _opts(warps_per_block=0, blocks=0, schedule="given", scores=None, root_nodes=None, intersect_mode=0,
           granularity=0, chunk=0, flags=0, work_bytes=None, root_cost=None, split=False, split_depth=0,
-          spill_kcycles=0, ctas_per_sm=0):
+          spill_kcycles=0, ctas_per_sm=0, wait_cycles=0):
     o = G2Opts()
+    o.wait_cycles = wait_cycles
     o.ctas_per_sm = ctas_per_sm
     o.split_depth = split_depth
     o.spill_kcycles = spill_kcycles

@@ -129,7 +129,10 @@ typedef struct g2_opts {
     uint32_t ctas_per_sm;       /* GMatch register budget, as CTAs of 256 threads per
                                    SM: 0 or 4 (64 registers), 6 (40 registers, more
                                    resident warps; pays on graphs larger than L2)   */
-    uint32_t reserved2;
+    uint32_t wait_cycles;       /* hang guard: the longest a warp waits for a handed-off
+                                   record, in SM cycles (0 = 2^37, about 70 s); a run
+                                   whose wait ran out returns G2_ERR_TIMEOUT and the
+                                   context stays usable                             */
 } g2_opts;
 
 /* g2_opts.flags */
