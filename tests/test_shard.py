@@ -179,3 +179,46 @@ def test_gloo_world2_view_bins(g2, orc):
         assert c == want["count"] and np.array_equal(np.array(h, np.uint64), want["hist"]), rank
         assert per == want_per, rank
         assert m == wm and sum(mper) == wm, rank
+
+
+def _lost_rank_main(rank, world, port, q):
+    import datetime
+    import time
+
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=4))
+    from g2aimd.shard import allreduce_counts
+    def report(msg):
+        q.put((rank, msg))
+        q.close()
+        q.join_thread()  # the message is out before the process ends
+
+    if rank == 1:
+        report("left")  # this rank leaves between steps: no collective in flight
+        os._exit(0)
+    t0 = time.time()
+    try:
+        allreduce_counts(5, np.zeros(3, np.uint64))
+        report("completed")
+    except Exception as e:  # the survivor learns of it from the collective's timeout
+        report(f"error after {time.time() - t0:.1f} s: {type(e).__name__}")
+    os._exit(0)
+
+
+def test_gloo_lost_rank_ends_in_an_error_not_a_hang():
+    """A rank that leaves before the final all-reduce: the other rank's
+    collective ends with an error within the process group's timeout."""
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_lost_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=90) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+    assert res[1] == "left"
+    assert res[0].startswith("error after"), res[0]
+    assert float(res[0].split()[2]) < 60
