@@ -466,6 +466,8 @@ uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Sha
                    uint32_t *bin_of, unsigned threads) {
     if (n == 0) return 0;
     unsigned T = n >= kParallelBinRoots ? std::max(1u, threads) : 1u;
+    // every range holds a byte per vertex of the whole graph: at most 8 GB in all
+    T = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(T, (8ull << 30) / n));
     if (T == 1) return plan_in_ranges(rp, ci, n, sh, max_bytes, bin_of, 1);
     // each range boundary adds at most one bin, so a first plan on T ranges
     // bounds the serial bin count from below; ranges are then sized to hold at

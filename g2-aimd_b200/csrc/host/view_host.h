@@ -104,8 +104,9 @@ class Builder {
 // the bin grows, up to 48 bytes of alignment; a bin holds at least one source).
 // Graphs of at least kParallelBinRoots vertices are cut into contiguous root
 // ranges of about equal edge counts, planned in parallel (a bin never spans two
-// ranges), as many as keep at least 8 bins per range (up to `threads`; one for
-// a graph of few bins).  bin_of[v] for every vertex; returns the number of bins.
+// ranges), as many as keep at least 8 bins per range (up to `threads` and to
+// 8 GB of per-range depth bytes, n each; one for a graph of few bins).  bin_of[v]
+// for every vertex; returns the number of bins.
 constexpr uint64_t kParallelBinRoots = 1u << 16;
 uint32_t plan_bins(const uint64_t *rp, const uint32_t *ci, uint64_t n, const Shape &shape, uint64_t max_bytes,
                    uint32_t *bin_of, unsigned threads = 1);

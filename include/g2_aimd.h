@@ -471,7 +471,8 @@ int g2_plan_view_radius(const g2_plan *plan, uint32_t *radius, uint32_t *row_rad
 /* Greedy bins over the roots 0..n-1 in id order: a bin closes when its view
  * would exceed max_bytes (its exact size, counted as the bin grows, up to 48
  * bytes of alignment; a bin holds at least one root).  bin_of: n entries (a
- * .vbmap body). */
+ * .vbmap body).  Host memory: a byte per vertex per planning thread (at most
+ * 8 GB); views cost each producer 4 bytes per vertex of the graph. */
 int g2_view_bins(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uint32_t radius,
                  uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
                  uint64_t max_bytes, uint32_t *bin_of, uint32_t *nbins);
