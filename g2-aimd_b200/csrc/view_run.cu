@@ -370,6 +370,9 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
         prod.device = ctx->device;
         const unsigned cores = g2view::host_threads();
         uint32_t np = vo && vo->producers ? vo->producers : std::min(8u, cores);
+        // by default at most 32 GB of builder marks (4 bytes and a bit per vertex each)
+        if (!(vo && vo->producers) && n)
+            np = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(np, (32ull << 30) / (4 * n + n / 8 + 1)));
         np = std::min<uint32_t>(np, std::max<uint32_t>(nbins, 1u));
         // the host's threads are shared out: few bins get several threads each
         prod.build_threads = std::max(1u, cores / np);

@@ -291,12 +291,14 @@ int g2_degeneracy_order_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core);
                                 allows upper balls and forward rows; G2_VIEW_EGO there asks
                                 for ego rows (radius-1 views only) */
 typedef struct g2_view_opts {
-    uint32_t producers;   /* host threads building views (0 = min(8, cores); the
-                             host's threads, or G2_HOST_THREADS, are shared out over
-                             the producers for large views)                      */
+    uint32_t producers;   /* host threads building views (0 = min(8, cores), fewer
+                             if their marks, 4 bytes and a bit per vertex each,
+                             would pass 32 GB); the host's threads, or
+                             G2_HOST_THREADS, are shared out over the producers
+                             for large views                                     */
     uint32_t radius;      /* ball radius (0 = from the query: 1 for MCE)         */
     uint32_t row_radius;  /* rows kept up to this distance (0 = from the query)  */
-    uint32_t flags;       /* G2_VIEW_NO_UPPER                                    */
+    uint32_t flags;       /* G2_VIEW_NO_UPPER, G2_VIEW_EGO                       */
 } g2_view_opts;
 typedef struct g2_view_stats {
     uint64_t bins;            /* views enumerated (bins with a root of enough degree) */
