@@ -8,6 +8,8 @@
 //   -h  <hop>         view-bin hop for BK (GMatch takes the plan's hop; must be unset)
 //   -cn <n>           consumers = GPUs 0..n-1
 //   -ss <0|1>         sort the sources of each bin
+//   -plan <0|1>       only plan view bins (-m GB each, -ds/-dr applied) and write
+//                     them to the .vbmap the other modes read; no GPU is used
 //   -ooc <0|1>        out of core: the CSR stays in host memory and each bin's view
 //                     is built by -pn host threads and uploaded (g2_view_mce /
 //                     g2_view_match); without a .vbmap, bins of at most -m GB
@@ -69,8 +71,9 @@ int main(int argc, char **argv) {
     const int ooc = atoi(opt(argc, argv, "-ooc", "0"));
     const int producers = std::max(1, atoi(opt(argc, argv, "-pn", "1")));
     const double mem_gb = atof(opt(argc, argv, "-m", "10"));
+    const int plan_only = atoi(opt(argc, argv, "-plan", "0"));
     if (data.empty()) {
-        fprintf(stderr, "usage: g2_worker -dg graph.bin [-q id] [-h hop] [-cn gpus] [-ss 0|1] [-ooc 0|1 -pn threads -m GB]\n");
+        fprintf(stderr, "usage: g2_worker -dg graph.bin [-q id] [-h hop] [-cn gpus] [-ss 0|1] [-ooc 0|1 -pn threads -m GB] [-plan 1]\n");
         return 2;
     }
     const bool bk = query == 1000;
@@ -98,19 +101,24 @@ int main(int argc, char **argv) {
     std::vector<uint32_t> bins(n, 0);
     uint32_t nbins = 1;
     const std::string vb = data + "." + std::to_string(hop) + ".hop.vbmap";
-    if (g2_read_vbmap(vb.c_str(), n, &nbins, bins.data()) != G2_OK) {
+    // bins of at most -m GB for the query's view shape (MCE: radius 1, full rows)
+    auto plan_bins = [&]() {
+        uint32_t radius = 1, row_radius = 1, root_degree = 1, flags = 0;
+        if (!bk) {
+            int r = g2_plan_view_radius(&plan, &radius, &row_radius, &root_degree, &flags);
+            if (r) return r;
+        }
+        int r = g2_view_bins(rp, ci, n, radius, row_radius, root_degree, flags, (uint64_t)(mem_gb * 1e9),
+                             bins.data(), &nbins);
+        if (!r) printf("view bins: %u (budget %.3f GB)\n", nbins, mem_gb);
+        return r;
+    };
+    if (plan_only || g2_read_vbmap(vb.c_str(), n, &nbins, bins.data()) != G2_OK) {
         nbins = 1;
         std::fill(bins.begin(), bins.end(), 0u);
-        if (ooc) {
-            uint32_t radius = 1, row_radius = 1, root_degree = 1, flags = 0;
-            if (!bk) {
-                rc = g2_plan_view_radius(&plan, &radius, &row_radius, &root_degree, &flags);
-                if (rc) return die("view shape", rc);
-            }
-            rc = g2_view_bins(rp, ci, n, radius, row_radius, root_degree, flags, (uint64_t)(mem_gb * 1e9),
-                              bins.data(), &nbins);
+        if (ooc || plan_only) {
+            rc = plan_bins();
             if (rc) return die("view bins", rc);
-            printf("view bins: %u (budget %.3f GB)\n", nbins, mem_gb);
         }
     }
     // -ds / -dst / -dr: the reference's split of heavy bins over the consumers
@@ -119,6 +127,16 @@ int main(int argc, char **argv) {
         rc = g2_view_bins_rebalance(rp, n, bins.data(), nbins, (uint32_t)consumers,
                                     do_split ? (uint32_t)std::max(1, split_times) : 0u, reorder, &nbins);
         if (rc) return die("bin split", rc);
+    }
+    if (plan_only) {
+        // the offline step of the reference's view_pack (kmeans/view_pack.cpp:
+        // 290-326): the bins go to the .vbmap that later runs read; no GPU is used
+        rc = g2_write_vbmap(vb.c_str(), nbins, bins.data(), n);
+        if (rc) return die(vb.c_str(), rc);
+        printf("wrote %s\n", vb.c_str());
+        g2_free(rp);
+        g2_free(ci);
+        return 0;
     }
     if (ooc) {
         // consumer c runs bins c, c + cn, ...: its bin_of maps them to 0, 1, ...

@@ -1,0 +1,39 @@
+"""g2_worker -plan 1 (no GPU): plans view bins for the query's view shape with
+the -m budget, applies -ds/-dst/-dr, and writes the .vbmap that later runs
+read, as the reference's offline view packing does."""
+import os
+import re
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+WORKER = os.path.join(ROOT, "g2-aimd_b200", "g2_worker")
+
+
+def run(*args):
+    out = subprocess.run([WORKER, *map(str, args)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    return out.stdout
+
+
+def test_plan_writes_the_bins_of_g2_view_bins(g2, tmp_path):
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(10, 8, seed=8).degeneracy_recoded()
+    path = tmp_path / "r10.bin"
+    g.write_bin(path)
+    # K4: the plan's hop names the file, the plan's view shape sizes the bins
+    out = run("-dg", path, "-q", 24, "-plan", 1, "-m", 0.00001)
+    nb = int(re.search(r"view bins: (\d+)", out).group(1))
+    hop = Plan.preset(24).raw.hop
+    vb = f"{path}.{hop}.hop.vbmap"
+    assert os.path.exists(vb) and f"wrote {vb}" in out
+    want_nb, want = g.view_bins(10000, **Plan.preset(24).view_shape())
+    got_nb, got = g.read_vbmap(vb)
+    assert nb == got_nb == want_nb > 1 and np.array_equal(got, want)
+    # maximal cliques (-h names the file), split over 4 consumers and reordered
+    out = run("-dg", path, "-h", 2, "-plan", 1, "-m", 0.0001, "-ds", 1, "-cn", 4, "-dr", 1)
+    nb0, b0 = g.view_bins(100000, radius=1, row_radius=1, min_root_degree=1)
+    want_nb, want = g.rebalance_bins(b0, nb0, devices=4, split_times=1, reorder=True)
+    got_nb, got = g.read_vbmap(f"{path}.2.hop.vbmap")
+    assert got_nb == want_nb == (nb0 // 4 + 1) * 4 and np.array_equal(got, want)
