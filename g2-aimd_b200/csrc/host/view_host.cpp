@@ -565,6 +565,22 @@ int g2_view_bins(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uin
     return G2_OK;
 }
 
+int g2_shell_bins(const uint32_t *core, uint64_t n, uint32_t nbins, uint32_t *bin_of) {
+    if (!core || !bin_of || !nbins) return G2_ERR_INVALID;
+    // kmeans/kcore.cpp:193-228 (writeBins): each core shell, a run of ids in
+    // degeneracy order, is dealt to the bins in consecutive chunks of
+    // window / nbins + 1 vertices (bin 0 first)
+    for (uint64_t i = 0; i < n;) {
+        uint64_t j = i;
+        while (j < n && core[j] == core[i]) j++;
+        if (j < n && core[j] < core[i]) return G2_ERR_INVALID;  // shells must ascend
+        const uint64_t share = (j - i) / nbins + 1;
+        for (uint64_t v = i; v < j; v++) bin_of[v] = (uint32_t)((v - i) / share);
+        i = j;
+    }
+    return G2_OK;
+}
+
 int g2_view_bins_rebalance(const uint64_t *row_ptrs, uint64_t n, uint32_t *bin_of, uint32_t nbins,
                            uint32_t devices, uint32_t split_times, int reorder, uint32_t *out_nbins) {
     if (!row_ptrs || !bin_of || !out_nbins || (split_times && !devices) || n >= (1ull << 32)) return G2_ERR_INVALID;

@@ -8,6 +8,9 @@
 //   -h  <hop>         view-bin hop for BK (GMatch takes the plan's hop; must be unset)
 //   -cn <n>           consumers = GPUs 0..n-1
 //   -ss <0|1>         sort the sources of each bin
+//   -recode 1 -o out.bin [-nb k]   the reference's kcore tool for a .bin input:
+//                     degeneracy order + recode to out.bin, k shell bins in
+//                     out.bin.2.hop.vbmap; no GPU is used
 //   -plan <0|1>       only plan view bins (-m GB each, -ds/-dr applied) and write
 //                     them to the .vbmap the other modes read; no GPU is used
 //   -ooc <0|1>        out of core: the CSR stays in host memory and each bin's view
@@ -72,9 +75,44 @@ int main(int argc, char **argv) {
     const int producers = std::max(1, atoi(opt(argc, argv, "-pn", "1")));
     const double mem_gb = atof(opt(argc, argv, "-m", "10"));
     const int plan_only = atoi(opt(argc, argv, "-plan", "0"));
+    const int recode = atoi(opt(argc, argv, "-recode", "0"));
+    const std::string out_bin = opt(argc, argv, "-o", "");
+    const uint32_t shell_bins = (uint32_t)std::max(1, atoi(opt(argc, argv, "-nb", "1")));
     if (data.empty()) {
         fprintf(stderr, "usage: g2_worker -dg graph.bin [-q id] [-h hop] [-cn gpus] [-ss 0|1] [-ooc 0|1 -pn threads -m GB] [-plan 1]\n");
         return 2;
+    }
+    if (recode) {
+        // the reference's kcore tool (kmeans/kcore.cpp:230-248) for a .bin input:
+        // degeneracy order + recode, the recoded .bin, and -nb shell bins in
+        // <out>.2.hop.vbmap; host only
+        if (out_bin.empty()) {
+            fprintf(stderr, "g2_worker: -recode 1 needs -o <out.bin>\n");
+            return 2;
+        }
+        uint64_t *rp = nullptr, n = 0, m = 0;
+        uint32_t *ci = nullptr;
+        int rc = g2_read_bin(data.c_str(), &rp, &ci, &n, &m);
+        if (rc) return die(data.c_str(), rc);
+        std::vector<uint32_t> perm(n), core(n), core_new(n), bins(n);
+        std::vector<uint64_t> rp2(n + 1);
+        std::vector<uint32_t> ci2(m);
+        rc = g2_degeneracy_order(rp, ci, n, perm.data(), core.data());
+        if (!rc) rc = g2_recode(rp, ci, n, perm.data(), rp2.data(), ci2.data());
+        if (rc) return die("degeneracy recode", rc);
+        for (uint64_t v = 0; v < n; v++) core_new[perm[v]] = core[v];
+        rc = g2_write_bin(out_bin.c_str(), rp2.data(), ci2.data(), n, m);
+        if (rc) return die(out_bin.c_str(), rc);
+        const std::string vbo = out_bin + ".2.hop.vbmap";
+        rc = g2_shell_bins(core_new.data(), n, shell_bins, bins.data());
+        if (!rc) rc = g2_write_vbmap(vbo.c_str(), shell_bins, bins.data(), n);
+        if (rc) return die(vbo.c_str(), rc);
+        printf("vertex_count=%llu, edge_count=%llu, degeneracy=%u\nwrote %s and %s\n", (unsigned long long)n,
+               (unsigned long long)m, n ? *std::max_element(core.begin(), core.end()) : 0u, out_bin.c_str(),
+               vbo.c_str());
+        g2_free(rp);
+        g2_free(ci);
+        return 0;
     }
     const bool bk = query == 1000;
     g2_plan plan;

@@ -113,6 +113,7 @@ def lib():
         "g2_plan_view_radius": (i32, [P(G2Plan), P(u32), P(u32), P(u32), P(u32)]),
         "g2_view_bins": (i32, [C.c_void_p, C.c_void_p, u64, u32, u32, u32, u32, u64, C.c_void_p, P(u32)]),
         "g2_view_bins_rebalance": (i32, [C.c_void_p, u64, C.c_void_p, u32, u32, u32, i32, P(u32)]),
+        "g2_shell_bins": (i32, [C.c_void_p, u64, u32, C.c_void_p]),
         "g2_load_core": (i32, [C.c_void_p, C.c_void_p]),
         "g2_root_features": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p]),
         "g2_model_train": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, u32, u32, C.c_float, u64, C.c_void_p,

@@ -479,6 +479,11 @@ int g2_view_bins(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uin
                  uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
                  uint64_t max_bytes, uint32_t *bin_of, uint32_t *nbins);
 
+/* The reference's kcore bins (kmeans/kcore.cpp:193-228): core[v] of a graph in
+ * degeneracy order (ascending, so every shell is a run of ids); each shell is
+ * dealt to the nbins bins in consecutive chunks of shell size / nbins + 1. */
+int g2_shell_bins(const uint32_t *core, uint64_t n, uint32_t nbins, uint32_t *bin_of);
+
 /* The reference's bin balancing for several devices (view/view_bin_manager.h:
  * 95-184, flags -ds / -dst / -dr): with split_times > 0 the bin whose factor
  * (degree sum of its roots) is furthest above the mean is cut in two until

@@ -37,3 +37,33 @@ def test_plan_writes_the_bins_of_g2_view_bins(g2, tmp_path):
     want_nb, want = g.rebalance_bins(b0, nb0, devices=4, split_times=1, reorder=True)
     got_nb, got = g.read_vbmap(f"{path}.2.hop.vbmap")
     assert got_nb == want_nb == (nb0 // 4 + 1) * 4 and np.array_equal(got, want)
+
+
+def py_shell_bins(core_new, nb):
+    """kmeans/kcore.cpp:193-228 restated: each core shell (a run of ids in
+    degeneracy order) in consecutive chunks of shell size // nb + 1 per bin."""
+    out = np.zeros(core_new.size, np.uint32)
+    i = 0
+    while i < core_new.size:
+        j = i
+        while j < core_new.size and core_new[j] == core_new[i]:
+            j += 1
+        share = (j - i) // nb + 1
+        out[i:j] = np.arange(j - i) // share
+        i = j
+    return out
+
+
+def test_recode_writes_the_kcore_files(g2, tmp_path):
+    g = g2.Graph.chung_lu(5000, 2.3, 8.0, seed=2)
+    src = tmp_path / "cl.bin"
+    dst = tmp_path / "cl_rec.bin"
+    g.write_bin(src)
+    out = run("-dg", src, "-recode", 1, "-o", dst, "-nb", 3)
+    assert f"wrote {dst}" in out
+    want = g.degeneracy_recoded()
+    got = g2.Graph.read_bin(dst)
+    assert np.array_equal(got.row_ptrs, want.row_ptrs) and np.array_equal(got.cols, want.cols)
+    nb, bins = got.read_vbmap(f"{dst}.2.hop.vbmap")
+    assert nb == 3 and np.array_equal(bins, py_shell_bins(want.core, 3))
+    assert bins.max() == 2
