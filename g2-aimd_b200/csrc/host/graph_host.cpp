@@ -177,6 +177,100 @@ int g2_read_bin(const char *path, uint64_t **row_ptrs, uint32_t **cols, uint64_t
     return G2_OK;
 }
 
+int g2_read_snap(const char *path, int preprocess, uint64_t **row_ptrs, uint32_t **cols, uint64_t *n,
+                 uint64_t *m) {
+    if (!path || !row_ptrs || !cols || !n || !m) return G2_ERR_INVALID;
+    // Graph::readSnapFile (common/graph.h:268-358): lines that start with a
+    // digit hold an edge "u v" (more columns ignored); ids are shifted by the
+    // smallest one; every edge is stored in both directions, rows sorted
+    FILE *f = fopen(path, "rb");
+    if (!f) return G2_ERR_IO;
+    std::vector<uint32_t> eu, ev;
+    uint64_t lo = UINT64_MAX, hi = 0;
+    char line[4096];
+    bool bad = false;
+    while (fgets(line, sizeof(line), f)) {
+        if (!(line[0] >= '0' && line[0] <= '9')) continue;
+        char *end = nullptr;
+        const unsigned long long a = strtoull(line, &end, 10);
+        char *end2 = nullptr;
+        const unsigned long long b = strtoull(end, &end2, 10);
+        if (end2 == end || a > UINT32_MAX || b > UINT32_MAX) {
+            bad = true;
+            break;
+        }
+        eu.push_back((uint32_t)a);
+        ev.push_back((uint32_t)b);
+        lo = std::min<uint64_t>(lo, std::min(a, b));
+        hi = std::max<uint64_t>(hi, std::max(a, b));
+    }
+    fclose(f);
+    if (bad) return G2_ERR_IO;
+    uint64_t nn = eu.empty() ? 0 : hi - lo + 1;
+    std::vector<uint64_t> rp(nn + 1, 0);
+    for (size_t i = 0; i < eu.size(); i++) {
+        rp[eu[i] - lo + 1]++;
+        rp[ev[i] - lo + 1]++;
+    }
+    for (uint64_t v = 0; v < nn; v++) rp[v + 1] += rp[v];
+    std::vector<uint32_t> ci(rp[nn]);
+    {
+        std::vector<uint64_t> pos(rp.begin(), rp.end() - 1);
+        for (size_t i = 0; i < eu.size(); i++) {
+            const uint32_t a = (uint32_t)(eu[i] - lo), b = (uint32_t)(ev[i] - lo);
+            ci[pos[a]++] = b;
+            ci[pos[b]++] = a;
+        }
+    }
+    std::vector<uint32_t>().swap(eu);
+    std::vector<uint32_t>().swap(ev);
+    parallel_for(nn, 4096, [&](uint64_t a, uint64_t b) {
+        for (uint64_t v = a; v < b; v++) std::sort(ci.begin() + rp[v], ci.begin() + rp[v + 1]);
+    });
+    if (preprocess) {
+        // Graph::Preprocess (common/graph.h:720-804): parallel edges and self
+        // loops go, then vertices left without neighbours, the others keeping
+        // their order
+        uint64_t w = 0;
+        std::vector<uint64_t> nrp(nn + 1, 0);
+        for (uint64_t u = 0; u < nn; u++) {
+            const uint64_t b = rp[u], e = rp[u + 1];
+            nrp[u] = w;
+            for (uint64_t j = b; j < e; j++) {
+                const uint32_t v = ci[j];
+                if ((j > b && v == ci[j - 1]) || v == u) continue;
+                ci[w++] = v;
+            }
+        }
+        nrp[nn] = w;
+        std::vector<uint32_t> id(nn, UINT32_MAX);
+        uint64_t k = 0;
+        for (uint64_t u = 0; u < nn; u++)
+            if (nrp[u + 1] > nrp[u]) id[u] = (uint32_t)k++;
+        rp.assign(k + 1, 0);
+        for (uint64_t u = 0; u < nn; u++)
+            if (id[u] != UINT32_MAX) rp[id[u]] = nrp[u];
+        rp[k] = w;
+        for (uint64_t j = 0; j < w; j++) ci[j] = id[ci[j]];
+        ci.resize(w);
+        nn = k;
+    }
+    uint64_t *orp = (uint64_t *)malloc(sizeof(uint64_t) * (nn + 1));
+    uint32_t *oci = (uint32_t *)malloc(sizeof(uint32_t) * (ci.size() ? ci.size() : 1));
+    if (!orp || !oci) {
+        free(orp);
+        free(oci);
+        return G2_ERR_OOM;
+    }
+    memcpy(orp, rp.data(), sizeof(uint64_t) * (nn + 1));
+    if (!ci.empty()) memcpy(oci, ci.data(), sizeof(uint32_t) * ci.size());
+    *row_ptrs = orp;
+    *cols = oci;
+    *n = nn;
+    *m = ci.size();
+    return G2_OK;
+}
+
 int g2_write_bin(const char *path, const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n, uint64_t m) {
     if (!path || !row_ptrs || (!cols && m)) return G2_ERR_INVALID;
     FILE *f = fopen(path, "wb");

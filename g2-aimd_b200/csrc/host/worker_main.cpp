@@ -8,6 +8,9 @@
 //   -h  <hop>         view-bin hop for BK (GMatch takes the plan's hop; must be unset)
 //   -cn <n>           consumers = GPUs 0..n-1
 //   -ss <0|1>         sort the sources of each bin
+//   -prep 1 [-o out.bin]  the reference's preprocess tool: the graph (a SNAP .txt
+//                     edge list, deduplicated, no self loops or isolated
+//                     vertices) written as <prefix>.bin; any mode reads .txt so
 //   -recode 1 -o out.bin [-nb k]   the reference's kcore tool for a .bin input:
 //                     degeneracy order + recode to out.bin, k shell bins in
 //                     out.bin.2.hop.vbmap; no GPU is used
@@ -76,11 +79,33 @@ int main(int argc, char **argv) {
     const double mem_gb = atof(opt(argc, argv, "-m", "10"));
     const int plan_only = atoi(opt(argc, argv, "-plan", "0"));
     const int recode = atoi(opt(argc, argv, "-recode", "0"));
+    const int prep = atoi(opt(argc, argv, "-prep", "0"));
     const std::string out_bin = opt(argc, argv, "-o", "");
     const uint32_t shell_bins = (uint32_t)std::max(1, atoi(opt(argc, argv, "-nb", "1")));
     if (data.empty()) {
         fprintf(stderr, "usage: g2_worker -dg graph.bin [-q id] [-h hop] [-cn gpus] [-ss 0|1] [-ooc 0|1 -pn threads -m GB] [-plan 1]\n");
         return 2;
+    }
+    // a .txt graph is a SNAP edge list, read and preprocessed as the reference's
+    // preprocess tool does (kmeans/preprocess.cpp); every other name is a .bin
+    const bool snap = data.size() > 4 && data.compare(data.size() - 4, 4, ".txt") == 0;
+    auto read_graph = [&](uint64_t **rp, uint32_t **ci, uint64_t *n, uint64_t *m) {
+        return snap ? g2_read_snap(data.c_str(), 1, rp, ci, n, m) : g2_read_bin(data.c_str(), rp, ci, n, m);
+    };
+    if (prep) {
+        // kmeans/preprocess.cpp: the preprocessed graph as <prefix>.bin (or -o)
+        uint64_t *rp = nullptr, n = 0, m = 0;
+        uint32_t *ci = nullptr;
+        int rc = read_graph(&rp, &ci, &n, &m);
+        if (rc) return die(data.c_str(), rc);
+        const std::string out = out_bin.empty() ? data.substr(0, data.rfind('.')) + ".bin" : out_bin;
+        rc = g2_write_bin(out.c_str(), rp, ci, n, m);
+        if (rc) return die(out.c_str(), rc);
+        printf("vertex_count=%llu, edge_count=%llu\nwrote %s\n", (unsigned long long)n, (unsigned long long)m,
+               out.c_str());
+        g2_free(rp);
+        g2_free(ci);
+        return 0;
     }
     if (recode) {
         // the reference's kcore tool (kmeans/kcore.cpp:230-248) for a .bin input:
@@ -92,7 +117,7 @@ int main(int argc, char **argv) {
         }
         uint64_t *rp = nullptr, n = 0, m = 0;
         uint32_t *ci = nullptr;
-        int rc = g2_read_bin(data.c_str(), &rp, &ci, &n, &m);
+        int rc = read_graph(&rp, &ci, &n, &m);
         if (rc) return die(data.c_str(), rc);
         std::vector<uint32_t> perm(n), core(n), core_new(n), bins(n);
         std::vector<uint64_t> rp2(n + 1);
@@ -132,7 +157,7 @@ int main(int argc, char **argv) {
     uint64_t *rp = nullptr, n = 0, m = 0;
     uint32_t *ci = nullptr;
     auto t0 = std::chrono::steady_clock::now();
-    int rc = g2_read_bin(data.c_str(), &rp, &ci, &n, &m);
+    int rc = read_graph(&rp, &ci, &n, &m);
     if (rc) return die(data.c_str(), rc);
     printf("vertex_count=%llu, edge_count=%llu\n", (unsigned long long)n, (unsigned long long)m);
     // view bins

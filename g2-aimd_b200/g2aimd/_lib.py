@@ -128,6 +128,7 @@ def lib():
         "g2_read_bin": (i32, [C.c_char_p, P(C.c_void_p), P(C.c_void_p), P(u64), P(u64)]),
         "g2_write_bin": (i32, [C.c_char_p, C.c_void_p, C.c_void_p, u64, u64]),
         "g2_free": (None, [C.c_void_p]),
+        "g2_read_snap": (i32, [C.c_char_p, i32, P(C.c_void_p), P(C.c_void_p), P(u64), P(u64)]),
         "g2_write_vbmap": (i32, [C.c_char_p, u32, C.c_void_p, u64]),
         "g2_read_vbmap": (i32, [C.c_char_p, u64, P(u32), C.c_void_p]),
         "g2_degeneracy_order": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p, C.c_void_p]),

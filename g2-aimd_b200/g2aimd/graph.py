@@ -94,6 +94,15 @@ class Graph:
               f"read {path}")
         return Graph(*_take(rp, ci, nn.value, mm.value), name=str(path))
 
+    @staticmethod
+    def read_snap(path, preprocess=True):
+        """SNAP text edge list (g2_read_snap); preprocess as the reference's
+        Graph::Preprocess (dedupe, no self loops, isolated vertices dropped)."""
+        rp, ci, nn, mm = C.c_void_p(), C.c_void_p(), C.c_uint64(), C.c_uint64()
+        check(lib().g2_read_snap(str(path).encode(), int(bool(preprocess)), C.byref(rp), C.byref(ci),
+                                 C.byref(nn), C.byref(mm)), f"read {path}")
+        return Graph(*_take(rp, ci, nn.value, mm.value), name=str(path))
+
     def write_bin(self, path):
         check(lib().g2_write_bin(str(path).encode(), _ptr(self.row_ptrs), _ptr(self.cols), self.n, self.m),
               f"write {path}")

@@ -423,6 +423,14 @@ int g2_read_bin(const char *path, uint64_t **row_ptrs, uint32_t **cols,
 int g2_write_bin(const char *path, const uint64_t *row_ptrs,
                  const uint32_t *cols, uint64_t n, uint64_t m);
 void g2_free(void *p);
+/* SNAP text edge list (Graph::readSnapFile, common/graph.h:268-358): lines that
+ * start with a digit hold an edge "u v"; ids are shifted by the smallest; rows
+ * symmetric and sorted.  preprocess != 0 applies Graph::Preprocess
+ * (common/graph.h:720-804): parallel edges and self loops removed, then vertices
+ * without neighbours, the rest renumbered in order; the enumeration needs this
+ * form.  Arrays malloc'd (g2_free). */
+int g2_read_snap(const char *path, int preprocess, uint64_t **row_ptrs, uint32_t **cols,
+                 uint64_t *n, uint64_t *m);
 
 /* .vbmap view-bin partition (view/view_bin_manager.h:34-94): "nbins b0 b1 ...".
  * Writes `n` bin ids; all-zero when nbins == 1. */

@@ -6,6 +6,7 @@ import re
 import subprocess
 
 import numpy as np
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 WORKER = os.path.join(ROOT, "g2-aimd_b200", "g2_worker")
@@ -67,3 +68,69 @@ def test_recode_writes_the_kcore_files(g2, tmp_path):
     nb, bins = got.read_vbmap(f"{dst}.2.hop.vbmap")
     assert nb == 3 and np.array_equal(bins, py_shell_bins(want.core, 3))
     assert bins.max() == 2
+
+
+SNAP = """# Directed graph (each unordered pair of nodes is saved once)
+# FromNodeId\tToNodeId
+5\t6
+6\t7
+7\t5
+5\t6
+9\t9
+9\t10\textra column
+12\t5
+
+10\t11
+"""
+
+
+def py_snap(text, preprocess):
+    """common/graph.h:268-358 and :720-804 restated."""
+    edges = [tuple(int(x) for x in line.split()[:2]) for line in text.splitlines() if line[:1].isdigit()]
+    lo = min(min(e) for e in edges)
+    n = max(max(e) for e in edges) - lo + 1
+    rows = [[] for _ in range(n)]
+    for a, b in edges:
+        rows[a - lo].append(b - lo)
+        rows[b - lo].append(a - lo)
+    rows = [sorted(r) for r in rows]
+    if preprocess:
+        rows = [sorted(set(v for v in r if v != u)) for u, r in enumerate(rows)]
+        keep = [u for u in range(n) if rows[u]]
+        new = {u: i for i, u in enumerate(keep)}
+        rows = [[new[v] for v in rows[u]] for u in keep]
+    rp = np.cumsum([0] + [len(r) for r in rows]).astype(np.uint64)
+    ci = np.array([v for r in rows for v in r], np.uint32)
+    return rp, ci
+
+
+def test_read_snap_follows_the_reference(g2, tmp_path):
+    path = tmp_path / "toy.txt"
+    path.write_text(SNAP)
+    for pre in (False, True):
+        g = g2.Graph.read_snap(path, preprocess=pre)
+        rp, ci = py_snap(SNAP, pre)
+        assert np.array_equal(g.row_ptrs, rp) and np.array_equal(g.cols, ci), pre
+    g = g2.Graph.read_snap(path)
+    assert g.n == 7 and g.m == 12  # 8 never appears; 9-9 and the repeat of 5-6 are gone
+
+
+def test_worker_prep_and_recode_read_snap_text(g2, tmp_path):
+    path = tmp_path / "toy.txt"
+    path.write_text(SNAP)
+    out = run("-dg", path, "-prep", 1)
+    assert f"wrote {tmp_path / 'toy.bin'}" in out
+    got = g2.Graph.read_bin(tmp_path / "toy.bin")
+    want = g2.Graph.read_snap(path)
+    assert np.array_equal(got.row_ptrs, want.row_ptrs) and np.array_equal(got.cols, want.cols)
+    run("-dg", path, "-recode", 1, "-o", tmp_path / "toy_rec.bin")
+    rec = g2.Graph.read_bin(tmp_path / "toy_rec.bin")
+    want = want.degeneracy_recoded()
+    assert np.array_equal(rec.row_ptrs, want.row_ptrs) and np.array_equal(rec.cols, want.cols)
+
+
+def test_read_snap_rejects_ids_beyond_32_bits(g2, tmp_path):
+    path = tmp_path / "big.txt"
+    path.write_text("1 4294967296\n")
+    with pytest.raises(Exception):
+        g2.Graph.read_snap(path)
