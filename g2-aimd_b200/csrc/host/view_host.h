@@ -10,8 +10,9 @@
 // scanned).  With `upper` (queries whose conditions put every matched vertex
 // above the root's image) the ball of source s is walked through vertices
 // larger than s only, and with `forward` (queries that order every position
-// above all earlier ones) rows keep only their entries above their own vertex.
-// Replaces the materialisation of view/view_bin.h:61-159,
+// above all earlier ones) rows keep only their entries above their own vertex;
+// with `ego` (radius 1) a row keeps only the entries (u, y) for which some
+// source s has u and y in N[s].  Replaces the materialisation of view/view_bin.h:61-159,
 // which keeps global ids and copies the full rows of the vertices within hop-1
 // of the sources.
 #pragma once
