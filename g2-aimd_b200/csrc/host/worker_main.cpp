@@ -21,7 +21,9 @@
 //                     g2_view_match); without a .vbmap, bins of at most -m GB
 //                     (default 10, the reference's view-bin budget) come from
 //                     g2_view_bins
-//   -m, -t, -qs, -pn, -dr, -ds, -dst  accepted for compatibility (see below)
+//   -t <threads>      host threads for view building and bin planning
+//                     (G2_HOST_THREADS); default: all
+//   -m, -qs, -pn, -dr, -ds, -dst  see below
 // Bins come from "<graph.bin>.<hop>.hop.vbmap" (view/view_bin_manager.h:34-94); a
 // missing file means one bin holding every vertex.  BK prints one
 // "Total No. of Cliques: N" line per bin (app_BK/BK.h:72-76), GMatch one final
@@ -80,6 +82,8 @@ int main(int argc, char **argv) {
     const int plan_only = atoi(opt(argc, argv, "-plan", "0"));
     const int recode = atoi(opt(argc, argv, "-recode", "0"));
     const int prep = atoi(opt(argc, argv, "-prep", "0"));
+    // -t: threads that build views (the reference's ViewBin thread_num) and plan bins
+    if (const char *t = opt(argc, argv, "-t", nullptr)) setenv("G2_HOST_THREADS", t, 1);
     const std::string out_bin = opt(argc, argv, "-o", "");
     const uint32_t shell_bins = (uint32_t)std::max(1, atoi(opt(argc, argv, "-nb", "1")));
     if (data.empty()) {

@@ -134,3 +134,17 @@ def test_read_snap_rejects_ids_beyond_32_bits(g2, tmp_path):
     path.write_text("1 4294967296\n")
     with pytest.raises(Exception):
         g2.Graph.read_snap(path)
+
+
+def test_plan_threads_flag(g2, tmp_path, monkeypatch):
+    """-t sets the planning threads: with -t 1 a large graph is planned in one
+    range, as g2_view_bins plans it on one thread."""
+    g = g2.Graph.chung_lu(1 << 17, 2.3, 10.0, seed=6).degeneracy_recoded()
+    path = tmp_path / "cl17.bin"
+    g.write_bin(path)
+    budget_gb = (g.row_ptrs.nbytes + g.cols.nbytes) / 40 / 1e9
+    run("-dg", path, "-h", 2, "-plan", 1, "-m", budget_gb, "-t", 1)
+    monkeypatch.setenv("G2_HOST_THREADS", "1")
+    want_nb, want = g.view_bins(int(budget_gb * 1e9), radius=1, row_radius=1, min_root_degree=1)
+    got_nb, got = g.read_vbmap(f"{path}.2.hop.vbmap")
+    assert got_nb == want_nb and np.array_equal(got, want)
