@@ -1,0 +1,28 @@
+"""Race detection for the host's threaded view code: tests/tsan_views.cpp is
+built with ThreadSanitizer together with csrc/host/view_host.cpp and run over
+every threaded path (row passes, radius-1 walk, ego filter, bin planning on
+several threads); any report fails the test."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_threaded_view_code_is_race_free(tmp_path):
+    exe = tmp_path / "tsan_views"
+    build = subprocess.run(
+        ["g++", "-O1", "-g", "-std=c++17", "-fsanitize=thread", "-pthread", "-I", os.path.join(ROOT, "include"),
+         "-I", os.path.join(ROOT, "g2-aimd_b200", "csrc"), os.path.join(HERE, "tsan_views.cpp"),
+         os.path.join(ROOT, "g2-aimd_b200", "csrc", "host", "view_host.cpp"), "-o", str(exe)],
+        capture_output=True, text=True, timeout=600)
+    assert build.returncode == 0, build.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ, TSAN_OPTIONS="halt_on_error=1 exitcode=66"))
+    assert run.returncode == 0, run.stderr[-4000:]
+    assert "ThreadSanitizer" not in run.stderr
+    assert run.stdout.count("mode") == 4
