@@ -26,3 +26,22 @@ def test_threaded_view_code_is_race_free(tmp_path):
     assert run.returncode == 0, run.stderr[-4000:]
     assert "ThreadSanitizer" not in run.stderr
     assert run.stdout.count("mode") == 4
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_view_code_is_memory_safe(tmp_path):
+    """The same paths under AddressSanitizer and UndefinedBehaviorSanitizer: no
+    out-of-bounds access, leak or undefined behaviour in building views and bins
+    (the views go to the GPU as they are)."""
+    exe = tmp_path / "asan_views"
+    build = subprocess.run(
+        ["g++", "-O1", "-g", "-std=c++17", "-fsanitize=address,undefined", "-fno-sanitize-recover=all",
+         "-pthread", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "g2-aimd_b200", "csrc"),
+         os.path.join(HERE, "tsan_views.cpp"), os.path.join(ROOT, "g2-aimd_b200", "csrc", "host", "view_host.cpp"),
+         "-o", str(exe)],
+        capture_output=True, text=True, timeout=600)
+    assert build.returncode == 0, build.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1"))
+    assert run.returncode == 0, run.stderr[-4000:]
+    assert run.stdout.count("mode") == 4

@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <random>
 #include <vector>
+#include "g2_aimd.h"
 #include "host/view_host.h"
 int main() {
     // a random power-law-ish symmetric graph, n = 70000 (threaded bin plans need 2^16)
@@ -35,5 +36,23 @@ int main() {
         uint32_t nb = g2view::plan_bins(rp.data(), ci.data(), n, sh, (8 * (n + 1) + 4 * ci.size()) / 30, bins.data(), 6);
         printf("mode %d view n %llu m %llu bins %u\n", mode, (unsigned long long)s.n, (unsigned long long)s.m, nb);
     }
+    // the C entry points: views of radius 2 (serial upper walk), bin split and
+    // reorder, shell bins
+    std::vector<uint32_t> some(src.begin(), src.begin() + 5000);
+    for (uint32_t flags : {0u, (uint32_t)G2_VIEW_UPPER}) {
+        g2_view v;
+        if (g2_view_materialize(rp.data(), ci.data(), n, some.data(), some.size(), 2, 1, 2, flags, &v) != G2_OK)
+            return 1;
+        printf("radius-2 view n %llu m %llu\n", (unsigned long long)v.n, (unsigned long long)v.m);
+        g2_view_free(&v);
+    }
+    std::vector<uint32_t> bins(n);
+    uint32_t nb = 0;
+    if (g2_view_bins(rp.data(), ci.data(), n, 1, 1, 1, 0, 200000, bins.data(), &nb) != G2_OK) return 1;
+    if (g2_view_bins_rebalance(rp.data(), n, bins.data(), nb, 4, 2, 1, &nb) != G2_OK) return 1;
+    std::vector<uint32_t> core(n);
+    for (uint32_t v = 0; v < n; v++) core[v] = v / 1000;  // ascending shells
+    if (g2_shell_bins(core.data(), n, 3, bins.data()) != G2_OK) return 1;
+    printf("rebalanced bins %u\n", nb);
     return 0;
 }
