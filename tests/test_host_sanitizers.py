@@ -1,4 +1,6 @@
-"""Race detection for the host's threaded view code: tests/tsan_views.cpp is
+"""Sanitizer builds of the host code: race detection for the threaded view code
+(ThreadSanitizer), memory and undefined-behaviour checks (ASan + UBSan) for it
+and for the graph and planner code.  Race detection: tests/tsan_views.cpp is
 built with ThreadSanitizer together with csrc/host/view_host.cpp and run over
 every threaded path (row passes, radius-1 walk, ego filter, bin planning on
 several threads); any report fails the test."""
@@ -45,3 +47,22 @@ def test_view_code_is_memory_safe(tmp_path):
                          env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1"))
     assert run.returncode == 0, run.stderr[-4000:]
     assert run.stdout.count("mode") == 4
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_graph_and_plan_host_code_is_memory_safe(tmp_path):
+    """Generators, .bin / .vbmap / SNAP I/O, degeneracy order and recode and the
+    planner under AddressSanitizer + UBSan (tests/sanitize_host.cpp)."""
+    exe = tmp_path / "asan_host"
+    host = os.path.join(ROOT, "g2-aimd_b200", "csrc", "host")
+    build = subprocess.run(
+        ["g++", "-O1", "-g", "-std=c++17", "-fsanitize=address,undefined", "-fno-sanitize-recover=all",
+         "-pthread", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "g2-aimd_b200", "csrc"),
+         os.path.join(HERE, "sanitize_host.cpp"), os.path.join(host, "graph_host.cpp"),
+         os.path.join(host, "plan_host.cpp"), "-o", str(exe)],
+        capture_output=True, text=True, timeout=600)
+    assert build.returncode == 0, build.stderr
+    run = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1"))
+    assert run.returncode == 0, run.stderr[-4000:]
+    assert "host ok" in run.stdout and "24 presets" in run.stdout, run.stdout

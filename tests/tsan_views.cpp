@@ -1,7 +1,7 @@
 // tsan_views.cpp - drives the threaded paths of the view builder and the bin
 // planner (parallel row passes, the atomic radius-1 walk, the ego filter,
 // range-parallel plans) so that a ThreadSanitizer build can check them for
-// data races (tests/test_host_tsan.py compiles and runs it).
+// data races (tests/test_host_sanitizers.py compiles and runs it).
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
