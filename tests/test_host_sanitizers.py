@@ -66,3 +66,21 @@ def test_graph_and_plan_host_code_is_memory_safe(tmp_path):
                          env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1"))
     assert run.returncode == 0, run.stderr[-4000:]
     assert "host ok" in run.stdout and "24 presets" in run.stdout, run.stdout
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_graph_host_threads_are_race_free(tmp_path):
+    """The generators and the SNAP reader fan out over host threads: the same
+    driver under ThreadSanitizer."""
+    exe = tmp_path / "tsan_host"
+    host = os.path.join(ROOT, "g2-aimd_b200", "csrc", "host")
+    build = subprocess.run(
+        ["g++", "-O1", "-g", "-std=c++17", "-fsanitize=thread", "-pthread", "-I", os.path.join(ROOT, "include"),
+         "-I", os.path.join(ROOT, "g2-aimd_b200", "csrc"), os.path.join(HERE, "sanitize_host.cpp"),
+         os.path.join(host, "graph_host.cpp"), os.path.join(host, "plan_host.cpp"), "-o", str(exe)],
+        capture_output=True, text=True, timeout=600)
+    assert build.returncode == 0, build.stderr
+    run = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ, TSAN_OPTIONS="halt_on_error=1 exitcode=66", G2_HOST_THREADS="6"))
+    assert run.returncode == 0, run.stderr[-4000:]
+    assert "ThreadSanitizer" not in run.stderr and "host ok" in run.stdout
