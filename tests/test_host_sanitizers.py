@@ -84,3 +84,27 @@ def test_graph_host_threads_are_race_free(tmp_path):
                          env=dict(os.environ, TSAN_OPTIONS="halt_on_error=1 exitcode=66", G2_HOST_THREADS="6"))
     assert run.returncode == 0, run.stderr[-4000:]
     assert "ThreadSanitizer" not in run.stderr and "host ok" in run.stdout
+
+
+@pytest.mark.skipif(shutil.which("g++") is None or shutil.which("gcc") is None, reason="needs gcc and g++")
+def test_oracle_is_memory_safe(tmp_path):
+    """The CPU oracle, the checker every parity test relies on, under
+    AddressSanitizer + UBSan on all of its entry points (tests/sanitize_oracle.cpp;
+    OpenMP threads included, so no ThreadSanitizer run here)."""
+    san = ["-fsanitize=address,undefined", "-fno-sanitize-recover=all", "-fopenmp", "-g", "-O1"]
+    obj = tmp_path / "oracle.o"
+    cc = subprocess.run(["gcc", *san, "-std=c11", "-c", os.path.join(ROOT, "oracle", "g2_oracle.c"), "-o", str(obj)],
+                        capture_output=True, text=True, timeout=600)
+    assert cc.returncode == 0, cc.stderr
+    exe = tmp_path / "asan_oracle"
+    host = os.path.join(ROOT, "g2-aimd_b200", "csrc", "host")
+    build = subprocess.run(
+        ["g++", *san, "-std=c++17", "-pthread", "-I", os.path.join(ROOT, "include"),
+         os.path.join(HERE, "sanitize_oracle.cpp"), str(obj), os.path.join(host, "graph_host.cpp"),
+         os.path.join(host, "plan_host.cpp"), "-o", str(exe)],
+        capture_output=True, text=True, timeout=600)
+    assert build.returncode == 0, build.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1"))
+    assert run.returncode == 0, run.stderr[-4000:]
+    assert "oracle ok" in run.stdout, run.stdout
