@@ -1,9 +1,10 @@
-"""Sanitizer builds of the host code: race detection for the threaded view code
-(ThreadSanitizer), memory and undefined-behaviour checks (ASan + UBSan) for it
-and for the graph and planner code.  Race detection: tests/tsan_views.cpp is
-built with ThreadSanitizer together with csrc/host/view_host.cpp and run over
-every threaded path (row passes, radius-1 walk, ego filter, bin planning on
-several threads); any report fails the test."""
+"""Sanitizer builds of the host code: race detection (ThreadSanitizer) and
+memory / undefined-behaviour checks (AddressSanitizer + UBSan).  Drivers in
+this directory call every host entry point on graphs large enough for the
+threaded paths; any sanitizer report fails the test.
+  tests/tsan_views.cpp      view builder, bin planner, view C entry points
+  tests/sanitize_host.cpp   generators, .bin / .vbmap / SNAP I/O, order, recode, planner
+  tests/sanitize_oracle.cpp the CPU oracle (the checker of every parity test)"""
 import os
 import shutil
 import subprocess
@@ -12,99 +13,67 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
+HOST = os.path.join(ROOT, "g2-aimd_b200", "csrc", "host")
+TSAN = ["-fsanitize=thread"]
+ASAN = ["-fsanitize=address,undefined", "-fno-sanitize-recover=all"]
+
+pytestmark = pytest.mark.skipif(shutil.which("g++") is None or shutil.which("gcc") is None,
+                                reason="needs gcc and g++")
 
 
-@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def build(exe, sources, san, extra=()):
+    cmd = ["g++", "-O1", "-g", "-std=c++17", "-pthread", *san, *extra, "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(ROOT, "g2-aimd_b200", "csrc"), *sources, "-o", str(exe)]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+
+
+def run(exe, args=(), **env):
+    env = dict(os.environ, TSAN_OPTIONS="halt_on_error=1 exitcode=66", ASAN_OPTIONS="detect_leaks=1", **env)
+    out = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=600, env=env)
+    assert out.returncode == 0, out.stderr[-4000:]
+    assert "Sanitizer" not in out.stderr, out.stderr[-4000:]
+    return out.stdout
+
+
+VIEWS = [os.path.join(HERE, "tsan_views.cpp"), os.path.join(HOST, "view_host.cpp")]
+GRAPH = [os.path.join(HERE, "sanitize_host.cpp"), os.path.join(HOST, "graph_host.cpp"),
+         os.path.join(HOST, "plan_host.cpp")]
+
+
 def test_threaded_view_code_is_race_free(tmp_path):
-    exe = tmp_path / "tsan_views"
-    build = subprocess.run(
-        ["g++", "-O1", "-g", "-std=c++17", "-fsanitize=thread", "-pthread", "-I", os.path.join(ROOT, "include"),
-         "-I", os.path.join(ROOT, "g2-aimd_b200", "csrc"), os.path.join(HERE, "tsan_views.cpp"),
-         os.path.join(ROOT, "g2-aimd_b200", "csrc", "host", "view_host.cpp"), "-o", str(exe)],
-        capture_output=True, text=True, timeout=600)
-    assert build.returncode == 0, build.stderr
-    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600,
-                         env=dict(os.environ, TSAN_OPTIONS="halt_on_error=1 exitcode=66"))
-    assert run.returncode == 0, run.stderr[-4000:]
-    assert "ThreadSanitizer" not in run.stderr
-    assert run.stdout.count("mode") == 4
+    """Row passes, the atomic radius-1 walk, the ego filter and range-parallel
+    bin plans on several threads."""
+    build(tmp_path / "t", VIEWS, TSAN)
+    assert run(tmp_path / "t").count("mode") == 4
 
 
-@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
 def test_view_code_is_memory_safe(tmp_path):
-    """The same paths under AddressSanitizer and UndefinedBehaviorSanitizer: no
-    out-of-bounds access, leak or undefined behaviour in building views and bins
-    (the views go to the GPU as they are)."""
-    exe = tmp_path / "asan_views"
-    build = subprocess.run(
-        ["g++", "-O1", "-g", "-std=c++17", "-fsanitize=address,undefined", "-fno-sanitize-recover=all",
-         "-pthread", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "g2-aimd_b200", "csrc"),
-         os.path.join(HERE, "tsan_views.cpp"), os.path.join(ROOT, "g2-aimd_b200", "csrc", "host", "view_host.cpp"),
-         "-o", str(exe)],
-        capture_output=True, text=True, timeout=600)
-    assert build.returncode == 0, build.stderr
-    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600,
-                         env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1"))
-    assert run.returncode == 0, run.stderr[-4000:]
-    assert run.stdout.count("mode") == 4
+    """The same paths and the view C entry points (the views go to the GPU as
+    they are)."""
+    build(tmp_path / "a", VIEWS, ASAN)
+    assert "rebalanced bins" in run(tmp_path / "a")
 
 
-@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
 def test_graph_and_plan_host_code_is_memory_safe(tmp_path):
-    """Generators, .bin / .vbmap / SNAP I/O, degeneracy order and recode and the
-    planner under AddressSanitizer + UBSan (tests/sanitize_host.cpp)."""
-    exe = tmp_path / "asan_host"
-    host = os.path.join(ROOT, "g2-aimd_b200", "csrc", "host")
-    build = subprocess.run(
-        ["g++", "-O1", "-g", "-std=c++17", "-fsanitize=address,undefined", "-fno-sanitize-recover=all",
-         "-pthread", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "g2-aimd_b200", "csrc"),
-         os.path.join(HERE, "sanitize_host.cpp"), os.path.join(host, "graph_host.cpp"),
-         os.path.join(host, "plan_host.cpp"), "-o", str(exe)],
-        capture_output=True, text=True, timeout=600)
-    assert build.returncode == 0, build.stderr
-    run = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=600,
-                         env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1"))
-    assert run.returncode == 0, run.stderr[-4000:]
-    assert "host ok" in run.stdout and "24 presets" in run.stdout, run.stdout
+    build(tmp_path / "a", GRAPH, ASAN)
+    out = run(tmp_path / "a", [tmp_path])
+    assert "host ok" in out and "24 presets" in out, out
 
 
-@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
 def test_graph_host_threads_are_race_free(tmp_path):
-    """The generators and the SNAP reader fan out over host threads: the same
-    driver under ThreadSanitizer."""
-    exe = tmp_path / "tsan_host"
-    host = os.path.join(ROOT, "g2-aimd_b200", "csrc", "host")
-    build = subprocess.run(
-        ["g++", "-O1", "-g", "-std=c++17", "-fsanitize=thread", "-pthread", "-I", os.path.join(ROOT, "include"),
-         "-I", os.path.join(ROOT, "g2-aimd_b200", "csrc"), os.path.join(HERE, "sanitize_host.cpp"),
-         os.path.join(host, "graph_host.cpp"), os.path.join(host, "plan_host.cpp"), "-o", str(exe)],
-        capture_output=True, text=True, timeout=600)
-    assert build.returncode == 0, build.stderr
-    run = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=600,
-                         env=dict(os.environ, TSAN_OPTIONS="halt_on_error=1 exitcode=66", G2_HOST_THREADS="6"))
-    assert run.returncode == 0, run.stderr[-4000:]
-    assert "ThreadSanitizer" not in run.stderr and "host ok" in run.stdout
+    """The generators and the SNAP reader fan out over host threads."""
+    build(tmp_path / "t", GRAPH, TSAN)
+    assert "host ok" in run(tmp_path / "t", [tmp_path], G2_HOST_THREADS="6")
 
 
-@pytest.mark.skipif(shutil.which("g++") is None or shutil.which("gcc") is None, reason="needs gcc and g++")
 def test_oracle_is_memory_safe(tmp_path):
-    """The CPU oracle, the checker every parity test relies on, under
-    AddressSanitizer + UBSan on all of its entry points (tests/sanitize_oracle.cpp;
-    OpenMP threads included, so no ThreadSanitizer run here)."""
-    san = ["-fsanitize=address,undefined", "-fno-sanitize-recover=all", "-fopenmp", "-g", "-O1"]
+    """OpenMP threads included, so ASan + UBSan only (no ThreadSanitizer)."""
     obj = tmp_path / "oracle.o"
-    cc = subprocess.run(["gcc", *san, "-std=c11", "-c", os.path.join(ROOT, "oracle", "g2_oracle.c"), "-o", str(obj)],
+    cc = subprocess.run(["gcc", "-O1", "-g", "-std=c11", "-fopenmp", *ASAN, "-c",
+                         os.path.join(ROOT, "oracle", "g2_oracle.c"), "-o", str(obj)],
                         capture_output=True, text=True, timeout=600)
     assert cc.returncode == 0, cc.stderr
-    exe = tmp_path / "asan_oracle"
-    host = os.path.join(ROOT, "g2-aimd_b200", "csrc", "host")
-    build = subprocess.run(
-        ["g++", *san, "-std=c++17", "-pthread", "-I", os.path.join(ROOT, "include"),
-         os.path.join(HERE, "sanitize_oracle.cpp"), str(obj), os.path.join(host, "graph_host.cpp"),
-         os.path.join(host, "plan_host.cpp"), "-o", str(exe)],
-        capture_output=True, text=True, timeout=600)
-    assert build.returncode == 0, build.stderr
-    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600,
-                         env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1"))
-    assert run.returncode == 0, run.stderr[-4000:]
-    assert "oracle ok" in run.stdout, run.stdout
+    build(tmp_path / "o", [os.path.join(HERE, "sanitize_oracle.cpp"), str(obj), os.path.join(HOST, "graph_host.cpp"),
+                           os.path.join(HOST, "plan_host.cpp")], ASAN, ["-fopenmp"])
+    assert "oracle ok" in run(tmp_path / "o")
