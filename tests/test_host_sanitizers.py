@@ -4,7 +4,8 @@ this directory call every host entry point on graphs large enough for the
 threaded paths; any sanitizer report fails the test.
   tests/tsan_views.cpp      view builder, bin planner, view C entry points
   tests/sanitize_host.cpp   generators, .bin / .vbmap / SNAP I/O, order, recode, planner
-  tests/sanitize_oracle.cpp the CPU oracle (the checker of every parity test)"""
+  tests/sanitize_oracle.cpp the CPU oracle (the checker of every parity test)
+  g2_worker's host-only modes, device entry points stubbed (tests/worker_gpu_stubs.cpp)"""
 import os
 import shutil
 import subprocess
@@ -77,3 +78,23 @@ def test_oracle_is_memory_safe(tmp_path):
     build(tmp_path / "o", [os.path.join(HERE, "sanitize_oracle.cpp"), str(obj), os.path.join(HOST, "graph_host.cpp"),
                            os.path.join(HOST, "plan_host.cpp")], ASAN, ["-fopenmp"])
     assert "oracle ok" in run(tmp_path / "o")
+
+
+def test_worker_host_modes_are_memory_safe(tmp_path):
+    """g2_worker's -prep, -recode and -plan under AddressSanitizer + UBSan (device
+    entry points stubbed: these modes use none)."""
+    build(tmp_path / "w", [os.path.join(HOST, "worker_main.cpp"), os.path.join(HERE, "worker_gpu_stubs.cpp"),
+                           os.path.join(HOST, "graph_host.cpp"), os.path.join(HOST, "plan_host.cpp"),
+                           os.path.join(HOST, "view_host.cpp")], ASAN)
+    txt = tmp_path / "g.txt"
+    with open(txt, "w") as f:
+        f.write("# toy\n")
+        for a in range(300):
+            for b in (a * 7 % 300, a * 13 % 300, (a + 1) % 300):
+                f.write(f"{a + 10} {b + 10}\n")
+    run(tmp_path / "w", ["-dg", txt, "-prep", 1])
+    run(tmp_path / "w", ["-dg", tmp_path / "g.bin", "-recode", 1, "-o", tmp_path / "r.bin", "-nb", 3])
+    out = run(tmp_path / "w", ["-dg", tmp_path / "r.bin", "-q", 24, "-plan", 1, "-m", 0.000002, "-ds", 1, "-cn", 2,
+                               "-dr", 1])
+    assert "wrote" in out and int(out.split("view bins: ")[1].split()[0]) > 1
+    run(tmp_path / "w", ["-dg", tmp_path / "r.bin", "-h", 2, "-plan", 1, "-m", 0.000004, "-t", 3])
