@@ -23,7 +23,9 @@
 //                     g2_view_bins
 //   -t <threads>      host threads for view building and bin planning
 //                     (G2_HOST_THREADS); default: all
-//   -m, -qs, -pn, -dr, -ds, -dst  see below
+//   -qs <k>           -ooc: pinned buffers holding built views (the reference's
+//                     view-bin holders; default producers + 2, at least 2)
+//   -m, -pn, -dr, -ds, -dst  see below
 // Bins come from "<graph.bin>.<hop>.hop.vbmap" (view/view_bin_manager.h:34-94); a
 // missing file means one bin holding every vertex.  BK prints one
 // "Total No. of Cliques: N" line per bin (app_BK/BK.h:72-76), GMatch one final
@@ -80,6 +82,7 @@ int main(int argc, char **argv) {
     const int producers = std::max(1, atoi(opt(argc, argv, "-pn", "1")));
     const double mem_gb = atof(opt(argc, argv, "-m", "10"));
     const int plan_only = atoi(opt(argc, argv, "-plan", "0"));
+    const int queue_size = std::max(0, atoi(opt(argc, argv, "-qs", "0")));
     const int recode = atoi(opt(argc, argv, "-recode", "0"));
     const int prep = atoi(opt(argc, argv, "-prep", "0"));
     // -t: threads that build views (the reference's ViewBin thread_num) and plan bins
@@ -228,6 +231,7 @@ int main(int argc, char **argv) {
                 g2_view_opts vo;
                 memset(&vo, 0, sizeof(vo));
                 vo.producers = (uint32_t)producers;
+                vo.slots = (uint32_t)queue_size;  // -qs: pinned view holders (0 = producers + 2)
                 g2_view_stats st;
                 memset(&st, 0, sizeof(st));
                 uint64_t count = 0;

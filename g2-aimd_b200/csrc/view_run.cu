@@ -376,7 +376,9 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
         np = std::min<uint32_t>(np, std::max<uint32_t>(nbins, 1u));
         // the host's threads are shared out: few bins get several threads each
         prod.build_threads = std::max(1u, cores / np);
-        if (!rc && nbins) prod.start(np, np + 2);
+        // the consumer holds one view while it waits for the next: at least 2 slots
+        const uint32_t nslots = vo && vo->slots ? std::max<uint32_t>(vo->slots, 2u) : np + 2;
+        if (!rc && nbins) prod.start(np, nslots);
         double wait_ms = 0;
         // next view with roots (bins that kept none count 0)
         auto take = [&](ReadyView *v) {

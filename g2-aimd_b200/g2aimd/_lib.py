@@ -52,7 +52,7 @@ class G2View(C.Structure):
 
 
 class G2ViewOpts(C.Structure):
-    _fields_ = [("producers", u32), ("radius", u32), ("row_radius", u32), ("flags", u32)]
+    _fields_ = [("producers", u32), ("radius", u32), ("row_radius", u32), ("flags", u32), ("slots", u32)]
 
 
 class G2ViewStats(C.Structure):

@@ -299,6 +299,10 @@ typedef struct g2_view_opts {
     uint32_t radius;      /* ball radius (0 = from the query: 1 for MCE)         */
     uint32_t row_radius;  /* rows kept up to this distance (0 = from the query)  */
     uint32_t flags;       /* G2_VIEW_NO_UPPER, G2_VIEW_EGO                       */
+    uint32_t slots;       /* pinned host buffers holding built views, each as
+                             large as the largest view (0 = producers + 2; at
+                             least 2): bounds pinned memory, as the reference's
+                             -qs holders do                                     */
 } g2_view_opts;
 typedef struct g2_view_stats {
     uint64_t bins;            /* views enumerated (bins with a root of enough degree) */
