@@ -64,7 +64,11 @@ struct ViewProducers {
     std::vector<std::thread> threads;
 
     void start(uint32_t producers, uint32_t nslots) {
-        if (slots->size() < nslots) slots->resize(nslots, {nullptr, 0});
+        // buffers kept from earlier calls beyond this call's count are released
+        // (nothing is in flight yet), so `nslots` bounds the pinned memory
+        for (size_t i = nslots; i < slots->size(); i++)
+            if ((*slots)[i].first) cudaFreeHost((*slots)[i].first);
+        slots->resize(nslots, {nullptr, 0});
         for (uint32_t i = 0; i < nslots; i++) free_slots.push_back((int)i);
         running = producers;
         for (uint32_t t = 0; t < producers; t++) threads.emplace_back([this] { produce(); });
