@@ -37,8 +37,6 @@ namespace g2 {
 
 namespace {
 
-__constant__ DevPlan c_plan;
-
 __device__ __forceinline__ bool cond_ok(uint32_t op, uint32_t w, uint32_t m) {
     return op == G2_COND_LESS_THAN ? w < m : op == G2_COND_LARGER_THAN ? w > m : w != m;
 }
@@ -51,8 +49,8 @@ struct Level {
 
 // Set up the scan window of position i given M[0..i-1].  Returns the sum of
 // the back neighbours' degrees (one partial embedding's share of the work model).
-__device__ uint64_t level_init(const uint64_t *rp, const uint32_t *ci, const uint32_t *M, uint32_t i, Level &L) {
-    const DevPlan &pl = c_plan;
+__device__ uint64_t level_init(const DevPlan &pl, const uint64_t *rp, const uint32_t *ci, const uint32_t *M,
+                               uint32_t i, Level &L) {
     uint32_t parent = pl.bn_pos[i][0];
     uint64_t pd = ldg(rp + M[parent] + 1) - ldg(rp + M[parent]);
     uint64_t dsum = pd;
@@ -84,9 +82,9 @@ __device__ uint64_t level_init(const uint64_t *rp, const uint32_t *ci, const uin
 }
 
 // Does w qualify for position i (conditions + other back neighbours)?
-__device__ __forceinline__ bool cand_ok(const uint64_t *rp, const uint32_t *ci, const uint32_t *M, uint32_t i,
+__device__ __forceinline__ bool cand_ok(const DevPlan &pl, const uint64_t *rp, const uint32_t *ci, const uint32_t *M,
+                                        uint32_t i,
                                         uint32_t parent, uint32_t w) {
-    const DevPlan &pl = c_plan;
     for (uint32_t c = 0; c < pl.cond_count[i]; c++)
         if (!cond_ok(pl.cond_op[i][c], w, M[pl.cond_pos[i][c]])) return false;
     for (uint32_t j = 0; j < pl.bn_count[i]; j++) {
@@ -192,10 +190,9 @@ __device__ __noinline__ bool match_donate_last(const MatchArgs &a, uint32_t task
 // Generic plan-driven walk of a root (rec == nullptr: M[0] = v) or of a handed-off
 // record; returns the number of embeddings and adds the work model (4 x
 // back-neighbour degrees per partial embedding) to work.
-__device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, uint32_t task, uint32_t v,
+__device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const DevPlan &pl, uint32_t task, uint32_t v,
                                                      const uint32_t *rec, uint32_t *S, unsigned long long &work,
                                                      uint32_t part, uint32_t nparts, long long c0) {
-    const DevPlan &pl = c_plan;
     const uint32_t k = pl.k;
     const uint32_t lane = lane_id();
     const uint64_t *rp = a.rp;
@@ -212,14 +209,14 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, uint32
     uint32_t base = 1;
     if (!rec) {
         M[0] = v;
-        const uint64_t w1 = 4ull * level_init(rp, ci, M, 1, Ls[1]);
+        const uint64_t w1 = 4ull * level_init(pl, rp, ci, M, 1, Ls[1]);
         if (part == 0) work += w1;
     } else {
         // record words are read past L1 (two records share a cache line)
         base = __ldcg(rec + 1);
         const uint32_t kind = __ldcg(rec + kRecKind);
         for (uint32_t j = 0; j < base; j++) M[j] = __ldcg(rec + kRecM + j);
-        const uint64_t d = level_init(rp, ci, M, base, Ls[base]);
+        const uint64_t d = level_init(pl, rp, ci, M, base, Ls[base]);
         if (kind == kRecPrefix) {
             work += 4ull * d;  // this partial embedding's share is counted where it starts
         } else if (kind == kRecWindow) {
@@ -259,7 +256,7 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, uint32
                     }
                 }
                 uint64_t x = e + lane;
-                bool ok = x < L.end && cand_ok(rp, ci, M, i, L.parent, ldg(ci + x));
+                bool ok = x < L.end && cand_ok(pl, rp, ci, M, i, L.parent, ldg(ci + x));
                 uint32_t b = __ballot_sync(G2_FULL, ok);
                 if (i == 1 && nparts > 1) {  // k == 2: split the candidates themselves
                     uint32_t keep = 0;
@@ -285,7 +282,7 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, uint32
             while (L.pos < L.end && len + 32 <= CH) {
                 uint64_t x = L.pos + lane;
                 uint32_t w = x < L.end ? ldg(ci + x) : 0u;
-                bool ok = x < L.end && cand_ok(rp, ci, M, i, L.parent, w);
+                bool ok = x < L.end && cand_ok(pl, rp, ci, M, i, L.parent, w);
                 uint32_t tot;
                 uint32_t pos = warp_scan(ok, tot);
                 if (ok) buf[len + pos] = w;
@@ -314,7 +311,7 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, uint32
             }
         }
         i++;
-        work += 4ull * level_init(rp, ci, M, i, Ls[i]);
+        work += 4ull * level_init(pl, rp, ci, M, i, Ls[i]);
     }
     return count;
 }
@@ -362,10 +359,10 @@ __device__ unsigned long long clique_count_lanes(const uint32_t *A, uint32_t p, 
 // Clique plans on P0 bitmaps.  Returns false if the root does not fit (caller
 // falls back to the generic walk).
 template <int WPL, bool METRICS>
-__device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, uint32_t *p0s, uint32_t *rowbuf,
+__device__ bool match_root_clique(const MatchArgs &a, const DevPlan &pl, uint32_t v, uint32_t *S, uint32_t *p0s,
+                                  uint32_t *rowbuf,
                                   unsigned long long &count, unsigned long long &work, uint32_t part,
                                   uint32_t nparts) {
-    const DevPlan &pl = c_plan;
     const uint32_t k = pl.k;
     const uint32_t lane = lane_id();
     const uint64_t *rp = a.rp;
@@ -475,7 +472,8 @@ __device__ bool match_root_clique(const MatchArgs &a, uint32_t v, uint32_t *S, u
 // registers; 6: 40 registers and more resident warps, which pays on graphs
 // larger than L2 where the rows' loads wait on memory).
 template <int WPL, bool METRICS, int MINB>
-__global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int clique_path) {
+__global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int clique_path,
+                                                          const __grid_constant__ DevPlan pl) {
     extern __shared__ uint32_t smem[];
     if (a.epoch_dev) a.epoch = *a.epoch_dev;
     const uint32_t wib = threadIdx.x >> 5;
@@ -512,8 +510,8 @@ __global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int cliqu
             if (lane_id() == 0) c0 = clock64();
             c0 = __shfl_sync(G2_FULL, c0, 0);
             unsigned long long c = 0;
-            if (!clique_path || !match_root_clique<WPL, METRICS>(a, v, S, p0s, rowbuf, c, work, part, nparts))
-                c = match_walk(a, (uint32_t)task, v, nullptr, S, work, part, nparts, c0);
+            if (!clique_path || !match_root_clique<WPL, METRICS>(a, pl, v, S, p0s, rowbuf, c, work, part, nparts))
+                c = match_walk(a, pl, (uint32_t)task, v, nullptr, S, work, part, nparts, c0);
             credit((uint32_t)task, c, c0);
         }
         outstanding_add(a, handoff, -1);
@@ -526,7 +524,7 @@ __global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int cliqu
             if (lane_id() == 0) c0 = clock64();
             c0 = __shfl_sync(G2_FULL, c0, 0);
             const uint32_t task = __ldcg(rec);
-            const unsigned long long c = match_walk(a, task, 0u, rec, S, work, 0u, 1u, c0);
+            const unsigned long long c = match_walk(a, pl, task, 0u, rec, S, work, 0u, 1u, c0);
             credit(task, c, c0);
         });
     if (lane_id() == 0 && total) atomicAdd(a.out, total);
@@ -540,9 +538,10 @@ size_t match_smem_bytes(int wpl, int warps_per_block) {
 }
 
 template <int WPL, bool M, int MINB>
-static void launch_match(const MatchArgs &a, dim3 g, dim3 b, size_t sm, cudaStream_t st, int cp) {
+static void launch_match(const DevPlan &pl, const MatchArgs &a, dim3 g, dim3 b, size_t sm, cudaStream_t st,
+                         int cp) {
     cudaFuncSetAttribute(match_kernel<WPL, M, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    match_kernel<WPL, M, MINB><<<g, b, sm, st>>>(a, cp);
+    match_kernel<WPL, M, MINB><<<g, b, sm, st>>>(a, cp, pl);
 }
 
 template <int WPL, bool M, int MINB>
@@ -572,21 +571,19 @@ int match_blocks_per_sm(int wpl, int warps_per_block, bool metrics, int ctas_per
 
 cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block, cudaStream_t st,
                          bool clique_path, int wpl, int ctas_per_sm) {
-    cudaError_t e = cudaMemcpyToSymbolAsync(c_plan, &plan, sizeof(DevPlan), 0, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return e;
     size_t sm = match_smem_bytes(wpl, warps_per_block);
     dim3 g(blocks), b(32 * warps_per_block);
     const int cp = clique_path ? 1 : 0;
     const bool m = a.work != nullptr;
     if (wide_budget(wpl, m, ctas_per_sm)) {
-        launch_match<1, false, 6>(a, g, b, sm, st, cp);
+        launch_match<1, false, 6>(plan, a, g, b, sm, st, cp);
         return cudaGetLastError();
     }
     switch (wpl) {
-        case 1: m ? launch_match<1, true, 4>(a, g, b, sm, st, cp) : launch_match<1, false, 4>(a, g, b, sm, st, cp); break;
-        case 2: m ? launch_match<2, true, 4>(a, g, b, sm, st, cp) : launch_match<2, false, 4>(a, g, b, sm, st, cp); break;
-        case 4: m ? launch_match<4, true, 4>(a, g, b, sm, st, cp) : launch_match<4, false, 4>(a, g, b, sm, st, cp); break;
-        case 8: m ? launch_match<8, true, 4>(a, g, b, sm, st, cp) : launch_match<8, false, 4>(a, g, b, sm, st, cp); break;
+        case 1: m ? launch_match<1, true, 4>(plan, a, g, b, sm, st, cp) : launch_match<1, false, 4>(plan, a, g, b, sm, st, cp); break;
+        case 2: m ? launch_match<2, true, 4>(plan, a, g, b, sm, st, cp) : launch_match<2, false, 4>(plan, a, g, b, sm, st, cp); break;
+        case 4: m ? launch_match<4, true, 4>(plan, a, g, b, sm, st, cp) : launch_match<4, false, 4>(plan, a, g, b, sm, st, cp); break;
+        case 8: m ? launch_match<8, true, 4>(plan, a, g, b, sm, st, cp) : launch_match<8, false, 4>(plan, a, g, b, sm, st, cp); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -20,15 +20,17 @@
 //     it is read;
 //   * two calls whose work overlaps on the GPU (different streams, or different
 //     host threads on one device) race on that array and give wrong counts:
-//     serialise them;
-//   * the first call on a device looks up the array's device address (once per
-//     device, with that device current); make that first call before any stream
-//     capture begins.
+//     serialise them.  The plan travels as a kernel argument, so a call may
+//     overlap context runs (g2_match_run*) of any plan;
+//   * every call looks up the array's device address on the current device
+//     (cudaGetSymbolAddress allocates nothing), so a context that was torn
+//     down and created again never sees a stale address;
+//   * a device-side failure (the kernel's status word non-zero, e.g. a
+//     candidate stack too small for the query) is reported on the stream:
+//     *d_count is set to G2_NOALLOC_FAILED (UINT64_MAX) instead of a count.
 #include <cuda_runtime.h>
 
-#include <atomic>
 #include <cstring>
-#include <mutex>
 
 #include "g2_aimd.h"
 #include "g2_kernels.h"
@@ -38,26 +40,23 @@ namespace {
 constexpr uint64_t kWords = G2_NOALLOC_SCRATCH_BYTES / sizeof(uint32_t);
 constexpr uint64_t kHeadWords = 64;  // [0..1] queue head (u64), [2] status word
 constexpr int kWarpsPerBlock = 4;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kWords];
 
-// Host copies of the array's device address, one per device.
-std::mutex g_setup_mu;
-uint32_t *g_scratch_addr[kMaxDevices] = {nullptr};
-
-int scratch_address(int dev, uint32_t **out) {
-    if (dev < 0 || dev >= kMaxDevices) return G2_ERR_UNSUPPORTED;
-    std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        // the current device is `dev` here: the symbol's address on this device
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) return G2_ERR_CUDA;
-        g_scratch_addr[dev] = static_cast<uint32_t *>(p);
-    }
-    *out = g_scratch_addr[dev];
+// The array's address on the current device.  In host code the symbol itself
+// is only a host-side stand-in; kernels must be given this address.
+int scratch_address(uint32_t **out) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return G2_ERR_CUDA;
+    *out = static_cast<uint32_t *>(p);
     return G2_OK;
+}
+
+// Runs after the count on the same stream: a non-zero status word replaces the
+// count by the failure sentinel.
+__global__ void noalloc_status_kernel(const int *status, unsigned long long *count) {
+    if (*status != 0) *count = G2_NOALLOC_FAILED;
 }
 
 // fo[v] (offset of the first neighbour larger than v) and the identity task list.
@@ -127,7 +126,7 @@ extern "C" int g2_match_count_noalloc(const uint64_t *d_row_ptrs, const uint32_t
     if (cudaGetDevice(&dev) != cudaSuccess) return G2_ERR_CUDA;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return G2_ERR_CUDA;
     uint32_t *S = nullptr;
-    rc = scratch_address(dev, &S);
+    rc = scratch_address(&S);
     if (rc) return rc;
     // layout: [head/status kHeadWords] [fo n] [tasks n] [per-warp slabs]
     uint32_t *fo = S + kHeadWords;
@@ -157,5 +156,7 @@ extern "C" int g2_match_count_noalloc(const uint64_t *d_row_ptrs, const uint32_t
     a.out = reinterpret_cast<unsigned long long *>(d_count);
     a.status = reinterpret_cast<int *>(S + 2);
     if (g2::match_launch(dp, a, blocks, wpb, st, clique, 1, 0) != cudaSuccess) return G2_ERR_CUDA;
+    noalloc_status_kernel<<<1, 1, 0, st>>>(a.status, a.out);
+    if (cudaGetLastError() != cudaSuccess) return G2_ERR_CUDA;
     return G2_OK;
 }

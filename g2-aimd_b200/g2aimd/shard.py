@@ -39,16 +39,25 @@ def shard(n: int, world: int, rank: int, cost=None) -> np.ndarray:
 
 
 def allreduce_counts(count: int, hist=None, device=None, group=None):
-    """Sum a count and an optional histogram over the ranks of `group`."""
+    """Sum a count and an optional histogram (uint64 values) over the ranks of
+    `group`.  Collectives have no uint64 sum, so every value travels as its low
+    and high 32-bit halves in int64 lanes (exact for up to 2^31 ranks) and is
+    put back together here; a total of 2^64 or more raises OverflowError."""
     import torch
     import torch.distributed as dist
-    h = np.zeros(0, np.int64) if hist is None else np.asarray(hist, dtype=np.int64)
-    t = torch.from_numpy(np.concatenate([[int(count)], h]).astype(np.int64))
+    vals = np.concatenate([np.asarray([int(count)], dtype=np.uint64),
+                           np.zeros(0, np.uint64) if hist is None else np.asarray(hist, dtype=np.uint64)])
+    halves = np.concatenate([vals & np.uint64(0xFFFFFFFF), vals >> np.uint64(32)]).astype(np.int64)
+    t = torch.from_numpy(halves)
     if device is not None:
         t = t.to(device)
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     t = t.cpu().numpy()
-    return int(t[0]), (None if hist is None else t[1:].astype(np.uint64))
+    k = vals.size
+    tot = [(int(t[k + i]) << 32) + int(t[i]) for i in range(k)]
+    if any(x >= 1 << 64 for x in tot):
+        raise OverflowError("a summed count does not fit in 64 bits")
+    return tot[0], (None if hist is None else np.asarray(tot[1:], dtype=np.uint64))
 
 
 def mce_sharded(ctx, world: int, rank: int, cost=None, hist_len: int = 256, device=None, group=None, **kw):

@@ -366,11 +366,16 @@ int g2_last_spill_stats(g2_ctx *ctx, uint64_t *records, uint64_t *pool_bytes);
  * GPU loading this library holds until exit.  Limits: n <= G2_NOALLOC_MAX_VERTICES,
  * otherwise G2_ERR_UNSUPPORTED (also when the query leaves too little scratch
  * per warp).  All calls on a device share that array: calls that overlap on the
- * GPU race and must be serialised.  The first call on each device looks up the
- * array's device address; make it before any stream capture.
+ * GPU race and must be serialised.  The plan is passed to the kernel as an
+ * argument, so a call may overlap context match runs of other plans.  Every
+ * call looks up the array's device address on the current device (no
+ * allocation).  A failure found on the device (the kernel's status word set)
+ * is reported in stream order: *d_count holds G2_NOALLOC_FAILED instead of a
+ * count.
  */
 #define G2_NOALLOC_SCRATCH_BYTES (32u << 20)
 #define G2_NOALLOC_MAX_VERTICES (1u << 21)
+#define G2_NOALLOC_FAILED 0xffffffffffffffffull
 int g2_match_count_noalloc(const uint64_t *d_row_ptrs, const uint32_t *d_cols,
                            uint64_t n, uint64_t m, const g2_plan *plan,
                            uint64_t *d_count, void *stream);

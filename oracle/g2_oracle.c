@@ -42,6 +42,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <math.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -530,4 +531,139 @@ int64_t orc_kcore(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint32_t *
     free(buf);
     free(removed);
     return kmax;
+}
+
+/* ------------------------------------------- seeded graphs, degeneracy recode */
+
+/*
+ * The synthetic inputs are defined by a seeded generator (the reference ships
+ * no datasets), so the checker can build the same graph without the library:
+ * orc_gen_rmat restates the counter-based R-MAT generator of the library's
+ * g2_gen_rmat (splitmix64 finaliser over (seed, stream 2, 8 * edge + level / 4),
+ * four 16-bit quadrant draws per 64-bit word, fixed-point thresholds a, a+b,
+ * a+b+c), then symmetrises, drops self loops and duplicates and sorts each row,
+ * as the reference's Preprocess does (common/graph.h:720-811) except that
+ * isolated vertices keep their ids (n = 2^scale).  Returns malloc'd arrays.
+ */
+static uint64_t orc_mix64(uint64_t z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+static uint64_t orc_rnd(uint64_t seed, uint64_t stream, uint64_t idx) {
+    return orc_mix64(orc_mix64(seed ^ orc_mix64(stream * 0x632be59bd9b4e019ull)) + idx);
+}
+static int cmp_u32(const void *a, const void *b) {
+    uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+    return x < y ? -1 : x > y;
+}
+
+int orc_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed,
+                 uint64_t **rp_out, uint32_t **ci_out, uint64_t *m_out) {
+    if (scale < 1 || scale > 31 || !edge_factor || !rp_out || !ci_out || !m_out) return ORC_ERR_INVALID;
+    const uint64_t n = 1ull << scale, ne = (uint64_t)edge_factor << scale;
+    const uint32_t ta = (uint32_t)llround(a * 65536.0), tb = (uint32_t)llround((a + b) * 65536.0),
+                   tc = (uint32_t)llround((a + b + c) * 65536.0);
+    uint32_t *src = (uint32_t *)malloc(sizeof(uint32_t) * ne), *dst = (uint32_t *)malloc(sizeof(uint32_t) * ne);
+    uint64_t *deg = (uint64_t *)calloc(n + 1, sizeof(uint64_t));
+    if (!src || !dst || !deg) { free(src); free(dst); free(deg); return ORC_ERR_OOM; }
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < (int64_t)ne; e++) {
+        uint32_t s = 0, d = 0;
+        uint64_t r = 0;
+        for (uint32_t l = 0; l < scale; l++) {
+            if ((l & 3) == 0) r = orc_rnd(seed, 2, (uint64_t)e * 8 + (l >> 2));
+            uint32_t x = (uint32_t)(r & 0xffff);
+            r >>= 16;
+            s = (s << 1) | (uint32_t)(x >= tb);
+            d = (d << 1) | (uint32_t)((x >= ta && x < tb) || x >= tc);
+        }
+        src[e] = s;
+        dst[e] = d;
+    }
+    for (uint64_t e = 0; e < ne; e++)
+        if (src[e] != dst[e]) { deg[src[e] + 1]++; deg[dst[e] + 1]++; }
+    for (uint64_t v = 0; v < n; v++) deg[v + 1] += deg[v];
+    uint32_t *tmp = (uint32_t *)malloc(sizeof(uint32_t) * (deg[n] ? deg[n] : 1));
+    uint64_t *fill = (uint64_t *)malloc(sizeof(uint64_t) * n);
+    if (!tmp || !fill) { free(src); free(dst); free(deg); free(tmp); free(fill); return ORC_ERR_OOM; }
+    memcpy(fill, deg, sizeof(uint64_t) * n);
+    for (uint64_t e = 0; e < ne; e++)
+        if (src[e] != dst[e]) { tmp[fill[src[e]]++] = dst[e]; tmp[fill[dst[e]]++] = src[e]; }
+    free(src);
+    free(dst);
+    /* sort and deduplicate each row; fill[v] becomes the row's kept length */
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t v = 0; v < (int64_t)n; v++) {
+        uint32_t *p = tmp + deg[v];
+        uint64_t len = deg[v + 1] - deg[v], k = 0;
+        qsort(p, len, sizeof(uint32_t), cmp_u32);
+        for (uint64_t i = 0; i < len; i++)
+            if (k == 0 || p[k - 1] != p[i]) p[k++] = p[i];
+        fill[v] = k;
+    }
+    uint64_t *rp = (uint64_t *)malloc(sizeof(uint64_t) * (n + 1));
+    if (!rp) { free(deg); free(tmp); free(fill); return ORC_ERR_OOM; }
+    rp[0] = 0;
+    for (uint64_t v = 0; v < n; v++) rp[v + 1] = rp[v] + fill[v];
+    uint32_t *ci = (uint32_t *)malloc(sizeof(uint32_t) * (rp[n] ? rp[n] : 1));
+    if (!ci) { free(deg); free(tmp); free(fill); free(rp); return ORC_ERR_OOM; }
+    for (uint64_t v = 0; v < n; v++) memcpy(ci + rp[v], tmp + deg[v], sizeof(uint32_t) * fill[v]);
+    free(deg);
+    free(tmp);
+    free(fill);
+    *rp_out = rp;
+    *ci_out = ci;
+    *m_out = rp[n];
+    return ORC_OK;
+}
+
+void orc_free(void *p) { free(p); }
+
+/*
+ * The degeneracy order that the reference's kcore tool writes
+ * (kmeans/kcore.cpp:126-191): core shells ascending, degree ascending inside a
+ * shell (ties by old id), ids renamed to positions in that order, rows sorted.
+ * Core numbers from orc_kcore.  orp (n+1) and oci (m) are the caller's; core_new
+ * (optional) receives core numbers under the new ids.
+ */
+static const uint64_t *g_sort_rp;
+static const uint32_t *g_sort_core;
+static int cmp_degeneracy(const void *pa, const void *pb) {
+    uint32_t x = *(const uint32_t *)pa, y = *(const uint32_t *)pb;
+    if (g_sort_core[x] != g_sort_core[y]) return g_sort_core[x] < g_sort_core[y] ? -1 : 1;
+    uint64_t dx = g_sort_rp[x + 1] - g_sort_rp[x], dy = g_sort_rp[y + 1] - g_sort_rp[y];
+    if (dx != dy) return dx < dy ? -1 : 1;
+    return x < y ? -1 : x > y;
+}
+
+int orc_degeneracy_recode(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint64_t *orp, uint32_t *oci,
+                          uint32_t *core_new) {
+    if (!rp || !orp || (!ci && rp[n]) || (!oci && rp[n])) return ORC_ERR_INVALID;
+    uint32_t *core = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t *ord = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t *perm = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    if (!core || !ord || !perm) { free(core); free(ord); free(perm); return ORC_ERR_OOM; }
+    if (orc_kcore(rp, ci, n, NULL, core) < 0) { free(core); free(ord); free(perm); return ORC_ERR_OOM; }
+    for (uint64_t v = 0; v < n; v++) ord[v] = (uint32_t)v;
+    g_sort_rp = rp;
+    g_sort_core = core;
+    qsort(ord, n, sizeof(uint32_t), cmp_degeneracy);
+    for (uint64_t i = 0; i < n; i++) perm[ord[i]] = (uint32_t)i;
+    orp[0] = 0;
+    for (uint64_t i = 0; i < n; i++) orp[i + 1] = orp[i] + (rp[ord[i] + 1] - rp[ord[i]]);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        uint32_t v = ord[i];
+        uint64_t o = orp[i];
+        for (uint64_t e = rp[v]; e < rp[v + 1]; e++) oci[o++] = perm[ci[e]];
+        qsort(oci + orp[i], orp[i + 1] - orp[i], sizeof(uint32_t), cmp_u32);
+    }
+    if (core_new)
+        for (uint64_t i = 0; i < n; i++) core_new[i] = core[ord[i]];
+    free(core);
+    free(ord);
+    free(perm);
+    return ORC_OK;
 }

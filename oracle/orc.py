@@ -38,6 +38,13 @@ def lib():
         L.orc_mce_bruteforce.restype = i32
         L.orc_kcore.argtypes = [vp, vp, u64, vp, vp]
         L.orc_kcore.restype = C.c_int64
+        L.orc_gen_rmat.argtypes = [u32, u32, C.c_double, C.c_double, C.c_double, u64, C.POINTER(vp),
+                                   C.POINTER(vp), C.POINTER(u64)]
+        L.orc_gen_rmat.restype = i32
+        L.orc_free.argtypes = [vp]
+        L.orc_free.restype = None
+        L.orc_degeneracy_recode.argtypes = [vp, vp, u64, vp, vp, vp]
+        L.orc_degeneracy_recode.restype = i32
         _lib = L
     return _lib
 
@@ -109,3 +116,68 @@ def kcore(g):
     core = np.zeros(g.n, np.uint32)
     kmax = lib().orc_kcore(_p(g.row_ptrs), _p(g.cols), g.n, _p(order), _p(core))
     return order, core, int(kmax)
+
+
+class CSR:
+    """A CSR graph held by the oracle alone (row_ptrs uint64, cols uint32), so
+    that a CPU measurement can build its input without the library."""
+
+    def __init__(self, row_ptrs, cols, core=None):
+        self.row_ptrs, self.cols, self.core = row_ptrs, cols, core
+
+    @property
+    def n(self):
+        return self.row_ptrs.size - 1
+
+    @property
+    def m(self):
+        return self.cols.size
+
+
+def gen_rmat(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=1):
+    """The seeded R-MAT graph of the library's generator (same ids, same rows)."""
+    rp, ci, m = C.c_void_p(), C.c_void_p(), C.c_uint64()
+    rc = lib().orc_gen_rmat(scale, edge_factor, a, b, c, seed, C.byref(rp), C.byref(ci), C.byref(m))
+    if rc != 0:
+        raise RuntimeError(f"orc_gen_rmat failed: {rc}")
+    n = 1 << scale
+    row_ptrs = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_uint64)), shape=(n + 1,)).copy()
+    cols = np.ctypeslib.as_array(C.cast(ci, C.POINTER(C.c_uint32)), shape=(max(m.value, 1),))[:m.value].copy()
+    lib().orc_free(rp)
+    lib().orc_free(ci)
+    return CSR(row_ptrs, cols)
+
+
+def degeneracy_recoded(g):
+    """g with ids in the reference kcore tool's order (core numbers attached)."""
+    orp = np.zeros(g.n + 1, np.uint64)
+    oci = np.zeros(max(g.m, 1), np.uint32)
+    core = np.zeros(g.n, np.uint32)
+    rc = lib().orc_degeneracy_recode(_p(g.row_ptrs), _p(g.cols), g.n, _p(orp), _p(oci), _p(core))
+    if rc != 0:
+        raise RuntimeError(f"orc_degeneracy_recode failed: {rc}")
+    return CSR(orp, oci[:g.m], core)
+
+
+class PresetPlan:
+    """A preset query's plan from the planner restatement (plan_oracle.py), in
+    the form orc.match takes (k and flat())."""
+
+    def __init__(self, query_id):
+        import plan_oracle
+        self.p = plan_oracle.preset_plan(query_id)
+        self.k = self.p["k"]
+
+    def flat(self):
+        k, p = self.k, self.p
+        bn = np.zeros(k * k, np.uint32)
+        cond = np.zeros(k * k * 2, np.uint32)
+        for i in range(k):
+            for j, b in enumerate(p["bn"][i]):
+                bn[i * k + j] = b
+            for j, (op, w) in enumerate(p["cond"][i]):
+                cond[(i * k + j) * 2] = op
+                cond[(i * k + j) * 2 + 1] = w
+        return (np.array(p["order"], np.uint32), np.array(p["id2order"], np.uint32),
+                np.array([len(b) for b in p["bn"]], np.uint32), bn,
+                np.array([len(c) for c in p["cond"]], np.uint32), cond)

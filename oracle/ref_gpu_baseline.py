@@ -10,10 +10,20 @@ formats), then runs, with the same flags,
   this repo:  g2-aimd_b200/g2_worker  (same flags, same result lines)
 and parses "Total counts:" / "Total No. of Cliques:" and the
 "In-memory Execution Time" lines (device loop only, both programs).
-Inputs (ids in degeneracy order): R-MAT scale 20 edge factor 16 (4-clique and
-triangle), Chung-Lu 2^18 gamma 2.3 degree 16 and ER(2000, 0.01) + 5 K12
-(maximal cliques).  Each run has a time limit; a reference run that does not
-finish is reported as such.
+Inputs (ids in degeneracy order, the generators in g2aimd.graph):
+  er2000_k12   ER(2000, 0.01) + 5 K12, seed 7               maximal cliques
+  rmat20       R-MAT scale 20 edge factor 16, seed 1          triangles, 4-, 5-cliques
+  rmat16       R-MAT scale 16 edge factor 16, seed 3          4-cycles, diamonds, 4-, 5-cliques
+  chunglu18    Chung-Lu 2^18 gamma 2.3 degree 16, seed 1      maximal cliques, triangles
+  cl_*         three Chung-Lu graphs shaped like the 64-graph batch members
+               (n 5e3 / 5e4 / 2e5)                            maximal cliques, triangles,
+                                                              4-cycles, diamonds
+  rmat13_k     R-MAT scale 13 edge factor 16 + 20 planted cliques of 20-60
+               vertices, seed 5                              maximal cliques
+Each run has a time limit; a reference run that does not finish is reported as
+such.  A reference GMatch run that printed a '--- chunk' line retried a chunk
+after a buffer overflow and double counts (its iterationFailed is a no-op), so
+such a count is marked untrusted; so is any run that printed 'Host overflow'.
 """
 import argparse
 import json
@@ -28,13 +38,33 @@ ROOT = os.path.dirname(HERE)
 sys.path.insert(0, os.path.join(ROOT, "g2-aimd_b200"))
 
 
+# graph name -> generator call (ids are then put in degeneracy order)
+GRAPHS = [
+    ("er2000_k12", "Graph.er(2000, 0.01, planted=5, planted_size=12, seed=7)",
+     lambda G: G.er(2000, 0.01, planted=5, planted_size=12, seed=7)),
+    ("rmat20", "Graph.rmat(20, 16, seed=1)", lambda G: G.rmat(20, 16, seed=1)),
+    ("rmat16", "Graph.rmat(16, 16, seed=3)", lambda G: G.rmat(16, 16, seed=3)),
+    ("chunglu18", "Graph.chung_lu(1 << 18, 2.3, 16.0, seed=1)", lambda G: G.chung_lu(1 << 18, 2.3, 16.0, seed=1)),
+    ("cl_5k", "Graph.chung_lu(5000, 2.5, 20.0, seed=11)", lambda G: G.chung_lu(5000, 2.5, 20.0, seed=11)),
+    ("cl_50k", "Graph.chung_lu(50000, 2.2, 30.0, seed=12)", lambda G: G.chung_lu(50000, 2.2, 30.0, seed=12)),
+    ("cl_200k", "Graph.chung_lu(200000, 2.8, 10.0, seed=13)", lambda G: G.chung_lu(200000, 2.8, 10.0, seed=13)),
+    ("rmat13_k", "Graph.rmat(13, 16, planted=20, pmin=20, pmax=60, seed=5)",
+     lambda G: G.rmat(13, 16, planted=20, pmin=20, pmax=60, seed=5)),
+]
+JOBS = [("er2000_k12", "mce"), ("rmat20", "q24"), ("rmat20", "q0"), ("rmat20", "q25"),
+        ("rmat16", "q1"), ("rmat16", "q2"), ("rmat16", "q24"), ("rmat16", "q25"),
+        ("chunglu18", "mce"), ("chunglu18", "q0")] + \
+       [(g, j) for g in ("cl_5k", "cl_50k", "cl_200k") for j in ("mce", "q0", "q1", "q2")] + \
+       [("rmat13_k", "mce")]
+
+
 def parse(out):
     t = sum(float(x) for x in re.findall(r"In-memory Execution Time, elapsed_time=([0-9.]+)ms", out))
     cl = [int(x) for x in re.findall(r"Total No\. of Cliques: (\d+)", out)]
     tc = re.findall(r"^Total counts: (\d+)", out, flags=re.M)
     tot = re.findall(r"total time, elapsed_time=([0-9.]+)ms", out)
     return {"in_memory_ms": t, "cliques": sum(cl) if cl else None, "counts": int(tc[-1]) if tc else None,
-            "total_ms": float(tot[-1]) if tot else None}
+            "total_ms": float(tot[-1]) if tot else None, "chunk_retries": len(re.findall(r"--- chunk", out))}
 
 
 def run(cmd, limit):
@@ -44,6 +74,7 @@ def run(cmd, limit):
         r["rc"] = p.returncode
         if "Host overflow" in p.stdout:
             r["note"] = "host overflow (reference cannot complete)"
+        r["trusted"] = p.returncode == 0 and "Host overflow" not in p.stdout and r["chunk_retries"] == 0
         return r
     except subprocess.TimeoutExpired:
         return {"rc": None, "note": f"did not finish within {limit} s"}
@@ -54,18 +85,18 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=None)
     ap.add_argument("--limit", type=int, default=600)
+    ap.add_argument("--only", default="", help="comma-separated graph names")
     a = ap.parse_args()
     ref_run, ref_bk = os.path.join(HERE, "_ref", "ref_run"), os.path.join(HERE, "_ref", "ref_bk")
     ours = os.path.join(ROOT, "g2-aimd_b200", "g2_worker")
     work = tempfile.mkdtemp(prefix="g2ref_")
-    graphs = {
-        "rmat20": g2aimd.Graph.rmat(20, 16, seed=1).degeneracy_recoded(),
-        "chunglu18": g2aimd.Graph.chung_lu(1 << 18, 2.3, 16.0, seed=1).degeneracy_recoded(),
-        "er2000_k12": g2aimd.Graph.er(2000, 0.01, planted=5, planted_size=12, seed=7).degeneracy_recoded(),
-    }
-    jobs = [("rmat20", "q24"), ("rmat20", "q0"), ("chunglu18", "mce"), ("er2000_k12", "mce")]
+    makers = {name: (text, fn) for name, text, fn in GRAPHS}
+    jobs = JOBS if not a.only else [j for j in JOBS if j[0] in a.only.split(",")]
+    graphs = {}
     results = []
     for name, job in jobs:
+        if name not in graphs:
+            graphs[name] = makers[name][1](g2aimd.Graph).degeneracy_recoded()
         g = graphs[name]
         path = os.path.join(work, f"{name}.bin")
         if not os.path.exists(path):
@@ -79,12 +110,13 @@ def main():
             args = ["-dg", path, "-q", job[1:], "-m", "1"]
             r = run([ref_run] + args, a.limit)
             o = run([ours] + args, a.limit)
-        res = {"graph": name, "n": g.n, "m": g.m, "job": job, "reference_gpu": r, "g2_worker": o}
+        res = {"graph": name, "make": makers[name][0], "n": g.n, "m": g.m, "job": job, "reference_gpu": r,
+               "g2_worker": o}
         print(json.dumps(res), flush=True)
         results.append(res)
-    if a.out:
-        with open(a.out, "w") as f:
-            json.dump(results, f, indent=1)
+        if a.out:  # rewritten after every job, so a cut-off run keeps what finished
+            with open(a.out, "w") as f:
+                json.dump(results, f, indent=1)
 
 
 if __name__ == "__main__":

@@ -103,3 +103,22 @@ def test_view_rejects_scores(vctx, c1_graph):
     bin_of = np.zeros(c1_graph.n, np.uint32)
     with pytest.raises(Exception):
         vctx.view_mce(c1_graph, bin_of, schedule="scores", scores=np.ones(c1_graph.n, np.float32))
+
+
+def test_view_runs_with_bounded_pinned_buffers(vctx, orc, c1_graph):
+    """g2_view_opts.slots (-qs) bounds the pinned view buffers: two of them for
+    four producers, then a second run on the same context with fewer buffers
+    than the first (the buffers beyond a call's count are released), each equal
+    to the run with the default count."""
+    g = c1_graph
+    bin_of = (np.arange(g.n) % 9).astype(np.uint32)
+    c0, h0, pb0, _ = vctx.view_mce(g, bin_of, hist_len=64, producers=4)
+    assert c0 == orc.mce(g, hist_len=64)["count"]
+    for slots in (4, 2):
+        c, h, pb, _ = vctx.view_mce(g, bin_of, hist_len=64, producers=4, slots=slots)
+        assert c == c0 and np.array_equal(h, h0) and np.array_equal(pb, pb0)
+    from g2aimd.context import Plan
+    want = orc.match(g, Plan.preset(24))["count"]
+    c, pb, _ = vctx.view_match(g, bin_of, Plan.preset(24), producers=4, slots=2)
+    assert c == want
+    vctx.load(g)

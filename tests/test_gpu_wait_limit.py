@@ -2,12 +2,11 @@
 is bounded (g2_opts.wait_cycles, default 2^37 SM cycles).  With the bound cut
 to one cycle the warps that wait give up, the run reports G2_ERR_TIMEOUT (a
 status word the host reads, no device fault), and the same context then runs
-normally.  Marked xfail without strictness until it has run on a B200: a
-failure here is reported without stopping a run at its first failure."""
+normally."""
 import numpy as np
 import pytest
 
-pytestmark = [pytest.mark.gpu, pytest.mark.xfail(strict=False, reason="not yet run on a GPU")]
+pytestmark = pytest.mark.gpu
 
 G2_ERR_TIMEOUT = -4
 

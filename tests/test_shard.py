@@ -222,3 +222,40 @@ def test_gloo_lost_rank_ends_in_an_error_not_a_hang():
     assert res[1] == "left"
     assert res[0].startswith("error after"), res[0]
     assert float(res[0].split()[2]) < 60
+
+
+def _big_rank_main(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        from g2aimd.shard import allreduce_counts
+        # totals at and above 2^63, where an int64 sum would wrap
+        mine = (1 << 63) + 5 if rank == 0 else 1 << 62
+        c, h = allreduce_counts(mine, np.array([(1 << 62) + rank, 7, 0], np.uint64))
+        try:
+            allreduce_counts((1 << 64) - 1)  # the sum needs 65 bits
+            over = False
+        except OverflowError:
+            over = True
+        q.put((rank, c, h.tolist(), over))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_world2_allreduce_is_exact_for_uint64():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_big_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, c, h, over in res:
+        assert c == (1 << 63) + (1 << 62) + 5, rank
+        assert h == [(1 << 63) + 1, 14, 0], rank
+        assert over, rank

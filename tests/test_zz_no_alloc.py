@@ -52,3 +52,35 @@ def test_noalloc_rejects_graphs_over_the_limit(g2):
     dummy = np.zeros(4, np.uint64)
     rc = f(dummy.ctypes.data, dummy.ctypes.data, (1 << 21) + 1, 0, C.addressof(plan.raw), dummy.ctypes.data, None)
     assert rc == -8  # G2_ERR_UNSUPPORTED, before any device work
+
+
+def test_noalloc_overlapping_a_context_run_of_another_plan(g2):
+    """The plan is a kernel argument: a no-alloc count of 4-cliques on one
+    stream and a context's diamond count on another stream, enqueued back to
+    back so that they may run at the same time, both give their own counts."""
+    import torch
+
+    from g2aimd.context import Context, Plan
+    g = g2.Graph.rmat(13, 16, seed=23).degeneracy_recoded()
+    k4, diamond = Plan.preset(24), Plan.preset(2)
+    dev = torch.device("cuda", 0)
+    rp = torch.from_numpy(g.row_ptrs.view(np.int64)).to(dev)
+    ci = torch.from_numpy(g.cols.view(np.int32)).to(dev)
+    f = _noalloc(g2.lib())
+    with Context(0) as ctx:
+        ctx.load(g)
+        want_d = ctx.match(diamond)
+        want_k4 = ctx.match(k4)
+        ctx.set_plan(diamond)
+        ctx.reserve()
+        s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        out1 = torch.zeros(1, dtype=torch.int64, device=dev)
+        out2 = torch.full((1,), -1, dtype=torch.int64, device=dev)
+        torch.cuda.synchronize(dev)
+        for _ in range(2):
+            ctx.match_device(out1.data_ptr(), stream=s1.cuda_stream)
+            rc = f(rp.data_ptr(), ci.data_ptr(), g.n, g.m, C.addressof(k4.raw), out2.data_ptr(), s2.cuda_stream)
+            assert rc == 0, g2.lib().g2_strerror(rc)
+            torch.cuda.synchronize(dev)
+            assert int(out1.item()) == want_d
+            assert int(out2.item()) == want_k4
