@@ -139,6 +139,10 @@ size_t match_smem_bytes(int wpl, int warps_per_block);
 cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block,
                          cudaStream_t st, bool clique_path, int wpl, int ctas_per_sm);
 
+// Sort each row of `in` (device CSR rows given by rp) into `out`, in calls of at
+// most max_chunk entries (kcore.cu); synchronous.
+cudaError_t sort_rows_device(const uint64_t *rp, uint64_t n, uint64_t m, const uint32_t *in, uint32_t *out,
+                             uint64_t max_chunk, int sms);
 // Degeneracy order of a CSR on the device (kcore.cu); synchronous.
 cudaError_t degeneracy_order_device(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint32_t *perm,
                                     uint32_t *core, int sms, uint64_t *rounds);

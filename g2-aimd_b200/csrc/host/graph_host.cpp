@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "g2_aimd.h"
+#include "host/gen_host.h"
 
 namespace {
 
@@ -139,6 +140,13 @@ int plant_cliques(uint64_t n, uint32_t count, uint32_t smin, uint32_t smax, uint
 }
 
 }  // namespace
+
+namespace g2host {
+int planted_edges(uint64_t n, uint32_t count, uint32_t smin, uint32_t smax, uint64_t seed,
+                  std::vector<uint64_t> &edges) {
+    return plant_cliques(n, count, smin, smax, seed, edges);
+}
+}  // namespace g2host
 
 extern "C" {
 

@@ -108,14 +108,13 @@ __global__ void chunk_offsets_kernel(const uint64_t *new_rp, uint64_t r0, uint64
 
 }  // namespace
 
-cudaError_t recode_device(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint64_t m, const uint32_t *perm,
-                          uint64_t max_chunk, int sms, uint64_t **new_rp, uint32_t **new_ci) {
-    *new_rp = nullptr;
-    *new_ci = nullptr;
-    if (n + 1 > (uint64_t)INT_MAX) return cudaErrorNotSupported;  // the scan counts items in int
+// Sort every row of a CSR whose row pointers (device, n+1) are rp: the rows of
+// `in` are sorted into `out`, in CUB segmented-sort calls of at most max_chunk
+// entries (CUB counts items and segments in int).  A row longer than max_chunk:
+// cudaErrorNotSupported.  Synchronous.
+cudaError_t sort_rows_device(const uint64_t *rp, uint64_t n, uint64_t m, const uint32_t *in, uint32_t *out,
+                             uint64_t max_chunk, int sms) {
     max_chunk = std::min<uint64_t>(std::max<uint64_t>(max_chunk, 1), (uint64_t)INT_MAX);
-    uint64_t *nrp = nullptr, *deg = nullptr;
-    uint32_t *tmp = nullptr, *nci = nullptr;
     int *off = nullptr;
     void *cub_tmp = nullptr;
     size_t cub_bytes = 0, need = 0;
@@ -125,21 +124,9 @@ cudaError_t recode_device(const uint64_t *rp, const uint32_t *ci, uint64_t n, ui
         return e == cudaSuccess;
     };
     const int G = sms * 8;
+    uint32_t *tmp = const_cast<uint32_t *>(in);
+    const uint64_t *nrp = rp;
     std::vector<uint64_t> cuts;  // row boundaries of the sort calls
-    if (!ok(cudaMalloc(&nrp, 8 * (n + 1))) || !ok(cudaMalloc(&deg, 8 * (n + 1))) ||
-        !ok(cudaMalloc(&tmp, 4 * std::max<uint64_t>(m, 1))) || !ok(cudaMalloc(&nci, 4 * std::max<uint64_t>(m, 1))) ||
-        !ok(cudaMemset(deg, 0, 8 * (n + 1))))
-        goto done;
-    recode_degrees_kernel<<<G, 256>>>(rp, perm, n, deg);
-    // exclusive scan: row pointers of the renamed rows (entry n = m)
-    if (!ok(cub::DeviceScan::ExclusiveSum(nullptr, need, deg, nrp, (int)(n + 1)))) goto done;
-    cub_bytes = need;
-    if (!ok(cudaMalloc(&cub_tmp, cub_bytes ? cub_bytes : 16)) ||
-        !ok(cub::DeviceScan::ExclusiveSum(cub_tmp, need, deg, nrp, (int)(n + 1))))
-        goto done;
-    recode_scatter_kernel<<<G, 256>>>(rp, ci, perm, nrp, n, tmp);
-    if (!ok(cudaGetLastError())) goto done;
-    // sort the rows, in calls of at most max_chunk entries
     if (m <= max_chunk) {
         cuts = {0, n};
     } else {
@@ -180,7 +167,7 @@ cudaError_t recode_device(const uint64_t *rp, const uint32_t *ci, uint64_t n, ui
         }
         chunk_offsets_kernel<<<G, 256>>>(nrp, r0, rows, off);
         need = 0;
-        if (!ok(cub::DeviceSegmentedSort::SortKeys(nullptr, need, tmp + base, nci + base, (int)items, (int)rows, off,
+        if (!ok(cub::DeviceSegmentedSort::SortKeys(nullptr, need, tmp + base, out + base, (int)items, (int)rows, off,
                                                     off + 1)))
             goto done;
         if (need > cub_bytes) {
@@ -189,16 +176,54 @@ cudaError_t recode_device(const uint64_t *rp, const uint32_t *ci, uint64_t n, ui
             cub_bytes = need;
             if (!ok(cudaMalloc(&cub_tmp, cub_bytes))) goto done;
         }
-        if (!ok(cub::DeviceSegmentedSort::SortKeys(cub_tmp, need, tmp + base, nci + base, (int)items, (int)rows, off,
+        if (!ok(cub::DeviceSegmentedSort::SortKeys(cub_tmp, need, tmp + base, out + base, (int)items, (int)rows, off,
                                                     off + 1)))
             goto done;
     }
     ok(cudaGetLastError());
     ok(cudaDeviceSynchronize());
 done:
+    cudaFree(off);
+    cudaFree(cub_tmp);
+    return e;
+}
+
+cudaError_t recode_device(const uint64_t *rp, const uint32_t *ci, uint64_t n, uint64_t m, const uint32_t *perm,
+                          uint64_t max_chunk, int sms, uint64_t **new_rp, uint32_t **new_ci) {
+    *new_rp = nullptr;
+    *new_ci = nullptr;
+    if (n + 1 > (uint64_t)INT_MAX) return cudaErrorNotSupported;  // the scan counts items in int
+    max_chunk = std::min<uint64_t>(std::max<uint64_t>(max_chunk, 1), (uint64_t)INT_MAX);
+    uint64_t *nrp = nullptr, *deg = nullptr;
+    uint32_t *tmp = nullptr, *nci = nullptr;
+    void *cub_tmp = nullptr;
+    size_t cub_bytes = 0, need = 0;
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+        return e == cudaSuccess;
+    };
+    const int G = sms * 8;
+    if (!ok(cudaMalloc(&nrp, 8 * (n + 1))) || !ok(cudaMalloc(&deg, 8 * (n + 1))) ||
+        !ok(cudaMalloc(&tmp, 4 * std::max<uint64_t>(m, 1))) || !ok(cudaMalloc(&nci, 4 * std::max<uint64_t>(m, 1))) ||
+        !ok(cudaMemset(deg, 0, 8 * (n + 1))))
+        goto done;
+    recode_degrees_kernel<<<G, 256>>>(rp, perm, n, deg);
+    // exclusive scan: row pointers of the renamed rows (entry n = m)
+    if (!ok(cub::DeviceScan::ExclusiveSum(nullptr, need, deg, nrp, (int)(n + 1)))) goto done;
+    cub_bytes = need;
+    if (!ok(cudaMalloc(&cub_tmp, cub_bytes ? cub_bytes : 16)) ||
+        !ok(cub::DeviceScan::ExclusiveSum(cub_tmp, need, deg, nrp, (int)(n + 1))))
+        goto done;
+    recode_scatter_kernel<<<G, 256>>>(rp, ci, perm, nrp, n, tmp);
+    if (!ok(cudaGetLastError())) goto done;
+    // sort the rows, in calls of at most max_chunk entries
+    if (!ok(sort_rows_device(nrp, n, m, tmp, nci, max_chunk, sms))) goto done;
+    ok(cudaGetLastError());
+    ok(cudaDeviceSynchronize());
+done:
     cudaFree(deg);
     cudaFree(tmp);
-    cudaFree(off);
     cudaFree(cub_tmp);
     if (e != cudaSuccess) {
         cudaFree(nrp);

@@ -1548,3 +1548,7 @@ int g2_set_model(g2_ctx *ctx, const float *params, const float *norm) {
 }
 
 }  // extern "C"
+
+namespace g2rt {
+int g2_after_load(g2_ctx *ctx) { return after_load(ctx); }
+}  // namespace g2rt

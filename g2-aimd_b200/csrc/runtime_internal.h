@@ -100,6 +100,8 @@ namespace g2rt {
 
 // Record a CUDA error in the context; G2_ERR_OOM for allocation failures.
 int fail_cuda(g2_ctx *c, cudaError_t e, const char *where);
+// Per-graph set-up after a new CSR is in the context (forward offsets, ...).
+int g2_after_load(g2_ctx *ctx);
 int fail_cuda_if(g2_ctx *c, cudaError_t e, const char *where);
 
 #define G2_TRY(call)                                             \

@@ -136,6 +136,8 @@ def lib():
         "g2_gen_er": (i32, [u64, C.c_double, u32, u32, u64, P(C.c_void_p), P(C.c_void_p), P(u64), P(u64)]),
         "g2_gen_rmat": (i32, [u32, u32, C.c_double, C.c_double, C.c_double, u32, u32, u32, u64,
                               P(C.c_void_p), P(C.c_void_p), P(u64), P(u64)]),
+        "g2_gen_rmat_device": (i32, [C.c_void_p, u32, u32, C.c_double, C.c_double, C.c_double, u32, u32, u32,
+                                     u64, P(u64)]),
         "g2_gen_chunglu": (i32, [u64, C.c_double, C.c_double, u64, P(C.c_void_p), P(C.c_void_p),
                                  P(u64), P(u64)]),
     }

@@ -273,6 +273,15 @@ class Context:
         self.n = n
         return self
 
+    def gen_rmat(self, scale, edge_factor, a=0.57, b=0.19, c=0.19, planted=0, pmin=0, pmax=0, seed=1):
+        """Build Graph.rmat(...)'s graph on the device as this context's graph
+        (g2_gen_rmat_device); returns its directed entry count m."""
+        m = C.c_uint64()
+        self._check(lib().g2_gen_rmat_device(self._h, scale, edge_factor, a, b, c, planted, pmin, pmax, seed,
+                                             C.byref(m)), "g2_gen_rmat_device")
+        self.graph, self.n, self.m = None, 1 << scale, m.value
+        return m.value
+
     def set_plan(self, plan: Plan):
         self._check(lib().g2_set_plan(self._h, C.byref(plan.raw)), "g2_set_plan")
         return self

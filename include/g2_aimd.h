@@ -545,6 +545,14 @@ int g2_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b,
                 double c, uint32_t nplanted, uint32_t planted_min,
                 uint32_t planted_max, uint64_t seed, uint64_t **row_ptrs,
                 uint32_t **cols, uint64_t *out_n, uint64_t *out_m);
+/* The same seeded R-MAT graph (same rows, planted cliques included) built on
+ * the device straight into the context, as if loaded by g2_load_csr; *m_out
+ * receives its directed entry count.  For scales whose host build is slow
+ * (scale 26, edge factor 28: 3.6 G entries).  scale <= 30.  Test and benchmark
+ * input; no counterpart in the reference, which reads graphs from files. */
+int g2_gen_rmat_device(g2_ctx *ctx, uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+                       uint32_t nplanted, uint32_t planted_min, uint32_t planted_max, uint64_t seed,
+                       uint64_t *m_out);
 int g2_gen_chunglu(uint64_t n, double gamma, double avg_degree, uint64_t seed,
                    uint64_t **row_ptrs, uint32_t **cols, uint64_t *out_n,
                    uint64_t *out_m);

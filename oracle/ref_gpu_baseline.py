@@ -24,6 +24,13 @@ Each run has a time limit; a reference run that does not finish is reported as
 such.  A reference GMatch run that printed a '--- chunk' line retried a chunk
 after a buffer overflow and double counts (its iterationFailed is a no-op), so
 such a count is marked untrusted; so is any run that printed 'Host overflow'.
+A clique count is also marked untrusted when the reference's deepest stored
+level cannot fit its 32-bit record indices (Index = unsigned int,
+common/gpu_env.h:79, used for the buffer tails in system/buffer.h): for a
+k-clique plan that level holds every (k-1)-clique with k-1 vertices each, so
+the (k-1)-clique count of the same graph (an earlier job) times k-1 must stay
+below 2^32; beyond it the tails wrap and records overwrite each other without
+any message.
 """
 import argparse
 import json
@@ -56,6 +63,25 @@ JOBS = [("er2000_k12", "mce"), ("rmat20", "q24"), ("rmat20", "q0"), ("rmat20", "
         ("chunglu18", "mce"), ("chunglu18", "q0")] + \
        [(g, j) for g in ("cl_5k", "cl_50k", "cl_200k") for j in ("mce", "q0", "q1", "q2")] + \
        [("rmat13_k", "mce")]
+
+
+# k-clique preset -> the (k-1)-clique preset whose matches the reference stores
+# at its deepest level, and k - 1
+CLIQUE_PREFIX = {"q24": ("q0", 3), "q25": ("q24", 4)}
+
+
+def index_overflow(results, name, job):
+    """Reason the reference's 32-bit record indices overflow on this job, or None."""
+    if job not in CLIQUE_PREFIX:
+        return None
+    pre, width = CLIQUE_PREFIX[job]
+    for r in results:
+        if r["graph"] == name and r["job"] == pre and r["g2_worker"].get("counts") is not None:
+            entries = r["g2_worker"]["counts"] * width
+            if entries >= 1 << 32:
+                return (f"level-{width} frontier of {entries} entries ({pre} matches x {width}) exceeds the "
+                        "32-bit record indices")
+    return None
 
 
 def parse(out):
@@ -110,6 +136,10 @@ def main():
             args = ["-dg", path, "-q", job[1:], "-m", "1"]
             r = run([ref_run] + args, a.limit)
             o = run([ours] + args, a.limit)
+        why = index_overflow(results, name, job)
+        if why:
+            r["trusted"] = False
+            r["note"] = why
         res = {"graph": name, "make": makers[name][0], "n": g.n, "m": g.m, "job": job, "reference_gpu": r,
                "g2_worker": o}
         print(json.dumps(res), flush=True)
