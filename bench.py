@@ -42,10 +42,6 @@ METRIC = "maximal cliques/s and 4-clique matches/s on 1 B200, learned vs plain s
 UNIT = "4-clique matches/s"
 HIST = 256
 K4 = 24
-# DRAM bytes (read + write) of one main-pass launch of the headline kernel on the
-# default graph (R-MAT s20 ef16, seed 1), from the ncu capture summarised in
-# profiles/match_kernel_k4_rmat_s20.md (dram__bytes_read.sum + dram__bytes_write.sum).
-TRAFFIC_K4_S20 = 859.611648e6 + 655.506176e6
 
 
 def parse():
@@ -58,6 +54,8 @@ def parse():
     ap.add_argument("--edge-factor", type=int, default=16)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-sample-s", type=float, default=12.0, help="target seconds of CPU baseline work")
+    ap.add_argument("--ref-budget-s", type=float, default=300.0,
+                    help="reference arm: projected CPU seconds above which only 1/M of the roots is timed")
     ap.add_argument("--no-extras", action="store_true", help="skip triangle / MCE / e2e / CPU legs")
     ap.add_argument("--scratch-mb", type=int, default=4096, help="device scratch for the DFS slabs")
     ap.add_argument("--fixed", action="store_true",
@@ -351,6 +349,41 @@ def c4_leg(Context, CostModel, Plan, models, local, seed, torch, stream):
     return out
 
 
+def headline_profile():
+    """Figures of the headline kernel's ncu capture committed under profiles/
+    (R-MAT s20 ef16 seed 1, 4-cliques): DRAM bytes per launch and warp
+    instructions per launch."""
+    path = os.path.join(ROOT, "profiles", "match_kernel_k4_rmat_s20.md")
+    out = {"file": "profiles/match_kernel_k4_rmat_s20.md"}
+    try:
+        text = open(path).read()
+    except OSError:
+        return out
+    import re
+    m = re.search(r"DRAM traffic per launch[^|]*\|\s*([0-9.,]+) MB", text)
+    if m:
+        out["traffic"] = float(m.group(1).replace(",", "")) * 1e6
+    m = re.search(r"smsp__inst_executed\.sum\s*\|\s*([0-9.,]+) G", text)
+    if m:
+        out["inst"] = float(m.group(1).replace(",", "")) * 1e9
+    return out
+
+
+def cpu_stride_sample(g, stride, threads):
+    """4-cliques of the roots v % stride == 0 by the CPU restatement of the
+    reference algorithm (oracle/g2_oracle.c), heaviest roots first."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    from g2aimd.context import Plan
+    ids = np.arange(g.n - 1, -1, -1, dtype=np.uint32)
+    roots = ids[ids % stride == 0]
+    orc.match(g, Plan.preset(K4), roots=roots[:64], threads=threads)  # thread pool start
+    t = time.perf_counter()
+    cnt = orc.match(g, Plan.preset(K4), roots=roots, threads=threads)["count"]
+    spent = time.perf_counter() - t
+    return {"value": cnt / spent, "roots": int(roots.size), "seconds": spent, "count": cnt}
+
+
 def cpu_sample(g, target_s, threads, what="k4"):
     """The CPU restatement of the reference algorithm (oracle/g2_oracle.c) on a
     bounded random sample of roots, grown until it takes about target_s.
@@ -376,32 +409,71 @@ def cpu_sample(g, target_s, threads, what="k4"):
     return {"value": cnt / spent, "roots": int(size), "seconds": spent, "count": cnt}
 
 
+def bench_config(a, n, m, world):
+    """The `config` of both arms' lines (identical for the same workload)."""
+    return {"workload": f"rmat-s{a.scale}-ef{a.edge_factor} (a=.57,b=c=.19, seed {a.seed}) degeneracy-ordered: "
+                        "4-clique count (preset 24 plan) over all roots",
+            "graph": {"n": int(n), "m": int(m), "seed": a.seed},
+            "parallelism": f"dp{world} (one graph instance per rank)"}
+
+
 def run_reference(a):
+    """The reference algorithm on the host cores, on the same graph and roots.
+
+    The reference has only a GPU implementation; its CPU restatement
+    (oracle/g2_oracle.c: plan-driven enumeration with the reference planner's
+    plan, all host threads) stands in for it.  The graph is built by the oracle
+    itself (the seeded generator and the kcore-tool recode restated in C), so
+    nothing of the library is loaded.  Timed step i counts the 4-cliques rooted
+    at the vertices v with v % (K * M) == i (heaviest roots first), so the K
+    timed steps together cover every root exactly once when M = 1: the line's
+    value is then the whole graph's count over the whole run's time, the same
+    workload as the GPU arm's.  M > 1 only if the warm-up steps (roots
+    v % 512 == j) project more than --ref-budget-s of CPU time for all roots;
+    the covered fraction 1/M is then reported."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
-    g, _ = make_graph(a.scale, a.edge_factor, a.seed)
-    threads = os.cpu_count() or 1
-    per = max(1.0, a.cpu_sample_s / 2)
-    for _ in range(a.warmup):
-        cpu_sample(g, min(per, 2.0), threads)
-    vals, samp = [], None
+    import math
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
     t0 = time.perf_counter()
-    for _ in range(a.steps):
-        samp = cpu_sample(g, per, threads)
-        vals.append(samp["value"])
-    wall = time.perf_counter() - t0
-    v = float(np.mean(vals))
+    g = orc.degeneracy_recoded(orc.gen_rmat(a.scale, a.edge_factor, 0.57, 0.19, 0.19, seed=a.seed))
+    build_s = time.perf_counter() - t0
+    plan = orc.PresetPlan(K4)
+    threads = os.cpu_count() or 1
+    ids = np.arange(g.n - 1, -1, -1, dtype=np.uint32)  # late (dense-core) roots first
+    spent, frac = 0.0, 0.0
+    for j in range(a.warmup):
+        roots = ids[ids % 512 == j]
+        t = time.perf_counter()
+        orc.match(g, plan, roots=roots, threads=threads)
+        if j or a.warmup == 1:  # the first call also starts the thread pool
+            spent += time.perf_counter() - t
+            frac += roots.size / g.n
+    projected = spent / frac if frac else 0.0
+    M = max(1, math.ceil(projected / a.ref_budget_s)) if projected else 1
+    stride = a.steps * M
+    counts, times = [], []
+    for i in range(a.steps):
+        roots = ids[ids % stride == i]
+        t = time.perf_counter()
+        counts.append(orc.match(g, plan, roots=roots, threads=threads)["count"])
+        times.append(time.perf_counter() - t)
+    total, secs = int(sum(counts)), float(sum(times))
+    v = total / secs
+    cover = "every root once over the timed steps" if M == 1 else f"1/{M} of the roots (v % {stride} < {a.steps})"
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 * wall / a.steps, "higher_is_better": True,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 * secs / a.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"rmat-s{a.scale}-ef{a.edge_factor} degeneracy-ordered, 4-clique (preset 24) "
-                               "count over sampled roots",
-                   "graph": {"n": g.n, "m": g.m, "seed": a.seed}},
+        "config": bench_config(a, g.n, g.m, world),
+        "count": total, "roots_covered": int(np.count_nonzero((ids % stride) < a.steps)),
+        "graph_build_s": round(build_s, 2), "projected_full_s": round(projected, 1),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{samp['roots']} random roots per step (~{per:.0f} s), plan-driven "
-                                   "enumeration with the reference planner's plan (oracle/g2_oracle.c)"},
+                         "sample": f"{cover}: step i takes the roots v % {stride} == i, plan-driven enumeration "
+                                   "with the reference planner's plan (oracle/g2_oracle.c, all host threads; "
+                                   "graph built by the oracle)"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -516,9 +588,17 @@ def run_ours(a):
         step_ms_all, total = step_ms, float(k4)
     value = total / (step_ms_all / 1000.0)
     kern_ms = float(np.mean(pass_ms)) if pass_ms else None
-    plain = float(np.mean(plain_ms))
+    # the plain heuristic schedule with everything else the learned run has
+    # (launch parameters, hand-off, heavy-root splits iff the learned run splits):
+    # the two differ in the schedule alone
+    plain_flags = tuned["flags"] | (0 if tuned["flags"] & 8 else 4)
+    same, _ = timed(lambda: run(schedule="heuristic", **dict(tuned, flags=plain_flags)), max(3, a.steps // 4), 1)
+    plain_same = float(np.mean(same))
     extras = {"schedules": {
-        "plain_heuristic_ms": plain, "learned_ms": step_ms, "learned_vs_plain": plain / step_ms,
+        "plain_heuristic_ms": plain_same, "learned_ms": step_ms, "learned_vs_plain": plain_same / step_ms,
+        "plain_default_launch_ms": float(np.mean(plain_ms)),
+        "note": "learned_vs_plain compares runs that differ in the schedule alone (same launch parameters, "
+                "same splitting); plain_default_launch_ms is the heuristic order with the default launch",
         "tuned": tuned, "tuning_log": [[c, round(t, 3)] for c, t in tlog]}}
     e2e, cpu = None, None
     if not a.no_extras:
@@ -635,32 +715,40 @@ def run_ours(a):
         if world == 1:
             extras["view_bins"] = view_legs(a, g, 2, 1)
         if rank == 0 and world == 1:
-            cs = cpu_sample(g, a.cpu_sample_s, os.cpu_count() or 1)
+            cs = cpu_stride_sample(g, 16, os.cpu_count() or 1)
             cpu = {"value": cs["value"], "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-                   "sample": f"{cs['roots']} random roots of the same graph, {cs['seconds']:.1f} s, plan-driven "
-                             "enumeration with the reference planner's plan (oracle/g2_oracle.c)"}
+                   "sample": f"the {cs['roots']} roots v % 16 == 0 of the same graph (every 16th root in "
+                             f"degeneracy order, heaviest first), {cs['seconds']:.1f} s, plan-driven enumeration "
+                             "with the reference planner's plan (oracle/g2_oracle.c, all host threads)"}
     peak, peak_kind = measured_peak()
     stream_bytes = g.clique_stream_bytes(4)
     achieved = stream_bytes / (kern_ms / 1000.0) / 1e9 if kern_ms else None
+    prof = headline_profile() if (a.scale, a.edge_factor, a.seed) == (20, 16, 1) else {}
+    csum = clk.summary()
+    issue = None
+    if prof.get("inst") and kern_ms and csum.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        slots = sms * 4 * csum["sm_mhz"] * 1e6 * (kern_ms / 1000.0)  # warp-instruction issue slots
+        issue = {"warp_instructions": prof["inst"], "issue_slots": slots, "frac": prof["inst"] / slots,
+                 "source": prof["file"] + " (instructions per launch, ncu); kernel time and SM clock live"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": step_ms_all, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"rmat-s{a.scale}-ef{a.edge_factor} (a=.57,b=c=.19) degeneracy-ordered: "
-                                   "4-clique count (preset 24 plan) over all roots, learned schedule "
-                                   "(cost-model order + heavy-root splits, autotuned launch parameters)",
-                       "graph": {"n": g.n, "m": g.m, "seed": a.seed, "gen_s": round(gen_s, 2)},
-                       "k4_matches": k4, "l2": "512 MiB flush before every timed step",
-                       "parallelism": f"dp{world} (one graph instance per rank)"},
+            "config": bench_config(a, g.n, g.m, world),
+            "count": k4, "schedule": "learned (cost-model order, autotuned launch parameters)",
+            "l2_flush": "512 MiB written before every timed step", "graph_gen_s": round(gen_s, 2),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
-                         "traffic": TRAFFIC_K4_S20 if (a.scale, a.edge_factor, a.seed) == (20, 16, 1) else None,
-                         "kernel": "match_kernel<1,0> (clique bitmap path), main pass", "kernel_ms": kern_ms,
+                         "traffic": prof.get("traffic"),
+                         "kernel": "match_kernel<1,0,6> (clique bitmap path), main pass", "kernel_ms": kern_ms,
                          "algorithmic_bytes": stream_bytes, "peak_kind": peak_kind,
+                         "binding": "instruction issue (see issue.frac); the HBM fraction is far from binding",
+                         "issue": issue,
                          "merge_model_bytes": work_bytes,
                          "merge_model_gbs": work_bytes / (kern_ms / 1000.0) / 1e9 if kern_ms else None},
-            "clocks": clk.summary(), "gpu_launches": int(launches_per_step * a.steps),
+            "clocks": csum, "gpu_launches": int(launches_per_step * a.steps),
             "e2e": e2e, "cpu_baseline": cpu, "extras": extras,
         }
         print(json.dumps(line), flush=True)

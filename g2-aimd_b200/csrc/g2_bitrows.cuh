@@ -212,6 +212,155 @@ __device__ __noinline__ static unsigned long long count_forward_edges(const uint
     return warp_sum_u64(c);
 }
 
+// ---------------------------------------------------------------------------
+// Membership filter of P0 (clique plans).  About 90 % of the forward-list
+// entries a row build scans are not in P0 (on R-MAT s20, 4.2e8 hits in 4.5e9
+// scanned entries), so a one-bit-per-hash filter in shared memory rejects most
+// of them with one shared load before any search; only filter hits binary-search
+// P0, which then stays in global memory (the root's own CSR slice, L1-resident).
+// The filter uses 2^fb bits, fb = log2 of about 32 bits per member (at most the
+// space given), so its false-positive rate is at most ~3 % for small P0 and
+// p / 2^fb for the largest.
+struct P0Filter {
+    const uint32_t *bits;
+    uint32_t shift;  // slot = (y * kFilterMul) >> shift
+};
+constexpr uint32_t kFilterMul = 0x9E3779B1u;  // Fibonacci hashing
+
+__device__ __forceinline__ P0Filter filter_build(uint32_t *bits, uint32_t max_words, const uint32_t *P0, uint32_t p) {
+    const uint32_t lane = lane_id();
+    uint32_t fb = 10;  // at least 1024 bits
+    while (fb < 31 && (1u << fb) < 32u * p && (1u << (fb + 1)) <= 32u * max_words) fb++;
+    const uint32_t words = 1u << (fb - 5), shift = 32u - fb;
+    for (uint32_t w = lane; w < words; w += 32) bits[w] = 0u;
+    __syncwarp();
+    for (uint32_t i = lane; i < p; i += 32) {
+        const uint32_t h = (ldg(P0 + i) * kFilterMul) >> shift;
+        atomicOr(bits + (h >> 5), 1u << (h & 31u));
+    }
+    __syncwarp();
+    return P0Filter{bits, shift};
+}
+
+__device__ __forceinline__ bool filter_maybe(const P0Filter &f, uint32_t y) {
+    const uint32_t h = (y * kFilterMul) >> f.shift;
+    return (f.bits[h >> 5] >> (h & 31u)) & 1u;
+}
+
+// First index in [lo, hi) of the global array a with a[i] >= key.
+__device__ __forceinline__ uint32_t gmem_lower_bound(const uint32_t *a, uint32_t lo, uint32_t hi, uint32_t key) {
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (ldg(a + mid) < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Upper adjacency rows of P0 (row i = bits j > i with P0[j] in N+(P0[i])), as
+// build_forward_rows(..., symmetric = false) builds them, with P0 = the root's
+// forward slice in global memory and the filter in `fbits` (fwords words of
+// shared memory).  One lane per row; forward lists longer than long_list are
+// scanned by the whole warp (coalesced) into rowbuf.
+__device__ __noinline__ static void build_upper_rows_filtered(const uint64_t *rp, const uint32_t *ci,
+                                                              const uint32_t *fo, const uint32_t *P0, uint32_t p,
+                                                              uint32_t W, uint32_t *A, uint32_t *rowbuf,
+                                                              uint32_t *fbits, uint32_t fwords, uint32_t long_list) {
+    const uint32_t lane = lane_id();
+    const uint32_t pmax = ldg(P0 + p - 1);
+    for (uint32_t i = lane; i < p; i += 32)
+        for (uint32_t w = i >> 5; w < W; w++) A[(uint64_t)i * W + w] = 0u;
+    const P0Filter f = filter_build(fbits, fwords, P0, p);
+    for (uint32_t i0 = 0; i0 < p; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        bool big = false;
+        if (i < p) {
+            const uint32_t u = ldg(P0 + i);
+            uint64_t e = ldg(rp + u) + ldg(fo + u);
+            const uint64_t end = ldg(rp + u + 1);
+            if (end - e > long_list) big = true;
+            else {
+                uint32_t *row = A + (uint64_t)i * W;
+                uint32_t j = i + 1;
+                for (; e < end; e++) {
+                    const uint32_t y = ldg(ci + e);
+                    if (y > pmax) break;
+                    if (!filter_maybe(f, y)) continue;
+                    j = gmem_lower_bound(P0, j, p, y);
+                    if (j < p && ldg(P0 + j) == y) row[j >> 5] |= 1u << (j & 31u);
+                }
+            }
+        }
+        uint32_t bigmask = __ballot_sync(G2_FULL, big);
+        while (bigmask) {
+            const uint32_t l = __ffs(bigmask) - 1;
+            bigmask &= bigmask - 1;
+            const uint32_t ii = i0 + l;
+            const uint32_t u = ldg(P0 + ii);
+            const uint64_t e0 = ldg(rp + u) + ldg(fo + u), end = ldg(rp + u + 1);
+            for (uint32_t w = lane; w < W; w += 32) rowbuf[w] = 0u;
+            __syncwarp();
+            for (uint64_t e = e0 + lane; e < end; e += 32) {
+                const uint32_t y = ldg(ci + e);
+                if (y > pmax) break;
+                if (!filter_maybe(f, y)) continue;
+                const uint32_t j = gmem_lower_bound(P0, ii + 1, p, y);
+                if (j < p && ldg(P0 + j) == y) atomicOr(rowbuf + (j >> 5), 1u << (j & 31u));
+            }
+            __syncwarp();
+            for (uint32_t w = (ii >> 5) + lane; w < W; w += 32) A[(uint64_t)ii * W + w] = rowbuf[w];
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+}
+
+// count_forward_edges with P0 in global memory and the filter in fbits.
+__device__ __noinline__ static unsigned long long count_forward_edges_filtered(
+    const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, const uint32_t *P0, uint32_t p, uint32_t part,
+    uint32_t nparts, uint32_t *fbits, uint32_t fwords) {
+    const uint32_t lane = lane_id();
+    const uint32_t pmax = ldg(P0 + p - 1);
+    const P0Filter f = filter_build(fbits, fwords, P0, p);
+    unsigned long long c = 0;
+    for (uint32_t i0 = 0; i0 < p; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        bool big = false;
+        if (i < p && (nparts <= 1 || i % nparts == part)) {
+            const uint32_t u = ldg(P0 + i);
+            uint64_t e = ldg(rp + u) + ldg(fo + u);
+            const uint64_t end = ldg(rp + u + 1);
+            if (end - e > kLongListMatch) big = true;
+            else {
+                uint32_t j = i + 1;
+                for (; e < end; e++) {
+                    const uint32_t y = ldg(ci + e);
+                    if (y > pmax) break;
+                    if (!filter_maybe(f, y)) continue;
+                    j = gmem_lower_bound(P0, j, p, y);
+                    c += j < p && ldg(P0 + j) == y;
+                }
+            }
+        }
+        uint32_t bigmask = __ballot_sync(G2_FULL, big);
+        while (bigmask) {
+            const uint32_t l = __ffs(bigmask) - 1;
+            bigmask &= bigmask - 1;
+            const uint32_t ii = i0 + l;
+            const uint32_t u = ldg(P0 + ii);
+            const uint64_t e0 = ldg(rp + u) + ldg(fo + u), end = ldg(rp + u + 1);
+            for (uint64_t e = e0 + lane; e < end; e += 32) {
+                const uint32_t y = ldg(ci + e);
+                if (y > pmax) break;
+                if (!filter_maybe(f, y)) continue;
+                const uint32_t j = gmem_lower_bound(P0, ii + 1, p, y);
+                c += j < p && ldg(P0 + j) == y;
+            }
+        }
+    }
+    return warp_sum_u64(c);
+}
+
 // B rows of the root's backward neighbours X0 = ci[lo, lo+nx) (ids < v):
 // row = N+(x) ∩ P0.  Only non-zero rows are kept, compacted in X0 order into
 // B (nb rows of W words); xv (optional) receives the vertex of each kept row.

@@ -388,21 +388,24 @@ __device__ bool match_root_clique(const MatchArgs &a, const DevPlan &pl, uint32_
     // slab: [A p*W] [frames (k) * (W + 1)]
     const uint64_t a0 = 0, f0 = (uint64_t)p * W;
     if (f0 + (uint64_t)k * (W + 1) > a.words_per_warp) return false;
-    for (uint32_t i = lane; i < p; i += 32) p0s[i] = ldg(ci + split + i);
-    __syncwarp();
+    // k <= 5 without metrics: P0 stays in global memory (the root's CSR slice)
+    // and its shared-memory region holds the membership filter instead
+    const uint32_t *P0 = ci + split;
     if (!METRICS && k == 3) {  // triangles: count forward-neighbourhood edges while scanning
-        count = count_forward_edges(rp, ci, a.fo, p0s, p, part, nparts);
+        count = count_forward_edges_filtered(rp, ci, a.fo, P0, p, part, nparts, p0s, 1024u * WPL);
         return true;
     }
     if (!METRICS && k <= 5) {
         // lane-parallel counting: lane takes the depth-1 vertices x = lane, lane+32, ...
         // (in ordinal order, so the split filter is x % nparts) and counts the
         // (k-2)-cliques above x serially; it reads only the upper part of rows.
-        build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf, false, kLongListMatch);
+        build_upper_rows_filtered(rp, ci, a.fo, P0, p, W, S + a0, rowbuf, p0s, 1024u * WPL, kLongListMatch);
         __syncwarp();
         count = clique_count_lanes(S + a0, p, W, k, part, nparts);
         return true;
     }
+    for (uint32_t i = lane; i < p; i += 32) p0s[i] = ldg(ci + split + i);
+    __syncwarp();
     build_forward_rows(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf, true, kLongListMatch);
     __syncwarp();
     // C = remaining candidates at the current depth; depth = vertices chosen (v included)
