@@ -85,6 +85,51 @@ __device__ __forceinline__ uint32_t smem_lower_bound(const uint32_t *a, uint32_t
     return lo;
 }
 
+// ---------------------------------------------------------------------------
+// Membership filter of P0 (clique plans).  About 90 % of the forward-list
+// entries a row build scans are not in P0 (on R-MAT s20, 4.2e8 hits in 4.5e9
+// scanned entries), so a one-bit-per-hash filter in shared memory rejects most
+// of them with one shared load before any search; only filter hits binary-search
+// P0, which then stays in global memory (the root's own CSR slice, L1-resident).
+// The filter uses 2^fb bits, fb = log2 of about 32 bits per member (at most the
+// space given), so its false-positive rate is at most ~3 % for small P0 and
+// p / 2^fb for the largest.
+struct P0Filter {
+    const uint32_t *bits;
+    uint32_t shift;  // slot = (y * kFilterMul) >> shift
+};
+constexpr uint32_t kFilterMul = 0x9E3779B1u;  // Fibonacci hashing
+
+__device__ __forceinline__ P0Filter filter_build(uint32_t *bits, uint32_t max_words, const uint32_t *P0, uint32_t p) {
+    const uint32_t lane = lane_id();
+    uint32_t fb = 10;  // at least 1024 bits
+    while (fb < 31 && (1u << fb) < 32u * p && (1u << (fb + 1)) <= 32u * max_words) fb++;
+    const uint32_t words = 1u << (fb - 5), shift = 32u - fb;
+    for (uint32_t w = lane; w < words; w += 32) bits[w] = 0u;
+    __syncwarp();
+    for (uint32_t i = lane; i < p; i += 32) {
+        const uint32_t h = (ldg(P0 + i) * kFilterMul) >> shift;
+        atomicOr(bits + (h >> 5), 1u << (h & 31u));
+    }
+    __syncwarp();
+    return P0Filter{bits, shift};
+}
+
+__device__ __forceinline__ bool filter_maybe(const P0Filter &f, uint32_t y) {
+    const uint32_t h = (y * kFilterMul) >> f.shift;
+    return (f.bits[h >> 5] >> (h & 31u)) & 1u;
+}
+
+// First index in [lo, hi) of the global array a with a[i] >= key.
+__device__ __forceinline__ uint32_t gmem_lower_bound(const uint32_t *a, uint32_t lo, uint32_t hi, uint32_t key) {
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (ldg(a + mid) < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
 // Forward lists longer than this are scanned by the whole warp (coalesced, one
 // row at a time) instead of by their row's lane.  The lane loop runs as long as
 // the warp's longest list, so a lower bound balances lanes better; the walks of
@@ -102,9 +147,12 @@ constexpr uint32_t kLongListMatch = 32;
 // transpose, added 32x32 tile by tile.
 // With symmetric = false only the upper part of each row (words from i / 32
 // on, bits j > i) is built: enough for walks that only look above the row.
+// With a filter (flt.bits non-null) an entry is binary-searched only if the
+// filter admits it.
 __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo,
                                    const uint32_t *p0s, uint32_t p, uint32_t W, uint32_t *A, uint32_t *rowbuf,
-                                   bool symmetric = true, uint32_t long_list = kLongList) {
+                                   bool symmetric = true, uint32_t long_list = kLongList,
+                                   P0Filter flt = P0Filter{nullptr, 0}) {
     const uint32_t lane = lane_id();
     const uint32_t pmax = p0s[p - 1];
     if (symmetric)
@@ -127,6 +175,7 @@ __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const
                 for (; e < end; e++) {
                     const uint32_t y = ldg(ci + e);
                     if (y > pmax) break;
+                    if (flt.bits && !filter_maybe(flt, y)) continue;
                     j = smem_lower_bound(p0s, j, p, y);
                     if (j < p && p0s[j] == y) row[j >> 5] |= 1u << (j & 31u);
                 }
@@ -144,6 +193,7 @@ __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const
             for (uint64_t e = e0 + lane; e < end; e += 32) {
                 const uint32_t y = ldg(ci + e);
                 if (y > pmax) break;
+                if (flt.bits && !filter_maybe(flt, y)) continue;
                 const uint32_t j = smem_lower_bound(p0s, ii + 1, p, y);
                 if (j < p && p0s[j] == y) atomicOr(rowbuf + (j >> 5), 1u << (j & 31u));
             }
@@ -210,51 +260,6 @@ __device__ __noinline__ static unsigned long long count_forward_edges(const uint
         }
     }
     return warp_sum_u64(c);
-}
-
-// ---------------------------------------------------------------------------
-// Membership filter of P0 (clique plans).  About 90 % of the forward-list
-// entries a row build scans are not in P0 (on R-MAT s20, 4.2e8 hits in 4.5e9
-// scanned entries), so a one-bit-per-hash filter in shared memory rejects most
-// of them with one shared load before any search; only filter hits binary-search
-// P0, which then stays in global memory (the root's own CSR slice, L1-resident).
-// The filter uses 2^fb bits, fb = log2 of about 32 bits per member (at most the
-// space given), so its false-positive rate is at most ~3 % for small P0 and
-// p / 2^fb for the largest.
-struct P0Filter {
-    const uint32_t *bits;
-    uint32_t shift;  // slot = (y * kFilterMul) >> shift
-};
-constexpr uint32_t kFilterMul = 0x9E3779B1u;  // Fibonacci hashing
-
-__device__ __forceinline__ P0Filter filter_build(uint32_t *bits, uint32_t max_words, const uint32_t *P0, uint32_t p) {
-    const uint32_t lane = lane_id();
-    uint32_t fb = 10;  // at least 1024 bits
-    while (fb < 31 && (1u << fb) < 32u * p && (1u << (fb + 1)) <= 32u * max_words) fb++;
-    const uint32_t words = 1u << (fb - 5), shift = 32u - fb;
-    for (uint32_t w = lane; w < words; w += 32) bits[w] = 0u;
-    __syncwarp();
-    for (uint32_t i = lane; i < p; i += 32) {
-        const uint32_t h = (ldg(P0 + i) * kFilterMul) >> shift;
-        atomicOr(bits + (h >> 5), 1u << (h & 31u));
-    }
-    __syncwarp();
-    return P0Filter{bits, shift};
-}
-
-__device__ __forceinline__ bool filter_maybe(const P0Filter &f, uint32_t y) {
-    const uint32_t h = (y * kFilterMul) >> f.shift;
-    return (f.bits[h >> 5] >> (h & 31u)) & 1u;
-}
-
-// First index in [lo, hi) of the global array a with a[i] >= key.
-__device__ __forceinline__ uint32_t gmem_lower_bound(const uint32_t *a, uint32_t lo, uint32_t hi, uint32_t key) {
-    while (lo < hi) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (ldg(a + mid) < key) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
 }
 
 // Upper adjacency rows of P0 (row i = bits j > i with P0[j] in N+(P0[i])), as
@@ -367,7 +372,8 @@ __device__ __noinline__ static unsigned long long count_forward_edges_filtered(
 // Returns nb, or ~0u if more than cap rows would be needed.
 __device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, uint32_t v,
                                     uint64_t lo, uint32_t nx, const uint32_t *p0s, uint32_t p, uint32_t W,
-                                    uint32_t *B, uint32_t *xv, uint32_t cap, uint32_t *rowbuf) {
+                                    uint32_t *B, uint32_t *xv, uint32_t cap, uint32_t *rowbuf,
+                                    P0Filter flt = P0Filter{nullptr, 0}) {
     const uint32_t lane = lane_id();
     const uint32_t pmin = p0s[0], pmax = p0s[p - 1];
     uint32_t nb = 0;
@@ -388,6 +394,7 @@ __device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, cons
                 for (uint64_t f = e; f < end; f++) {
                     const uint32_t y = ldg(ci + f);
                     if (y > pmax) break;
+                    if (flt.bits && !filter_maybe(flt, y)) continue;
                     j = smem_lower_bound(p0s, j, p, y);
                     if (j < p && p0s[j] == y) {
                         hit = true;
@@ -413,7 +420,7 @@ __device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, cons
                 const uint32_t y = f < b1 ? ldg(ci + f) : 0xffffffffu;
                 const bool inr = f < b1 && y <= pmax;
                 bool found = false;
-                if (inr) {
+                if (inr && (!flt.bits || filter_maybe(flt, y))) {
                     const uint32_t j = smem_lower_bound(p0s, 0, p, y);
                     found = j < p && p0s[j] == y;
                 }
@@ -438,6 +445,7 @@ __device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, cons
             for (uint64_t f = e; f < end; f++) {
                 const uint32_t y = ldg(ci + f);
                 if (y > pmax) break;
+                if (flt.bits && !filter_maybe(flt, y)) continue;
                 j = smem_lower_bound(p0s, j, p, y);
                 if (j < p && p0s[j] == y) row[j >> 5] |= 1u << (j & 31u);
             }
@@ -458,6 +466,7 @@ __device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, cons
             for (uint64_t f = s + lane; f < b1; f += 32) {
                 const uint32_t y = ldg(ci + f);
                 if (y > pmax) break;
+                if (flt.bits && !filter_maybe(flt, y)) continue;
                 const uint32_t j = smem_lower_bound(p0s, 0, p, y);
                 if (j < p && p0s[j] == y) atomicOr(rowbuf + (j >> 5), 1u << (j & 31u));
             }

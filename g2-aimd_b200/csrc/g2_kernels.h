@@ -17,6 +17,7 @@ constexpr int kStatusHistOverflow = 2;   // clique larger than the histogram
 constexpr int kStatusStackOverflow = 4;  // GMatch candidate stack exhausted
 constexpr int kStatusBadPlan = 8;        // plan arrays inconsistent
 constexpr int kStatusWaitLimit = 16;     // a bounded device wait ran out
+constexpr int kStatusDeadline = 32;      // the run's time budget ran out (MCE)
 
 // An MCE pass entry with this bit set is a spilled record id, else a task id.
 constexpr uint32_t kRecordBit = 0x80000000u;
@@ -64,6 +65,8 @@ struct MceArgs {
     uint32_t epoch;                 // ready word of records published in this run (read from epoch_dev)
     const uint32_t *epoch_dev;      // the run's epoch, bumped on the device at the run's start
     uint64_t wait_cycles;           // longest wait of a warp for its ticket's record
+    const unsigned long long *deadline;  // optional: %globaltimer (ns) past which roots are
+                                         // dropped (set on the device by deadline_set)
 };
 constexpr int kQHead = 0, kQOut = 1;
 constexpr uint32_t kMatchRecordWords = 32;  // stride of a plan-walk record
@@ -77,6 +80,8 @@ cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_bloc
 // never-published ready word), so runs captured in a CUDA graph stay distinct
 // when the graph is replayed.
 cudaError_t epoch_bump(uint32_t *epoch_dev, cudaStream_t st);
+// *deadline = the device's %globaltimer now + budget_ns, in stream order.
+cudaError_t deadline_set(unsigned long long *deadline, unsigned long long budget_ns, cudaStream_t st);
 
 // Plan in device-friendly form: everything by POSITION.
 struct DevPlan {

@@ -318,6 +318,20 @@ __device__ __noinline__ bool spill_all(const MceArgs &a, uint32_t task, uint32_t
 
 enum : int { kTaskDone = 0, kTaskDeferred = 1 };
 
+// Shared-memory words per warp of the P0 membership filter used while a root's
+// rows are built (16384 bits: a false-positive rate of p / 16384).
+constexpr uint32_t kMceFilterWords = 512;
+
+// Has the run's time budget (MceArgs::deadline, %globaltimer ns) run out?
+// Warp-uniform.
+__device__ __forceinline__ bool deadline_passed(const MceArgs &a) {
+    if (!a.deadline) return false;
+    unsigned long long now = 0;
+    if (lane_id() == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    now = __shfl_sync(G2_FULL, now, 0);
+    return now > *a.deadline;
+}
+
 // Run one entry: a root task (entry < 2^31) or a handed-off record (entry has
 // kRecordBit set).  With METRICS the work model W (in 4-byte words) of the
 // reference's tree is accumulated: per node with P ∪ X non-empty,
@@ -389,14 +403,15 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
         const uint64_t xv0 = a0 + (uint64_t)p * W;
         const uint64_t b0 = xv0 + (METRICS ? nx : 0);
         if (fr0 < b0 + 64) return kTaskDeferred;
-        // stage P0 in shared memory, then the rows
+        // stage P0 in shared memory and its membership filter, then the rows
         for (uint32_t i = lane; i < p; i += 32) cand[i] = ldg(ci + split + i);
-        __syncwarp();
-        build_forward_rows(rp, ci, a.fo, cand, p, W, S + a0, rowbuf);
+        const P0Filter flt = filter_build(rowbuf + 32u * WPL, kMceFilterWords, ci + split, p);
+        build_forward_rows(rp, ci, a.fo, cand, p, W, S + a0, rowbuf, true, kLongList, flt);
         // kept B rows plus their root-list entries must stay below the frames
         const uint64_t cap64 = (fr0 - b0 - 64) / (W + 1);
         const uint32_t cap = cap64 > 0xfffffff0ull ? 0xfffffff0u : (uint32_t)cap64;
-        nb = build_back_rows(rp, ci, a.fo, v, lo, nx, cand, p, W, S + b0, METRICS ? S + xv0 : nullptr, cap, rowbuf);
+        nb = build_back_rows(rp, ci, a.fo, v, lo, nx, cand, p, W, S + b0, METRICS ? S + xv0 : nullptr, cap, rowbuf,
+                             flt);
         if (nb == ~0u) return kTaskDeferred;
         __syncwarp();
         rows.A = S + a0;
@@ -451,7 +466,7 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
     uint32_t d = 0;  // depth below the entry node
     unsigned long long nodes = 0, cliques = 0, work = 0;
     bool enter = true;
-    bool overflow = false, spilled = false;
+    bool overflow = false, spilled = false, expired = false;
     bool donated = false;  // some branches went to records: the entry can no longer be re-run
     bool may_spill = a.spill_cycles != 0 && nparts == 1 && W <= a.rec_words;
     long long next_check = (long long)a.spill_cycles;
@@ -459,6 +474,10 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
         bool want_pop = false;
         if (enter) {
             enter = false;
+            if (a.deadline && (nodes & 255u) == 0 && deadline_passed(a)) {  // time budget: drop the root
+                expired = true;
+                break;
+            }
             const bool own = d >= D || part == 0;  // this part counts the node
             const bool at_root = !is_rec && d == 0;
             if (own) nodes++;
@@ -654,6 +673,11 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
         }
         __syncwarp();
     }
+    if (expired) {  // nothing of this entry is committed (deadline runs never hand off)
+        if (lane == 0) atomicOr(a.status, kStatusDeadline);
+        __syncwarp();
+        return kTaskDone;
+    }
     if (overflow && !spilled) {
         if (!donated) return kTaskDeferred;  // re-run from scratch by a pass with a bigger slab
         if (lane == 0) atomicOr(a.status, kStatusDeferOverflow);  // record buffers full: incomplete
@@ -699,8 +723,8 @@ __global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
     extern __shared__ uint32_t smem[];
     if (a.epoch_dev) a.epoch = *a.epoch_dev;
     const uint32_t wib = threadIdx.x >> 5;
-    uint32_t *cand = smem + wib * (32u * 32u * WPL + 32u * WPL);
-    uint32_t *rowbuf = cand + 32u * 32u * WPL;
+    uint32_t *cand = smem + wib * (32u * 32u * WPL + 32u * WPL + kMceFilterWords);
+    uint32_t *rowbuf = cand + 32u * 32u * WPL;  // then the P0 filter (kMceFilterWords)
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t *S = a.scratch + gw * a.words_per_warp;
     const bool handoff = a.spill_cycles != 0;
@@ -717,8 +741,13 @@ __global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
             break;
         }
         const unsigned long long t1 = t0 + a.chunk < n ? t0 + a.chunk : n;
-        for (unsigned long long t = t0; t < t1; t++)
+        for (unsigned long long t = t0; t < t1; t++) {
+            if (deadline_passed(a)) {  // time budget spent: start no new root
+                if (lane_id() == 0) atomicOr(a.status, kStatusDeadline);
+                continue;
+            }
             run_entry<WPL, METRICS>(a, a.task_index ? a.task_index[t] : (uint32_t)t, S, cand, rowbuf);
+        }
         outstanding_add(a, handoff, -1);
     }
     if (handoff)
@@ -730,7 +759,7 @@ __global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
 }  // namespace
 
 size_t mce_smem_bytes(int wpl, int warps_per_block) {
-    return (size_t)warps_per_block * (32u * 32u * wpl + 32u * wpl) * sizeof(uint32_t);
+    return (size_t)warps_per_block * (32u * 32u * wpl + 32u * wpl + kMceFilterWords) * sizeof(uint32_t);
 }
 
 template <int WPL, bool M>
@@ -767,6 +796,17 @@ __global__ void epoch_bump_kernel(uint32_t *e) {
 
 cudaError_t epoch_bump(uint32_t *epoch_dev, cudaStream_t st) {
     epoch_bump_kernel<<<1, 1, 0, st>>>(epoch_dev);
+    return cudaGetLastError();
+}
+
+__global__ void deadline_set_kernel(unsigned long long *d, unsigned long long budget_ns) {
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    *d = now + budget_ns;
+}
+
+cudaError_t deadline_set(unsigned long long *deadline, unsigned long long budget_ns, cudaStream_t st) {
+    deadline_set_kernel<<<1, 1, 0, st>>>(deadline, budget_ns);
     return cudaGetLastError();
 }
 

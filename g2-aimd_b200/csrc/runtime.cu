@@ -386,6 +386,7 @@ int ensure_handoff(g2_ctx *ctx, cudaStream_t st) {
 int ensure_counters(g2_ctx *ctx) {
     if (!ctx->d_ctr) G2_TRY(cudaMalloc(&ctx->d_ctr, sizeof(unsigned long long) * kCtrWords));
     if (!ctx->d_status) G2_TRY(cudaMalloc(&ctx->d_status, sizeof(int)));
+    if (!ctx->d_deadline) G2_TRY(cudaMalloc(&ctx->d_deadline, sizeof(unsigned long long)));
     return G2_OK;
 }
 
@@ -399,6 +400,7 @@ int status_to_code(int st) {
     if (st & g2::kStatusBadPlan) return G2_ERR_INVALID;
     if (st & g2::kStatusHistOverflow) return G2_ERR_HIST;
     if (st & g2::kStatusWaitLimit) return G2_ERR_TIMEOUT;
+    if (st & g2::kStatusDeadline) return G2_ERR_DEADLINE;
     return G2_OK;
 }
 
@@ -528,7 +530,10 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     if (rc) return rc;
     if (ctx->max_fwd > 32u * 32u * 8u) return G2_ERR_UNSUPPORTED;
     const uint32_t flags = o ? o->flags : 0u;
-    const bool spill = !(flags & G2_FLAG_NO_SPILL);
+    const uint32_t deadline_ms = o ? o->deadline_ms : 0u;
+    // a run with a time budget drops unfinished roots whole, which needs every
+    // root walked by one warp: no hand-off
+    const bool spill = !(flags & G2_FLAG_NO_SPILL) && !deadline_ms;
     if (spill) {
         rc = ensure_handoff(ctx, st);
         if (rc) return rc;
@@ -578,6 +583,12 @@ int mce_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned long
     base.qctl = ctx->d_ctr + kCtrQueue;
     base.epoch_dev = spill ? ctx->d_epoch : nullptr;
     base.wait_cycles = (o && o->wait_cycles) ? o->wait_cycles : kWaitCycles;
+    if (deadline_ms) {
+        cudaError_t e = g2::deadline_set(ctx->d_deadline, 1000000ull * deadline_ms, st);
+        if (e != cudaSuccess) return fail_cuda(ctx, e, "deadline_set");
+        ctx->launches++;
+        base.deadline = ctx->d_deadline;
+    }
     if (ctx->timed) G2_TRY(cudaEventRecord(ctx->ev[0], st));
     L2Window l2(ctx, st, flags);
     {  // main pass: every task, WPL=1, one slab per resident warp; long walks
@@ -798,6 +809,7 @@ const char *g2_strerror(int code) {
         case G2_ERR_UNSUPPORTED: return "unsupported size";
         case G2_ERR_IO: return "I/O error";
         case G2_ERR_HIST: return "clique larger than the histogram";
+        case G2_ERR_DEADLINE: return "time budget ran out (outputs hold the roots that finished)";
         default: return "unknown error";
     }
 }
@@ -997,7 +1009,7 @@ int g2_close(g2_ctx *ctx) {
                     ctx->d_roots,  ctx->d_S,       ctx->d_part,    ctx->d_xroots, ctx->d_xparts,     ctx->d_cost,
                     ctx->d_total,  ctx->d_ntask,   ctx->d_cub,     ctx->d_model,  ctx->d_work,
                     ctx->d_feat,   ctx->d_rec,     ctx->d_pool,    ctx->d_ready,  ctx->d_goff,    ctx->d_fwdmax,
-                    ctx->d_epoch,
+                    ctx->d_epoch,  ctx->d_deadline,
                     ctx->d_root_cliques, ctx->d_gcount};
     for (void *b : bufs)
         if (b) cudaFree(b);

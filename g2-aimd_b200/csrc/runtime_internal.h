@@ -44,6 +44,7 @@ struct g2_ctx {
     uint32_t *d_epoch = nullptr;          // epoch of the current run (bumped on the device)
     uint32_t *d_pool = nullptr;           // MCE spill row pool
     int *d_status = nullptr;
+    unsigned long long *d_deadline = nullptr;  // %globaltimer ns of a run's time budget
     unsigned long long *d_out = nullptr;  // counters for the host entry points
     uint64_t out_cap = 0;
     // schedule

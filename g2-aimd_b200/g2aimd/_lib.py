@@ -43,6 +43,7 @@ class G2Opts(C.Structure):
         ("root_nodes", P(u64)), ("work_bytes", P(u64)),
         ("intersect_mode", u32), ("flags", u32), ("split_depth", u32), ("root_cost", P(u64)),
         ("chunk", u32), ("spill_kcycles", u32), ("ctas_per_sm", u32), ("wait_cycles", u32),
+        ("deadline_ms", u32),
     ]
 
 

@@ -85,8 +85,9 @@ class Plan:
 
 def _opts(warps_per_block=0, blocks=0, schedule="given", scores=None, root_nodes=None, intersect_mode=0,
           granularity=0, chunk=0, flags=0, work_bytes=None, root_cost=None, split=False, split_depth=0,
-          spill_kcycles=0, ctas_per_sm=0, wait_cycles=0):
+          spill_kcycles=0, ctas_per_sm=0, wait_cycles=0, deadline_ms=0):
     o = G2Opts()
+    o.deadline_ms = deadline_ms
     o.wait_cycles = wait_cycles
     o.ctas_per_sm = ctas_per_sm
     o.split_depth = split_depth
@@ -112,6 +113,9 @@ def _opts(warps_per_block=0, blocks=0, schedule="given", scores=None, root_nodes
     return o, keep
 
 
+G2_ERR_DEADLINE = -11
+
+
 class Context:
     """One device context (g2_open).  Load a graph, then run enumerations."""
 
@@ -120,6 +124,7 @@ class Context:
         check(lib().g2_open(device, scratch_bytes, C.byref(self._h)), "g2_open")
         self.graph = None
         self.n = 0
+        self.expired = False  # the last MCE run's time budget (deadline_ms) ran out
 
     def close(self):
         if self._h:
@@ -292,13 +297,17 @@ class Context:
         uint64 array passed as root_cost receives SM cycles per source."""
         src = None if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
         nsrc = 0 if src is None else src.size
-        rn = np.zeros(nsrc if src is not None else self.graph.n, np.uint64) if root_nodes else None
+        rn = np.zeros(nsrc if src is not None else self.n, np.uint64) if root_nodes else None
         o, keep = _opts(root_nodes=rn, root_cost=root_cost, **kw)
         count = C.c_uint64()
         hist = np.zeros(hist_len, np.uint64)
-        self._check(lib().g2_mce_run(self._h, None if src is None else src.ctypes.data_as(C.c_void_p), nsrc,
-                                     C.byref(o), C.byref(count), hist.ctypes.data_as(C.c_void_p), hist_len),
-                    "g2_mce_run")
+        rc = lib().g2_mce_run(self._h, None if src is None else src.ctypes.data_as(C.c_void_p), nsrc,
+                              C.byref(o), C.byref(count), hist.ctypes.data_as(C.c_void_p), hist_len)
+        # with a time budget (deadline_ms), G2_ERR_DEADLINE is a result: the
+        # outputs hold the roots that finished (root_nodes > 0)
+        self.expired = rc == G2_ERR_DEADLINE and o.deadline_ms != 0
+        if not self.expired:
+            self._check(rc, "g2_mce_run")
         del keep
         return (count.value, hist, rn) if root_nodes else (count.value, hist)
 
@@ -389,7 +398,7 @@ class Context:
 
     def root_features(self, sources=None):
         src = None if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
-        n = self.graph.n if src is None else src.size
+        n = self.n if src is None else src.size
         out = np.zeros((n, MODEL_FEATURES), np.float32)
         self._check(lib().g2_root_features(self._h, None if src is None else src.ctypes.data_as(C.c_void_p),
                                            0 if src is None else src.size, out.ctypes.data_as(C.c_void_p)),

@@ -41,6 +41,9 @@ extern "C" {
 #define G2_ERR_UNSUPPORTED (-8)  /* e.g. query larger than G2_MAX_QUERY        */
 #define G2_ERR_IO (-9)           /* file could not be read or written          */
 #define G2_ERR_HIST (-10)        /* clique larger than the histogram supplied  */
+#define G2_ERR_DEADLINE (-11)    /* g2_opts.deadline_ms ran out: the outputs hold
+                                    the roots that finished (per-root outputs of
+                                    the others stay 0)                          */
 
 /* Largest query pattern: the reference keeps a partial embedding in
  * partial_subgraphs[WARPS_EACH_BLK][8] (app_gmatch/gmatch.h:87). */
@@ -133,6 +136,13 @@ typedef struct g2_opts {
                                    record, in SM cycles (0 = 2^37, about 70 s); a run
                                    whose wait ran out returns G2_ERR_TIMEOUT and the
                                    context stays usable                             */
+    uint32_t deadline_ms;       /* MCE: time budget of the run on the device (0 =
+                                   none).  Past it, warps start no new root and drop
+                                   the root they are walking (nothing of it counted),
+                                   so the run ends soon after; it returns
+                                   G2_ERR_DEADLINE with the totals, histogram and
+                                   per-root outputs (root_nodes > 0 = finished) of
+                                   the roots that finished.  Implies no hand-off.   */
 } g2_opts;
 
 /* g2_opts.flags */

@@ -1,0 +1,37 @@
+"""MCE with a time budget (g2_opts.deadline_ms): past the budget warps start no
+new root and drop the root they walk, so the run ends soon after and returns
+G2_ERR_DEADLINE with the results of the roots that finished.  Those results are
+exact: the count and histogram equal the oracle's over exactly the roots whose
+search-tree node count is non-zero.  The limit is a device clock read, not a
+fault: the context stays usable."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_generous_budget_changes_nothing(orc, c1_graph):
+    from g2aimd.context import Context
+    g = c1_graph
+    want = orc.mce(g, hist_len=64)
+    with Context(0) as c:
+        c.load(g)
+        count, hist, _rn = c.mce(hist_len=64, root_nodes=True, deadline_ms=60000)
+        assert not c.expired
+        assert count == want["count"] and np.array_equal(hist, want["hist"])
+
+
+def test_budget_run_out_keeps_finished_roots_exact(g2, orc):
+    from g2aimd.context import Context
+    g = g2.Graph.rmat(14, 16, seed=1).degeneracy_recoded()
+    with Context(0) as c:
+        c.load(g)
+        count, hist, rn = c.mce(hist_len=128, root_nodes=True, deadline_ms=5)
+        assert c.expired
+        done = np.flatnonzero(rn > 0).astype(np.uint32)
+        assert 0 < done.size < g.n
+        want = orc.mce(g, roots=done, hist_len=128, threads=8)
+        assert count == want["count"] and np.array_equal(hist, want["hist"])
+        # the context runs normally afterwards
+        c2, _h2 = c.mce(sources=done[:256], hist_len=128)
+        assert c2 == orc.mce(g, roots=done[:256], hist_len=128)["count"] and not c.expired
