@@ -92,7 +92,7 @@ def wall_ms(torch, fn):
     return r, 1000.0 * (time.perf_counter() - t)
 
 
-def c5_leg(a, local, torch, stream, scale=26, ef=28, k5_stride=1024, mce_budget_ms=20000):
+def c5_leg(a, local, torch, stream, scale=26, ef=28, k5_stride=16384, mce_budget_ms=20000):
     """C5: R-MAT scale 26, edge factor 28, seed 1 (67 M vertices, 3.6 G directed
     entries, 15 GB CSR), built on the device (g2_gen_rmat_device) and put in
     degeneracy order on the device.  4-cliques and triangles over every root;

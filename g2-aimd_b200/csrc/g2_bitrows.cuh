@@ -262,11 +262,77 @@ __device__ __noinline__ static unsigned long long count_forward_edges(const uint
     return warp_sum_u64(c);
 }
 
+// Hits of one long forward list N+(u) = ci[e0, end) in P0[lo, p) (P0 in global
+// memory, sorted), found by the whole warp; on_hit(j) runs on some lane for
+// every index j with P0[j] in the list.  Two ways, by the cheaper side:
+//  * forward: the warp reads the list 32 entries at a time (coalesced), the
+//    filter drops most entries, and the survivors are compacted into `queue`
+//    (64 words of shared memory) so that every binary search in P0 runs with
+//    all 32 lanes busy (without compaction one survivor per 32 entries kept the
+//    whole warp searching);
+//  * reverse, when |P0[lo, p)| x log |list| is much smaller than the list (a
+//    small P0 next to a long list of the dense core): each lane takes P0
+//    entries and binary-searches them in the list.
+template <class F>
+__device__ __forceinline__ void warp_list_hits(const uint32_t *ci, uint64_t e0, uint64_t end, const uint32_t *P0,
+                                               uint32_t lo, uint32_t p, uint32_t pmax, const P0Filter &f,
+                                               uint32_t *queue, F on_hit) {
+    const uint32_t lane = lane_id();
+    if (lo >= p || e0 >= end) return;
+    // the list's part up to pmax (one search by lane 0)
+    uint64_t cut = 0;
+    if (lane == 0) cut = lower_bound(ci, e0, end, pmax + 1u);
+    cut = __shfl_sync(G2_FULL, cut, 0);
+    const uint64_t L = cut - e0;
+    const uint32_t R = p - lo;
+    if (L == 0) return;
+    if ((uint64_t)R * (ilog2p1(L) + 1u) * 2u < L) {
+        for (uint32_t j = lo + lane; j < p; j += 32) {
+            const uint32_t x = ldg(P0 + j);
+            const uint64_t k = lower_bound(ci, e0, cut, x);
+            if (k < cut && ldg(ci + k) == x) on_hit(j);
+        }
+        return;
+    }
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t qn = 0;
+    for (uint64_t base = e0; base < cut; base += 32) {
+        const uint64_t e = base + lane;
+        const uint32_t y = e < cut ? ldg(ci + e) : 0u;
+        const bool pass = e < cut && filter_maybe(f, y);
+        const uint32_t m = __ballot_sync(G2_FULL, pass);
+        if (pass) queue[qn + __popc(m & lt)] = y;
+        qn += __popc(m);
+        __syncwarp();
+        if (qn >= 32) {
+            const uint32_t yq = queue[lane];
+            const uint32_t jq = gmem_lower_bound(P0, lo, p, yq);
+            if (jq < p && ldg(P0 + jq) == yq) on_hit(jq);
+            const uint32_t rest = qn - 32u;
+            const uint32_t keep = lane < rest ? queue[32 + lane] : 0u;
+            __syncwarp();
+            if (lane < rest) queue[lane] = keep;
+            qn = rest;
+            __syncwarp();
+        }
+    }
+    if (lane < qn) {
+        const uint32_t yq = queue[lane];
+        const uint32_t jq = gmem_lower_bound(P0, lo, p, yq);
+        if (jq < p && ldg(P0 + jq) == yq) on_hit(jq);
+    }
+    __syncwarp();
+}
+
+// Shared-memory layout of the clique path's per-warp P0 region (fwords words):
+// the filter in the first fwords - kQueueWords words, the hit queue after it.
+constexpr uint32_t kQueueWords = 64;
+
 // Upper adjacency rows of P0 (row i = bits j > i with P0[j] in N+(P0[i])), as
 // build_forward_rows(..., symmetric = false) builds them, with P0 = the root's
-// forward slice in global memory and the filter in `fbits` (fwords words of
-// shared memory).  One lane per row; forward lists longer than long_list are
-// scanned by the whole warp (coalesced) into rowbuf.
+// forward slice in global memory and the filter and queue in `fbits` (fwords
+// words of shared memory).  One lane per short forward list; lists longer than
+// long_list are taken by the whole warp (warp_list_hits) into rowbuf.
 __device__ __noinline__ static void build_upper_rows_filtered(const uint64_t *rp, const uint32_t *ci,
                                                               const uint32_t *fo, const uint32_t *P0, uint32_t p,
                                                               uint32_t W, uint32_t *A, uint32_t *rowbuf,
@@ -275,7 +341,8 @@ __device__ __noinline__ static void build_upper_rows_filtered(const uint64_t *rp
     const uint32_t pmax = ldg(P0 + p - 1);
     for (uint32_t i = lane; i < p; i += 32)
         for (uint32_t w = i >> 5; w < W; w++) A[(uint64_t)i * W + w] = 0u;
-    const P0Filter f = filter_build(fbits, fwords, P0, p);
+    uint32_t *queue = fbits + fwords - kQueueWords;
+    const P0Filter f = filter_build(fbits, fwords - kQueueWords, P0, p);
     for (uint32_t i0 = 0; i0 < p; i0 += 32) {
         const uint32_t i = i0 + lane;
         bool big = false;
@@ -305,13 +372,8 @@ __device__ __noinline__ static void build_upper_rows_filtered(const uint64_t *rp
             const uint64_t e0 = ldg(rp + u) + ldg(fo + u), end = ldg(rp + u + 1);
             for (uint32_t w = lane; w < W; w += 32) rowbuf[w] = 0u;
             __syncwarp();
-            for (uint64_t e = e0 + lane; e < end; e += 32) {
-                const uint32_t y = ldg(ci + e);
-                if (y > pmax) break;
-                if (!filter_maybe(f, y)) continue;
-                const uint32_t j = gmem_lower_bound(P0, ii + 1, p, y);
-                if (j < p && ldg(P0 + j) == y) atomicOr(rowbuf + (j >> 5), 1u << (j & 31u));
-            }
+            warp_list_hits(ci, e0, end, P0, ii + 1, p, pmax, f, queue,
+                           [&](uint32_t j) { atomicOr(rowbuf + (j >> 5), 1u << (j & 31u)); });
             __syncwarp();
             for (uint32_t w = (ii >> 5) + lane; w < W; w += 32) A[(uint64_t)ii * W + w] = rowbuf[w];
             __syncwarp();
@@ -320,13 +382,14 @@ __device__ __noinline__ static void build_upper_rows_filtered(const uint64_t *rp
     __syncwarp();
 }
 
-// count_forward_edges with P0 in global memory and the filter in fbits.
+// count_forward_edges with P0 in global memory and the filter and queue in fbits.
 __device__ __noinline__ static unsigned long long count_forward_edges_filtered(
     const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, const uint32_t *P0, uint32_t p, uint32_t part,
     uint32_t nparts, uint32_t *fbits, uint32_t fwords) {
     const uint32_t lane = lane_id();
     const uint32_t pmax = ldg(P0 + p - 1);
-    const P0Filter f = filter_build(fbits, fwords, P0, p);
+    uint32_t *queue = fbits + fwords - kQueueWords;
+    const P0Filter f = filter_build(fbits, fwords - kQueueWords, P0, p);
     unsigned long long c = 0;
     for (uint32_t i0 = 0; i0 < p; i0 += 32) {
         const uint32_t i = i0 + lane;
@@ -354,13 +417,7 @@ __device__ __noinline__ static unsigned long long count_forward_edges_filtered(
             const uint32_t ii = i0 + l;
             const uint32_t u = ldg(P0 + ii);
             const uint64_t e0 = ldg(rp + u) + ldg(fo + u), end = ldg(rp + u + 1);
-            for (uint64_t e = e0 + lane; e < end; e += 32) {
-                const uint32_t y = ldg(ci + e);
-                if (y > pmax) break;
-                if (!filter_maybe(f, y)) continue;
-                const uint32_t j = gmem_lower_bound(P0, ii + 1, p, y);
-                c += j < p && ldg(P0 + j) == y;
-            }
+            warp_list_hits(ci, e0, end, P0, ii + 1, p, pmax, f, queue, [&](uint32_t) { c++; });
         }
     }
     return warp_sum_u64(c);

@@ -15,7 +15,7 @@ entries) is checked instead against the plan walk (an independent device path)
 and, per root, against the CPU oracle on a sample of roots.
 
 Also at the headline size: per-root 4-clique counts on R-MAT s20 equal the
-oracle's on 4,096 random roots plus the 64 heaviest.
+oracle's on 2,048 random roots plus the 16 heaviest.
 """
 import json
 import os
@@ -89,7 +89,7 @@ def test_rmat20_k4_per_root_equals_oracle(g2, orc, ctx):
     per = np.zeros(g.n, np.uint64)
     total = ctx.match(plan, root_counts=per)
     assert total == int(per.sum()) == 17038400522
-    roots = _sample_roots(g.n, per, 4096, 64, 7)
+    roots = _sample_roots(g.n, per, 2048, 16, 7)
     want = orc.match(g, plan, roots=roots, threads=os.cpu_count() or 1, per_root=True)["root_counts"]
     assert np.array_equal(per[roots], want)
 
@@ -105,10 +105,12 @@ def test_rmat20_k5_where_the_reference_cannot_count(g2, orc, ctx):
     total = ctx.match(plan, root_counts=per)
     assert total == int(per.sum())
     # the generic plan walk (candidate lists + binary searches, hand-off) is
-    # an independent device path: same total, same count for every root
-    per_walk = np.zeros(g.n, np.uint64)
-    assert ctx.match(plan, root_counts=per_walk, intersect_mode=1) == total
-    assert np.array_equal(per, per_walk)
+    # an independent device path: the same count for every root of a stride
+    # sample (all roots through the walk take minutes)
+    sample = np.arange(0, g.n, 128, dtype=np.uint32)
+    per_walk = np.zeros(sample.size, np.uint64)
+    assert ctx.match(plan, sources=sample, root_counts=per_walk, intersect_mode=1) == int(per[sample].sum())
+    assert np.array_equal(per[sample], per_walk)
     # oracle on random roots and moderately heavy ones (the heaviest hold
     # ~1e9 5-cliques each, minutes of CPU time)
     order = np.argsort(per, kind="stable")
