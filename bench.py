@@ -106,7 +106,8 @@ def c5_leg(a, local, torch, stream, scale=26, ef=28, k5_stride=16384, mce_budget
     models = os.path.join(ROOT, "g2-aimd_b200", "models")
     launch = {"warps_per_block": 4, "chunk": 1, "ctas_per_sm": 6}
     out = {"workload": f"rmat-s{scale}-ef{ef} (a=.57,b=c=.19, seed 1) degeneracy-ordered, built on the device"}
-    with Context(local, 8 << 30) as ctx:
+    # 48 GiB of slabs: the dense core's roots (|P0| up to ~4500) need 2.5 MB of rows each
+    with Context(local, 48 << 30) as ctx:
         t0 = time.perf_counter()
         m = ctx.gen_rmat(scale, ef, seed=1)
         out["gen_s"] = round(time.perf_counter() - t0, 2)

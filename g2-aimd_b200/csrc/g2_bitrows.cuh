@@ -279,27 +279,24 @@ __device__ __forceinline__ void warp_list_hits(const uint32_t *ci, uint64_t e0, 
                                                uint32_t *queue, F on_hit) {
     const uint32_t lane = lane_id();
     if (lo >= p || e0 >= end) return;
-    // the list's part up to pmax (one search by lane 0)
-    uint64_t cut = 0;
-    if (lane == 0) cut = lower_bound(ci, e0, end, pmax + 1u);
-    cut = __shfl_sync(G2_FULL, cut, 0);
-    const uint64_t L = cut - e0;
+    const uint64_t L = end - e0;  // entries beyond pmax are not scanned, so this bounds the forward cost
     const uint32_t R = p - lo;
-    if (L == 0) return;
     if ((uint64_t)R * (ilog2p1(L) + 1u) * 2u < L) {
         for (uint32_t j = lo + lane; j < p; j += 32) {
             const uint32_t x = ldg(P0 + j);
-            const uint64_t k = lower_bound(ci, e0, cut, x);
-            if (k < cut && ldg(ci + k) == x) on_hit(j);
+            const uint64_t k = lower_bound(ci, e0, end, x);
+            if (k < end && ldg(ci + k) == x) on_hit(j);
         }
         return;
     }
     const uint32_t lt = (1u << lane) - 1u;
     uint32_t qn = 0;
-    for (uint64_t base = e0; base < cut; base += 32) {
+    for (uint64_t base = e0; base < end; base += 32) {
         const uint64_t e = base + lane;
-        const uint32_t y = e < cut ? ldg(ci + e) : 0u;
-        const bool pass = e < cut && filter_maybe(f, y);
+        const uint32_t y = e < end ? ldg(ci + e) : 0xffffffffu;
+        const bool inr = e < end && y <= pmax;
+        if (!__any_sync(G2_FULL, inr)) break;  // sorted: the rest lies beyond P0
+        const bool pass = inr && filter_maybe(f, y);
         const uint32_t m = __ballot_sync(G2_FULL, pass);
         if (pass) queue[qn + __popc(m & lt)] = y;
         qn += __popc(m);

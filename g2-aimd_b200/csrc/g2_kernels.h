@@ -74,7 +74,7 @@ constexpr uint32_t kMatchRecordWords = 32;  // stride of a plan-walk record
 size_t mce_smem_bytes(int wpl, int warps_per_block);
 // Resident CTAs per SM of the kernel a launch with these parameters runs (0 on error).
 int mce_blocks_per_sm(int wpl, int warps_per_block, bool metrics);
-int match_blocks_per_sm(int wpl, int warps_per_block, bool metrics, int ctas_per_sm);
+int match_blocks_per_sm(int wpl, int warps_per_block, bool metrics, int ctas_per_sm, uint32_t p0_words);
 cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_block, cudaStream_t st);
 // Advance a run's hand-off epoch in stream order (skipping 0, the value of a
 // never-published ready word), so runs captured in a CUDA graph stay distinct
@@ -138,9 +138,15 @@ struct MatchArgs {
     const uint32_t *epoch_dev;      // the run's epoch, bumped on the device at the run's start
     uint64_t wait_cycles;
     uint64_t spill_cycles;          // 0: no hand-off
+    uint32_t p0_words;              // shared words per warp for P0 (see match_p0_words)
 };
 
-size_t match_smem_bytes(int wpl, int warps_per_block);
+// Shared-memory words per warp the clique path needs besides its row buffer:
+// P0 staged for the symmetric-row walk (k > 5 or the metrics build), or the
+// P0 filter and hit queue of the lane-parallel counting (k <= 5); none for
+// plan walks (non-clique plans).
+uint32_t match_p0_words(int wpl, bool clique_path, uint32_t k, bool metrics);
+size_t match_smem_bytes(int wpl, int warps_per_block, uint32_t p0_words);
 cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block,
                          cudaStream_t st, bool clique_path, int wpl, int ctas_per_sm);
 

@@ -392,14 +392,14 @@ __device__ bool match_root_clique(const MatchArgs &a, const DevPlan &pl, uint32_
     // and its shared-memory region holds the membership filter instead
     const uint32_t *P0 = ci + split;
     if (!METRICS && k == 3) {  // triangles: count forward-neighbourhood edges while scanning
-        count = count_forward_edges_filtered(rp, ci, a.fo, P0, p, part, nparts, p0s, 1024u * WPL);
+        count = count_forward_edges_filtered(rp, ci, a.fo, P0, p, part, nparts, p0s, a.p0_words);
         return true;
     }
     if (!METRICS && k <= 5) {
         // lane-parallel counting: lane takes the depth-1 vertices x = lane, lane+32, ...
         // (in ordinal order, so the split filter is x % nparts) and counts the
         // (k-2)-cliques above x serially; it reads only the upper part of rows.
-        build_upper_rows_filtered(rp, ci, a.fo, P0, p, W, S + a0, rowbuf, p0s, 1024u * WPL, kLongListMatch);
+        build_upper_rows_filtered(rp, ci, a.fo, P0, p, W, S + a0, rowbuf, p0s, a.p0_words, kLongListMatch);
         __syncwarp();
         count = clique_count_lanes(S + a0, p, W, k, part, nparts);
         return true;
@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int cliqu
     extern __shared__ uint32_t smem[];
     if (a.epoch_dev) a.epoch = *a.epoch_dev;
     const uint32_t wib = threadIdx.x >> 5;
-    uint32_t *rowbuf = smem + wib * (32u * WPL + 1024u * WPL);
+    uint32_t *rowbuf = smem + wib * (32u * WPL + a.p0_words);
     uint32_t *p0s = rowbuf + 32u * WPL;
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t *S = a.scratch + gw * a.words_per_warp;
@@ -536,8 +536,13 @@ __global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int cliqu
 
 }  // namespace
 
-size_t match_smem_bytes(int wpl, int warps_per_block) {
-    return (size_t)warps_per_block * (32u * wpl + 1024u * wpl) * sizeof(uint32_t);
+uint32_t match_p0_words(int wpl, bool clique_path, uint32_t k, bool metrics) {
+    if (!clique_path) return 0u;
+    return (k <= 5 && !metrics) ? 1024u : 1024u * (uint32_t)wpl;
+}
+
+size_t match_smem_bytes(int wpl, int warps_per_block, uint32_t p0_words) {
+    return (size_t)warps_per_block * (32u * wpl + p0_words) * sizeof(uint32_t);
 }
 
 template <int WPL, bool M, int MINB>
@@ -548,8 +553,8 @@ static void launch_match(const DevPlan &pl, const MatchArgs &a, dim3 g, dim3 b, 
 }
 
 template <int WPL, bool M, int MINB>
-static int match_occ(int warps_per_block) {
-    const size_t sm = match_smem_bytes(WPL, warps_per_block);
+static int match_occ(int warps_per_block, uint32_t p0_words) {
+    const size_t sm = match_smem_bytes(WPL, warps_per_block, p0_words);
     cudaFuncSetAttribute(match_kernel<WPL, M, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, match_kernel<WPL, M, MINB>, 32 * warps_per_block, sm) !=
@@ -561,20 +566,22 @@ static int match_occ(int warps_per_block) {
 // The 40-register build exists for the hot case only: WPL 1, no metrics.
 static bool wide_budget(int wpl, bool metrics, int ctas_per_sm) { return ctas_per_sm == 6 && wpl == 1 && !metrics; }
 
-int match_blocks_per_sm(int wpl, int warps_per_block, bool metrics, int ctas_per_sm) {
-    if (wide_budget(wpl, metrics, ctas_per_sm)) return match_occ<1, false, 6>(warps_per_block);
+int match_blocks_per_sm(int wpl, int warps_per_block, bool metrics, int ctas_per_sm, uint32_t p0_words) {
+    const int w = warps_per_block;
+    const uint32_t q = p0_words;
+    if (wide_budget(wpl, metrics, ctas_per_sm)) return match_occ<1, false, 6>(w, q);
     switch (wpl) {
-        case 1: return metrics ? match_occ<1, true, 4>(warps_per_block) : match_occ<1, false, 4>(warps_per_block);
-        case 2: return metrics ? match_occ<2, true, 4>(warps_per_block) : match_occ<2, false, 4>(warps_per_block);
-        case 4: return metrics ? match_occ<4, true, 4>(warps_per_block) : match_occ<4, false, 4>(warps_per_block);
-        case 8: return metrics ? match_occ<8, true, 4>(warps_per_block) : match_occ<8, false, 4>(warps_per_block);
+        case 1: return metrics ? match_occ<1, true, 4>(w, q) : match_occ<1, false, 4>(w, q);
+        case 2: return metrics ? match_occ<2, true, 4>(w, q) : match_occ<2, false, 4>(w, q);
+        case 4: return metrics ? match_occ<4, true, 4>(w, q) : match_occ<4, false, 4>(w, q);
+        case 8: return metrics ? match_occ<8, true, 4>(w, q) : match_occ<8, false, 4>(w, q);
         default: return 0;
     }
 }
 
 cudaError_t match_launch(const DevPlan &plan, const MatchArgs &a, int blocks, int warps_per_block, cudaStream_t st,
                          bool clique_path, int wpl, int ctas_per_sm) {
-    size_t sm = match_smem_bytes(wpl, warps_per_block);
+    size_t sm = match_smem_bytes(wpl, warps_per_block, a.p0_words);
     dim3 g(blocks), b(32 * warps_per_block);
     const int cp = clique_path ? 1 : 0;
     const bool m = a.work != nullptr;

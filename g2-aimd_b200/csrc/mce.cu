@@ -318,10 +318,6 @@ __device__ __noinline__ bool spill_all(const MceArgs &a, uint32_t task, uint32_t
 
 enum : int { kTaskDone = 0, kTaskDeferred = 1 };
 
-// Shared-memory words per warp of the P0 membership filter used while a root's
-// rows are built (16384 bits: a false-positive rate of p / 16384).
-constexpr uint32_t kMceFilterWords = 512;
-
 // Has the run's time budget (MceArgs::deadline, %globaltimer ns) run out?
 // Warp-uniform.
 __device__ __forceinline__ bool deadline_passed(const MceArgs &a) {
@@ -403,15 +399,14 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
         const uint64_t xv0 = a0 + (uint64_t)p * W;
         const uint64_t b0 = xv0 + (METRICS ? nx : 0);
         if (fr0 < b0 + 64) return kTaskDeferred;
-        // stage P0 in shared memory and its membership filter, then the rows
+        // stage P0 in shared memory, then the rows
         for (uint32_t i = lane; i < p; i += 32) cand[i] = ldg(ci + split + i);
-        const P0Filter flt = filter_build(rowbuf + 32u * WPL, kMceFilterWords, ci + split, p);
-        build_forward_rows(rp, ci, a.fo, cand, p, W, S + a0, rowbuf, true, kLongList, flt);
+        __syncwarp();
+        build_forward_rows(rp, ci, a.fo, cand, p, W, S + a0, rowbuf);
         // kept B rows plus their root-list entries must stay below the frames
         const uint64_t cap64 = (fr0 - b0 - 64) / (W + 1);
         const uint32_t cap = cap64 > 0xfffffff0ull ? 0xfffffff0u : (uint32_t)cap64;
-        nb = build_back_rows(rp, ci, a.fo, v, lo, nx, cand, p, W, S + b0, METRICS ? S + xv0 : nullptr, cap, rowbuf,
-                             flt);
+        nb = build_back_rows(rp, ci, a.fo, v, lo, nx, cand, p, W, S + b0, METRICS ? S + xv0 : nullptr, cap, rowbuf);
         if (nb == ~0u) return kTaskDeferred;
         __syncwarp();
         rows.A = S + a0;
@@ -723,8 +718,8 @@ __global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
     extern __shared__ uint32_t smem[];
     if (a.epoch_dev) a.epoch = *a.epoch_dev;
     const uint32_t wib = threadIdx.x >> 5;
-    uint32_t *cand = smem + wib * (32u * 32u * WPL + 32u * WPL + kMceFilterWords);
-    uint32_t *rowbuf = cand + 32u * 32u * WPL;  // then the P0 filter (kMceFilterWords)
+    uint32_t *cand = smem + wib * (32u * 32u * WPL + 32u * WPL);
+    uint32_t *rowbuf = cand + 32u * 32u * WPL;
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t *S = a.scratch + gw * a.words_per_warp;
     const bool handoff = a.spill_cycles != 0;
@@ -759,7 +754,7 @@ __global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
 }  // namespace
 
 size_t mce_smem_bytes(int wpl, int warps_per_block) {
-    return (size_t)warps_per_block * (32u * 32u * wpl + 32u * wpl + kMceFilterWords) * sizeof(uint32_t);
+    return (size_t)warps_per_block * (32u * 32u * wpl + 32u * wpl) * sizeof(uint32_t);
 }
 
 template <int WPL, bool M>

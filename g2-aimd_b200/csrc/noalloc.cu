@@ -155,6 +155,7 @@ extern "C" int g2_match_count_noalloc(const uint64_t *d_row_ptrs, const uint32_t
     a.words_per_warp = wpw;
     a.out = reinterpret_cast<unsigned long long *>(d_count);
     a.status = reinterpret_cast<int *>(S + 2);
+    a.p0_words = g2::match_p0_words(1, clique, dp.k, false);
     if (g2::match_launch(dp, a, blocks, wpb, st, clique, 1, 0) != cudaSuccess) return G2_ERR_CUDA;
     noalloc_status_kernel<<<1, 1, 0, st>>>(a.status, a.out);
     if (cudaGetLastError() != cudaSuccess) return G2_ERR_CUDA;

@@ -686,12 +686,15 @@ int mce_host_spill(g2_ctx *ctx, cudaStream_t st) {
 namespace {
 
 // Persistent-grid geometry of the match kernel.
-void match_geometry(g2_ctx *ctx, const g2_opts *o, int *wpl, int *wpb, int *blocks) {
+void match_geometry(g2_ctx *ctx, const g2_opts *o, int *wpl, int *wpb, int *blocks, uint32_t *p0_words) {
     *wpl = wpl_for(ctx->max_fwd);
     *wpb = default_warps(o);
-    while (*wpb > 1 && g2::match_smem_bytes(*wpl, *wpb) > 200 * 1024) *wpb /= 2;
     const bool metrics = o && (o->flags & G2_FLAG_WORK_MODEL);
-    *blocks = default_blocks(ctx, o, *wpb, g2::match_blocks_per_sm(*wpl, *wpb, metrics, o ? (int)o->ctas_per_sm : 0));
+    const bool clique = ctx->clique_plan && !(o && o->intersect_mode == 1);
+    *p0_words = g2::match_p0_words(*wpl, clique, ctx->plan.k, metrics);
+    while (*wpb > 1 && g2::match_smem_bytes(*wpl, *wpb, *p0_words) > 200 * 1024) *wpb /= 2;
+    *blocks = default_blocks(
+        ctx, o, *wpb, g2::match_blocks_per_sm(*wpl, *wpb, metrics, o ? (int)o->ctas_per_sm : 0, *p0_words));
 }
 
 }  // namespace
@@ -711,8 +714,10 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
     rc = prepare_flags(ctx, flags, st);
     if (rc) return rc;
     int wpl, wpb, blocks;
-    match_geometry(ctx, o, &wpl, &wpb, &blocks);
+    uint32_t p0_words;
+    match_geometry(ctx, o, &wpl, &wpb, &blocks, &p0_words);
     g2::MatchArgs a{};
+    a.p0_words = p0_words;
     a.rp = ctx->d_rp;
     a.ci = ctx->d_ci;
     a.fo = ctx->d_fo;
@@ -782,7 +787,8 @@ namespace g2rt {
 
 uint64_t match_warps(g2_ctx *ctx, const g2_opts *o) {
     int wpl, wpb, blocks;
-    match_geometry(ctx, o, &wpl, &wpb, &blocks);
+    uint32_t p0_words;
+    match_geometry(ctx, o, &wpl, &wpb, &blocks, &p0_words);
     return (uint64_t)blocks * wpb;
 }
 

@@ -13,10 +13,12 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def c5_small(g2):
-    from g2aimd.context import Context
+    from g2aimd.context import Context, CostModel
     c = Context(0)
     m = c.gen_rmat(15, 28, seed=1)
     c.degeneracy_recode()
+    c.set_model(CostModel.load(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                            "g2-aimd_b200", "models", "k4.npz")))
     g = c.copy_csr(m)
     yield c, g
     c.close()
