@@ -902,6 +902,14 @@ def run_ours(a):
                                  and np.array_equal(dev_rec.cols, host_rec.cols))})
         # ---- a batch of 64 power-law graphs, one launch per job
         extras["batch_chung_lu_64"] = c4_leg(Context, CostModel, Plan, models, local, a.seed + rank, torch, stream)
+        # ---- C3 (maximal cliques of R-MAT with planted cliques) and C5 (R-MAT s26 ef28)
+        for key, leg in (("c3_rmat_planted", lambda: c3_leg(a, local, torch, stream, reps=2, budget_ms=10000)),
+                         ("c5_rmat_s26_ef28", lambda: c5_leg(a, local, torch, stream, k5_stride=65536,
+                                                              mce_budget_ms=10000))):
+            try:
+                extras[key] = leg()
+            except Exception as exc:  # a failed leg is reported, the headline line still prints
+                extras[key] = {"error": f"{type(exc).__name__}: {exc}"}
         # ---- the same graph out of core: view bins against in-core runs
         if world == 1:
             extras["view_bins"] = view_legs(a, g, 2, 1)

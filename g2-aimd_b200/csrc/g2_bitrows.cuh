@@ -147,12 +147,9 @@ constexpr uint32_t kLongListMatch = 32;
 // transpose, added 32x32 tile by tile.
 // With symmetric = false only the upper part of each row (words from i / 32
 // on, bits j > i) is built: enough for walks that only look above the row.
-// With a filter (flt.bits non-null) an entry is binary-searched only if the
-// filter admits it.
 __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo,
                                    const uint32_t *p0s, uint32_t p, uint32_t W, uint32_t *A, uint32_t *rowbuf,
-                                   bool symmetric = true, uint32_t long_list = kLongList,
-                                   P0Filter flt = P0Filter{nullptr, 0}) {
+                                   bool symmetric = true, uint32_t long_list = kLongList) {
     const uint32_t lane = lane_id();
     const uint32_t pmax = p0s[p - 1];
     if (symmetric)
@@ -175,7 +172,6 @@ __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const
                 for (; e < end; e++) {
                     const uint32_t y = ldg(ci + e);
                     if (y > pmax) break;
-                    if (flt.bits && !filter_maybe(flt, y)) continue;
                     j = smem_lower_bound(p0s, j, p, y);
                     if (j < p && p0s[j] == y) row[j >> 5] |= 1u << (j & 31u);
                 }
@@ -193,7 +189,6 @@ __device__ __noinline__ static void build_forward_rows(const uint64_t *rp, const
             for (uint64_t e = e0 + lane; e < end; e += 32) {
                 const uint32_t y = ldg(ci + e);
                 if (y > pmax) break;
-                if (flt.bits && !filter_maybe(flt, y)) continue;
                 const uint32_t j = smem_lower_bound(p0s, ii + 1, p, y);
                 if (j < p && p0s[j] == y) atomicOr(rowbuf + (j >> 5), 1u << (j & 31u));
             }
@@ -291,9 +286,13 @@ __device__ __forceinline__ void warp_list_hits(const uint32_t *ci, uint64_t e0, 
     }
     const uint32_t lt = (1u << lane) - 1u;
     uint32_t qn = 0;
+    // the next chunk's entry is loaded before this chunk is filtered (its
+    // L2 latency overlaps the filter work)
+    uint32_t y_next = e0 + lane < end ? ldg(ci + e0 + lane) : 0xffffffffu;
     for (uint64_t base = e0; base < end; base += 32) {
         const uint64_t e = base + lane;
-        const uint32_t y = e < end ? ldg(ci + e) : 0xffffffffu;
+        const uint32_t y = y_next;
+        y_next = e + 32 < end ? ldg(ci + e + 32) : 0xffffffffu;
         const bool inr = e < end && y <= pmax;
         if (!__any_sync(G2_FULL, inr)) break;  // sorted: the rest lies beyond P0
         const bool pass = inr && filter_maybe(f, y);
@@ -426,8 +425,7 @@ __device__ __noinline__ static unsigned long long count_forward_edges_filtered(
 // Returns nb, or ~0u if more than cap rows would be needed.
 __device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, uint32_t v,
                                     uint64_t lo, uint32_t nx, const uint32_t *p0s, uint32_t p, uint32_t W,
-                                    uint32_t *B, uint32_t *xv, uint32_t cap, uint32_t *rowbuf,
-                                    P0Filter flt = P0Filter{nullptr, 0}) {
+                                    uint32_t *B, uint32_t *xv, uint32_t cap, uint32_t *rowbuf) {
     const uint32_t lane = lane_id();
     const uint32_t pmin = p0s[0], pmax = p0s[p - 1];
     uint32_t nb = 0;
@@ -448,7 +446,6 @@ __device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, cons
                 for (uint64_t f = e; f < end; f++) {
                     const uint32_t y = ldg(ci + f);
                     if (y > pmax) break;
-                    if (flt.bits && !filter_maybe(flt, y)) continue;
                     j = smem_lower_bound(p0s, j, p, y);
                     if (j < p && p0s[j] == y) {
                         hit = true;
@@ -474,7 +471,7 @@ __device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, cons
                 const uint32_t y = f < b1 ? ldg(ci + f) : 0xffffffffu;
                 const bool inr = f < b1 && y <= pmax;
                 bool found = false;
-                if (inr && (!flt.bits || filter_maybe(flt, y))) {
+                if (inr) {
                     const uint32_t j = smem_lower_bound(p0s, 0, p, y);
                     found = j < p && p0s[j] == y;
                 }
@@ -499,7 +496,6 @@ __device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, cons
             for (uint64_t f = e; f < end; f++) {
                 const uint32_t y = ldg(ci + f);
                 if (y > pmax) break;
-                if (flt.bits && !filter_maybe(flt, y)) continue;
                 j = smem_lower_bound(p0s, j, p, y);
                 if (j < p && p0s[j] == y) row[j >> 5] |= 1u << (j & 31u);
             }
@@ -520,7 +516,6 @@ __device__ __noinline__ static uint32_t build_back_rows(const uint64_t *rp, cons
             for (uint64_t f = s + lane; f < b1; f += 32) {
                 const uint32_t y = ldg(ci + f);
                 if (y > pmax) break;
-                if (flt.bits && !filter_maybe(flt, y)) continue;
                 const uint32_t j = smem_lower_bound(p0s, 0, p, y);
                 if (j < p && p0s[j] == y) atomicOr(rowbuf + (j >> 5), 1u << (j & 31u));
             }

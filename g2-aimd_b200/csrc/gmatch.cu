@@ -95,6 +95,60 @@ __device__ __forceinline__ bool cand_ok(const DevPlan &pl, const uint64_t *rp, c
     return true;
 }
 
+// First index in [c, stop) of the sorted list ci with ci[index] >= w, found by
+// exponential search from c (the previous answer: candidates come in ascending
+// order, so a cursor only moves forward).
+__device__ __forceinline__ uint64_t gallop(const uint32_t *ci, uint64_t c, uint64_t stop, uint32_t w) {
+    if (c >= stop || ldg(ci + c) >= w) return c;
+    uint64_t step = 1;
+    while (c + step < stop && ldg(ci + c + step) < w) {
+        c += step;
+        step <<= 1;
+    }
+    const uint64_t hi = c + step < stop ? c + step : stop;
+    return lower_bound(ci, c + 1, hi, w);
+}
+
+// Windows of the last position up to this many entries are counted by
+// count_last_sliced; longer ones keep the chunked scan, which can hand off.
+constexpr uint64_t kSlicedMax = 32ull * 256ull;
+
+// The last position's count over the window [pos, end) of the parent's list:
+// every lane takes a contiguous slice of the window and tests its candidates
+// against the conditions and the other back neighbours' lists through cursors
+// that only move forward (galloping), instead of a full binary search per
+// candidate and list.  Per-lane count.
+__device__ __noinline__ unsigned long long count_last_sliced(const DevPlan &pl, const uint64_t *rp,
+                                                             const uint32_t *ci, const uint32_t *M, uint32_t i,
+                                                             uint32_t parent, uint64_t pos, uint64_t end) {
+    const uint32_t lane = lane_id();
+    const uint64_t per = (end - pos + 31) >> 5;
+    const uint64_t lo = pos + (uint64_t)lane * per;
+    const uint64_t hi = lo + per < end ? lo + per : end;
+    uint64_t cur[G2_MAX_QUERY], stop[G2_MAX_QUERY];
+    uint32_t nb = 0;
+    for (uint32_t j = 0; j < pl.bn_count[i]; j++) {
+        const uint32_t b = pl.bn_pos[i][j];
+        if (b == parent) continue;
+        cur[nb] = ldg(rp + M[b]);
+        stop[nb] = ldg(rp + M[b] + 1);
+        nb++;
+    }
+    unsigned long long c = 0;
+    for (uint64_t x = lo; x < hi; x++) {
+        const uint32_t w = ldg(ci + x);
+        bool ok = true;
+        for (uint32_t t = 0; t < pl.cond_count[i] && ok; t++)
+            ok = cond_ok(pl.cond_op[i][t], w, M[pl.cond_pos[i][t]]);
+        for (uint32_t t = 0; t < nb && ok; t++) {
+            cur[t] = gallop(ci, cur[t], stop[t], w);
+            ok = cur[t] < stop[t] && ldg(ci + cur[t]) == w;
+        }
+        c += ok;
+    }
+    return c;
+}
+
 // Record layout of a handed-off plan walk (kMatchRecordWords words): the walk
 // resumes at position `level` with M[0..level-1]; kind 0 (prefix) initialises
 // that level from the plan, kind 1 (window) scans only [pos, end) of its
@@ -238,6 +292,13 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
     long long next_check = (long long)a.spill_cycles;
     for (;;) {
         Level &L = Ls[i];
+        if (i == k - 1 && L.end - L.pos <= kSlicedMax && !(i == 1 && nparts > 1)) {
+            // last position, short window: sliced count with forward-moving cursors
+            if (L.pos < L.end) count += warp_sum_u64(count_last_sliced(pl, rp, ci, M, i, L.parent, L.pos, L.end));
+            if (i == base) break;
+            i--;
+            continue;
+        }
         if (i == k - 1) {
             // last position: count, never materialise (a long scan hands off its upper half)
             uint32_t iter = 0;

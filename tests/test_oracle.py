@@ -78,3 +78,23 @@ def test_kcore_oracle_vs_library_order(g2, orc):
     same = np.diff(c) == 0
     assert np.all(np.diff(d)[same] >= 0)
     assert kmax == int(core.max())
+
+
+def test_oracle_builds_the_librarys_rmat_graphs(g2, orc):
+    """The CPU measurement of the reference algorithm builds its input without
+    the library: the oracle's generator and kcore-order recode give the same CSR
+    (and core numbers) as g2_gen_rmat + the library's recode."""
+    for scale, ef, seed in ((8, 8, 1), (12, 16, 3), (13, 28, 5)):
+        o = orc.degeneracy_recoded(orc.gen_rmat(scale, ef, seed=seed))
+        g = g2.Graph.rmat(scale, ef, seed=seed).degeneracy_recoded()
+        assert np.array_equal(o.row_ptrs, g.row_ptrs)
+        assert np.array_equal(o.cols, g.cols)
+        assert np.array_equal(o.core, g.core)
+
+
+def test_oracle_preset_plans_equal_the_librarys(g2, orc):
+    from g2aimd.context import Plan
+    for q in (0, 1, 2, 23, 24, 25):
+        a, b = orc.PresetPlan(q), Plan.preset(q)
+        assert a.k == b.k
+        assert all(np.array_equal(x, y) for x, y in zip(a.flat(), b.flat()))
