@@ -452,13 +452,15 @@ def c4_work_estimate(g):
     return float((s1 * pf).sum() / 2)
 
 
-def c4_leg(Context, CostModel, Plan, models, local, seed, torch, stream):
+def c4_leg(Context, CostModel, Plan, models, local, seed, torch, stream, budget_ms=1000):
     """64 Chung-Lu graphs (n log-uniform in [1e3, 1e6], exponent in [2.1, 2.8],
     average degree in [8, 40]): triangles over all of them, maximal cliques over
     the ones of degeneracy <= 160 (the densest cores hold 5e9 to over 3e10
     maximal cliques each), 4-cycles and diamonds over the ones whose estimated
     walk is at most 1e10; each job is one launch over the batch (disjoint union),
-    compared with one run per graph."""
+    compared with one run per graph.  The members left out of a job then run it
+    alone with a device time budget (budget_ms), reporting the roots that
+    finished and their exact counts."""
     from g2aimd.graph import chung_lu_batch
     t0 = time.perf_counter()
     gs = chung_lu_batch(count=64, seed=seed)
@@ -508,6 +510,32 @@ def c4_leg(Context, CostModel, Plan, models, local, seed, torch, stream):
             assert cnt == out[name]["total"], (name, cnt, out[name]["total"])
             out[name]["per_graph_loop_ms"] = tot
             out[name]["batched_vs_loop"] = tot / out[name]["batched_ms"]
+        # the members left out above, each job with a device time budget: the
+        # roots that finished and their exact counts (MCE: root_nodes > 0;
+        # matches: root_cost > 0)
+        heavy = []
+        for gi, g in enumerate(gs):
+            jobs_g = ([("mce", None)] if g not in mce_set else []) + \
+                     ([("4-cycle", 1), ("diamond", 2)] if g not in light else [])
+            if not jobs_g:
+                continue
+            bc.load(g)
+            bc.load_core(g.core)
+            rec = {"graph": gi, "n": g.n, "m": g.m, "degeneracy": int(g.core.max()), "walk_estimate": est[gi]}
+            for name, q in jobs_g:
+                t0 = time.perf_counter()
+                if q is None:
+                    c, _h, rn = bc.mce(hist_len=4096, root_nodes=True, flags=1, deadline_ms=budget_ms)
+                    done = int(np.count_nonzero(rn))
+                else:
+                    cost = np.zeros(g.n, np.uint64)
+                    c = bc.match(Plan.preset(q), root_cost=cost, schedule="heuristic", flags=1,
+                                 deadline_ms=budget_ms)
+                    done = int(np.count_nonzero(cost))
+                rec[name] = {"count_of_finished_roots": int(c), "roots_finished": done, "complete": not bc.expired,
+                             "wall_s": round(time.perf_counter() - t0, 2)}
+            heavy.append(rec)
+        out["left_out_members_budgeted"] = {"budget_ms": budget_ms, "graphs": heavy}
     return out
 
 

@@ -139,6 +139,7 @@ struct MatchArgs {
     uint64_t wait_cycles;
     uint64_t spill_cycles;          // 0: no hand-off
     uint32_t p0_words;              // shared words per warp for P0 (see match_p0_words)
+    const unsigned long long *deadline;  // optional: %globaltimer (ns) past which roots are dropped
 };
 
 // Shared-memory words per warp the clique path needs besides its row buffer:

@@ -41,6 +41,20 @@ __device__ __forceinline__ bool cond_ok(uint32_t op, uint32_t w, uint32_t m) {
     return op == G2_COND_LESS_THAN ? w < m : op == G2_COND_LARGER_THAN ? w > m : w != m;
 }
 
+// Count returned by a walk that the run's time budget cut short (nothing of it
+// is credited).
+constexpr unsigned long long kExpired = ~0ull;
+
+// Has the run's time budget (MatchArgs::deadline, %globaltimer ns) run out?
+// Warp-uniform; false without a budget.
+__device__ __forceinline__ bool match_deadline_passed(const MatchArgs &a) {
+    if (!a.deadline) return false;
+    unsigned long long now = 0;
+    if (lane_id() == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    now = __shfl_sync(G2_FULL, now, 0);
+    return now > *a.deadline;
+}
+
 struct Level {
     uint64_t pos, end;   // scan window in the parent's neighbour list
     uint32_t len, idx;   // materialised chunk
@@ -288,6 +302,7 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
     }
     uint32_t i = base;
     uint32_t ord = 0;  // ordinal of the next position-1 candidate (heavy-root split)
+    uint32_t budget_tick = 0;  // time-budget checks every 64 partial embeddings / scan chunks
     bool may_spill = a.spill_cycles != 0 && nparts == 1;
     long long next_check = (long long)a.spill_cycles;
     for (;;) {
@@ -303,6 +318,7 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
             // last position: count, never materialise (a long scan hands off its upper half)
             uint32_t iter = 0;
             for (uint64_t e = L.pos; e < L.end; e += 32) {
+                if (a.deadline && (++budget_tick & 63u) == 0 && match_deadline_passed(a)) return kExpired;
                 if (may_spill && (++iter & 63u) == 0) {
                     long long el = 0;
                     if (lane == 0) el = clock64() - c0;
@@ -357,6 +373,7 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
         }
         M[i] = buf[L.idx];
         L.idx++;
+        if (a.deadline && (++budget_tick & 63u) == 0 && match_deadline_passed(a)) return kExpired;
         if (i == 1 && nparts > 1 && (ord++ % nparts) != part) continue;  // another part's candidate
         if (may_spill) {  // every spill_cycles: hand work to idle warps
             long long el = 0;
@@ -386,11 +403,12 @@ __device__ __forceinline__ uint32_t above(uint32_t x, uint32_t w) {
 // Number of (k-1)-cliques of the local graph rows A (p rows x W words) with
 // increasing indices, k = 3, 4 or 5, summed over the warp.  Lane l owns the
 // first indices x = l, l+32, ... with x % nparts == part.
-__device__ unsigned long long clique_count_lanes(const uint32_t *A, uint32_t p, uint32_t W, uint32_t k,
-                                                 uint32_t part, uint32_t nparts) {
+__device__ unsigned long long clique_count_lanes(const MatchArgs &a, const uint32_t *A, uint32_t p, uint32_t W,
+                                                 uint32_t k, uint32_t part, uint32_t nparts) {
     unsigned long long c = 0;
-    for (uint32_t x = lane_id(); x < p; x += 32) {
-        if (nparts > 1 && x % nparts != part) continue;
+    for (uint32_t x = lane_id(); x - lane_id() < p; x += 32) {  // warp-uniform trip count
+        if (a.deadline && match_deadline_passed(a)) return kExpired;
+        if (x >= p || (nparts > 1 && x % nparts != part)) continue;
         const uint32_t *ax = A + (uint64_t)x * W;
         if (k == 3) {
             for (uint32_t w = x >> 5; w < W; w++) c += __popc(ax[w] & above(x, w));
@@ -462,7 +480,7 @@ __device__ bool match_root_clique(const MatchArgs &a, const DevPlan &pl, uint32_
         // (k-2)-cliques above x serially; it reads only the upper part of rows.
         build_upper_rows_filtered(rp, ci, a.fo, P0, p, W, S + a0, rowbuf, p0s, a.p0_words, kLongListMatch);
         __syncwarp();
-        count = clique_count_lanes(S + a0, p, W, k, part, nparts);
+        count = clique_count_lanes(a, S + a0, p, W, k, part, nparts);
         return true;
     }
     for (uint32_t i = lane; i < p; i += 32) p0s[i] = ldg(ci + split + i);
@@ -549,6 +567,10 @@ __global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int cliqu
     const bool handoff = a.spill_cycles != 0;
     const unsigned long long ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
     auto credit = [&](uint32_t task, unsigned long long c, long long c0) {
+        if (c == kExpired) {  // dropped by the time budget: nothing counted, no cost recorded
+            if (lane_id() == 0) atomicOr(a.status, kStatusDeadline);
+            return;
+        }
         total += c;
         if (lane_id() == 0) {
             if (a.root_nodes && c) atomicAdd(reinterpret_cast<unsigned long long *>(a.root_nodes + task), c);
@@ -574,6 +596,10 @@ __global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int cliqu
             if (lane_id() == 0) c0 = clock64();
             c0 = __shfl_sync(G2_FULL, c0, 0);
             unsigned long long c = 0;
+            if (match_deadline_passed(a)) {  // time budget spent: start no new root
+                credit((uint32_t)task, kExpired, c0);
+                continue;
+            }
             if (!clique_path || !match_root_clique<WPL, METRICS>(a, pl, v, S, p0s, rowbuf, c, work, part, nparts))
                 c = match_walk(a, pl, (uint32_t)task, v, nullptr, S, work, part, nparts, c0);
             credit((uint32_t)task, c, c0);

@@ -333,7 +333,7 @@ __device__ __forceinline__ bool deadline_passed(const MceArgs &a) {
 // reference's tree is accumulated: per node with P ∪ X non-empty,
 // sum_{u in P∪X} (|P| + deg u) for pivot scoring plus
 // sum_{q in P \ N(pivot)} (|P ∪ X| + deg q) for the children.
-template <int WPL, bool METRICS>
+template <int WPL, bool METRICS, bool BUDGET>
 __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t *cand, uint32_t *rowbuf,
                         long long c0, uint32_t *task_out) {
     const uint32_t lane = lane_id();
@@ -469,7 +469,7 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
         bool want_pop = false;
         if (enter) {
             enter = false;
-            if (a.deadline && (nodes & 255u) == 0 && deadline_passed(a)) {  // time budget: drop the root
+            if (BUDGET && (nodes & 255u) == 0 && deadline_passed(a)) {  // time budget: drop the root
                 expired = true;
                 break;
             }
@@ -668,7 +668,7 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
         }
         __syncwarp();
     }
-    if (expired) {  // nothing of this entry is committed (deadline runs never hand off)
+    if (BUDGET && expired) {  // nothing of this entry is committed (budgeted runs never hand off)
         if (lane == 0) atomicOr(a.status, kStatusDeadline);
         __syncwarp();
         return kTaskDone;
@@ -697,14 +697,14 @@ __device__ int mce_task(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t 
     return kTaskDone;
 }
 
-template <int WPL, bool METRICS>
+template <int WPL, bool METRICS, bool BUDGET>
 __device__ __forceinline__ void run_entry(const MceArgs &a, uint32_t entry, uint32_t *S, uint32_t *cand,
                                           uint32_t *rowbuf) {
     long long c0 = 0;
     if (lane_id() == 0) c0 = clock64();
     c0 = __shfl_sync(G2_FULL, c0, 0);
     uint32_t task = 0;
-    if (mce_task<WPL, METRICS>(a, entry, S, cand, rowbuf, c0, &task) == kTaskDeferred)
+    if (mce_task<WPL, METRICS, BUDGET>(a, entry, S, cand, rowbuf, c0, &task) == kTaskDeferred)
         defer_entry(a, entry);
     else if (a.root_cost && lane_id() == 0 && task != ~0u)
         atomicAdd(reinterpret_cast<unsigned long long *>(a.root_cost + task), (unsigned long long)(clock64() - c0));
@@ -713,7 +713,9 @@ __device__ __forceinline__ void run_entry(const MceArgs &a, uint32_t entry, uint
 // Persistent pass.  Phase 1: entries from the task queue (or a deferred list).
 // Phase 2 (passes that hand off work): records through the ticket queue of
 // g2_handoff.cuh until no work is outstanding.
-template <int WPL, bool METRICS>
+// BUDGET: the build for runs with a time budget (MceArgs::deadline set); the
+// others carry no deadline check.
+template <int WPL, bool METRICS, bool BUDGET>
 __global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
     extern __shared__ uint32_t smem[];
     if (a.epoch_dev) a.epoch = *a.epoch_dev;
@@ -737,17 +739,17 @@ __global__ void __launch_bounds__(256, 3) mce_kernel(MceArgs a) {
         }
         const unsigned long long t1 = t0 + a.chunk < n ? t0 + a.chunk : n;
         for (unsigned long long t = t0; t < t1; t++) {
-            if (deadline_passed(a)) {  // time budget spent: start no new root
+            if (BUDGET && deadline_passed(a)) {  // time budget spent: start no new root
                 if (lane_id() == 0) atomicOr(a.status, kStatusDeadline);
                 continue;
             }
-            run_entry<WPL, METRICS>(a, a.task_index ? a.task_index[t] : (uint32_t)t, S, cand, rowbuf);
+            run_entry<WPL, METRICS, BUDGET>(a, a.task_index ? a.task_index[t] : (uint32_t)t, S, cand, rowbuf);
         }
         outstanding_add(a, handoff, -1);
     }
     if (handoff)
         run_record_queue(a, [&](unsigned long long h) {
-            run_entry<WPL, METRICS>(a, kRecordBit | (uint32_t)h, S, cand, rowbuf);
+            run_entry<WPL, METRICS, BUDGET>(a, kRecordBit | (uint32_t)h, S, cand, rowbuf);
         });
 }
 
@@ -759,16 +761,21 @@ size_t mce_smem_bytes(int wpl, int warps_per_block) {
 
 template <int WPL, bool M>
 static void launch_one(const MceArgs &a, dim3 g, dim3 b, size_t sm, cudaStream_t st) {
-    cudaFuncSetAttribute(mce_kernel<WPL, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    mce_kernel<WPL, M><<<g, b, sm, st>>>(a);
+    if (!M && a.deadline) {  // budgeted runs (never the metrics build)
+        cudaFuncSetAttribute(mce_kernel<WPL, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        mce_kernel<WPL, false, true><<<g, b, sm, st>>>(a);
+        return;
+    }
+    cudaFuncSetAttribute(mce_kernel<WPL, M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    mce_kernel<WPL, M, false><<<g, b, sm, st>>>(a);
 }
 
 template <int WPL, bool M>
 static int mce_occ(int warps_per_block) {
     const size_t sm = mce_smem_bytes(WPL, warps_per_block);
-    cudaFuncSetAttribute(mce_kernel<WPL, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(mce_kernel<WPL, M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mce_kernel<WPL, M>, 32 * warps_per_block, sm) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mce_kernel<WPL, M, false>, 32 * warps_per_block, sm) !=
         cudaSuccess)
         return 0;
     return nb;

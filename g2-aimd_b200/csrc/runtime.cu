@@ -736,8 +736,15 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
     a.status = ctx->d_status;
     a.work = (flags & G2_FLAG_WORK_MODEL) ? ctx->d_work : nullptr;
     const bool clique = ctx->clique_plan && !(o && o->intersect_mode == 1);
+    const uint32_t deadline_ms = o ? o->deadline_ms : 0u;
+    if (deadline_ms) {  // time budget: unfinished roots are dropped whole, so no hand-off
+        cudaError_t ed = g2::deadline_set(ctx->d_deadline, 1000000ull * deadline_ms, st);
+        if (ed != cudaSuccess) return fail_cuda(ctx, ed, "deadline_set");
+        ctx->launches++;
+        a.deadline = ctx->d_deadline;
+    }
     // plan walks (non-clique plans) hand pending work to idle warps
-    if (!clique && !(flags & G2_FLAG_NO_SPILL)) {
+    if (!clique && !(flags & G2_FLAG_NO_SPILL) && !deadline_ms) {
         rc = ensure_handoff(ctx, st);
         if (rc) return rc;
         cudaError_t eb = g2::epoch_bump(ctx->d_epoch, st);

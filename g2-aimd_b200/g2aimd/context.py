@@ -320,8 +320,13 @@ class Context:
         src = None if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
         o, keep = _opts(root_nodes=root_counts, root_cost=root_cost, **kw)
         count = C.c_uint64()
-        self._check(lib().g2_match_run(self._h, None if src is None else src.ctypes.data_as(C.c_void_p),
-                                       0 if src is None else src.size, C.byref(o), C.byref(count)), "g2_match_run")
+        rc = lib().g2_match_run(self._h, None if src is None else src.ctypes.data_as(C.c_void_p),
+                                0 if src is None else src.size, C.byref(o), C.byref(count))
+        # with a time budget (deadline_ms), G2_ERR_DEADLINE is a result: the count
+        # covers the roots that finished (root_cost > 0)
+        self.expired = rc == G2_ERR_DEADLINE and o.deadline_ms != 0
+        if not self.expired:
+            self._check(rc, "g2_match_run")
         del keep
         return count.value
 

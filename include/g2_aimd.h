@@ -136,13 +136,13 @@ typedef struct g2_opts {
                                    record, in SM cycles (0 = 2^37, about 70 s); a run
                                    whose wait ran out returns G2_ERR_TIMEOUT and the
                                    context stays usable                             */
-    uint32_t deadline_ms;       /* MCE: time budget of the run on the device (0 =
-                                   none).  Past it, warps start no new root and drop
-                                   the root they are walking (nothing of it counted),
-                                   so the run ends soon after; it returns
-                                   G2_ERR_DEADLINE with the totals, histogram and
-                                   per-root outputs (root_nodes > 0 = finished) of
-                                   the roots that finished.  Implies no hand-off.   */
+    uint32_t deadline_ms;       /* time budget of the run on the device (0 = none).
+                                   Past it, warps start no new root and drop the root
+                                   they are walking (nothing of it counted), so the
+                                   run ends soon after; it returns G2_ERR_DEADLINE
+                                   with the totals and per-root outputs of the roots
+                                   that finished: MCE root_nodes > 0, match
+                                   root_cost > 0 mark them.  Implies no hand-off.   */
 } g2_opts;
 
 /* g2_opts.flags */

@@ -35,3 +35,28 @@ def test_budget_run_out_keeps_finished_roots_exact(g2, orc):
         # the context runs normally afterwards
         c2, _h2 = c.mce(sources=done[:256], hist_len=128)
         assert c2 == orc.mce(g, roots=done[:256], hist_len=128)["count"] and not c.expired
+
+
+@pytest.mark.parametrize("q,budget", [(24, 1), (25, 2), (1, 5), (2, 5)])
+def test_match_budget_keeps_finished_roots_exact(g2, orc, q, budget):
+    """Plan-driven counts with a time budget: clique plans (bitmap path) and
+    plan walks (4-cycles, diamonds).  Finished roots are the ones with a
+    recorded cost; the count equals the oracle's over exactly those roots."""
+    from g2aimd.context import Context, Plan
+    g = g2.Graph.rmat(16, 16, seed=3).degeneracy_recoded()
+    plan = Plan.preset(q)
+    with Context(0) as c:
+        c.load(g)
+        c.load_core(g.core)
+        full = c.match(plan, schedule="heuristic", flags=1)
+        cost = np.zeros(g.n, np.uint64)
+        got = c.match(plan, root_cost=cost, schedule="heuristic", flags=1, deadline_ms=budget)
+        done = np.flatnonzero(cost > 0).astype(np.uint32)
+        if c.expired:
+            assert done.size < g.n and got <= full
+        else:
+            assert got == full
+        want = orc.match(g, plan, roots=done, threads=8)["count"]
+        assert got == want
+        # generous budget: everything finishes
+        assert c.match(plan, schedule="heuristic", flags=1, deadline_ms=600000) == full and not c.expired
