@@ -100,6 +100,15 @@ struct P0Filter {
 };
 constexpr uint32_t kFilterMul = 0x9E3779B1u;  // Fibonacci hashing
 
+// P0 entry j: from shared memory when P0 is staged there (SH), else from the
+// root's CSR slice in global memory.
+template <bool SH>
+__device__ __forceinline__ uint32_t p0_at(const uint32_t *P0, uint32_t j) {
+    if constexpr (SH) return P0[j];
+    else return ldg(P0 + j);
+}
+
+template <bool SH = false>
 __device__ __forceinline__ P0Filter filter_build(uint32_t *bits, uint32_t max_words, const uint32_t *P0, uint32_t p) {
     const uint32_t lane = lane_id();
     uint32_t fb = 10;  // at least 1024 bits
@@ -108,7 +117,7 @@ __device__ __forceinline__ P0Filter filter_build(uint32_t *bits, uint32_t max_wo
     for (uint32_t w = lane; w < words; w += 32) bits[w] = 0u;
     __syncwarp();
     for (uint32_t i = lane; i < p; i += 32) {
-        const uint32_t h = (ldg(P0 + i) * kFilterMul) >> shift;
+        const uint32_t h = (p0_at<SH>(P0, i) * kFilterMul) >> shift;
         atomicOr(bits + (h >> 5), 1u << (h & 31u));
     }
     __syncwarp();
@@ -120,11 +129,12 @@ __device__ __forceinline__ bool filter_maybe(const P0Filter &f, uint32_t y) {
     return (f.bits[h >> 5] >> (h & 31u)) & 1u;
 }
 
-// First index in [lo, hi) of the global array a with a[i] >= key.
-__device__ __forceinline__ uint32_t gmem_lower_bound(const uint32_t *a, uint32_t lo, uint32_t hi, uint32_t key) {
+// First index in [lo, hi) of P0 with P0[i] >= key (shared or global memory).
+template <bool SH>
+__device__ __forceinline__ uint32_t p0_lower_bound(const uint32_t *a, uint32_t lo, uint32_t hi, uint32_t key) {
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
-        if (ldg(a + mid) < key) lo = mid + 1;
+        if (p0_at<SH>(a, mid) < key) lo = mid + 1;
         else hi = mid;
     }
     return lo;
@@ -268,7 +278,7 @@ __device__ __noinline__ static unsigned long long count_forward_edges(const uint
 //  * reverse, when |P0[lo, p)| x log |list| is much smaller than the list (a
 //    small P0 next to a long list of the dense core): each lane takes P0
 //    entries and binary-searches them in the list.
-template <class F>
+template <bool SH, class F>
 __device__ __forceinline__ void warp_list_hits(const uint32_t *ci, uint64_t e0, uint64_t end, const uint32_t *P0,
                                                uint32_t lo, uint32_t p, uint32_t pmax, const P0Filter &f,
                                                uint32_t *queue, F on_hit) {
@@ -278,7 +288,7 @@ __device__ __forceinline__ void warp_list_hits(const uint32_t *ci, uint64_t e0, 
     const uint32_t R = p - lo;
     if ((uint64_t)R * (ilog2p1(L) + 1u) * 2u < L) {
         for (uint32_t j = lo + lane; j < p; j += 32) {
-            const uint32_t x = ldg(P0 + j);
+            const uint32_t x = p0_at<SH>(P0, j);
             const uint64_t k = lower_bound(ci, e0, end, x);
             if (k < end && ldg(ci + k) == x) on_hit(j);
         }
@@ -302,8 +312,8 @@ __device__ __forceinline__ void warp_list_hits(const uint32_t *ci, uint64_t e0, 
         __syncwarp();
         if (qn >= 32) {
             const uint32_t yq = queue[lane];
-            const uint32_t jq = gmem_lower_bound(P0, lo, p, yq);
-            if (jq < p && ldg(P0 + jq) == yq) on_hit(jq);
+            const uint32_t jq = p0_lower_bound<SH>(P0, lo, p, yq);
+            if (jq < p && p0_at<SH>(P0, jq) == yq) on_hit(jq);
             const uint32_t rest = qn - 32u;
             const uint32_t keep = lane < rest ? queue[32 + lane] : 0u;
             __syncwarp();
@@ -314,8 +324,8 @@ __device__ __forceinline__ void warp_list_hits(const uint32_t *ci, uint64_t e0, 
     }
     if (lane < qn) {
         const uint32_t yq = queue[lane];
-        const uint32_t jq = gmem_lower_bound(P0, lo, p, yq);
-        if (jq < p && ldg(P0 + jq) == yq) on_hit(jq);
+        const uint32_t jq = p0_lower_bound<SH>(P0, lo, p, yq);
+        if (jq < p && p0_at<SH>(P0, jq) == yq) on_hit(jq);
     }
     __syncwarp();
 }
@@ -329,21 +339,22 @@ constexpr uint32_t kQueueWords = 64;
 // forward slice in global memory and the filter and queue in `fbits` (fwords
 // words of shared memory).  One lane per short forward list; lists longer than
 // long_list are taken by the whole warp (warp_list_hits) into rowbuf.
+template <bool SH>
 __device__ __noinline__ static void build_upper_rows_filtered(const uint64_t *rp, const uint32_t *ci,
                                                               const uint32_t *fo, const uint32_t *P0, uint32_t p,
                                                               uint32_t W, uint32_t *A, uint32_t *rowbuf,
                                                               uint32_t *fbits, uint32_t fwords, uint32_t long_list) {
     const uint32_t lane = lane_id();
-    const uint32_t pmax = ldg(P0 + p - 1);
+    const uint32_t pmax = p0_at<SH>(P0, p - 1);
     for (uint32_t i = lane; i < p; i += 32)
         for (uint32_t w = i >> 5; w < W; w++) A[(uint64_t)i * W + w] = 0u;
     uint32_t *queue = fbits + fwords - kQueueWords;
-    const P0Filter f = filter_build(fbits, fwords - kQueueWords, P0, p);
+    const P0Filter f = filter_build<SH>(fbits, fwords - kQueueWords, P0, p);
     for (uint32_t i0 = 0; i0 < p; i0 += 32) {
         const uint32_t i = i0 + lane;
         bool big = false;
         if (i < p) {
-            const uint32_t u = ldg(P0 + i);
+            const uint32_t u = p0_at<SH>(P0, i);
             uint64_t e = ldg(rp + u) + ldg(fo + u);
             const uint64_t end = ldg(rp + u + 1);
             if (end - e > long_list) big = true;
@@ -354,8 +365,8 @@ __device__ __noinline__ static void build_upper_rows_filtered(const uint64_t *rp
                     const uint32_t y = ldg(ci + e);
                     if (y > pmax) break;
                     if (!filter_maybe(f, y)) continue;
-                    j = gmem_lower_bound(P0, j, p, y);
-                    if (j < p && ldg(P0 + j) == y) row[j >> 5] |= 1u << (j & 31u);
+                    j = p0_lower_bound<SH>(P0, j, p, y);
+                    if (j < p && p0_at<SH>(P0, j) == y) row[j >> 5] |= 1u << (j & 31u);
                 }
             }
         }
@@ -364,11 +375,11 @@ __device__ __noinline__ static void build_upper_rows_filtered(const uint64_t *rp
             const uint32_t l = __ffs(bigmask) - 1;
             bigmask &= bigmask - 1;
             const uint32_t ii = i0 + l;
-            const uint32_t u = ldg(P0 + ii);
+            const uint32_t u = p0_at<SH>(P0, ii);
             const uint64_t e0 = ldg(rp + u) + ldg(fo + u), end = ldg(rp + u + 1);
             for (uint32_t w = lane; w < W; w += 32) rowbuf[w] = 0u;
             __syncwarp();
-            warp_list_hits(ci, e0, end, P0, ii + 1, p, pmax, f, queue,
+            warp_list_hits<SH>(ci, e0, end, P0, ii + 1, p, pmax, f, queue,
                            [&](uint32_t j) { atomicOr(rowbuf + (j >> 5), 1u << (j & 31u)); });
             __syncwarp();
             for (uint32_t w = (ii >> 5) + lane; w < W; w += 32) A[(uint64_t)ii * W + w] = rowbuf[w];
@@ -379,19 +390,20 @@ __device__ __noinline__ static void build_upper_rows_filtered(const uint64_t *rp
 }
 
 // count_forward_edges with P0 in global memory and the filter and queue in fbits.
+template <bool SH>
 __device__ __noinline__ static unsigned long long count_forward_edges_filtered(
     const uint64_t *rp, const uint32_t *ci, const uint32_t *fo, const uint32_t *P0, uint32_t p, uint32_t part,
     uint32_t nparts, uint32_t *fbits, uint32_t fwords) {
     const uint32_t lane = lane_id();
-    const uint32_t pmax = ldg(P0 + p - 1);
+    const uint32_t pmax = p0_at<SH>(P0, p - 1);
     uint32_t *queue = fbits + fwords - kQueueWords;
-    const P0Filter f = filter_build(fbits, fwords - kQueueWords, P0, p);
+    const P0Filter f = filter_build<SH>(fbits, fwords - kQueueWords, P0, p);
     unsigned long long c = 0;
     for (uint32_t i0 = 0; i0 < p; i0 += 32) {
         const uint32_t i = i0 + lane;
         bool big = false;
         if (i < p && (nparts <= 1 || i % nparts == part)) {
-            const uint32_t u = ldg(P0 + i);
+            const uint32_t u = p0_at<SH>(P0, i);
             uint64_t e = ldg(rp + u) + ldg(fo + u);
             const uint64_t end = ldg(rp + u + 1);
             if (end - e > kLongListMatch) big = true;
@@ -401,8 +413,8 @@ __device__ __noinline__ static unsigned long long count_forward_edges_filtered(
                     const uint32_t y = ldg(ci + e);
                     if (y > pmax) break;
                     if (!filter_maybe(f, y)) continue;
-                    j = gmem_lower_bound(P0, j, p, y);
-                    c += j < p && ldg(P0 + j) == y;
+                    j = p0_lower_bound<SH>(P0, j, p, y);
+                    c += j < p && p0_at<SH>(P0, j) == y;
                 }
             }
         }
@@ -411,9 +423,9 @@ __device__ __noinline__ static unsigned long long count_forward_edges_filtered(
             const uint32_t l = __ffs(bigmask) - 1;
             bigmask &= bigmask - 1;
             const uint32_t ii = i0 + l;
-            const uint32_t u = ldg(P0 + ii);
+            const uint32_t u = p0_at<SH>(P0, ii);
             const uint64_t e0 = ldg(rp + u) + ldg(fo + u), end = ldg(rp + u + 1);
-            warp_list_hits(ci, e0, end, P0, ii + 1, p, pmax, f, queue, [&](uint32_t) { c++; });
+            warp_list_hits<SH>(ci, e0, end, P0, ii + 1, p, pmax, f, queue, [&](uint32_t) { c++; });
         }
     }
     return warp_sum_u64(c);

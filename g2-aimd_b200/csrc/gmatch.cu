@@ -467,18 +467,29 @@ __device__ bool match_root_clique(const MatchArgs &a, const DevPlan &pl, uint32_
     // slab: [A p*W] [frames (k) * (W + 1)]
     const uint64_t a0 = 0, f0 = (uint64_t)p * W;
     if (f0 + (uint64_t)k * (W + 1) > a.words_per_warp) return false;
-    // k <= 5 without metrics: P0 stays in global memory (the root's CSR slice)
-    // and its shared-memory region holds the membership filter instead
-    const uint32_t *P0 = ci + split;
-    if (!METRICS && k == 3) {  // triangles: count forward-neighbourhood edges while scanning
-        count = count_forward_edges_filtered(rp, ci, a.fo, P0, p, part, nparts, p0s, a.p0_words);
-        return true;
-    }
+    // k <= 5 without metrics: the shared region holds P0's membership filter and
+    // hit queue; P0 itself is staged in the region's first half when it fits
+    // there (the searches of filter hits then read shared memory), else it stays
+    // in its CSR slice in global memory.
     if (!METRICS && k <= 5) {
+        const uint32_t half = a.p0_words / 2;
+        const bool sh = p <= half;
+        if (sh) {
+            for (uint32_t i = lane; i < p; i += 32) p0s[i] = ldg(ci + split + i);
+            __syncwarp();
+        }
+        uint32_t *fb = sh ? p0s + half : p0s;
+        const uint32_t fw = sh ? a.p0_words - half : a.p0_words;
+        if (k == 3) {  // triangles: count forward-neighbourhood edges while scanning
+            count = sh ? count_forward_edges_filtered<true>(rp, ci, a.fo, p0s, p, part, nparts, fb, fw)
+                       : count_forward_edges_filtered<false>(rp, ci, a.fo, ci + split, p, part, nparts, fb, fw);
+            return true;
+        }
         // lane-parallel counting: lane takes the depth-1 vertices x = lane, lane+32, ...
         // (in ordinal order, so the split filter is x % nparts) and counts the
         // (k-2)-cliques above x serially; it reads only the upper part of rows.
-        build_upper_rows_filtered(rp, ci, a.fo, P0, p, W, S + a0, rowbuf, p0s, a.p0_words, kLongListMatch);
+        if (sh) build_upper_rows_filtered<true>(rp, ci, a.fo, p0s, p, W, S + a0, rowbuf, fb, fw, kLongListMatch);
+        else build_upper_rows_filtered<false>(rp, ci, a.fo, ci + split, p, W, S + a0, rowbuf, fb, fw, kLongListMatch);
         __syncwarp();
         count = clique_count_lanes(a, S + a0, p, W, k, part, nparts);
         return true;
