@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--scratch-mb", type=int, default=4096, help="device scratch for the DFS slabs")
     ap.add_argument("--fixed", action="store_true",
                     help="skip the plain-schedule timing and the autotuner (profiling runs)")
-    ap.add_argument("--leg", choices=["all", "mce", "view", "view-host", "c5", "c3"], default="all",
+    ap.add_argument("--leg", choices=["all", "mce", "view", "view-host", "c5", "c3", "walk"], default="all",
                     help="mce: only the maximal-clique workload (Chung-Lu 2^18), for profiling; "
                          "view: out-of-core runs over view bins against in-core runs; "
                          "view-host: the views' sizes and host build time alone (no GPU)")
@@ -229,6 +229,32 @@ def run_c5_leg(a):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     print(json.dumps(c5_leg(a, 0, torch, stream)), flush=True)
+
+
+def run_walk_leg(a):
+    """Plan walks alone (for profiling): 4-cycles (preset 1) on a Chung-Lu graph
+    shaped like the larger C4 members (n = 2e5, gamma 2.2, average degree 20),
+    heuristic order with hand-off, W warm-up and K timed runs; one JSON line."""
+    import torch
+
+    import g2aimd
+    from g2aimd.context import Context, Plan
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    g = g2aimd.Graph.chung_lu(200000, 2.2, 20.0, seed=1).degeneracy_recoded()
+    out = torch.zeros(1, dtype=torch.int64, device=dev)
+    with Context(0) as ctx:
+        ctx.load(g)
+        ctx.load_core(g.core)
+        ctx.set_plan(Plan.preset(1))
+        run = lambda: ctx.match_device(out.data_ptr(), stream=stream.cuda_stream, schedule="heuristic", flags=1)  # noqa
+        for _ in range(a.warmup):
+            run()
+        times = [ev_time(torch, stream, run)[1] for _ in range(a.steps)]
+        print(json.dumps({"workload": "4-cycles, chung-lu n=2e5 gamma 2.2 avg degree 20", "count": int(out[0].item()),
+                          "ms": times}), flush=True)
 
 
 def run_mce_leg(a):
@@ -994,6 +1020,8 @@ def main():
         run_c5_leg(a)
     elif a.leg == "c3":
         run_c3_leg(a)
+    elif a.leg == "walk":
+        run_walk_leg(a)
     elif a.leg == "mce":
         run_mce_leg(a)
     elif a.leg == "view":

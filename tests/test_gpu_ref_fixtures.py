@@ -107,15 +107,15 @@ def test_rmat20_k5_where_the_reference_cannot_count(g2, orc, ctx):
     # the generic plan walk (candidate lists + binary searches, hand-off) is
     # an independent device path: the same count for every root of a stride
     # sample (all roots through the walk take minutes)
-    sample = np.arange(0, g.n, 128, dtype=np.uint32)
+    sample = np.arange(0, g.n, 512, dtype=np.uint32)
     per_walk = np.zeros(sample.size, np.uint64)
     assert ctx.match(plan, sources=sample, root_counts=per_walk, intersect_mode=1) == int(per[sample].sum())
     assert np.array_equal(per[sample], per_walk)
-    # oracle on random roots and the 32 heaviest roots of at most 2e7 5-cliques
+    # oracle on random roots and the 16 heaviest roots of at most 2e7 5-cliques
     # each (the heaviest hold ~1e9 each: minutes of CPU time per root)
     order = np.argsort(per, kind="stable")
     light = order[per[order] <= 20_000_000]
     rng = np.random.default_rng(11)
-    roots = np.unique(np.concatenate([light[-32:], rng.choice(g.n, 2048, replace=False)])).astype(np.uint32)
+    roots = np.unique(np.concatenate([light[-16:], rng.choice(g.n, 1024, replace=False)])).astype(np.uint32)
     want = orc.match(g, plan, roots=roots, threads=os.cpu_count() or 1, per_root=True)["root_counts"]
     assert np.array_equal(per[roots], want)
