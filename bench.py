@@ -300,7 +300,7 @@ def view_legs(a, g, steps, warmup):
         pci = torch.from_numpy(g.cols.view(np.int32)).pin_memory()
         return g2aimd.Graph(prp.numpy().view(np.uint64), pci.numpy().view(np.uint32)), (prp, pci)
 
-    def leg(name, g, shape, view_fn, core_fn):
+    def leg(name, g, shape, view_fn, core_fn, device_fn=None):
         csr = g.row_ptrs.nbytes + g.cols.nbytes
         budget = csr // a.view_split
         t0 = time.perf_counter()
@@ -315,6 +315,14 @@ def view_legs(a, g, steps, warmup):
                 t0 = time.perf_counter()
                 c_view, st = view_fn(ctx, pg, bins, nb)
                 vt.append((time.perf_counter() - t0) * 1e3)
+            dvt, c_dev, st_dev = [], None, None
+            if device_fn is not None:  # the same views built by the GPU (G2_VIEW_DEVICE)
+                for _ in range(warmup):
+                    c_dev, st_dev = device_fn(ctx, pg, bins, nb)
+                for _ in range(steps):
+                    t0 = time.perf_counter()
+                    c_dev, st_dev = device_fn(ctx, pg, bins, nb)
+                    dvt.append((time.perf_counter() - t0) * 1e3)
             for _ in range(warmup):
                 ctx.load(pg)
                 c_core = core_fn(ctx)
@@ -325,22 +333,31 @@ def view_legs(a, g, steps, warmup):
                 c_core = core_fn(ctx)
                 ct.append((time.perf_counter() - t0) * 1e3)
         assert c_view == c_core, (name, c_view, c_core)
+        assert c_dev is None or c_dev == c_core, (name, c_dev, c_core)
         del keep
         out[name] = {"graph": {"n": g.n, "m": g.m}, "shape": shape, "csr_bytes": int(csr),
                      "bin_budget_bytes": int(budget), "bins": nb, "bin_plan_s": round(bin_s, 3),
                      "count": int(c_view), "view_ms": float(np.mean(vt)), "in_core_ms": float(np.mean(ct)),
                      "view_vs_in_core": float(np.mean(ct)) / float(np.mean(vt)), "stats": st}
+        if dvt:
+            out[name].update({"device_built_view_ms": float(np.mean(dvt)),
+                              "device_built_vs_in_core": float(np.mean(ct)) / float(np.mean(dvt)),
+                              "device_built_stats": st_dev})
 
     k4 = Plan.preset(K4)
     leg(f"k4_rmat_s{a.scale}", g, k4.view_shape(),
         lambda ctx, pg, bins, nb: (lambda c, _pb, st: (c, st))(
             *ctx.view_match(pg, bins, k4, nbins=nb, producers=producers, schedule="heuristic", **launch)),
-        lambda ctx: ctx.match(k4, schedule="heuristic", **launch))
+        lambda ctx: ctx.match(k4, schedule="heuristic", **launch),
+        lambda ctx, pg, bins, nb: (lambda c, _pb, st: (c, st))(
+            *ctx.view_match(pg, bins, k4, nbins=nb, device=True, schedule="heuristic", **launch)))
     cl = g2aimd.Graph.chung_lu(1 << 18, 2.3, 16.0, seed=a.seed).degeneracy_recoded()
     leg("mce_chung_lu_2^18", cl, {"radius": 1, "row_radius": 1, "min_root_degree": 1, "upper": False},
         lambda ctx, pg, bins, nb: (lambda c, _h, _pb, st: (c, st))(
             *ctx.view_mce(pg, bins, nbins=nb, hist_len=HIST, producers=producers, schedule="heuristic")),
-        lambda ctx: ctx.mce(hist_len=HIST, schedule="heuristic")[0])
+        lambda ctx: ctx.mce(hist_len=HIST, schedule="heuristic")[0],
+        lambda ctx, pg, bins, nb: (lambda c, _h, _pb, st: (c, st))(
+            *ctx.view_mce(pg, bins, nbins=nb, hist_len=HIST, device=True, schedule="heuristic")))
     return out
 
 

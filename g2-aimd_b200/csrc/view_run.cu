@@ -20,6 +20,7 @@
 #include "g2_aimd.h"
 #include "host/view_host.h"
 #include "runtime_internal.h"
+#include "view_device.h"
 
 using namespace g2rt;
 
@@ -314,7 +315,9 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
     if (vo && vo->row_radius) shape.row_radius = vo->row_radius;
     if (vo && (vo->flags & G2_VIEW_NO_UPPER)) shape.upper = shape.forward = false;
     if (vo && (vo->flags & G2_VIEW_EGO)) shape.ego = true;
-    if (vo && (vo->flags & ~(uint32_t)(G2_VIEW_NO_UPPER | G2_VIEW_EGO))) return G2_ERR_INVALID;
+    if (vo && (vo->flags & ~(uint32_t)(G2_VIEW_NO_UPPER | G2_VIEW_EGO | G2_VIEW_DEVICE))) return G2_ERR_INVALID;
+    const bool device_build = vo && (vo->flags & G2_VIEW_DEVICE);
+    if (device_build && (shape.radius != 1 || shape.row_radius != 1 || shape.ego)) return G2_ERR_UNSUPPORTED;
     if (shape.row_radius > shape.radius || shape.radius > 15) return G2_ERR_INVALID;
     if (shape.ego && (shape.radius != 1 || shape.row_radius != 1)) return G2_ERR_INVALID;
     // roots grouped by bin, ascending inside a bin
@@ -359,7 +362,65 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
     if (bin_counts) memset(bin_counts, 0, sizeof(uint64_t) * nbins);
     g2_view_stats st{};
     uint32_t *saved_fo = ctx->d_fo;
-    {
+    if (device_build) {
+        // the GPU builds each view into a device slot on the copy stream; the
+        // next view's build overlaps the current run on the legacy stream
+        ViewDevice dev(ctx);
+        DeviceViewBuilder vb;
+        rc = dev.init();
+        if (!rc) rc = vb.init(ctx, rp, ci, n, shape);
+        int d = 0;
+        uint32_t b = 0;
+        ReadyView cur, nxt;
+        auto build_next = [&](ReadyView *v, int slot) -> int {
+            // next bin with a kept source; its view in device slot `slot`
+            for (; b < nbins; b++) {
+                const auto t0 = std::chrono::steady_clock::now();
+                int r = fail_cuda_if(ctx, cudaStreamWaitEvent(dev.copy, dev.done[slot], 0), "view wait");
+                if (!r) r = fail_cuda_if(ctx, cudaEventRecord(dev.t_copy[slot][0], dev.copy), "view record");
+                g2view::Sizes sz;
+                if (!r)
+                    r = vb.build(roots.data() + start[b], start[b + 1] - start[b], &dev.buf[slot], &dev.cap[slot],
+                                 dev.copy, &sz);
+                if (!r) r = fail_cuda_if(ctx, cudaEventRecord(dev.t_copy[slot][1], dev.copy), "view record");
+                if (!r) r = fail_cuda_if(ctx, cudaEventRecord(dev.copied[slot], dev.copy), "view record");
+                st.build_ms += ms_between(t0, std::chrono::steady_clock::now());
+                if (r) return r;
+                if (sz.nsrc) {
+                    v->bin = b++;
+                    v->slot = slot;
+                    v->sizes = sz;
+                    return G2_OK;
+                }
+            }
+            v->slot = -1;
+            return G2_OK;
+        };
+        if (!rc) rc = build_next(&cur, d);
+        while (!rc && cur.slot >= 0) {
+            rc = fail_cuda_if(ctx, cudaStreamWaitEvent(nullptr, dev.copied[d], 0), "view wait");
+            if (rc) break;
+            const uint32_t *d_src = dev.bind(cur, d);
+            rc = fail_cuda_if(ctx, cudaEventRecord(dev.t_run[0], nullptr), "view record");
+            if (!rc) rc = job.enqueue(ctx, d_src, cur.sizes.nsrc);
+            if (!rc) rc = fail_cuda_if(ctx, cudaEventRecord(dev.t_run[1], nullptr), "view record");
+            if (!rc) rc = fail_cuda_if(ctx, cudaEventRecord(dev.done[d], nullptr), "view record");
+            if (!rc) rc = build_next(&nxt, d ^ 1);
+            if (!rc) rc = job.finish(ctx);
+            if (rc) break;
+            total += job.h[0];
+            for (uint32_t s = 0; s < job.hist_len; s++) hsum[s] += job.h[1 + s];
+            if (bin_counts) bin_counts[cur.bin] = job.h[0];
+            st.bins++;
+            st.view_vertices += cur.sizes.n;
+            st.view_edges += cur.sizes.m;
+            st.max_view_bytes = std::max(st.max_view_bytes, g2view::Layout(cur.sizes).bytes);
+            st.copy_ms += dev.copy_ms(d);  // device time of the view's build
+            st.run_ms += dev.run_ms();
+            cur = nxt;
+            d ^= 1;
+        }
+    } else {
         ViewProducers prod;  // destroyed after dev, whose destructor waits for uploads from its slots
         ViewDevice dev(ctx);
         rc = dev.init();

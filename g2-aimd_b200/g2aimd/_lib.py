@@ -66,7 +66,7 @@ class G2ViewStats(C.Structure):
 
 
 G2_VIEW_NO_BIN = 0xFFFFFFFF
-G2_VIEW_UPPER, G2_VIEW_NO_UPPER, G2_VIEW_FORWARD, G2_VIEW_EGO = 1, 2, 4, 8
+G2_VIEW_UPPER, G2_VIEW_NO_UPPER, G2_VIEW_FORWARD, G2_VIEW_EGO, G2_VIEW_DEVICE = 1, 2, 4, 8, 16
 
 _lib = None
 

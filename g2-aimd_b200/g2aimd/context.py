@@ -331,22 +331,26 @@ class Context:
         return count.value
 
     # out-of-core runs over view bins: the graph stays in host memory
-    def _view_args(self, graph, bin_of, nbins, producers, radius, row_radius, no_upper, ego=False, slots=0):
-        from ._lib import G2_VIEW_EGO, G2_VIEW_NO_UPPER, G2ViewOpts
+    def _view_args(self, graph, bin_of, nbins, producers, radius, row_radius, no_upper, ego=False, slots=0,
+                   device=False):
+        from ._lib import G2_VIEW_DEVICE, G2_VIEW_EGO, G2_VIEW_NO_UPPER, G2ViewOpts
         bins = np.ascontiguousarray(bin_of, dtype=np.uint32)
         if nbins is None:
             valid = bins[bins != 0xFFFFFFFF]
             nbins = int(valid.max()) + 1 if valid.size else 0
         vo = G2ViewOpts(producers, radius, row_radius,
-                        (G2_VIEW_NO_UPPER if no_upper else 0) | (G2_VIEW_EGO if ego else 0), slots)
+                        (G2_VIEW_NO_UPPER if no_upper else 0) | (G2_VIEW_EGO if ego else 0) |
+                        (G2_VIEW_DEVICE if device else 0), slots)
         return bins, nbins, vo
 
     def view_mce(self, graph, bin_of, nbins=None, hist_len=256, producers=0, radius=0, row_radius=0, ego=False,
-                 slots=0, **kw):
+                 slots=0, device=False, **kw):
         """(count, hist, per-bin counts, stats) of maximal cliques of a host graph
-        enumerated view bin by view bin (g2_view_mce); ego: ego-network rows."""
+        enumerated view bin by view bin (g2_view_mce); ego: ego-network rows;
+        device: views built by the GPU (G2_VIEW_DEVICE)."""
         from ._lib import G2ViewStats
-        bins, nbins, vo = self._view_args(graph, bin_of, nbins, producers, radius, row_radius, False, ego, slots)
+        bins, nbins, vo = self._view_args(graph, bin_of, nbins, producers, radius, row_radius, False, ego, slots,
+                                          device)
         o, keep = _opts(**kw)
         count = C.c_uint64()
         hist = np.zeros(hist_len, np.uint64)
@@ -362,13 +366,14 @@ class Context:
         return count.value, hist, per_bin[:nbins], st.to_dict()
 
     def view_match(self, graph, bin_of, plan: Plan = None, nbins=None, producers=0, radius=0, row_radius=0,
-                   no_upper=False, ego=False, slots=0, **kw):
+                   no_upper=False, ego=False, slots=0, device=False, **kw):
         """(count, per-bin counts, stats) of the plan's matches in a host graph,
         view bin by view bin (g2_view_match)."""
         from ._lib import G2ViewStats
         if plan is not None:
             self.set_plan(plan)
-        bins, nbins, vo = self._view_args(graph, bin_of, nbins, producers, radius, row_radius, no_upper, ego, slots)
+        bins, nbins, vo = self._view_args(graph, bin_of, nbins, producers, radius, row_radius, no_upper, ego, slots,
+                                          device)
         o, keep = _opts(**kw)
         count = C.c_uint64()
         per_bin = np.zeros(max(nbins, 1), np.uint64)

@@ -300,6 +300,12 @@ int g2_degeneracy_order_device(g2_ctx *ctx, uint32_t *perm, uint32_t *core);
 #define G2_VIEW_NO_UPPER 2u  /* g2_view_opts: full balls and rows even where the query
                                 allows upper balls and forward rows; G2_VIEW_EGO there asks
                                 for ego rows (radius-1 views only) */
+#define G2_VIEW_DEVICE 16u   /* g2_view_opts: the GPU builds each view (same bytes as the
+                                host build) straight into its device slot, reading the
+                                host CSR through mapped pinned memory (registered for the
+                                call if it is not pinned); radius-1 views without ego rows
+                                (MCE, triangles, cliques), else G2_ERR_UNSUPPORTED.  No
+                                host producers, no uploads                       */
 typedef struct g2_view_opts {
     uint32_t producers;   /* host threads building views (0 = min(8, cores), fewer
                              if their marks, 4 bytes and a bit per vertex each,
@@ -308,7 +314,7 @@ typedef struct g2_view_opts {
                              for large views                                     */
     uint32_t radius;      /* ball radius (0 = from the query: 1 for MCE)         */
     uint32_t row_radius;  /* rows kept up to this distance (0 = from the query)  */
-    uint32_t flags;       /* G2_VIEW_NO_UPPER, G2_VIEW_EGO                       */
+    uint32_t flags;       /* G2_VIEW_NO_UPPER, G2_VIEW_EGO, G2_VIEW_DEVICE        */
     uint32_t slots;       /* pinned host buffers holding built views, each as
                              large as the largest view (0 = producers + 2; at
                              least 2): bounds pinned memory, as the reference's

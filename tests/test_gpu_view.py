@@ -122,3 +122,43 @@ def test_view_runs_with_bounded_pinned_buffers(vctx, orc, c1_graph):
     c, pb, _ = vctx.view_match(g, bin_of, Plan.preset(24), producers=4, slots=2)
     assert c == want
     vctx.load(g)
+
+
+@pytest.mark.parametrize("nbins", [1, 7, 64])
+def test_device_built_views_mce(vctx, orc, c1_graph, nbins):
+    """Views built by the GPU from the mapped host CSR (G2_VIEW_DEVICE) give
+    the host-built views' sizes and per-bin results, and the oracle's totals."""
+    g = c1_graph
+    want = orc.mce(g, hist_len=64)
+    bin_of = np.random.default_rng(nbins + 100).integers(0, nbins, g.n).astype(np.uint32)
+    c_h, h_h, pb_h, st_h = vctx.view_mce(g, bin_of, nbins=nbins, hist_len=64, producers=2)
+    c_d, h_d, pb_d, st_d = vctx.view_mce(g, bin_of, nbins=nbins, hist_len=64, device=True)
+    assert c_d == c_h == want["count"]
+    assert np.array_equal(h_d, want["hist"]) and np.array_equal(pb_d, pb_h)
+    assert (st_d["bins"], st_d["view_vertices"], st_d["view_edges"]) == \
+        (st_h["bins"], st_h["view_vertices"], st_h["view_edges"])
+    vctx.load(g)
+
+
+@pytest.mark.parametrize("q", [0, 24, 25])
+def test_device_built_views_cliques(vctx, orc, g2, q):
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(12, 16, seed=4).degeneracy_recoded()
+    plan = Plan.preset(q)
+    nb, bin_of = g.view_bins(max_bytes=64 << 10, **plan.view_shape())
+    assert nb > 2
+    want = orc.match(g, plan, threads=8)["count"]
+    c_h, pb_h, st_h = vctx.view_match(g, bin_of, plan, producers=2)
+    c_d, pb_d, st_d = vctx.view_match(g, bin_of, plan, device=True)
+    assert c_d == c_h == want and np.array_equal(pb_d, pb_h)
+    assert (st_d["view_vertices"], st_d["view_edges"]) == (st_h["view_vertices"], st_h["view_edges"])
+    vctx.load(g)
+
+
+def test_device_built_views_need_radius_one(vctx, g2):
+    from g2aimd._lib import G2Error
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(10, 8, seed=5).degeneracy_recoded()
+    with pytest.raises(G2Error):  # 4-cycles need radius-2 views: host-built only
+        vctx.view_match(g, (np.arange(g.n) % 3).astype(np.uint32), Plan.preset(1), device=True)
+    vctx.load(g)
