@@ -28,6 +28,8 @@
 #include "runtime_internal.h"
 #include "view_device.h"
 
+using namespace g2rt;
+
 namespace {
 
 constexpr uint64_t kLongRow = 256;  // rows longer than this find their start by binary search
@@ -384,3 +386,73 @@ DeviceViewBuilder::~DeviceViewBuilder() {
 }
 
 }  // namespace g2rt
+
+extern "C" int g2_view_materialize_device(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n,
+                                          const uint32_t *sources, uint64_t nsrc, uint32_t min_root_degree,
+                                          uint32_t flags, g2_view *out) {
+    if (!ctx || !row_ptrs || !out || (!sources && nsrc) || (!cols && row_ptrs[n]) || n >= (1ull << 32))
+        return G2_ERR_INVALID;
+    if (flags & ~(uint32_t)(G2_VIEW_UPPER | G2_VIEW_FORWARD)) return G2_ERR_UNSUPPORTED;
+    for (uint64_t i = 0; i < nsrc; i++)
+        if (sources[i] >= n) return G2_ERR_INVALID;
+    memset(out, 0, sizeof(*out));
+    G2_TRY(cudaSetDevice(ctx->device));
+    g2view::Shape sh;
+    sh.radius = sh.row_radius = 1;
+    sh.min_deg = min_root_degree;
+    sh.upper = (flags & G2_VIEW_UPPER) != 0;
+    sh.forward = (flags & G2_VIEW_FORWARD) != 0;
+    // the view lands in the context's first view slot: its graph gives way
+    if (ctx->owns_csr) {
+        cudaFree(ctx->d_rp);
+        cudaFree(ctx->d_ci);
+        ctx->rp_cap = ctx->ci_cap = 0;
+    }
+    ctx->d_rp = nullptr;
+    ctx->d_ci = nullptr;
+    ctx->owns_csr = false;
+    ctx->n = ctx->m = 0;
+    g2view::Sizes s;
+    uint32_t *ball_host = nullptr;
+    {
+        g2rt::DeviceViewBuilder vb;
+        int rc = vb.init(ctx, row_ptrs, cols, n, sh);
+        if (!rc) rc = vb.build(sources, nsrc, &ctx->view_dev[0], &ctx->view_dev_cap[0], nullptr, &s);
+        if (rc) return rc;
+        G2_TRY(cudaStreamSynchronize(nullptr));
+        ball_host = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.n, 1)));
+        if (!ball_host) return G2_ERR_OOM;
+        if (s.n && cudaMemcpy(ball_host, vb.ball, 4 * s.n, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            free(ball_host);
+            return fail_cuda(ctx, cudaGetLastError(), "view ids");
+        }
+    }
+    const g2view::Layout L(s);
+    auto *rp = static_cast<uint64_t *>(malloc(8 * (s.n + 1)));
+    auto *fo = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.n, 1)));
+    auto *ci = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.m, 1)));
+    auto *src = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.nsrc, 1)));
+    if (!rp || !fo || !ci || !src) {
+        free(rp), free(fo), free(ci), free(src), free(ball_host);
+        return G2_ERR_OOM;
+    }
+    const char *b = static_cast<const char *>(ctx->view_dev[0]);
+    cudaError_t e = cudaMemcpy(rp, b, 8 * (s.n + 1), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && s.n) e = cudaMemcpy(fo, b + L.fo, 4 * s.n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && s.m) e = cudaMemcpy(ci, b + L.ci, 4 * s.m, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && s.nsrc) e = cudaMemcpy(src, b + L.src, 4 * s.nsrc, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        free(rp), free(fo), free(ci), free(src), free(ball_host);
+        return fail_cuda(ctx, e, "view copy-back");
+    }
+    out->row_ptrs = rp;
+    out->cols = ci;
+    out->fwd_offsets = fo;
+    out->sources = src;
+    out->ids = ball_host;
+    out->n = s.n;
+    out->m = s.m;
+    out->nsrc = s.nsrc;
+    out->max_fwd = s.max_fwd;
+    return G2_OK;
+}

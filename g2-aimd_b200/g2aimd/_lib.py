@@ -111,6 +111,8 @@ def lib():
         "g2_view_materialize": (i32, [C.c_void_p, C.c_void_p, u64, C.c_void_p, u64, u32, u32, u32, u32,
                                       P(G2View)]),
         "g2_view_free": (None, [P(G2View)]),
+        "g2_view_materialize_device": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, C.c_void_p, u64, u32, u32,
+                                             P(G2View)]),
         "g2_plan_view_radius": (i32, [P(G2Plan), P(u32), P(u32), P(u32), P(u32)]),
         "g2_view_bins": (i32, [C.c_void_p, C.c_void_p, u64, u32, u32, u32, u32, u64, C.c_void_p, P(u32)]),
         "g2_view_bins_rebalance": (i32, [C.c_void_p, u64, C.c_void_p, u32, u32, u32, i32, P(u32)]),

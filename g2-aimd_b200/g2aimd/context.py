@@ -287,6 +287,34 @@ class Context:
         self.graph, self.n, self.m = None, 1 << scale, m.value
         return m.value
 
+    def view_device(self, graph, sources, min_root_degree=0, upper=False, forward=False):
+        """Graph.view's radius-1 view of `sources` built by this context's GPU
+        (g2_view_materialize_device): (view graph, local sources, global ids).
+        Releases the context's loaded graph."""
+        from ._lib import G2View
+        from .graph import Graph
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        v = G2View()
+        self._check(lib().g2_view_materialize_device(
+            self._h, graph.row_ptrs.ctypes.data_as(C.c_void_p), graph.cols.ctypes.data_as(C.c_void_p), graph.n,
+            src.ctypes.data_as(C.c_void_p), src.size, min_root_degree,
+            int(bool(upper)) | 4 * int(bool(forward)), C.byref(v)), "g2_view_materialize_device")
+        self.graph, self.n = None, 0
+        try:
+            n, m, ns = v.n, v.m, v.nsrc
+            rp = np.ctypeslib.as_array(v.row_ptrs, shape=(n + 1,)).copy()
+            ci = np.ctypeslib.as_array(v.cols, shape=(max(m, 1),))[:m].copy()
+            fo = np.ctypeslib.as_array(v.fwd_offsets, shape=(max(n, 1),))[:n].copy()
+            lsrc = np.ctypeslib.as_array(v.sources, shape=(max(ns, 1),))[:ns].copy()
+            ids = np.ctypeslib.as_array(v.ids, shape=(max(n, 1),))[:n].copy()
+            max_fwd = v.max_fwd
+        finally:
+            lib().g2_view_free(C.byref(v))
+        g = Graph(rp, ci, f"{graph.name}+view")
+        g.fwd_offsets = fo
+        g.max_fwd = max_fwd
+        return g, lsrc, ids
+
     def set_plan(self, plan: Plan):
         self._check(lib().g2_set_plan(self._h, C.byref(plan.raw)), "g2_set_plan")
         return self

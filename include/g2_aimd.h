@@ -498,6 +498,13 @@ int g2_view_materialize(const uint64_t *row_ptrs, const uint32_t *cols, uint64_t
                         uint32_t row_radius, uint32_t min_root_degree, uint32_t flags,
                         g2_view *out);
 void g2_view_free(g2_view *view);
+/* The same view built by the GPU of `ctx` (the builder G2_VIEW_DEVICE uses in
+ * view runs), copied back into malloc'd arrays (release with g2_view_free):
+ * radius 1, row radius 1, no G2_VIEW_EGO (else G2_ERR_UNSUPPORTED).  The
+ * context's loaded graph is released.  No counterpart in the reference. */
+int g2_view_materialize_device(g2_ctx *ctx, const uint64_t *row_ptrs, const uint32_t *cols, uint64_t n,
+                               const uint32_t *sources, uint64_t nsrc, uint32_t min_root_degree,
+                               uint32_t flags, g2_view *out);
 /* Radius, row radius, root degree and flags (G2_VIEW_UPPER, G2_VIEW_FORWARD) a plan's views
  * need (system/plan.h:51-73 derives the reference's single hop count from the
  * same query distances). */

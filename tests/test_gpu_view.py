@@ -162,3 +162,20 @@ def test_device_built_views_need_radius_one(vctx, g2):
     with pytest.raises(G2Error):  # 4-cycles need radius-2 views: host-built only
         vctx.view_match(g, (np.arange(g.n) % 3).astype(np.uint32), Plan.preset(1), device=True)
     vctx.load(g)
+
+
+@pytest.mark.parametrize("shape", [dict(), dict(upper=True), dict(upper=True, forward=True), dict(forward=True)])
+def test_device_built_view_bytes_equal_host_build(vctx, g2, shape):
+    """g2_view_materialize_device gives the host builder's view exactly: row
+    pointers, columns, forward offsets, sources, global ids, max forward degree
+    (R-MAT s13 with a hub-heavy and a light root set; minimum root degree 3)."""
+    g = g2.Graph.rmat(13, 16, seed=6).degeneracy_recoded()
+    rng = np.random.default_rng(3)
+    for src in (np.arange(g.n - 600, g.n, dtype=np.uint32), np.sort(rng.choice(g.n, 900, replace=False))):
+        src = src.astype(np.uint32)
+        h, hs, hid = g.view(src, radius=1, row_radius=1, min_root_degree=3, **shape)
+        d, ds, did = vctx.view_device(g, src, min_root_degree=3, **shape)
+        assert np.array_equal(h.row_ptrs, d.row_ptrs) and np.array_equal(h.cols, d.cols)
+        assert np.array_equal(h.fwd_offsets, d.fwd_offsets) and h.max_fwd == d.max_fwd
+        assert np.array_equal(hs, ds) and np.array_equal(hid, did)
+    vctx.load(g)
