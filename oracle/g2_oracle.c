@@ -32,6 +32,12 @@
  *              (core number = peel level).
  *   orc_embeddings  brute-force count of injective edge-preserving maps of a
  *              query into a graph (independent check: count = embeddings/|Aut|).
+ *   orc_gen_rmat, orc_degeneracy_recode  the seeded R-MAT input (the library's
+ *              generator, restated) and the kcore tool's degeneracy order and
+ *              recode (kmeans/kcore.cpp:126-191), so that a CPU measurement of
+ *              the reference algorithm builds its input without the library.
+ * Roots are taken one at a time by the OpenMP threads (dynamic, 1): a few
+ * dense-core roots carry most of the work.
  *
  * Parity status: pinned.  The MCE count and histogram are graph invariants
  * (number of maximal cliques with >= 2 vertices, by size), checked against a
@@ -278,7 +284,7 @@ int orc_mce(const uint64_t *rp, const uint32_t *ci, uint64_t n, const uint32_t *
         c.ci = ci;
         c.hist_len = hist_len;
         if (hist) c.hist = (uint64_t *)calloc(hist_len, sizeof(uint64_t));
-#pragma omp for schedule(dynamic, 16)
+#pragma omp for schedule(dynamic, 1)
         for (int64_t t = 0; t < (int64_t)nroots; t++) {
             uint32_t v = roots ? roots[t] : (uint32_t)t;
             uint64_t lo = rp[v], hi = rp[v + 1];
@@ -405,7 +411,7 @@ int orc_match(const uint64_t *rp, const uint32_t *ci, uint64_t n, const uint32_t
         c.rp = rp;
         c.ci = ci;
         c.pl = &pl;
-#pragma omp for schedule(dynamic, 64)
+#pragma omp for schedule(dynamic, 1)
         for (int64_t t = 0; t < (int64_t)nroots; t++) {
             uint64_t c0 = c.count;
             c.M[0] = roots ? roots[t] : (uint32_t)t;
