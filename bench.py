@@ -131,14 +131,19 @@ def c5_leg(a, local, torch, stream, scale=26, ef=28, k5_stride=16384, mce_budget
         out["triangle"] = {"count": count(), "ms": ms, "per_s": count() / (ms / 1000.0)}
         ctx.set_plan(Plan.preset(24))
         _, plain_ms = ev_time(torch, stream, lambda: ctx.match_device(
-            d_out.data_ptr(), stream=sptr, schedule="heuristic", flags=1, **launch))
+            d_out.data_ptr(), stream=sptr, schedule="given", flags=1, **launch))
         k4 = count()
+        _, heur_ms = ev_time(torch, stream, lambda: ctx.match_device(
+            d_out.data_ptr(), stream=sptr, schedule="heuristic", flags=1, **launch))
+        assert count() == k4
         _, learned_ms = ev_time(torch, stream, lambda: ctx.match_device(
             d_out.data_ptr(), stream=sptr, schedule="learned", flags=1 | 8, **launch))
         assert count() == k4, (count(), k4)
-        out["k4"] = {"count": k4, "plain_heuristic_ms": plain_ms, "learned_ms": learned_ms,
-                     "learned_vs_plain": plain_ms / learned_ms, "per_s": k4 / (learned_ms / 1000.0),
-                     "launch": launch, "note": "both schedules without heavy-root splits, same launch parameters"}
+        out["k4"] = {"count": k4, "plain_kcore_order_ms": plain_ms, "plain_heuristic_ms": heur_ms,
+                     "learned_ms": learned_ms, "learned_vs_plain": plain_ms / learned_ms,
+                     "learned_vs_degree_core_heuristic": heur_ms / learned_ms, "per_s": k4 / (learned_ms / 1000.0),
+                     "launch": launch, "note": "plain = the reference's kcore root order; no heavy-root splits, "
+                                               "same launch parameters"}
         roots = np.arange(0, 1 << scale, k5_stride, dtype=np.uint32)
         d_roots = torch.from_numpy(roots.view(np.int32)).to(d_out.device)
         ctx.set_plan(Plan.preset(25))
@@ -194,7 +199,7 @@ def c3_leg(a, local, torch, stream, reps=3, budget_ms=30000):
             ctx.degeneracy_recode()
             rec = {"graph": f"rmat-s{sc}-ef16 + 200 planted cliques of 20-60 vertices (seed 1)", "m": int(m)}
             res = {}
-            for sched in ("heuristic", "learned"):
+            for sched in ("given", "heuristic", "learned"):
                 run = lambda sched=sched: ctx.mce(hist_len=256, schedule=sched, flags=1)  # noqa: E731
                 run()
                 times = []
@@ -202,11 +207,13 @@ def c3_leg(a, local, torch, stream, reps=3, budget_ms=30000):
                     (c, h), ms = wall_ms(torch, run)
                     times.append(ms)
                 res[sched] = (int(c), h, float(np.median(times)))
-            assert res["heuristic"][0] == res["learned"][0]
-            assert np.array_equal(res["heuristic"][1], res["learned"][1])
-            rec.update({"maximal_cliques": res["learned"][0], "plain_heuristic_ms": res["heuristic"][2],
-                        "learned_ms": res["learned"][2],
-                        "learned_vs_plain": res["heuristic"][2] / res["learned"][2],
+            for sched in ("given", "heuristic"):
+                assert res[sched][0] == res["learned"][0]
+                assert np.array_equal(res[sched][1], res["learned"][1])
+            rec.update({"maximal_cliques": res["learned"][0], "plain_kcore_order_ms": res["given"][2],
+                        "plain_heuristic_ms": res["heuristic"][2], "learned_ms": res["learned"][2],
+                        "learned_vs_plain": res["given"][2] / res["learned"][2],
+                        "learned_vs_degree_core_heuristic": res["heuristic"][2] / res["learned"][2],
                         "largest_clique": int(np.flatnonzero(res["learned"][1])[-1]),
                         "note": "same hand-off and launch parameters; histograms equal"})
             out["planted"].append(rec)
@@ -879,13 +886,21 @@ def run_ours(a):
     # (launch parameters, hand-off, heavy-root splits iff the learned run splits):
     # the two differ in the schedule alone
     plain_flags = tuned["flags"] | (0 if tuned["flags"] & 8 else 4)
-    same, _ = timed(lambda: run(schedule="heuristic", **dict(tuned, flags=plain_flags)), max(3, a.steps // 4), 1)
+    reps = max(3, a.steps // 4)
+    same, _ = timed(lambda: run(schedule="heuristic", **dict(tuned, flags=plain_flags)), reps, 1)
     plain_same = float(np.mean(same))
+    # the reference's own root order: ids after its kcore recode (degeneracy
+    # order, degree-sorted inside each shell), taken as given
+    kc, _ = timed(lambda: run(schedule="given", **tuned), reps, 1)
+    kcore_ms = float(np.mean(kc))
     extras = {"schedules": {
-        "plain_heuristic_ms": plain_same, "learned_ms": step_ms, "learned_vs_plain": plain_same / step_ms,
+        "plain_kcore_order_ms": kcore_ms, "plain_heuristic_ms": plain_same, "learned_ms": step_ms,
+        "learned_vs_plain": kcore_ms / step_ms, "learned_vs_degree_core_heuristic": plain_same / step_ms,
         "plain_default_launch_ms": float(np.mean(plain_ms)),
-        "note": "learned_vs_plain compares runs that differ in the schedule alone (same launch parameters, "
-                "same splitting); plain_default_launch_ms is the heuristic order with the default launch",
+        "note": "plain = the reference's root order (its kcore tool's degeneracy order, degree-sorted inside each "
+                "shell: the 'plain degree/core heuristic'); every ratio compares runs that differ in the order "
+                "alone (same launch parameters and flags). degree_core_heuristic orders roots by descending "
+                "degree x core number. plain_default_launch_ms: the heuristic order with the default launch",
         "tuned": tuned, "tuning_log": [[c, round(t, 3)] for c, t in tlog]}}
     e2e, cpu = None, None
     if not a.no_extras:
@@ -920,23 +935,33 @@ def run_ours(a):
         mwork = work_of(mctx)
         cliques = count()
         cur["ctx"] = mctx
-        # plain: one warp per root, no hand-off; then walks handing branches to idle warps
+        # one warp per root (no hand-off), then walks handing branches to idle
+        # warps; each order under the same settings (the learned run's tuned ones
+        # for the hand-off rows)
+        mgiven, _ = timed(lambda: mrun(schedule="given", flags=1 | FLAG_NO_SPILL), 3, 1)
         mplain, _ = timed(lambda: mrun(schedule="heuristic", flags=1 | FLAG_NO_SPILL), 3, 1)
         mlplain, _ = timed(lambda: mrun(schedule="learned", flags=1 | FLAG_NO_SPILL), 3, 1)
-        mhand, _ = timed(lambda: mrun(schedule="heuristic", flags=1), 3, 1)
         mtuned, _, _ = tune(lambda **kw: mrun(schedule="learned", **kw), {"flags": 1, "chunk": 1}, MCE_SPACE)
+        mgh, _ = timed(lambda: mrun(schedule="given", **mtuned), 3, 1)
+        mhand, _ = timed(lambda: mrun(schedule="heuristic", **mtuned), 3, 1)
         mms, mpass = timed(lambda: mrun(schedule="learned", **mtuned), 3, 1)
         assert count() == cliques
         cur["ctx"] = ctx
         mk = float(np.mean(mpass)) if mpass else None
         mstream = cl.mce_stream_bytes()
+        ml = float(np.mean(mms))
         extras["mce_chung_lu"] = {
             "graph": {"n": cl.n, "m": cl.m, "gamma": 2.3, "avg_degree": 16},
             "stream_bytes": mstream, "stream_gbs": mstream / (mk / 1000.0) / 1e9 if mk else None,
-            "maximal_cliques": cliques, "plain_heuristic_ms": float(np.mean(mplain)),
-            "learned_no_handoff_ms": float(np.mean(mlplain)), "heuristic_handoff_ms": float(np.mean(mhand)),
-            "learned_ms": float(np.mean(mms)), "learned_vs_plain": float(np.mean(mplain)) / float(np.mean(mms)),
-            "tuned": mtuned, "per_s": cliques / (float(np.mean(mms)) / 1000.0), "kernel_ms": mk,
+            "maximal_cliques": cliques,
+            "no_handoff_ms": {"kcore_order": float(np.mean(mgiven)), "heuristic": float(np.mean(mplain)),
+                              "learned": float(np.mean(mlplain))},
+            "handoff_ms": {"kcore_order": float(np.mean(mgh)), "heuristic": float(np.mean(mhand)), "learned": ml},
+            "learned_ms": ml, "learned_vs_plain": float(np.mean(mgh)) / ml,
+            "learned_vs_degree_core_heuristic": float(np.mean(mhand)) / ml,
+            "learned_vs_plain_no_handoff": float(np.mean(mgiven)) / float(np.mean(mlplain)),
+            "note": "plain = the reference's kcore root order; each ratio compares the same settings",
+            "tuned": mtuned, "per_s": cliques / (ml / 1000.0), "kernel_ms": mk,
             "merge_model_bytes": mwork, "merge_model_gbs": mwork / (mk / 1000.0) / 1e9 if mk else None}
         if rank == 0 and world == 1:
             cs = cpu_sample(cl, a.cpu_sample_s / 2, os.cpu_count() or 1, what="mce")

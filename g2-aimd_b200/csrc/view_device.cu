@@ -13,8 +13,9 @@
 //      population prefix); the ball list is the bitmap's set bits in order;
 //   4. rows: every ball vertex's row restricted to the ball (forward views:
 //      entries above the vertex; otherwise from the ball's smallest vertex on),
-//      counted (degree, entries <= the vertex) and then written as local ids
-//      (warp ballots keep the order), row pointers by a scan;
+//      copied once from host memory into a device staging area, then counted
+//      (degree, entries <= the vertex) and written as local ids (warp ballots
+//      keep the order), row pointers by a scan;
 //   5. sources as local ids.
 // The result is byte for byte the host builder's (same Layout, same rp, fo, ci,
 // src) for shapes with radius 1 and row radius 1 without ego rows.
@@ -33,6 +34,7 @@ using namespace g2rt;
 namespace {
 
 constexpr uint64_t kLongRow = 256;  // rows longer than this find their start by binary search
+constexpr uint64_t kStageMax = 1ull << 29;  // row entries staged in device memory per view (2 GiB)
 
 __device__ __forceinline__ uint32_t lane_of() { return threadIdx.x & 31u; }
 
@@ -60,6 +62,50 @@ __device__ __forceinline__ uint64_t row_start(const uint64_t *rp, const uint32_t
 }
 
 __device__ __forceinline__ bool bit_of(const uint32_t *bits, uint32_t x) { return (bits[x >> 5] >> (x & 31u)) & 1u; }
+
+// Row of ball vertex i (global id g): from the device staging copy when there is
+// one (srp indexed by i, the row already cut at its start), else from the host CSR.
+__device__ __forceinline__ const uint32_t *ball_row(const uint64_t *rp, const uint32_t *ci, const uint64_t *srp,
+                                                    const uint32_t *sci, uint64_t i, uint32_t g, uint32_t from,
+                                                    uint64_t *b, uint64_t *end) {
+    if (srp) {
+        *b = srp[i];
+        *end = srp[i + 1];
+        return sci;
+    }
+    *b = row_start(rp, ci, g, from, end);
+    return ci;
+}
+
+// A warp per ball vertex: where its row's scan starts in the host CSR, and its length.
+__global__ void row_span_kernel(const uint64_t *rp, const uint32_t *ci, const uint32_t *ball, uint64_t nv,
+                                bool forward, uint64_t *start, unsigned long long *len) {
+    const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t lo = nv ? ball[0] : 0u;
+    for (uint64_t i = w0; i < nv; i += nw) {
+        const uint32_t g = ball[i];
+        uint64_t end;
+        const uint64_t b = row_start(rp, ci, g, forward ? g + 1 : lo, &end);
+        if (lane_of() == 0) {
+            start[i] = b;
+            len[i] = end - b;
+        }
+    }
+}
+
+// A warp per ball vertex: its row from the host CSR into the device staging copy
+// (the one pass over host memory).
+__global__ void row_stage_kernel(const uint32_t *ci, const uint64_t *start, const uint64_t *soff, uint64_t nv,
+                                 uint32_t *sci) {
+    const uint32_t lane = lane_of();
+    const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = w0; i < nv; i += nw) {
+        const uint64_t b = start[i], o = soff[i], l = soff[i + 1] - o;
+        for (uint64_t k = lane; k < l; k += 32) sci[o + k] = ci[b + k];
+    }
+}
 
 // Rank of a set bit x in the bitmap: its local id.
 __device__ __forceinline__ uint32_t rank_of(const uint32_t *bits, const uint32_t *pre, uint32_t x) {
@@ -117,9 +163,9 @@ __global__ void ball_list_kernel(const uint32_t *bits, const uint32_t *pre, uint
 }
 
 // A warp per ball vertex: degree inside the ball and entries <= the vertex.
-__global__ void row_count_kernel(const uint64_t *rp, const uint32_t *ci, const uint32_t *ball, uint64_t nv,
-                                 const uint32_t *bits, bool forward, unsigned long long *deg, uint32_t *fo,
-                                 unsigned int *max_fwd) {
+__global__ void row_count_kernel(const uint64_t *rp, const uint32_t *ci, const uint64_t *srp, const uint32_t *sci,
+                                 const uint32_t *ball, uint64_t nv, const uint32_t *bits, bool forward,
+                                 unsigned long long *deg, uint32_t *fo, unsigned int *max_fwd) {
     const uint32_t lane = lane_of();
     const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -127,11 +173,11 @@ __global__ void row_count_kernel(const uint64_t *rp, const uint32_t *ci, const u
     for (uint64_t i = w0; i < nv; i += nw) {
         const uint32_t g = ball[i];
         const uint32_t from = forward ? g + 1 : lo;
-        uint64_t end;
-        const uint64_t b = row_start(rp, ci, g, from, &end);
+        uint64_t b, end;
+        const uint32_t *row = ball_row(rp, ci, srp, sci, i, g, from, &b, &end);
         uint32_t d = 0, back = 0;
         for (uint64_t e = b + lane; e < end; e += 32) {
-            const uint32_t u = ci[e];
+            const uint32_t u = row[e];
             if (u < from || !bit_of(bits, u)) continue;
             d++;
             back += u <= g;
@@ -149,9 +195,9 @@ __global__ void row_count_kernel(const uint64_t *rp, const uint32_t *ci, const u
 }
 
 // A warp per ball vertex: its kept entries as local ids, in order.
-__global__ void row_write_kernel(const uint64_t *rp, const uint32_t *ci, const uint32_t *ball, uint64_t nv,
-                                 const uint32_t *bits, const uint32_t *pre, bool forward, const uint64_t *vrp,
-                                 uint32_t *vci) {
+__global__ void row_write_kernel(const uint64_t *rp, const uint32_t *ci, const uint64_t *srp, const uint32_t *sci,
+                                 const uint32_t *ball, uint64_t nv, const uint32_t *bits, const uint32_t *pre,
+                                 bool forward, const uint64_t *vrp, uint32_t *vci) {
     const uint32_t lane = lane_of();
     const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -161,11 +207,11 @@ __global__ void row_write_kernel(const uint64_t *rp, const uint32_t *ci, const u
         if (vrp[i + 1] == o) continue;
         const uint32_t g = ball[i];
         const uint32_t from = forward ? g + 1 : lo;
-        uint64_t end;
-        const uint64_t b = row_start(rp, ci, g, from, &end);
+        uint64_t b, end;
+        const uint32_t *row = ball_row(rp, ci, srp, sci, i, g, from, &b, &end);
         for (uint64_t base = b; base < end; base += 32) {
             const uint64_t e = base + lane;
-            const uint32_t u = e < end ? ci[e] : 0u;
+            const uint32_t u = e < end ? row[e] : 0u;
             const bool keep = e < end && u >= from && bit_of(bits, u);
             const uint32_t m = __ballot_sync(0xffffffffu, keep);
             if (keep) vci[o + __popc(m & ((1u << lane) - 1u))] = rank_of(bits, pre, u);
@@ -292,13 +338,17 @@ int DeviceViewBuilder::grow_rows(uint64_t need) {
     cudaFree(deg);
     cudaFree(fo);
     cudaFree(vrp);
+    cudaFree(sstart);
+    cudaFree(soff);
     deg = nullptr;
     fo = nullptr;
-    vrp = nullptr;
+    vrp = sstart = soff = nullptr;
     rows_cap = 0;
     G2_TRY(cudaMalloc(&deg, 8 * (need + 1)));
     G2_TRY(cudaMalloc(&fo, 4 * (need + 1)));
     G2_TRY(cudaMalloc(&vrp, 8 * (need + 1)));
+    G2_TRY(cudaMalloc(&sstart, 8 * (need + 1)));
+    G2_TRY(cudaMalloc(&soff, 8 * (need + 1)));
     rows_cap = need;
     return G2_OK;
 }
@@ -335,9 +385,33 @@ int DeviceViewBuilder::build(const uint32_t *roots, uint64_t nroots, void **buf,
     rc = grow_rows(std::max<uint64_t>(nv, 1));
     if (rc) return rc;
     ball_list_kernel<<<G, 256, 0, st>>>(bits, wpre, words, ball);
-    // 4. rows: counts, row pointers, then columns
+    // 4. rows: staged once into device memory (up to kStageMax entries; the
+    //    row count and row write then read them there), counts, row pointers,
+    //    then columns
+    const uint64_t *srp = nullptr;
+    const uint32_t *sci = nullptr;
+    if (nv) {
+        row_span_kernel<<<G, 256, 0, st>>>(hrp, hci, ball, nv, sh.forward, sstart, deg);
+        G2_TRY(cudaMemsetAsync(deg + nv, 0, 8, st));
+        G2_TRY(scan(deg, soff, (uint64_t)nv + 1, &cub_tmp, &cub_cap, st));
+        uint64_t T = 0;
+        G2_TRY(cudaMemcpyAsync(&T, soff + nv, 8, cudaMemcpyDeviceToHost, st));
+        G2_TRY(cudaStreamSynchronize(st));
+        if (T <= kStageMax) {
+            if (T > stage_cap) {
+                cudaFree(stage);
+                stage = nullptr;
+                stage_cap = 0;
+                G2_TRY(cudaMalloc(&stage, 4 * std::max<uint64_t>(T, 1)));
+                stage_cap = T;
+            }
+            row_stage_kernel<<<G, 256, 0, st>>>(hci, sstart, soff, nv, stage);
+            srp = soff;
+            sci = stage;
+        }
+    }
     auto *mx = reinterpret_cast<unsigned int *>(scalars);
-    if (nv) row_count_kernel<<<G, 256, 0, st>>>(hrp, hci, ball, nv, bits, sh.forward, deg, fo, mx);
+    if (nv) row_count_kernel<<<G, 256, 0, st>>>(hrp, hci, srp, sci, ball, nv, bits, sh.forward, deg, fo, mx);
     G2_TRY(cudaMemsetAsync(deg + nv, 0, 8, st));
     G2_TRY(scan(deg, vrp, (uint64_t)nv + 1, &cub_tmp, &cub_cap, st));
     uint64_t m = 0;
@@ -366,7 +440,8 @@ int DeviceViewBuilder::build(const uint32_t *roots, uint64_t nroots, void **buf,
     auto *out_src = reinterpret_cast<uint32_t *>(b + L.src);
     G2_TRY(cudaMemcpyAsync(out_rp, vrp, 8 * ((uint64_t)nv + 1), cudaMemcpyDeviceToDevice, st));
     if (nv) G2_TRY(cudaMemcpyAsync(out_fo, fo, 4 * (uint64_t)nv, cudaMemcpyDeviceToDevice, st));
-    if (nv && m) row_write_kernel<<<G, 256, 0, st>>>(hrp, hci, ball, nv, bits, wpre, sh.forward, vrp, out_ci);
+    if (nv && m)
+        row_write_kernel<<<G, 256, 0, st>>>(hrp, hci, srp, sci, ball, nv, bits, wpre, sh.forward, vrp, out_ci);
     // 5. sources
     if (nk) src_local_kernel<<<G, 256, 0, st>>>(kept, nk, bits, wpre, out_src);
     G2_TRY(cudaGetLastError());
@@ -378,7 +453,8 @@ int DeviceViewBuilder::build(const uint32_t *roots, uint64_t nroots, void **buf,
 DeviceViewBuilder::~DeviceViewBuilder() {
     cudaDeviceSynchronize();  // builds and runs that read these buffers or the mapped CSR have ended
     for (void *p : {(void *)bits, (void *)wcnt, (void *)wpre, (void *)ball, (void *)scalars, (void *)d_roots,
-                    (void *)keep, (void *)pos, (void *)kept, (void *)deg, (void *)fo, (void *)vrp, cub_tmp})
+                    (void *)keep, (void *)pos, (void *)kept, (void *)deg, (void *)fo, (void *)vrp, (void *)sstart,
+                    (void *)soff, (void *)stage, cub_tmp})
         if (p) cudaFree(p);
     for (int k = 0; k < nreg; k++) cudaHostUnregister(reg[k]);
     if (stage_rp) cudaFreeHost(stage_rp);

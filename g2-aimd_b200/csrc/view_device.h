@@ -42,7 +42,10 @@ struct DeviceViewBuilder {
     unsigned long long *deg = nullptr;
     uint32_t *fo = nullptr;
     uint64_t *vrp = nullptr;
+    uint64_t *sstart = nullptr, *soff = nullptr;  // staged rows: host start, device offset
     uint64_t rows_cap = 0;
+    uint32_t *stage = nullptr;  // the ball's rows copied from host memory
+    uint64_t stage_cap = 0;
     void *cub_tmp = nullptr;
     size_t cub_cap = 0;
 

@@ -156,3 +156,45 @@ def test_learned_order_tracks_measured_cost(g2, ctx):
     s_model, s_heur = spearman(pred[busy], cost[busy]), spearman(heur[busy], cost[busy])
     print(f"spearman on the costlier half: model {s_model:.3f}, heuristic {s_heur:.3f}")
     assert s_model >= s_heur - 0.02
+
+
+def test_learned_schedule_beats_the_kcore_order(g2):
+    """On a held-out graph (R-MAT s19, seed 77: no training graph), the learned
+    schedule against the reference's own root order (its kcore tool's
+    degeneracy order, which puts the dense core's heavy roots last), every
+    other parameter identical: 4-cliques on the shipped model, device time of
+    the whole run (task generation included), best of 5 runs each."""
+    import os
+
+    import torch
+
+    from g2aimd.context import Context, CostModel, Plan
+    g = g2.Graph.rmat(19, 16, seed=77).degeneracy_recoded()
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.Stream(dev)
+    out = torch.zeros(1, dtype=torch.int64, device=dev)
+    models = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "g2-aimd_b200", "models")
+    launch = dict(warps_per_block=8, chunk=1, flags=8)  # no heavy-root splits: the order alone differs
+    with Context(0) as c:
+        c.load(g)
+        c.load_core(g.core)
+        c.set_model(CostModel.load(os.path.join(models, "k4.npz")))
+        c.set_plan(Plan.preset(24))
+
+        def best(schedule):
+            ms, cnt = [], None
+            for _ in range(6):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                c.match_device(out.data_ptr(), stream=st.cuda_stream, schedule=schedule, **launch)
+                e1.record(st)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+                cnt = int(out[0].item())
+            return min(ms[1:]), cnt
+
+        kcore_ms, k1 = best("given")
+        learned_ms, k2 = best("learned")
+        assert k1 == k2
+        print(f"kcore order {kcore_ms:.2f} ms, learned {learned_ms:.2f} ms: {kcore_ms / learned_ms:.2f}x")
+        assert learned_ms * 1.3 < kcore_ms
