@@ -1033,6 +1033,7 @@ int g2_close(g2_ctx *ctx) {
         if (h.first) cudaFreeHost(h.first);
     for (void *b : ctx->view_dev)
         if (b) cudaFree(b);
+    g2rt::view_builder_free(ctx->view_builder);
     delete ctx;
     return G2_OK;
 }

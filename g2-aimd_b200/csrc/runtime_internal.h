@@ -90,6 +90,7 @@ struct g2_ctx {
     // between calls (pinning and device allocation stall other CUDA calls)
     std::vector<std::pair<void *, uint64_t>> view_host;
     void *view_dev[2] = {nullptr, nullptr};
+    void *view_builder = nullptr;  // g2rt::DeviceViewBuilder kept between view runs (its work arrays)
     uint64_t view_dev_cap[2] = {0, 0};
     bool timed = false;
     int timed_passes = 0;  // enumeration passes the last timed run recorded (MCE 3, match 1)
@@ -103,6 +104,8 @@ namespace g2rt {
 int fail_cuda(g2_ctx *c, cudaError_t e, const char *where);
 // Per-graph set-up after a new CSR is in the context (forward offsets, ...).
 int g2_after_load(g2_ctx *ctx);
+// Release a context's device view builder (view_device.cu).
+void view_builder_free(void *builder);
 int fail_cuda_if(g2_ctx *c, cudaError_t e, const char *where);
 
 #define G2_TRY(call)                                             \

@@ -309,11 +309,18 @@ int DeviceViewBuilder::init(g2_ctx *c, const uint64_t *host_rp, const uint32_t *
     hrp = static_cast<const uint64_t *>(drp);
     hci = static_cast<const uint32_t *>(dci);
     words = (n + 31) / 32;
-    G2_TRY(cudaMalloc(&bits, 4 * (words + 1)));
-    G2_TRY(cudaMalloc(&wcnt, 4 * (words + 1)));
-    G2_TRY(cudaMalloc(&wpre, 4 * (words + 1)));
-    G2_TRY(cudaMalloc(&ball, 4 * std::max<uint64_t>(n, 1)));
-    G2_TRY(cudaMalloc(&scalars, 64));
+    if (n_cap < std::max<uint64_t>(n, 1) || !bits) {
+        for (void *p : {(void *)bits, (void *)wcnt, (void *)wpre, (void *)ball}) cudaFree(p);
+        bits = wcnt = wpre = ball = nullptr;
+        n_cap = 0;
+        const uint64_t w = (std::max<uint64_t>(n, 1) + 31) / 32;
+        G2_TRY(cudaMalloc(&bits, 4 * (w + 1)));
+        G2_TRY(cudaMalloc(&wcnt, 4 * (w + 1)));
+        G2_TRY(cudaMalloc(&wpre, 4 * (w + 1)));
+        G2_TRY(cudaMalloc(&ball, 4 * std::max<uint64_t>(n, 1)));
+        n_cap = std::max<uint64_t>(n, 1);
+    }
+    if (!scalars) G2_TRY(cudaMalloc(&scalars, 64));
     return G2_OK;
 }
 
@@ -450,16 +457,26 @@ int DeviceViewBuilder::build(const uint32_t *roots, uint64_t nroots, void **buf,
     return G2_OK;
 }
 
+void DeviceViewBuilder::release_host() {
+    cudaDeviceSynchronize();  // builds and runs that read the mapped CSR have ended
+    for (int k = 0; k < nreg; k++) cudaHostUnregister(reg[k]);
+    nreg = 0;
+    if (stage_rp) cudaFreeHost(stage_rp);
+    if (stage_ci) cudaFreeHost(stage_ci);
+    stage_rp = stage_ci = nullptr;
+    hrp = nullptr;
+    hci = nullptr;
+}
+
 DeviceViewBuilder::~DeviceViewBuilder() {
-    cudaDeviceSynchronize();  // builds and runs that read these buffers or the mapped CSR have ended
+    release_host();
     for (void *p : {(void *)bits, (void *)wcnt, (void *)wpre, (void *)ball, (void *)scalars, (void *)d_roots,
                     (void *)keep, (void *)pos, (void *)kept, (void *)deg, (void *)fo, (void *)vrp, (void *)sstart,
                     (void *)soff, (void *)stage, cub_tmp})
         if (p) cudaFree(p);
-    for (int k = 0; k < nreg; k++) cudaHostUnregister(reg[k]);
-    if (stage_rp) cudaFreeHost(stage_rp);
-    if (stage_ci) cudaFreeHost(stage_ci);
 }
+
+void view_builder_free(void *builder) { delete static_cast<DeviceViewBuilder *>(builder); }
 
 }  // namespace g2rt
 
@@ -491,16 +508,21 @@ extern "C" int g2_view_materialize_device(g2_ctx *ctx, const uint64_t *row_ptrs,
     g2view::Sizes s;
     uint32_t *ball_host = nullptr;
     {
-        g2rt::DeviceViewBuilder vb;
+        if (!ctx->view_builder) ctx->view_builder = new g2rt::DeviceViewBuilder();
+        auto &vb = *static_cast<g2rt::DeviceViewBuilder *>(ctx->view_builder);
         int rc = vb.init(ctx, row_ptrs, cols, n, sh);
         if (!rc) rc = vb.build(sources, nsrc, &ctx->view_dev[0], &ctx->view_dev_cap[0], nullptr, &s);
-        if (rc) return rc;
-        G2_TRY(cudaStreamSynchronize(nullptr));
-        ball_host = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.n, 1)));
-        if (!ball_host) return G2_ERR_OOM;
-        if (s.n && cudaMemcpy(ball_host, vb.ball, 4 * s.n, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        if (!rc) rc = fail_cuda_if(ctx, cudaStreamSynchronize(nullptr), "view build");
+        if (!rc) {
+            ball_host = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.n, 1)));
+            if (!ball_host) rc = G2_ERR_OOM;
+            else if (s.n && cudaMemcpy(ball_host, vb.ball, 4 * s.n, cudaMemcpyDeviceToHost) != cudaSuccess)
+                rc = fail_cuda(ctx, cudaGetLastError(), "view ids");
+        }
+        vb.release_host();
+        if (rc) {
             free(ball_host);
-            return fail_cuda(ctx, cudaGetLastError(), "view ids");
+            return rc;
         }
     }
     const g2view::Layout L(s);

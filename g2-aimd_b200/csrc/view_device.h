@@ -20,6 +20,9 @@ struct DeviceViewBuilder {
     // for the call, else copied to mapped staging buffers) and allocate the
     // n-sized work arrays.
     int init(g2_ctx *ctx, const uint64_t *host_rp, const uint32_t *host_ci, uint64_t n, const g2view::Shape &shape);
+    // Undo init's host mapping (registrations, staging copies); the device
+    // work arrays stay for the next call.
+    void release_host();
     // The view of `roots` (host array) into *buf (a device slot, grown to fit),
     // enqueued on st; returns once its sizes are known (the writes may still be
     // in flight on st).
@@ -35,6 +38,7 @@ struct DeviceViewBuilder {
     void *reg[2] = {nullptr, nullptr};  // page ranges registered for the call
     int nreg = 0;
     void *stage_rp = nullptr, *stage_ci = nullptr;  // mapped copies if registering failed
+    uint64_t n_cap = 0;  // graph size the n-sized arrays were allocated for
     uint32_t *bits = nullptr, *wcnt = nullptr, *wpre = nullptr, *ball = nullptr;
     unsigned long long *scalars = nullptr;
     uint32_t *d_roots = nullptr, *keep = nullptr, *pos = nullptr, *kept = nullptr;

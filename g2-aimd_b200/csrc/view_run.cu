@@ -366,7 +366,12 @@ int view_run(g2_ctx *ctx, bool mce, const uint64_t *rp, const uint32_t *ci, uint
         // the GPU builds each view into a device slot on the copy stream; the
         // next view's build overlaps the current run on the legacy stream
         ViewDevice dev(ctx);
-        DeviceViewBuilder vb;
+        if (!ctx->view_builder) ctx->view_builder = new DeviceViewBuilder();
+        DeviceViewBuilder &vb = *static_cast<DeviceViewBuilder *>(ctx->view_builder);
+        struct Unmap {  // the host CSR's mapping ends with the call (device arrays stay)
+            DeviceViewBuilder &b;
+            ~Unmap() { b.release_host(); }
+        } unmap{vb};
         rc = dev.init();
         if (!rc) rc = vb.init(ctx, rp, ci, n, shape);
         int d = 0;
