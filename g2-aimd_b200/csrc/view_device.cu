@@ -254,8 +254,12 @@ int DeviceViewBuilder::init(g2_ctx *c, const uint64_t *host_rp, const uint32_t *
     const uint64_t m = host_rp[n];
     // The host CSR seen from the device: pinned and mapped memory (cudaHostAlloc,
     // a pinning allocator) is used in place; other memory is registered for the
-    // call, whole pages, one range if the two arrays' pages meet; if that fails,
-    // the CSR is copied once into mapped pinned staging buffers.
+    // call, the arrays' exact byte ranges (one range spanning both if they
+    // share a page), else copied once into mapped pinned staging buffers.  Exact
+    // ranges matter: the driver counts a registered range as pinned memory, so
+    // a range rounded out to whole pages would take in the neighbouring heap
+    // blocks, and a pageable copy to or from a block that starts inside the
+    // range and ends past it is refused (cudaErrorInvalidValue).
     auto mapped = [](const void *p) -> const void * {
         cudaPointerAttributes at{};
         if (cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost && at.devicePointer)
@@ -266,12 +270,11 @@ int DeviceViewBuilder::init(g2_ctx *c, const uint64_t *host_rp, const uint32_t *
     const void *drp = mapped(host_rp), *dci = m ? mapped(host_ci) : host_ci;
     if (!drp || !dci) {
         const uint64_t pg = 4096;
-        auto lo = [&](const void *p) { return (uintptr_t)p & ~(uintptr_t)(pg - 1); };
-        auto hi = [&](const void *p, uint64_t b) { return ((uintptr_t)p + b + pg - 1) & ~(uintptr_t)(pg - 1); };
-        uintptr_t a0 = lo(host_rp), a1 = hi(host_rp, 8 * (n + 1));
-        uintptr_t b0 = m ? lo(host_ci) : a0, b1 = m ? hi(host_ci, 4 * m) : a1;
+        auto page = [&](uintptr_t a) { return a & ~(uintptr_t)(pg - 1); };
+        const uintptr_t a0 = (uintptr_t)host_rp, a1 = a0 + 8 * (n + 1);
+        const uintptr_t b0 = m ? (uintptr_t)host_ci : a0, b1 = m ? b0 + 4 * m : a1;
         bool ok = true;
-        if (b0 <= a1 && a0 <= b1) {  // the pages meet: one range
+        if (page(b0) <= page(a1 - 1) && page(a0) <= page(b1 - 1)) {  // a page in common: one range
             const uintptr_t u0 = std::min(a0, b0), u1 = std::max(a1, b1);
             ok = cudaHostRegister((void *)u0, u1 - u0, cudaHostRegisterMapped) == cudaSuccess;
             if (ok) reg[nreg++] = (void *)u0;
@@ -513,13 +516,13 @@ extern "C" int g2_view_materialize_device(g2_ctx *ctx, const uint64_t *row_ptrs,
         int rc = vb.init(ctx, row_ptrs, cols, n, sh);
         if (!rc) rc = vb.build(sources, nsrc, &ctx->view_dev[0], &ctx->view_dev_cap[0], nullptr, &s);
         if (!rc) rc = fail_cuda_if(ctx, cudaStreamSynchronize(nullptr), "view build");
+        vb.release_host();  // the build has ended: the host CSR is no longer read
         if (!rc) {
             ball_host = static_cast<uint32_t *>(malloc(4 * std::max<uint64_t>(s.n, 1)));
             if (!ball_host) rc = G2_ERR_OOM;
-            else if (s.n && cudaMemcpy(ball_host, vb.ball, 4 * s.n, cudaMemcpyDeviceToHost) != cudaSuccess)
-                rc = fail_cuda(ctx, cudaGetLastError(), "view ids");
+            else if (s.n) rc = fail_cuda_if(ctx, cudaMemcpy(ball_host, vb.ball, 4 * s.n, cudaMemcpyDeviceToHost),
+                                            "view ids");
         }
-        vb.release_host();
         if (rc) {
             free(ball_host);
             return rc;

@@ -179,3 +179,32 @@ def test_device_built_view_bytes_equal_host_build(vctx, g2, shape):
         assert np.array_equal(h.fwd_offsets, d.fwd_offsets) and h.max_fwd == d.max_fwd
         assert np.array_equal(hs, ds) and np.array_equal(hid, did)
     vctx.load(g)
+
+
+def test_device_built_view_csr_sharing_pages_with_other_arrays(vctx, g2):
+    """The host CSR is registered by its exact byte ranges: a pageable array
+    that starts on the page where the columns end and runs past it (here the
+    sources, copied to the device while the CSR is mapped) still copies."""
+    g = g2.Graph.rmat(12, 16, seed=7).degeneracy_recoded()
+    src = np.arange(g.n - 700, g.n, dtype=np.uint32)
+    n, m = g.n, g.m
+    buf = np.zeros(8 * (n + 1) + 4 * m + 4 * src.size + 3 * 4096, np.uint8)
+    base = (-buf.ctypes.data) % 4096 + 64
+    rp_at = base
+    ci_at = rp_at + 8 * (n + 1)
+    src_at = ci_at + 4 * m  # the offsets within a page are fixed: base is 64 bytes past a page start
+    rp = buf[rp_at:rp_at + 8 * (n + 1)].view(np.uint64)
+    ci = buf[ci_at:ci_at + 4 * m].view(np.uint32)
+    sv = buf[src_at:src_at + 4 * src.size].view(np.uint32)
+    rp[:], ci[:], sv[:] = g.row_ptrs, g.cols, src
+    # the sources start on the page of the columns' last byte, and end past it
+    assert src_at // 4096 == (ci_at + 4 * m - 1) // 4096 < (src_at + 4 * src.size - 1) // 4096
+    gb = g2.Graph(rp, ci)
+    assert gb.row_ptrs.ctypes.data == rp.ctypes.data and gb.cols.ctypes.data == ci.ctypes.data
+    for shape in (dict(), dict(upper=True, forward=True)):
+        h, hs, hid = g.view(src, radius=1, row_radius=1, min_root_degree=2, **shape)
+        d, ds, did = vctx.view_device(gb, sv, min_root_degree=2, **shape)
+        assert np.array_equal(h.row_ptrs, d.row_ptrs) and np.array_equal(h.cols, d.cols)
+        assert np.array_equal(hs, ds) and np.array_equal(hid, did)
+    vctx.load(g)
+
