@@ -64,10 +64,12 @@ def parse():
     ap.add_argument("--scratch-mb", type=int, default=4096, help="device scratch for the DFS slabs")
     ap.add_argument("--fixed", action="store_true",
                     help="skip the plain-schedule timing and the autotuner (profiling runs)")
-    ap.add_argument("--leg", choices=["all", "mce", "view", "view-host", "c5", "c3", "walk"], default="all",
+    ap.add_argument("--leg", choices=["all", "mce", "view", "view-host", "c5", "c3", "c4", "walk"], default="all",
                     help="mce: only the maximal-clique workload (Chung-Lu 2^18), for profiling; "
                          "view: out-of-core runs over view bins against in-core runs; "
-                         "view-host: the views' sizes and host build time alone (no GPU)")
+                         "view-host: the views' sizes and host build time alone (no GPU); "
+                         "c4: the batch of 64 power-law graphs alone")
+    ap.add_argument("--walk-query", type=int, default=1, help="preset plan of the walk leg (1: 4-cycles, 2: diamonds)")
     ap.add_argument("--view-split", type=int, default=2,
                     help="view leg: bin budget = CSR bytes / this")
     return ap.parse_args()
@@ -238,10 +240,23 @@ def run_c5_leg(a):
     print(json.dumps(c5_leg(a, 0, torch, stream)), flush=True)
 
 
+def run_c4_leg(a):
+    import torch
+
+    from g2aimd.context import Context, CostModel, Plan
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    models = os.path.join(ROOT, "g2-aimd_b200", "models")
+    print(json.dumps(c4_leg(Context, CostModel, Plan, models, 0, a.seed, torch, stream)), flush=True)
+
+
 def run_walk_leg(a):
-    """Plan walks alone (for profiling): 4-cycles (preset 1) on a Chung-Lu graph
-    shaped like the larger C4 members (n = 2e5, gamma 2.2, average degree 20),
-    heuristic order with hand-off, W warm-up and K timed runs; one JSON line."""
+    """Plan walks alone (for profiling): 4-cycles (preset 1; --walk-query picks
+    another preset) on a Chung-Lu graph shaped like the larger C4 members
+    (n = 2e5, gamma 2.2, average degree 20), heuristic order with hand-off, W
+    warm-up and K timed runs; one JSON line."""
     import torch
 
     import g2aimd
@@ -255,12 +270,13 @@ def run_walk_leg(a):
     with Context(0) as ctx:
         ctx.load(g)
         ctx.load_core(g.core)
-        ctx.set_plan(Plan.preset(1))
+        ctx.set_plan(Plan.preset(a.walk_query))
         run = lambda: ctx.match_device(out.data_ptr(), stream=stream.cuda_stream, schedule="heuristic", flags=1)  # noqa
         for _ in range(a.warmup):
             run()
         times = [ev_time(torch, stream, run)[1] for _ in range(a.steps)]
-        print(json.dumps({"workload": "4-cycles, chung-lu n=2e5 gamma 2.2 avg degree 20", "count": int(out[0].item()),
+        name = {1: "4-cycles", 2: "diamonds"}.get(a.walk_query, f"preset {a.walk_query}")
+        print(json.dumps({"workload": f"{name}, chung-lu n=2e5 gamma 2.2 avg degree 20", "count": int(out[0].item()),
                           "ms": times}), flush=True)
 
 
@@ -1064,6 +1080,8 @@ def main():
         run_c3_leg(a)
     elif a.leg == "walk":
         run_walk_leg(a)
+    elif a.leg == "c4":
+        run_c4_leg(a)
     elif a.leg == "mce":
         run_mce_leg(a)
     elif a.leg == "view":

@@ -82,6 +82,9 @@ cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_bloc
 cudaError_t epoch_bump(uint32_t *epoch_dev, cudaStream_t st);
 // *deadline = the device's %globaltimer now + budget_ns, in stream order.
 cudaError_t deadline_set(unsigned long long *deadline, unsigned long long budget_ns, cudaStream_t st);
+// In stream order: kStatusDeferOverflow into *status if *left (entries no pass
+// walked) is nonzero.
+cudaError_t flag_left(const unsigned long long *left, int *status, cudaStream_t st);
 
 // Plan in device-friendly form: everything by POSITION.
 struct DevPlan {

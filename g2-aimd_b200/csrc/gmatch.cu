@@ -163,6 +163,118 @@ __device__ __noinline__ unsigned long long count_last_sliced(const DevPlan &pl, 
     return c;
 }
 
+// Shared candidate set of the last position: the reference's PREFIX store
+// strategy (system/plan.h:151-172, app_gmatch/gmatch.h:273-509: a position's
+// intersection over the back neighbours that precede its previous position is
+// computed once and filtered per previous image), applied to the last
+// position k-1.  When no back neighbour of k-1 is position k-2, its candidates
+// depend on M[0..k-3] alone: the set S is built once per such prefix (the
+// least-degree back neighbour's list filtered by the other back neighbours'
+// lists and by the conditions against positions before k-2), and each
+// candidate c of position k-2 completes |{x in S : x op c}| embeddings for the
+// conditions between k-1 and k-2 - one binary search per candidate instead of
+// a scan of the last position's window per candidate.
+__device__ __forceinline__ bool last_is_shared(const DevPlan &pl) {
+    if (pl.k < 3 || pl.bn_count[pl.k - 1] == 0) return false;
+    for (uint32_t j = 0; j < pl.bn_count[pl.k - 1]; j++)
+        if (pl.bn_pos[pl.k - 1][j] == pl.k - 2) return false;
+    return true;
+}
+
+constexpr uint32_t kSharedUnbuilt = 0xffffffffu, kSharedTooLarge = 0xfffffffeu;
+
+// Build S for M[0..k-3] into out (at most cap entries, ascending); returns its
+// length or kSharedTooLarge.  *dsum = sum of the back neighbours' degrees (the
+// work model's share of every partial embedding of length k-1).
+__device__ __noinline__ uint32_t shared_last_build(const DevPlan &pl, const uint64_t *rp, const uint32_t *ci,
+                                                   const uint32_t *M, uint32_t *out, uint32_t cap, uint64_t *dsum) {
+    const uint32_t i = pl.k - 1, prev = pl.k - 2;
+    const uint32_t lane = lane_id();
+    uint32_t parent = pl.bn_pos[i][0];
+    uint64_t pd = ldg(rp + M[parent] + 1) - ldg(rp + M[parent]);
+    uint64_t ds = pd;
+    for (uint32_t j = 1; j < pl.bn_count[i]; j++) {
+        const uint32_t b = pl.bn_pos[i][j];
+        const uint64_t d = ldg(rp + M[b] + 1) - ldg(rp + M[b]);
+        ds += d;
+        if (d < pd) pd = d, parent = b;
+    }
+    *dsum = ds;
+    uint32_t lo = 0, hi = 0xffffffffu;
+    bool hi_set = false;
+    for (uint32_t c = 0; c < pl.cond_count[i]; c++) {
+        if (pl.cond_pos[i][c] == prev) continue;
+        const uint32_t m = M[pl.cond_pos[i][c]];
+        if (pl.cond_op[i][c] == G2_COND_LARGER_THAN) lo = m + 1 > lo ? m + 1 : lo;
+        else if (pl.cond_op[i][c] == G2_COND_LESS_THAN) hi = m < hi ? m : hi, hi_set = true;
+    }
+    const uint64_t s = ldg(rp + M[parent]), e = ldg(rp + M[parent] + 1);
+    uint64_t ps = s, pe = e;
+    if (lane == 0) {
+        ps = lo ? lower_bound(ci, s, e, lo) : s;
+        pe = hi_set ? lower_bound(ci, ps, e, hi) : e;
+    }
+    ps = __shfl_sync(G2_FULL, ps, 0);
+    pe = __shfl_sync(G2_FULL, pe, 0);
+    uint32_t len = 0;
+    for (uint64_t x0 = ps; x0 < pe; x0 += 32) {
+        const uint64_t x = x0 + lane;
+        const uint32_t w = x < pe ? ldg(ci + x) : 0u;
+        bool ok = x < pe;
+        for (uint32_t c = 0; c < pl.cond_count[i] && ok; c++)
+            if (pl.cond_pos[i][c] != prev) ok = cond_ok(pl.cond_op[i][c], w, M[pl.cond_pos[i][c]]);
+        for (uint32_t j = 0; j < pl.bn_count[i] && ok; j++) {
+            const uint32_t b = pl.bn_pos[i][j];
+            if (b != parent) ok = contains(ci, ldg(rp + M[b]), ldg(rp + M[b] + 1), w);
+        }
+        uint32_t tot;
+        const uint32_t pos = warp_scan(ok, tot);
+        if (len + tot > cap) return kSharedTooLarge;  // warp-uniform
+        if (ok) out[len + pos] = w;
+        len += tot;
+    }
+    __syncwarp();
+    return len;
+}
+
+// Embeddings completed by the candidates buf[0..n) of position k-2 against
+// S[0..ns); with nparts > 1 only candidates of ordinal ord0 + j with
+// (ord0 + j) % nparts == part count (a split root's part).  Per-lane count;
+// *taken = this lane's candidates of the part.
+__device__ __noinline__ unsigned long long shared_last_count(const DevPlan &pl, const uint32_t *Sv, uint32_t ns,
+                                                             const uint32_t *buf, uint32_t n, uint32_t ord0,
+                                                             uint32_t part, uint32_t nparts, uint32_t *taken) {
+    const uint32_t i = pl.k - 1, prev = pl.k - 2;
+    bool lt = false, gt = false, ne = false;
+    for (uint32_t c = 0; c < pl.cond_count[i]; c++) {
+        if (pl.cond_pos[i][c] != prev) continue;
+        const uint32_t op = pl.cond_op[i][c];
+        lt |= op == G2_COND_LESS_THAN;
+        gt |= op == G2_COND_LARGER_THAN;
+        ne |= op == G2_COND_NON_EQUAL;
+    }
+    unsigned long long cnt = 0;
+    uint32_t tk = 0;
+    for (uint32_t j = lane_id(); j < n; j += 32) {
+        if (nparts > 1 && (ord0 + j) % nparts != part) continue;
+        tk++;
+        const uint32_t w = buf[j];
+        uint32_t a = 0, b = ns;  // first index of S with S[a] >= w
+        while (a < b) {
+            const uint32_t m = (a + b) >> 1;
+            if (Sv[m] < w) a = m + 1;
+            else b = m;
+        }
+        const bool in = a < ns && Sv[a] == w;
+        const uint32_t lo = gt ? a + (in ? 1u : 0u) : 0u, hi = lt ? a : ns;
+        uint32_t c = hi > lo ? hi - lo : 0u;
+        if (ne && in && a >= lo && a < hi) c--;
+        cnt += c;
+    }
+    *taken = tk;
+    return cnt;
+}
+
 // Record layout of a handed-off plan walk (kMatchRecordWords words): the walk
 // resumes at position `level` with M[0..level-1]; kind 0 (prefix) initialises
 // that level from the plan, kind 1 (window) scans only [pos, end) of its
@@ -267,8 +379,14 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
     const uint32_t *ci = a.ci;
     uint32_t M[G2_MAX_QUERY];
     Level Ls[G2_MAX_QUERY];
-    const uint32_t nlists = k > 2 ? k - 2 : 1;
+    // slab: candidate chunks of positions 1..k-2, then the last position's
+    // shared set when the plan has one (and the slab holds 64-entry chunks)
+    const bool shared = last_is_shared(pl) && ((a.words_per_warp / (k - 1)) & ~31ull) >= 64;
+    const uint32_t nlists = shared ? k - 1 : k > 2 ? k - 2 : 1;
     const uint32_t CH = (uint32_t)((a.words_per_warp / nlists) & ~31ull);
+    uint32_t *Sset = S + (uint64_t)(k - 2) * CH;
+    uint32_t s_len = kSharedUnbuilt;  // S for the current M[0..k-3]
+    uint64_t s_dsum = 0;
     unsigned long long count = 0;
     if (CH < 64) {  // a chunk must hold at least two warp-widths of candidates
         if (lane == 0) atomicOr(a.status, kStatusStackOverflow);
@@ -371,11 +489,7 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
             L.idx = 0;
             continue;
         }
-        M[i] = buf[L.idx];
-        L.idx++;
-        if (a.deadline && (++budget_tick & 63u) == 0 && match_deadline_passed(a)) return kExpired;
-        if (i == 1 && nparts > 1 && (ord++ % nparts) != part) continue;  // another part's candidate
-        if (may_spill) {  // every spill_cycles: hand work to idle warps
+        auto maybe_donate = [&]() {  // every spill_cycles: hand work to idle warps
             long long el = 0;
             if (lane == 0) el = clock64() - c0;
             el = __shfl_sync(G2_FULL, el, 0);
@@ -387,9 +501,33 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
                 }
                 next_check = el + (long long)a.spill_cycles;
             }
+        };
+        if (shared && i == k - 2 && s_len != kSharedTooLarge) {
+            // the whole chunk against the last position's shared set
+            if (s_len == kSharedUnbuilt) s_len = shared_last_build(pl, rp, ci, M, Sset, CH, &s_dsum);
+            if (s_len != kSharedTooLarge) {
+                const uint32_t n = L.len - L.idx;
+                const bool split = i == 1 && nparts > 1;
+                uint32_t tk = 0;
+                const unsigned long long c =
+                    shared_last_count(pl, Sset, s_len, buf + L.idx, n, ord, part, split ? nparts : 1u, &tk);
+                count += warp_sum_u64(c);
+                work += 4ull * s_dsum * warp_sum_u64(tk);
+                if (split) ord += n;
+                L.idx = L.len;
+                if (a.deadline && match_deadline_passed(a)) return kExpired;
+                if (may_spill) maybe_donate();
+                continue;
+            }
         }
+        M[i] = buf[L.idx];
+        L.idx++;
+        if (a.deadline && (++budget_tick & 63u) == 0 && match_deadline_passed(a)) return kExpired;
+        if (i == 1 && nparts > 1 && (ord++ % nparts) != part) continue;  // another part's candidate
+        if (may_spill) maybe_donate();
         i++;
         work += 4ull * level_init(pl, rp, ci, M, i, Ls[i]);
+        if (i == k - 2) s_len = kSharedUnbuilt;
     }
     return count;
 }

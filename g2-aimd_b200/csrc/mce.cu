@@ -812,6 +812,15 @@ cudaError_t deadline_set(unsigned long long *deadline, unsigned long long budget
     return cudaGetLastError();
 }
 
+__global__ void flag_left_kernel(const unsigned long long *left, int *status) {
+    if (*left) atomicOr(status, kStatusDeferOverflow);
+}
+
+cudaError_t flag_left(const unsigned long long *left, int *status, cudaStream_t st) {
+    flag_left_kernel<<<1, 1, 0, st>>>(left, status);
+    return cudaGetLastError();
+}
+
 cudaError_t mce_launch(int wpl, const MceArgs &a, int blocks, int warps_per_block, cudaStream_t st) {
     size_t sm = mce_smem_bytes(wpl, warps_per_block);
     dim3 g(blocks), b(32 * warps_per_block);

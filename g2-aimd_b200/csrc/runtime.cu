@@ -647,19 +647,22 @@ namespace {
 
 namespace g2rt {
 
-int mce_host_spill(g2_ctx *ctx, cudaStream_t st) {
-    unsigned long long left = 0;
-    G2_TRY(cudaMemcpy(&left, ctx->d_ctr + kCtrDefer + 2, sizeof(left), cudaMemcpyDeviceToHost));
-    if (!left) return G2_OK;
-    if (!ctx->host_spill_bytes || left > ctx->tasks_cap) return G2_ERR_OVERFLOW;
-    if (ctx->scratch_words < 2ull * (ctx->max_fwd + 2)) return G2_ERR_OVERFLOW;  // room for the histogram
-    if (ctx->h_spill_bytes != ctx->host_spill_bytes) {
-        if (ctx->h_spill) cudaFree(ctx->h_spill);
-        ctx->h_spill = nullptr;
-        ctx->h_spill_bytes = 0;
-        G2_TRY(cudaMallocManaged(&ctx->h_spill, ctx->host_spill_bytes));
-        ctx->h_spill_bytes = ctx->host_spill_bytes;
-    }
+// The spill slab (managed memory of g2_set_host_spill's size), allocated or
+// resized on first need.
+static int ensure_spill_slab(g2_ctx *ctx) {
+    if (ctx->h_spill_bytes == ctx->host_spill_bytes) return G2_OK;
+    if (ctx->h_spill) cudaFree(ctx->h_spill);
+    ctx->h_spill = nullptr;
+    ctx->h_spill_bytes = 0;
+    G2_TRY(cudaMallocManaged(&ctx->h_spill, ctx->host_spill_bytes));
+    ctx->h_spill_bytes = ctx->host_spill_bytes;
+    return G2_OK;
+}
+
+// The spill pass over the one-warp pass's leftover entries (count read on the
+// device: the kernel exits at once when there are none); its own leftovers
+// go to kCtrSpillDefer.
+static int launch_spill_pass(g2_ctx *ctx, cudaStream_t st) {
     g2::MceArgs a = ctx->last_mce;
     a.scratch = static_cast<uint32_t *>(ctx->h_spill);
     // the root's clique-size counters go to the idle device scratch
@@ -677,8 +680,44 @@ int mce_host_spill(g2_ctx *ctx, cudaStream_t st) {
     cudaError_t e = g2::mce_launch(ctx->last_mce_wpl, a, 1, 1, st);
     if (e != cudaSuccess) return fail_cuda(ctx, e, "mce_launch (host spill)");
     ctx->launches++;
-    G2_TRY(cudaMemcpy(&left, a.ndeferred, sizeof(left), cudaMemcpyDeviceToHost));
+    return G2_OK;
+}
+
+int mce_host_spill(g2_ctx *ctx, cudaStream_t st) {
+    unsigned long long left = 0;
+    G2_TRY(cudaMemcpy(&left, ctx->d_ctr + kCtrDefer + 2, sizeof(left), cudaMemcpyDeviceToHost));
+    if (!left) return G2_OK;
+    if (!ctx->host_spill_bytes || left > ctx->tasks_cap) return G2_ERR_OVERFLOW;
+    if (ctx->scratch_words < 2ull * (ctx->max_fwd + 2)) return G2_ERR_OVERFLOW;  // room for the histogram
+    int rc = ensure_spill_slab(ctx);
+    if (!rc) rc = launch_spill_pass(ctx, st);
+    if (rc) return rc;
+    G2_TRY(cudaMemcpy(&left, ctx->d_ctr + kCtrSpillDefer, sizeof(left), cudaMemcpyDeviceToHost));
     return left ? G2_ERR_OVERFLOW : G2_OK;
+}
+
+// Device-stream MCE runs: the same spill pass in stream order, without a host
+// read of the leftover count, then a one-thread kernel that flags entries still
+// left (read with g2_run_status).  The slab must exist before a CUDA graph
+// capture: inside one, a slab not yet allocated means no spill pass.
+int mce_stream_spill(g2_ctx *ctx, cudaStream_t st) {
+    const unsigned long long *left = ctx->d_ctr + kCtrDefer + 2;
+    bool can = ctx->host_spill_bytes && ctx->scratch_words >= 2ull * (ctx->max_fwd + 2);
+    if (can && ctx->h_spill_bytes != ctx->host_spill_bytes) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        G2_TRY(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone) can = false;
+        else if (int rc = ensure_spill_slab(ctx)) return rc;
+    }
+    if (can) {
+        int rc = launch_spill_pass(ctx, st);
+        if (rc) return rc;
+        left = ctx->d_ctr + kCtrSpillDefer;
+    }
+    cudaError_t e = g2::flag_left(left, ctx->d_status, st);
+    if (e != cudaSuccess) return fail_cuda(ctx, e, "flag_left");
+    ctx->launches++;
+    return G2_OK;
 }
 
 }  // namespace g2rt
@@ -1169,8 +1208,19 @@ int g2_mce_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc, con
     if (rc) return rc;
     ctx->last_split = tl.split;
     ctx->last_cap = tl.cap;
-    return mce_enqueue(ctx, tl, opts, reinterpret_cast<unsigned long long *>(d_out), hist_len, nullptr, nullptr,
-                       st);
+    rc = mce_enqueue(ctx, tl, opts, reinterpret_cast<unsigned long long *>(d_out), hist_len, nullptr, nullptr, st);
+    if (rc) return rc;
+    return mce_stream_spill(ctx, st);
+}
+
+int g2_run_status(g2_ctx *ctx, void *stream) {
+    if (!ctx) return G2_ERR_INVALID;
+    if (!ctx->d_status) return G2_OK;  // nothing has run
+    G2_TRY(cudaSetDevice(ctx->device));
+    G2_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    int status = 0;
+    G2_TRY(cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    return status_to_code(status);
 }
 
 int g2_mce_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc, const g2_opts *opts, uint64_t *count,

@@ -142,6 +142,8 @@ int match_enqueue(g2_ctx *ctx, const TaskList &tl, const g2_opts *o, unsigned lo
                   uint64_t *d_root_nodes, uint64_t *d_root_cost, cudaStream_t st);
 // After a synchronous MCE run: roots no device slab held, on the managed spill slab.
 int mce_host_spill(g2_ctx *ctx, cudaStream_t st);
+// Device-stream MCE runs: the same pass in stream order, then a flag for entries left.
+int mce_stream_spill(g2_ctx *ctx, cudaStream_t st);
 // Resident warps of the persistent grids (split targets).
 uint64_t mce_warps(g2_ctx *ctx, const g2_opts *o);
 uint64_t match_warps(g2_ctx *ctx, const g2_opts *o);

@@ -92,6 +92,7 @@ def lib():
         "g2_match_run": (i32, [C.c_void_p, C.c_void_p, u64, P(G2Opts), P(u64)]),
         "g2_mce_run_device": (i32, [C.c_void_p, C.c_void_p, u64, P(G2Opts), C.c_void_p, u32, C.c_void_p]),
         "g2_match_run_device": (i32, [C.c_void_p, C.c_void_p, u64, P(G2Opts), C.c_void_p, C.c_void_p]),
+        "g2_run_status": (i32, [C.c_void_p, C.c_void_p]),
         "g2_last_launch_count": (u64, [C.c_void_p]),
         "g2_pass_time_ms": (i32, [C.c_void_p, i32, P(C.c_float)]),
         "g2_last_work_bytes": (i32, [C.c_void_p, P(u64)]),

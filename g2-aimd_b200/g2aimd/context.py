@@ -428,6 +428,11 @@ class Context:
                                               C.byref(o), C.c_void_p(d_out), C.c_void_p(stream)),
                     "g2_match_run_device")
 
+    def run_status(self, stream: int = 0) -> int:
+        """Outcome code of the last device-stream run on `stream` (g2_run_status;
+        waits for the stream): 0, or the G2_ERR_* the synchronous entry point
+        would have returned."""
+        return lib().g2_run_status(self._h, C.c_void_p(stream))
 
     # ------------------------------------------------------ cost model
     def load_core(self, core):

@@ -249,13 +249,26 @@ int g2_match_run(g2_ctx *ctx, const uint32_t *sources, uint64_t nsrc,
  * synchronising.  d_out receives the counters:
  *   MCE:   d_out[0] = count, d_out[1 + s] = hist[s] for s < hist_len;
  *   match: d_out[0] = count.
- * d_out must hold 1 + hist_len (MCE) or 1 (match) uint64_t.
+ * d_out must hold 1 + hist_len (MCE) or 1 (match) uint64_t.  The run's outcome
+ * (what the synchronous entry point would return) is read with g2_run_status.
  */
 int g2_mce_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc,
                       const g2_opts *opts, uint64_t *d_out, uint32_t hist_len,
                       void *stream);
 int g2_match_run_device(g2_ctx *ctx, const uint32_t *d_sources, uint64_t nsrc,
                         const g2_opts *opts, uint64_t *d_out, void *stream);
+
+/*
+ * Outcome of the last device-stream run (g2_mce_run_device,
+ * g2_match_run_device) of this context, enqueued on `stream`: waits for the
+ * stream, then returns what the synchronous entry point would have returned:
+ * G2_OK; G2_ERR_OVERFLOW (entries that no slab, spill slab included, held: the
+ * counts leave them out); G2_ERR_TIMEOUT (a bounded device wait ran out);
+ * G2_ERR_DEADLINE (the time budget ran out: the counts cover the roots that
+ * finished); G2_ERR_HIST; G2_ERR_INVALID (inconsistent plan).  The status word
+ * belongs to the context: the next run on it starts a new one.
+ */
+int g2_run_status(g2_ctx *ctx, void *stream);
 
 /* Number of kernels the last run launched (for launch accounting). */
 uint64_t g2_last_launch_count(const g2_ctx *ctx);
@@ -361,7 +374,10 @@ int g2_copy_csr(g2_ctx *ctx, uint64_t *row_ptrs, uint32_t *cols);
  * after the deferral passes: managed memory (default 1 GiB, allocated on first
  * need) whose pages live on the GPU while used and in host memory when device
  * memory runs out; 0 = none: such roots make the run return G2_ERR_OVERFLOW.
- * The device-stream entry points never spill and report G2_ERR_OVERFLOW. */
+ * g2_mce_run_device enqueues the same pass in stream order, allocating the
+ * slab on its first run since it cannot know the need (managed pages are only
+ * placed when touched); under a CUDA graph capture a slab not yet allocated
+ * means no pass.  g2_run_status reports the roots it could not hold. */
 int g2_set_host_spill(g2_ctx *ctx, uint64_t bytes);
 
 /* Search-tree nodes the last MCE run handed from long walks to idle warps

@@ -60,3 +60,31 @@ def test_match_budget_keeps_finished_roots_exact(g2, orc, q, budget):
         assert got == want
         # generous budget: everything finishes
         assert c.match(plan, schedule="heuristic", flags=1, deadline_ms=600000) == full and not c.expired
+
+
+def test_device_stream_status_reports_the_budget(g2):
+    """g2_run_status gives a device-stream run's outcome: G2_ERR_DEADLINE when
+    its budget ran out before every root finished (a run that takes more than
+    ten times the budget), 0 for a run without one."""
+    import torch
+    from g2aimd.context import Context, Plan
+    g = g2.Graph.rmat(16, 16, seed=3).degeneracy_recoded()
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.Stream(dev)
+    out = torch.zeros(1, dtype=torch.int64, device=dev)
+    with Context(0) as c:
+        c.load(g)
+        c.load_core(g.core)
+        c.set_plan(Plan.preset(1))  # 4-cycles: the plan walk
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        c.match_device(out.data_ptr(), stream=st.cuda_stream, schedule="heuristic", flags=1)
+        e1.record(st)
+        assert c.run_status(st.cuda_stream) == 0
+        full, full_ms = int(out[0].item()), e0.elapsed_time(e1)
+        c.match_device(out.data_ptr(), stream=st.cuda_stream, schedule="heuristic", flags=1, deadline_ms=1)
+        code = c.run_status(st.cuda_stream)
+        if full_ms > 10.0:
+            assert code == -11 and int(out[0].item()) < full  # G2_ERR_DEADLINE
+        else:
+            assert code in (0, -11)

@@ -108,3 +108,50 @@ def test_l2_persistence_window_keeps_counts(g2, orc, ctx):
         ctx.match_device(out.data_ptr(), stream=s.cuda_stream, flags=32)
         s.synchronize()
         assert int(out[0].item()) == orc.match(g, plan, threads=8)["count"], q
+
+
+@pytest.mark.parametrize("q", [2, 5, 7, 9, 11, 13])
+def test_shared_last_position_small_slabs(g2, orc, q):
+    """Plans whose last position has no back neighbour at the position before
+    it (diamonds, presets 5, 7, 9-15) count it from one candidate set per
+    prefix.  With 256 scratch words per warp (512 for k = 6) that set holds at
+    most 64 entries (96 for k = 6): larger sets (the hubs' at k = 4, 5) take
+    the per-candidate scan, the rest the shared set.  Per-root counts and the work
+    model stay the oracle's, hand-off on and off."""
+    from g2aimd.context import Context, Plan
+    plan = Plan.preset(q)
+    scale, ef, words = {4: (11, 16, 256), 5: (9, 16, 256), 6: (8, 8, 512)}[plan.k]
+    g = g2.Graph.rmat(scale, ef, seed=8).degeneracy_recoded()
+    want = orc.match(g, plan, threads=8, per_root=True)
+    if q == 2:  # the heaviest edge's common neighbourhood exceeds the 64-entry set
+        adj = [set(g.cols[g.row_ptrs[v]:g.row_ptrs[v + 1]].tolist()) for v in range(g.n)]
+        top = np.argsort(-np.diff(g.row_ptrs.astype(np.int64)))[:2]
+        assert len(adj[top[0]] & adj[top[1]]) > 64
+    launch = dict(blocks=148, warps_per_block=8, intersect_mode=1)
+    with Context(0, scratch_bytes=148 * 8 * words * 4) as c:
+        c.load(g)
+        for kw in ({}, {"spill_kcycles": 1}, {"flags": 16}):
+            rc = np.zeros(g.n, np.uint64)
+            assert c.match(plan, root_counts=rc, **launch, **kw) == want["count"], (q, kw)
+            assert np.array_equal(rc, want["root_counts"]), (q, kw)
+            w = np.zeros(1, np.uint64)
+            c.match(plan, work_bytes=w, **launch, **kw)
+            assert int(w[0]) == want["work"], (q, kw)
+
+
+@pytest.mark.parametrize("k", [3, 4])
+def test_shared_last_position_split_roots(g2, orc, ctx, k):
+    """Wedges and 3-stars rooted at the centre (last position adjacent to the
+    root only): with heavy roots split into parts, each part counts its own
+    position-1 candidates against the shared set, so per-root sums stay the
+    oracle's."""
+    from g2aimd.context import Plan
+    plan = Plan.from_edges(k, [(0, j) for j in range(1, k)])
+    assert all(b == [0] for b in plan.to_dict()["bn"][1:])
+    g = g2.Graph.rmat(11 if k == 3 else 9, 16, seed=9).degeneracy_recoded()
+    want = orc.match(g, plan, threads=8, per_root=True)
+    ctx.load(g)
+    for kw in ({}, {"split": True, "schedule": "heuristic", "granularity": 64}, {"spill_kcycles": 1}):
+        rc = np.zeros(g.n, np.uint64)
+        assert ctx.match(plan, root_counts=rc, **kw) == want["count"], (k, kw)
+        assert np.array_equal(rc, want["root_counts"]), (k, kw)

@@ -157,3 +157,32 @@ def test_host_spill_pass(g2, orc):
         c.set_host_spill(0)
         with pytest.raises(g2.G2Error):
             c.mce(flags=16)
+
+
+def test_stream_spill_and_status(g2, orc):
+    """g2_mce_run_device enqueues the spill pass in stream order: with a 256 KiB
+    scratch the device counters still equal the oracle's and g2_run_status
+    reports 0; without a spill slab it reports the roots left out
+    (G2_ERR_OVERFLOW)."""
+    import torch
+    from g2aimd.context import Context
+    g = g2.Graph.rmat(11, 16, seed=21)
+    want = orc.mce(g, threads=8, hist_len=256)
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.Stream(dev)
+    out = torch.zeros(257, dtype=torch.int64, device=dev)
+    with Context(0, scratch_bytes=256 << 10) as c:
+        c.load(g)
+        c.mce_device(out.data_ptr(), 256, stream=st.cuda_stream, flags=16)
+        assert c.run_status(st.cuda_stream) == 0
+        h = out.cpu().numpy().astype(np.uint64)
+        _same((int(h[0]), h[1:]), want, "stream spill")
+        c.set_host_spill(0)
+        c.mce_device(out.data_ptr(), 256, stream=st.cuda_stream, flags=16)
+        assert c.run_status(st.cuda_stream) == -5  # G2_ERR_OVERFLOW
+        assert int(out[0].item()) <= want["count"]
+    with Context(0) as c:
+        c.load(g)
+        c.mce_device(out.data_ptr(), 256, stream=st.cuda_stream)
+        assert c.run_status(st.cuda_stream) == 0 and int(out[0].item()) == want["count"]
+
