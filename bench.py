@@ -522,11 +522,11 @@ def c4_leg(Context, CostModel, Plan, models, local, seed, torch, stream, budget_
     """64 Chung-Lu graphs (n log-uniform in [1e3, 1e6], exponent in [2.1, 2.8],
     average degree in [8, 40]): triangles over all of them, maximal cliques over
     the ones of degeneracy <= 160 (the densest cores hold 5e9 to over 3e10
-    maximal cliques each), 4-cycles and diamonds over the ones whose estimated
-    walk is at most 1e10; each job is one launch over the batch (disjoint union),
-    compared with one run per graph.  The members left out of a job then run it
-    alone with a device time budget (budget_ms), reporting the roots that
-    finished and their exact counts."""
+    maximal cliques each), diamonds over all of them, 4-cycles over the ones
+    whose estimated walk is at most 1e10; each job is one launch over the batch
+    (disjoint union), compared with one run per graph.  The members left out of
+    a job then run it alone with a device time budget (budget_ms), reporting the
+    roots that finished and their exact counts."""
     from g2aimd.graph import chung_lu_batch
     t0 = time.perf_counter()
     gs = chung_lu_batch(count=64, seed=seed)
@@ -543,10 +543,10 @@ def c4_leg(Context, CostModel, Plan, models, local, seed, torch, stream, budget_
         e1.synchronize()
         return e0.elapsed_time(e1), r
 
-    jobs = [("triangle", 0, gs), ("mce", None, mce_set), ("4-cycle", 1, light), ("diamond", 2, light)]
+    jobs = [("triangle", 0, gs), ("diamond", 2, gs), ("mce", None, mce_set), ("4-cycle", 1, light)]
     out = {"graphs": len(gs), "vertices": int(sum(g.n for g in gs)), "directed_edges": int(sum(g.m for g in gs)),
            "generation_s": round(gen_s, 1), "mce_graphs": len(mce_set), "mce_rule": "degeneracy <= 160",
-           "light_graphs": len(light), "light_rule": "estimated 4-vertex walk <= 1e10"}
+           "light_graphs": len(light), "light_rule": "4-cycles: estimated 4-vertex walk <= 1e10; diamonds: all"}
     with Context(local) as bc:
         bc.set_model(CostModel.load(os.path.join(models, "mce.npz")))
         loaded = None
@@ -581,8 +581,7 @@ def c4_leg(Context, CostModel, Plan, models, local, seed, torch, stream, budget_
         # matches: root_cost > 0)
         heavy = []
         for gi, g in enumerate(gs):
-            jobs_g = ([("mce", None)] if g not in mce_set else []) + \
-                     ([("4-cycle", 1), ("diamond", 2)] if g not in light else [])
+            jobs_g = ([("mce", None)] if g not in mce_set else []) + ([("4-cycle", 1)] if g not in light else [])
             if not jobs_g:
                 continue
             bc.load(g)

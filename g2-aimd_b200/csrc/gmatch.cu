@@ -183,9 +183,41 @@ __device__ __forceinline__ bool last_is_shared(const DevPlan &pl) {
 
 constexpr uint32_t kSharedUnbuilt = 0xffffffffu, kSharedTooLarge = 0xfffffffeu;
 
+// Does position k-2 have exactly the last position's candidate set for every
+// prefix?  Same back neighbours and the same conditions against every position
+// before k-2 (diamonds, presets 9 and 15, stars: the reference's moving_lvl of
+// two positions, system/plan.h:340-371).
+__device__ __forceinline__ bool last_pair_same_set(const DevPlan &pl) {
+    const uint32_t a = pl.k - 2, b = pl.k - 1;
+    if (pl.bn_count[a] != pl.bn_count[b]) return false;
+    for (uint32_t j = 0; j < pl.bn_count[a]; j++) {
+        bool found = false;
+        for (uint32_t t = 0; t < pl.bn_count[b]; t++) found |= pl.bn_pos[b][t] == pl.bn_pos[a][j];
+        if (!found) return false;
+    }
+    for (uint32_t p = 0; p < a; p++) {  // conditions against position p: op set of a == op set of b
+        uint32_t ma = 0, mb = 0;
+        for (uint32_t c = 0; c < pl.cond_count[a]; c++)
+            if (pl.cond_pos[a][c] == p) ma |= 1u << pl.cond_op[a][c];
+        for (uint32_t c = 0; c < pl.cond_count[b]; c++)
+            if (pl.cond_pos[b][c] == p) mb |= 1u << pl.cond_op[b][c];
+        if (ma != mb) return false;
+    }
+    return true;
+}
+
+// Windows longer than this are filtered by galloping lane slices (below);
+// shorter ones by one binary search per entry, which costs less there.
+constexpr uint64_t kGallopMin = 32ull * 32ull;
+
 // Build S for M[0..k-3] into out (at most cap entries, ascending); returns its
 // length or kSharedTooLarge.  *dsum = sum of the back neighbours' degrees (the
-// work model's share of every partial embedding of length k-1).
+// work model's share of every partial embedding of length k-1).  Short windows:
+// 32 entries at a time, each tested by binary search in the other back
+// neighbours' lists, survivors compacted by a warp scan.  Long windows: each
+// lane takes a contiguous slice and tests it through cursors that only move
+// forward (galloping): a counting pass, a warp scan for the offsets, a writing
+// pass.
 __device__ __noinline__ uint32_t shared_last_build(const DevPlan &pl, const uint64_t *rp, const uint32_t *ci,
                                                    const uint32_t *M, uint32_t *out, uint32_t cap, uint64_t *dsum) {
     const uint32_t i = pl.k - 1, prev = pl.k - 2;
@@ -216,25 +248,70 @@ __device__ __noinline__ uint32_t shared_last_build(const DevPlan &pl, const uint
     }
     ps = __shfl_sync(G2_FULL, ps, 0);
     pe = __shfl_sync(G2_FULL, pe, 0);
-    uint32_t len = 0;
-    for (uint64_t x0 = ps; x0 < pe; x0 += 32) {
-        const uint64_t x = x0 + lane;
-        const uint32_t w = x < pe ? ldg(ci + x) : 0u;
-        bool ok = x < pe;
-        for (uint32_t c = 0; c < pl.cond_count[i] && ok; c++)
-            if (pl.cond_pos[i][c] != prev) ok = cond_ok(pl.cond_op[i][c], w, M[pl.cond_pos[i][c]]);
-        for (uint32_t j = 0; j < pl.bn_count[i] && ok; j++) {
-            const uint32_t b = pl.bn_pos[i][j];
-            if (b != parent) ok = contains(ci, ldg(rp + M[b]), ldg(rp + M[b] + 1), w);
+    if (pe - ps <= kGallopMin) {
+        uint32_t len = 0;
+        for (uint64_t x0 = ps; x0 < pe; x0 += 32) {
+            const uint64_t x = x0 + lane;
+            const uint32_t w = x < pe ? ldg(ci + x) : 0u;
+            bool ok = x < pe;
+            for (uint32_t c = 0; c < pl.cond_count[i] && ok; c++)
+                if (pl.cond_pos[i][c] != prev) ok = cond_ok(pl.cond_op[i][c], w, M[pl.cond_pos[i][c]]);
+            for (uint32_t j = 0; j < pl.bn_count[i] && ok; j++) {
+                const uint32_t b = pl.bn_pos[i][j];
+                if (b != parent) ok = contains(ci, ldg(rp + M[b]), ldg(rp + M[b] + 1), w);
+            }
+            uint32_t tot;
+            const uint32_t pos = warp_scan(ok, tot);
+            if (len + tot > cap) return kSharedTooLarge;  // warp-uniform
+            if (ok) out[len + pos] = w;
+            len += tot;
         }
-        uint32_t tot;
-        const uint32_t pos = warp_scan(ok, tot);
-        if (len + tot > cap) return kSharedTooLarge;  // warp-uniform
-        if (ok) out[len + pos] = w;
-        len += tot;
+        __syncwarp();
+        return len;
     }
+    uint64_t beg[G2_MAX_QUERY], stop[G2_MAX_QUERY];
+    uint32_t nb = 0;
+    for (uint32_t j = 0; j < pl.bn_count[i]; j++) {
+        const uint32_t b = pl.bn_pos[i][j];
+        if (b == parent) continue;
+        beg[nb] = ldg(rp + M[b]);
+        stop[nb] = ldg(rp + M[b] + 1);
+        nb++;
+    }
+    const uint64_t per = (pe - ps + 31) >> 5;
+    const uint64_t x0 = ps + (uint64_t)lane * per < pe ? ps + (uint64_t)lane * per : pe;
+    const uint64_t x1 = x0 + per < pe ? x0 + per : pe;
+    auto pass = [&](uint32_t *dst) -> uint32_t {
+        uint64_t cur[G2_MAX_QUERY];
+        for (uint32_t t = 0; t < nb; t++) cur[t] = beg[t];
+        uint32_t n = 0;
+        for (uint64_t x = x0; x < x1; x++) {
+            const uint32_t w = ldg(ci + x);
+            bool ok = true;
+            for (uint32_t c = 0; c < pl.cond_count[i] && ok; c++)
+                if (pl.cond_pos[i][c] != prev) ok = cond_ok(pl.cond_op[i][c], w, M[pl.cond_pos[i][c]]);
+            for (uint32_t t = 0; t < nb && ok; t++) {
+                cur[t] = gallop(ci, cur[t], stop[t], w);
+                ok = cur[t] < stop[t] && ldg(ci + cur[t]) == w;
+            }
+            if (ok) {
+                if (dst) dst[n] = w;
+                n++;
+            }
+        }
+        return n;
+    };
+    const uint32_t n = pass(nullptr);
+    uint32_t off = n;  // inclusive scan over the lanes
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(G2_FULL, off, d);
+        if (lane >= d) off += t;
+    }
+    const uint32_t total = __shfl_sync(G2_FULL, off, 31);
+    if (total > cap) return kSharedTooLarge;  // warp-uniform
+    pass(out + (off - n));
     __syncwarp();
-    return len;
+    return total;
 }
 
 // Embeddings completed by the candidates buf[0..n) of position k-2 against
@@ -269,6 +346,35 @@ __device__ __noinline__ unsigned long long shared_last_count(const DevPlan &pl, 
         const uint32_t lo = gt ? a + (in ? 1u : 0u) : 0u, hi = lt ? a : ns;
         uint32_t c = hi > lo ? hi - lo : 0u;
         if (ne && in && a >= lo && a < hi) c--;
+        cnt += c;
+    }
+    *taken = tk;
+    return cnt;
+}
+
+// Embeddings completed when position k-2's candidates are S itself (in
+// order): candidate j completes |{x in S : x op S[j]}|, an index range; with
+// nparts > 1 only ordinals ord0 + j with (ord0 + j) % nparts == part count.
+// Per-lane count; *taken = this lane's candidates of the part.
+__device__ __noinline__ unsigned long long shared_pair_count(const DevPlan &pl, uint32_t ns, uint32_t ord0,
+                                                             uint32_t part, uint32_t nparts, uint32_t *taken) {
+    const uint32_t i = pl.k - 1, prev = pl.k - 2;
+    bool lt = false, gt = false, ne = false;
+    for (uint32_t c = 0; c < pl.cond_count[i]; c++) {
+        if (pl.cond_pos[i][c] != prev) continue;
+        const uint32_t op = pl.cond_op[i][c];
+        lt |= op == G2_COND_LESS_THAN;
+        gt |= op == G2_COND_LARGER_THAN;
+        ne |= op == G2_COND_NON_EQUAL;
+    }
+    unsigned long long cnt = 0;
+    uint32_t tk = 0;
+    for (uint32_t j = lane_id(); j < ns; j += 32) {
+        if (nparts > 1 && (ord0 + j) % nparts != part) continue;
+        tk++;
+        const uint32_t lo = gt ? j + 1 : 0u, hi = lt ? j : ns;
+        uint32_t c = hi > lo ? hi - lo : 0u;
+        if (ne && j >= lo && j < hi) c--;
         cnt += c;
     }
     *taken = tk;
@@ -387,6 +493,10 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
     uint32_t *Sset = S + (uint64_t)(k - 2) * CH;
     uint32_t s_len = kSharedUnbuilt;  // S for the current M[0..k-3]
     uint64_t s_dsum = 0;
+    // position k-2's candidates are S itself: counted by index, never scanned,
+    // when its level starts with its whole window (k2_full)
+    const bool pair = shared && last_pair_same_set(pl);
+    bool k2_full = k == 3;
     unsigned long long count = 0;
     if (CH < 64) {  // a chunk must hold at least two warp-widths of candidates
         if (lane == 0) atomicOr(a.status, kStatusStackOverflow);
@@ -401,6 +511,7 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
         // record words are read past L1 (two records share a cache line)
         base = __ldcg(rec + 1);
         const uint32_t kind = __ldcg(rec + kRecKind);
+        k2_full = base == k - 2 && kind == kRecPrefix;
         for (uint32_t j = 0; j < base; j++) M[j] = __ldcg(rec + kRecM + j);
         const uint64_t d = level_init(pl, rp, ci, M, base, Ls[base]);
         if (kind == kRecPrefix) {
@@ -465,6 +576,21 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
             i--;
             continue;
         }
+        if (pair && i == k - 2 && k2_full) {
+            k2_full = false;
+            if (s_len == kSharedUnbuilt) s_len = shared_last_build(pl, rp, ci, M, Sset, CH, &s_dsum);
+            if (s_len != kSharedTooLarge) {
+                const bool split = i == 1 && nparts > 1;
+                uint32_t tk = 0;
+                count += warp_sum_u64(shared_pair_count(pl, s_len, ord, part, split ? nparts : 1u, &tk));
+                work += 4ull * s_dsum * warp_sum_u64(tk);
+                if (split) ord += s_len;
+                L.pos = L.end;  // the level is done
+                L.len = L.idx = 0;
+                if (a.deadline && match_deadline_passed(a)) return kExpired;
+                continue;
+            }
+        }
         uint32_t *buf = S + (uint64_t)(i - 1) * CH;
         if (L.idx == L.len) {
             if (L.pos >= L.end) {
@@ -527,7 +653,7 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
         if (may_spill) maybe_donate();
         i++;
         work += 4ull * level_init(pl, rp, ci, M, i, Ls[i]);
-        if (i == k - 2) s_len = kSharedUnbuilt;
+        if (i == k - 2) s_len = kSharedUnbuilt, k2_full = true;
     }
     return count;
 }
