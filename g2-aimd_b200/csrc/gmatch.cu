@@ -206,18 +206,11 @@ __device__ __forceinline__ bool last_pair_same_set(const DevPlan &pl) {
     return true;
 }
 
-// Windows longer than this are filtered by galloping lane slices (below);
-// shorter ones by one binary search per entry, which costs less there.
-constexpr uint64_t kGallopMin = 32ull * 32ull;
-
 // Build S for M[0..k-3] into out (at most cap entries, ascending); returns its
 // length or kSharedTooLarge.  *dsum = sum of the back neighbours' degrees (the
-// work model's share of every partial embedding of length k-1).  Short windows:
-// 32 entries at a time, each tested by binary search in the other back
-// neighbours' lists, survivors compacted by a warp scan.  Long windows: each
-// lane takes a contiguous slice and tests it through cursors that only move
-// forward (galloping): a counting pass, a warp scan for the offsets, a writing
-// pass.
+// work model's share of every partial embedding of length k-1).  The window is
+// read 32 entries at a time, each tested by binary search in the other back
+// neighbours' lists, survivors compacted by a warp scan.
 __device__ __noinline__ uint32_t shared_last_build(const DevPlan &pl, const uint64_t *rp, const uint32_t *ci,
                                                    const uint32_t *M, uint32_t *out, uint32_t cap, uint64_t *dsum) {
     const uint32_t i = pl.k - 1, prev = pl.k - 2;
@@ -248,70 +241,25 @@ __device__ __noinline__ uint32_t shared_last_build(const DevPlan &pl, const uint
     }
     ps = __shfl_sync(G2_FULL, ps, 0);
     pe = __shfl_sync(G2_FULL, pe, 0);
-    if (pe - ps <= kGallopMin) {
-        uint32_t len = 0;
-        for (uint64_t x0 = ps; x0 < pe; x0 += 32) {
-            const uint64_t x = x0 + lane;
-            const uint32_t w = x < pe ? ldg(ci + x) : 0u;
-            bool ok = x < pe;
-            for (uint32_t c = 0; c < pl.cond_count[i] && ok; c++)
-                if (pl.cond_pos[i][c] != prev) ok = cond_ok(pl.cond_op[i][c], w, M[pl.cond_pos[i][c]]);
-            for (uint32_t j = 0; j < pl.bn_count[i] && ok; j++) {
-                const uint32_t b = pl.bn_pos[i][j];
-                if (b != parent) ok = contains(ci, ldg(rp + M[b]), ldg(rp + M[b] + 1), w);
-            }
-            uint32_t tot;
-            const uint32_t pos = warp_scan(ok, tot);
-            if (len + tot > cap) return kSharedTooLarge;  // warp-uniform
-            if (ok) out[len + pos] = w;
-            len += tot;
+    uint32_t len = 0;
+    for (uint64_t x0 = ps; x0 < pe; x0 += 32) {
+        const uint64_t x = x0 + lane;
+        const uint32_t w = x < pe ? ldg(ci + x) : 0u;
+        bool ok = x < pe;
+        for (uint32_t c = 0; c < pl.cond_count[i] && ok; c++)
+            if (pl.cond_pos[i][c] != prev) ok = cond_ok(pl.cond_op[i][c], w, M[pl.cond_pos[i][c]]);
+        for (uint32_t j = 0; j < pl.bn_count[i] && ok; j++) {
+            const uint32_t b = pl.bn_pos[i][j];
+            if (b != parent) ok = contains(ci, ldg(rp + M[b]), ldg(rp + M[b] + 1), w);
         }
-        __syncwarp();
-        return len;
+        uint32_t tot;
+        const uint32_t pos = warp_scan(ok, tot);
+        if (len + tot > cap) return kSharedTooLarge;  // warp-uniform
+        if (ok) out[len + pos] = w;
+        len += tot;
     }
-    uint64_t beg[G2_MAX_QUERY], stop[G2_MAX_QUERY];
-    uint32_t nb = 0;
-    for (uint32_t j = 0; j < pl.bn_count[i]; j++) {
-        const uint32_t b = pl.bn_pos[i][j];
-        if (b == parent) continue;
-        beg[nb] = ldg(rp + M[b]);
-        stop[nb] = ldg(rp + M[b] + 1);
-        nb++;
-    }
-    const uint64_t per = (pe - ps + 31) >> 5;
-    const uint64_t x0 = ps + (uint64_t)lane * per < pe ? ps + (uint64_t)lane * per : pe;
-    const uint64_t x1 = x0 + per < pe ? x0 + per : pe;
-    auto pass = [&](uint32_t *dst) -> uint32_t {
-        uint64_t cur[G2_MAX_QUERY];
-        for (uint32_t t = 0; t < nb; t++) cur[t] = beg[t];
-        uint32_t n = 0;
-        for (uint64_t x = x0; x < x1; x++) {
-            const uint32_t w = ldg(ci + x);
-            bool ok = true;
-            for (uint32_t c = 0; c < pl.cond_count[i] && ok; c++)
-                if (pl.cond_pos[i][c] != prev) ok = cond_ok(pl.cond_op[i][c], w, M[pl.cond_pos[i][c]]);
-            for (uint32_t t = 0; t < nb && ok; t++) {
-                cur[t] = gallop(ci, cur[t], stop[t], w);
-                ok = cur[t] < stop[t] && ldg(ci + cur[t]) == w;
-            }
-            if (ok) {
-                if (dst) dst[n] = w;
-                n++;
-            }
-        }
-        return n;
-    };
-    const uint32_t n = pass(nullptr);
-    uint32_t off = n;  // inclusive scan over the lanes
-    for (uint32_t d = 1; d < 32; d <<= 1) {
-        const uint32_t t = __shfl_up_sync(G2_FULL, off, d);
-        if (lane >= d) off += t;
-    }
-    const uint32_t total = __shfl_sync(G2_FULL, off, 31);
-    if (total > cap) return kSharedTooLarge;  // warp-uniform
-    pass(out + (off - n));
     __syncwarp();
-    return total;
+    return len;
 }
 
 // Embeddings completed by the candidates buf[0..n) of position k-2 against
