@@ -14,7 +14,9 @@
 //    scan, which removes only candidates the filter rejects.  Candidate lists
 //    live in the warp's HBM slab and are generated in chunks (the reference's
 //    TEMPSIZE chunking, :617-622), so any degree fits.  The last position is
-//    counted, never materialised (:602-609).  Long walks hand half of their
+//    counted, never materialised (:602-609); when it has no back neighbour at
+//    position k-2 its candidate set is built once per prefix and counted
+//    against (the reference's PREFIX strategy, see shared_last_build).  Long walks hand half of their
 //    shallowest pending level (window half, candidate batches) or half of a long
 //    last-position scan to idle warps through the record queue of
 //    g2_handoff.cuh; records resume from a matched prefix.
