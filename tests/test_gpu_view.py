@@ -198,7 +198,9 @@ def test_device_built_view_csr_sharing_pages_with_other_arrays(vctx, g2):
     sv = buf[src_at:src_at + 4 * src.size].view(np.uint32)
     rp[:], ci[:], sv[:] = g.row_ptrs, g.cols, src
     # the sources start on the page of the columns' last byte, and end past it
-    assert src_at // 4096 == (ci_at + 4 * m - 1) // 4096 < (src_at + 4 * src.size - 1) // 4096
+    # (pages of absolute addresses)
+    a = buf.ctypes.data
+    assert (a + src_at) // 4096 == (a + ci_at + 4 * m - 1) // 4096 < (a + src_at + 4 * src.size - 1) // 4096
     gb = g2.Graph(rp, ci)
     assert gb.row_ptrs.ctypes.data == rp.ctypes.data and gb.cols.ctypes.data == ci.ctypes.data
     for shape in (dict(), dict(upper=True, forward=True)):
