@@ -331,6 +331,100 @@ __device__ __noinline__ unsigned long long shared_pair_count(const DevPlan &pl, 
     return cnt;
 }
 
+// Conditions of position i against position p, as a bit set of operators.
+__device__ __forceinline__ uint32_t cond_mask(const DevPlan &pl, uint32_t i, uint32_t p) {
+    uint32_t m = 0;
+    for (uint32_t c = 0; c < pl.cond_count[i]; c++)
+        if (pl.cond_pos[i][c] == p) m |= 1u << pl.cond_op[i][c];
+    return m;
+}
+
+// The 4-cycle plan (preset 1): M1 and M2 neighbours of M0 with M0 < M1 < M2,
+// M3 > M0 a neighbour of both (its `!=` conditions are implied by adjacency).
+__device__ __forceinline__ bool plan_is_cycle4(const DevPlan &pl) {
+    if (pl.k != 4 || pl.bn_count[1] != 1 || pl.bn_count[2] != 1 || pl.bn_count[3] != 2) return false;
+    if (pl.bn_pos[1][0] != 0 || pl.bn_pos[2][0] != 0) return false;
+    const uint32_t b0 = pl.bn_pos[3][0], b1 = pl.bn_pos[3][1];
+    if (!((b0 == 1 && b1 == 2) || (b0 == 2 && b1 == 1))) return false;
+    const uint32_t gt = 1u << G2_COND_LARGER_THAN, ne = 1u << G2_COND_NON_EQUAL;
+    return cond_mask(pl, 1, 0) == gt && cond_mask(pl, 2, 0) == gt && cond_mask(pl, 2, 1) == gt &&
+           cond_mask(pl, 3, 0) == gt && (cond_mask(pl, 3, 1) & ~ne) == 0 && (cond_mask(pl, 3, 2) & ~ne) == 0;
+}
+
+// 4-cycles rooted at v for that plan, counted through the opposite vertex:
+// every x > v closes C(c_x, 2) of them, c_x = |{y in N(v) : y > v, x in N(y)}|
+// (the pair M1 < M2 is any two of those y).  The c_x live in the warp's slab as
+// a dense array over id ranges [lo, lo + slab words), filled by atomics from
+// the forward neighbours' lists (each list entry visited once) and summed.
+// Taken only when that costs less than the walk's per-pair intersections
+// (4 x (ids spanned + the forward neighbours' degrees) <= (d - 1) x those
+// degrees, d forward neighbours); false leaves the root to the walk.  count = kExpired when the time budget ran out.
+__device__ __noinline__ bool cycle4_root(const MatchArgs &a, uint32_t v, uint32_t *S, unsigned long long &count) {
+    const uint32_t lane = lane_id();
+    const uint64_t *rp = a.rp;
+    const uint32_t *ci = a.ci;
+    const uint64_t b = ldg(rp + v), e = ldg(rp + v + 1);
+    uint64_t fs = b;
+    if (lane == 0) fs = lower_bound(ci, b, e, v + 1);
+    fs = __shfl_sync(G2_FULL, fs, 0);
+    const uint64_t d = e - fs;
+    if (d < 2) return false;
+    unsigned long long sdeg = 0, xmax = 0;
+    for (uint64_t j = fs + lane; j < e; j += 32) {
+        const uint32_t y = ldg(ci + j);
+        const uint64_t yb = ldg(rp + y), ye = ldg(rp + y + 1);
+        sdeg += ye - yb;
+        if (ye > yb) {
+            const unsigned long long last = ldg(ci + ye - 1);
+            xmax = last > xmax ? last : xmax;
+        }
+    }
+    sdeg = warp_sum_u64(sdeg);
+    xmax = warp_max_u64(xmax);
+    if (xmax <= v) {
+        count = 0;
+        return true;
+    }
+    // the walk intersects d (d - 1) / 2 pairs of forward neighbours' lists, about
+    // half the mean degree each; this path clears and sums the id span once and
+    // adds every list entry once
+    const unsigned long long span = xmax - v;
+    if (4ull * (span + sdeg) > (d - 1) * sdeg) return false;
+    const uint64_t R = a.words_per_warp;
+    unsigned long long total = 0;
+    for (uint64_t lo = (uint64_t)v + 1; lo <= xmax; lo += R) {
+        const uint64_t hi = lo + R <= xmax + 1 ? lo + R : xmax + 1;  // x in [lo, hi)
+        const uint32_t len = (uint32_t)(hi - lo);
+        for (uint32_t j = lane; j < len; j += 32) S[j] = 0u;
+        __syncwarp();
+        for (uint64_t t = fs; t < e; t++) {
+            if (a.deadline && ((t - fs) & 63u) == 0 && match_deadline_passed(a)) {
+                count = kExpired;
+                return true;
+            }
+            const uint32_t y = ldg(ci + t);
+            const uint64_t yb = ldg(rp + y), ye = ldg(rp + y + 1);
+            uint64_t ws = yb, we = ye;
+            if (lane == 0) {
+                ws = lower_bound(ci, yb, ye, (uint32_t)lo);
+                we = lower_bound(ci, ws, ye, (uint32_t)(hi - 1)) ;
+                if (we < ye && ldg(ci + we) == (uint32_t)(hi - 1)) we++;  // entries <= hi - 1
+            }
+            ws = __shfl_sync(G2_FULL, ws, 0);
+            we = __shfl_sync(G2_FULL, we, 0);
+            for (uint64_t x = ws + lane; x < we; x += 32) atomicAdd(S + (ldg(ci + x) - (uint32_t)lo), 1u);
+        }
+        __syncwarp();
+        for (uint32_t j = lane; j < len; j += 32) {
+            const unsigned long long c = __ldcg(S + j);
+            total += c ? c * (c - 1) / 2 : 0ull;
+        }
+        __syncwarp();  // the sums have read the range before the next one clears it
+    }
+    count = warp_sum_u64(total);
+    return true;
+}
+
 // Record layout of a handed-off plan walk (kMatchRecordWords words): the walk
 // resumes at position `level` with M[0..level-1]; kind 0 (prefix) initialises
 // that level from the plan, kind 1 (window) scans only [pos, end) of its
@@ -608,6 +702,18 @@ __device__ __noinline__ unsigned long long match_walk(const MatchArgs &a, const 
     return count;
 }
 
+// A root of a non-clique plan (or a clique root whose rows do not fit): the
+// 4-cycle count through opposite vertices where that is cheaper, else the walk.
+// (Runs with the work model keep the walk: the model counts its steps.)
+template <bool METRICS>
+__device__ __noinline__ unsigned long long match_root_plan(const MatchArgs &a, const DevPlan &pl, uint32_t task,
+                                                           uint32_t v, uint32_t *S, unsigned long long &work,
+                                                           uint32_t part, uint32_t nparts, long long c0) {
+    unsigned long long c = 0;
+    if (!METRICS && nparts == 1 && plan_is_cycle4(pl) && cycle4_root(a, v, S, c)) return c;
+    return match_walk(a, pl, task, v, nullptr, S, work, part, nparts, c0);
+}
+
 // Bits of word w of the mask {j : j > x}.
 __device__ __forceinline__ uint32_t above(uint32_t x, uint32_t w) {
     const uint32_t xw = x >> 5;
@@ -826,7 +932,7 @@ __global__ void __launch_bounds__(256, MINB) match_kernel(MatchArgs a, int cliqu
                 continue;
             }
             if (!clique_path || !match_root_clique<WPL, METRICS>(a, pl, v, S, p0s, rowbuf, c, work, part, nparts))
-                c = match_walk(a, pl, (uint32_t)task, v, nullptr, S, work, part, nparts, c0);
+                c = match_root_plan<METRICS>(a, pl, (uint32_t)task, v, S, work, part, nparts, c0);
             credit((uint32_t)task, c, c0);
         }
         outstanding_add(a, handoff, -1);

@@ -155,3 +155,37 @@ def test_shared_last_position_split_roots(g2, orc, ctx, k):
         rc = np.zeros(g.n, np.uint64)
         assert ctx.match(plan, root_counts=rc, **kw) == want["count"], (k, kw)
         assert np.array_equal(rc, want["root_counts"]), (k, kw)
+
+
+@pytest.mark.parametrize("words", [0, 256])
+def test_cycle4_through_opposite_vertices(g2, orc, words):
+    """4-cycles (preset 1): a root whose forward neighbours make the walk's
+    per-pair intersections dearer than one count per id above the root
+    (4 (ids spanned + the forward neighbours' degrees) <= (d - 1) x those
+    degrees) counts every cycle through its vertex opposite the root.  Per-root counts equal the
+    oracle's with the default slab and with 256-word slabs (up to six id ranges
+    per root), in id and heuristic order, hand-off on and off."""
+    from g2aimd.context import Context, Plan
+    plan = Plan.preset(1)
+    g = g2.Graph.rmat(12, 16, seed=11).degeneracy_recoded()
+    rp = g.row_ptrs.astype(np.int64)
+    deg = np.diff(rp)
+    taken = 0  # roots that take the opposite-vertex count (the device's rule)
+    for v in range(g.n):
+        row = g.cols[rp[v]:rp[v + 1]]
+        fw = row[row > v]
+        nz = fw[deg[fw] > 0]
+        if fw.size < 2 or nz.size == 0:
+            continue
+        xmax = int(max(g.cols[rp[y + 1] - 1] for y in nz))
+        sdeg = int(deg[fw].sum())
+        taken += xmax > v and 4 * ((xmax - v) + sdeg) <= (fw.size - 1) * sdeg
+    assert 0 < taken < g.n
+    want = orc.match(g, plan, threads=8, per_root=True)
+    launch = dict(blocks=148, warps_per_block=8) if words else {}
+    with Context(0, scratch_bytes=148 * 8 * words * 4) as c:
+        c.load(g)
+        for kw in ({}, {"schedule": "heuristic"}, {"flags": 16}):
+            rc = np.zeros(g.n, np.uint64)
+            assert c.match(plan, root_counts=rc, **launch, **kw) == want["count"], (words, kw)
+            assert np.array_equal(rc, want["root_counts"]), (words, kw)
