@@ -98,3 +98,45 @@ def test_oracle_preset_plans_equal_the_librarys(g2, orc):
         a, b = orc.PresetPlan(q), Plan.preset(q)
         assert a.k == b.k
         assert all(np.array_equal(x, y) for x, y in zip(a.flat(), b.flat()))
+
+
+def _adjacency(g):
+    rp = g.row_ptrs.astype(np.int64)
+    return [g.cols[rp[v]:rp[v + 1]].astype(np.int64) for v in range(g.n)]
+
+
+@pytest.mark.parametrize("seed", [11, 12])
+def test_cycle4_count_through_opposite_vertices(g2, orc, seed):
+    """The identity behind the GPU's opposite-vertex 4-cycle count: for the
+    4-cycle plan, the oracle's count of root v equals the sum over x > v of
+    C(c_x, 2), c_x = the neighbours y > v of v adjacent to x."""
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(10, 16, seed=seed).degeneracy_recoded()
+    want = orc.match(g, Plan.preset(1), threads=4, per_root=True)["root_counts"]
+    adj = _adjacency(g)
+    got = np.zeros(g.n, np.uint64)
+    for v in range(g.n):
+        fw = adj[v][adj[v] > v]
+        if fw.size < 2:
+            continue
+        xs = np.concatenate([adj[y][adj[y] > v] for y in fw])
+        c = np.bincount(xs - v - 1) if xs.size else np.zeros(0, np.int64)
+        got[v] = int((c * (c - 1) // 2).sum())
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("seed", [11, 12])
+def test_diamond_count_from_one_shared_set(g2, orc, seed):
+    """The identity behind the GPU's shared last-position set for diamonds
+    (positions 2 and 3 share their candidates): the oracle's count of root v
+    equals the sum over neighbours u > v of C(|N(v) & N(u)|, 2)."""
+    from g2aimd.context import Plan
+    g = g2.Graph.rmat(10, 16, seed=seed).degeneracy_recoded()
+    want = orc.match(g, Plan.preset(2), threads=4, per_root=True)["root_counts"]
+    adj = _adjacency(g)
+    got = np.zeros(g.n, np.uint64)
+    for v in range(g.n):
+        for u in adj[v][adj[v] > v]:
+            s = np.intersect1d(adj[v], adj[u], assume_unique=True).size
+            got[v] += s * (s - 1) // 2
+    assert np.array_equal(got, want)
